@@ -1,0 +1,224 @@
+/*
+ * ssim2b200.h -- C ABI of the B200-native SSIMULACRA2 engine.
+ *
+ * The engine is a drop-in for the `Ssimulacra2` type of the turbo-metrics
+ * crate `ssimulacra2-cuda` (crates/ssimulacra2-cuda/src/lib.rs).  Every entry
+ * point below names the reference interface it replaces.  Signatures use
+ * plain pointers and sizes only; `stream` arguments are `cudaStream_t` values
+ * passed as `void *` (NULL = the legacy default stream).
+ *
+ * Images:
+ *   linear f32   packed interleaved RGB, 3 floats per pixel, rows `pitch`
+ *                bytes apart (the NPP C3 layout the reference binds)
+ *   sRGB8        packed interleaved RGB, 3 bytes per pixel, gamma-2.4 sRGB
+ *   NV12         8-bit 4:2:0, Y plane then interleaved CbCr plane (w/2 pairs
+ *                per row, h/2 rows), both with the same `pitch`
+ *   RGB16        packed RGB uint16 code values of `bits` bits (10 or 12),
+ *                BT.2020 primaries, BT.709/BT.2020 transfer
+ * Device pointers must stay valid until the stream work completes.
+ *
+ * Results: the score and the 108 pooled statistics, in the order of the
+ * reference weight table: index = c*36 + scale*6 + norm*3 + map, c in
+ * {X, Y, B}, norm 0 = mean (L1), 1 = (mean d^4)^(1/4) (L4), map 0 = SSIM
+ * error, 1 = artifact, 2 = detail loss.  Unscored scales hold 0.
+ *
+ * Thread safety: one context per thread, or external synchronisation.  No
+ * process-global state except the no-allocation entry point's scratch.
+ */
+#ifndef SSIM2B200_H
+#define SSIM2B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define S2_ABI_VERSION 1
+#define S2_NUM_STATS 108
+#define S2_NUM_SCALES 6
+
+typedef enum {
+    S2_OK = 0,
+    S2_ERR_OOM = 1,            /* device allocation failed or over the HBM budget */
+    S2_ERR_INVALID_SIZE = 2,   /* width or height below 8 (or above the limit) */
+    S2_ERR_DIM_MISMATCH = 3,   /* image does not match the context's size */
+    S2_ERR_NO_REFERENCE = 4,   /* compute_with_reference without a cached reference */
+    S2_ERR_CUDA = 5,           /* a CUDA runtime call failed (see s2_last_error) */
+    S2_ERR_TIMEOUT = 6,        /* a bounded wait ran out */
+    S2_ERR_BUSY = 7,           /* server queue full / admission refused */
+    S2_ERR_INVALID_ARG = 8,    /* NULL pointer, bad enum, bad pitch */
+    S2_ERR_NOT_READY = 9,      /* result not computed yet */
+    S2_ERR_CANCELLED = 10      /* job cancelled by the caller */
+} s2_status;
+
+/* Blur arithmetic. */
+enum {
+    /* Default.  Separable 9-tap FIR (the exact closed form of the reference's
+     * recursive Gaussian), fused with the error maps in one pass per scale,
+     * f32 arithmetic on block-shifted moments.  Scores within ~1e-4 of the
+     * FP64 oracle. */
+    S2_BLUR_FIR = 0,
+    /* The reference's own f32 recursive walk (ssimulacra2-kernel blur.rs:95-136),
+     * vertical then horizontal, reproduced operation for operation, so that
+     * the 108 statistics match ssimulacra2-cuda's arithmetic. */
+    S2_BLUR_IIR_REF = 1
+};
+
+/* Storage type of the intermediate pyramid levels and reference caches. */
+enum { S2_STORAGE_F32 = 0, S2_STORAGE_F16 = 1, S2_STORAGE_BF16 = 2 };
+
+/* Which pyramid scales are scored. */
+enum {
+    S2_SCALES_CPU = 0,  /* CPU crate ssimulacra2 0.5.1 (examples/cpu.rs:359-361) */
+    S2_SCALES_MIN8 = 1, /* ssim2-gpu (pipeline.rs:194-206): scales >= 8x8 only */
+    S2_SCALES_ALL6 = 2  /* ssimulacra2-cuda (lib.rs:138-143): always 6 */
+};
+
+/* NV12 matrix / range selectors. */
+enum { S2_MATRIX_BT709 = 0 };
+enum { S2_RANGE_LIMITED = 0 };
+
+typedef struct {
+    uint32_t struct_size;  /* sizeof(s2_config) */
+    int32_t device;        /* CUDA device ordinal */
+    int32_t blur;          /* S2_BLUR_* */
+    int32_t storage;       /* S2_STORAGE_* */
+    int32_t scale_rule;    /* S2_SCALES_* */
+    int32_t strip_rows;    /* rows per fused tile: 0 = autotuned, else 16/32/64 */
+    uint64_t hbm_budget;   /* bytes this context may allocate; 0 = no limit */
+} s2_config;
+
+typedef struct {
+    double score;
+    double stats[S2_NUM_STATS];
+    double sums[S2_NUM_STATS]; /* raw pooled sums: sum d (L1 slots), sum d^4 (L4 slots) */
+    int32_t n_scales;
+    int32_t status;            /* s2_status of this pair */
+} s2_result;
+
+typedef struct s2_ctx s2_ctx;
+
+/* ---- library ---------------------------------------------------------- */
+const char *s2_version(void);
+const char *s2_status_string(s2_status st);
+/* Message of the last failing CUDA call on this thread (empty if none). */
+const char *s2_last_error(void);
+void s2_config_default(s2_config *cfg);
+/* Number of scales scored for a w x h pair under a rule (0 if too small). */
+int s2_num_scales(uint32_t w, uint32_t h, int32_t scale_rule);
+
+/* ---- single pair (the drop-in) ----------------------------------------- */
+
+/* Replaces Ssimulacra2::new (ssimulacra2-cuda/src/lib.rs:80-197).  Allocates
+ * every intermediate for a w x h pair.  Unlike the reference, the context is
+ * not bound to input pointers: they are passed per call.  Errors instead of
+ * panics: S2_ERR_INVALID_SIZE (< 8 under the CPU/MIN8 rules), S2_ERR_OOM
+ * (pre-flight estimate over the free memory or the budget, or a failed
+ * allocation), S2_ERR_CUDA. */
+s2_status s2_create(const s2_config *cfg, uint32_t width, uint32_t height, s2_ctx **out);
+/* Replaces Drop for Ssimulacra2 (lib.rs:1195-1202); synchronises only this
+ * context's own work, then frees. */
+void s2_destroy(s2_ctx *ctx);
+/* Replaces Ssimulacra2::mem_usage (lib.rs:207-235): device bytes owned. */
+s2_status s2_mem_usage(const s2_ctx *ctx, size_t *bytes);
+s2_status s2_dimensions(const s2_ctx *ctx, uint32_t *width, uint32_t *height);
+
+/* Replaces Ssimulacra2::compute (lib.rs:421-424): enqueue the whole pair
+ * pipeline on `stream`, asynchronously.  Inputs are linear RGB on the device. */
+s2_status s2_compute_linear_f32(s2_ctx *ctx, const float *ref, size_t ref_pitch,
+                                const float *dis, size_t dis_pitch, void *stream);
+/* Replaces compute_srgb_sync / compute_from_cpu_srgb_sync (lib.rs:329-345,
+ * 391-404) without the sync: sRGB8 inputs on the device (on_host = 0) or in
+ * host memory (on_host = 1; copied through the context's staging buffers). */
+s2_status s2_compute_srgb8(s2_ctx *ctx, const uint8_t *ref, size_t ref_pitch,
+                           const uint8_t *dis, size_t dis_pitch, int32_t on_host,
+                           void *stream);
+/* NV12 pair (cuda-colorspace biplanaryuv420_to_linearrgb_8_l_bt709 followed
+ * by Ssimulacra2::compute; cuda-colorspace/src/lib.rs:33-51), conversion fused. */
+s2_status s2_compute_nv12(s2_ctx *ctx, const uint8_t *ref_y, const uint8_t *ref_uv,
+                          size_t ref_pitch, const uint8_t *dis_y, const uint8_t *dis_uv,
+                          size_t dis_pitch, int32_t matrix, int32_t range, int32_t on_host,
+                          void *stream);
+/* 10/12-bit BT.2020 RGB pair (no reference counterpart: the reference has no
+ * BT.2020 path; cuda-colorspace/src/lib.rs:46-68 are todo!()). */
+s2_status s2_compute_rgb16(s2_ctx *ctx, const uint16_t *ref, size_t ref_pitch,
+                           const uint16_t *dis, size_t dis_pitch, int32_t bits,
+                           int32_t on_host, void *stream);
+
+/* Replaces Ssimulacra2::get_score (lib.rs:427-429, post_process_scores
+ * :1018-1192).  Waits for the last enqueued compute of this context and
+ * returns its result.  Idempotent (the reference re-weights its buffer in
+ * place on every call).  `stats` / `sums` may be NULL. */
+s2_status s2_get_result(s2_ctx *ctx, double *score, double stats[S2_NUM_STATS],
+                        double sums[S2_NUM_STATS]);
+/* Replaces Ssimulacra2::compute_sync (lib.rs:409-416). */
+s2_status s2_compute_sync_linear_f32(s2_ctx *ctx, const float *ref, size_t ref_pitch,
+                                     const float *dis, size_t dis_pitch, void *stream,
+                                     double *score);
+
+/* ---- cached reference -------------------------------------------------- */
+/* Replaces set_reference_linear (lib.rs:440-546): keeps the reference's
+ * pyramid, XYB and blurred moments resident on the device. */
+s2_status s2_set_reference_linear_f32(s2_ctx *ctx, const float *ref, size_t pitch, void *stream);
+s2_status s2_set_reference_srgb8(s2_ctx *ctx, const uint8_t *ref, size_t pitch,
+                                 int32_t on_host, void *stream);
+/* Replaces compute_with_reference_linear (lib.rs:556-590); returns
+ * S2_ERR_NO_REFERENCE where the reference panics.  Asynchronous: read the
+ * result with s2_get_result. */
+s2_status s2_compute_with_reference_linear_f32(s2_ctx *ctx, const float *dis, size_t pitch,
+                                               void *stream);
+s2_status s2_compute_with_reference_srgb8(s2_ctx *ctx, const uint8_t *dis, size_t pitch,
+                                          int32_t on_host, void *stream);
+/* Replaces clear_reference / has_reference (lib.rs:595-602). */
+s2_status s2_clear_reference(s2_ctx *ctx);
+int32_t s2_has_reference(const s2_ctx *ctx);
+
+/* ---- batches of pairs of uneven sizes ---------------------------------- */
+/* Semantics from ssim2-gpu Ssim2Batch (pipeline_batch.rs:120-382), widened to
+ * mixed sizes: all pairs of a submission run as one pyramid launch, one
+ * persistent tile launch over every (pair, scale, strip) and one finalize
+ * launch.  Pairs are sRGB8 or linear f32 or NV12, on the device. */
+typedef enum { S2_FMT_LINEAR_F32 = 0, S2_FMT_SRGB8 = 1, S2_FMT_NV12 = 2, S2_FMT_RGB16 = 3 } s2_format;
+
+typedef struct {
+    uint32_t width, height;
+    int32_t format;          /* s2_format */
+    int32_t bits;            /* RGB16 only */
+    const void *ref, *dis;   /* packed image, or NV12 Y plane */
+    const void *ref_uv, *dis_uv; /* NV12 CbCr planes */
+    size_t ref_pitch, dis_pitch;
+} s2_pair_desc;
+
+typedef struct s2_batch s2_batch;
+
+/* max_pairs: most pairs per submission; max_pixels: most scale-0 pixels of
+ * all pairs of one submission together. */
+s2_status s2_batch_create(const s2_config *cfg, uint32_t max_pairs, uint64_t max_pixels,
+                          s2_batch **out);
+void s2_batch_destroy(s2_batch *b);
+/* Enqueue n pairs on `stream` (asynchronous).  A pair below 8x8 gets
+ * S2_ERR_INVALID_SIZE in its result; the others run. */
+s2_status s2_batch_submit(s2_batch *b, const s2_pair_desc *pairs, uint32_t n, void *stream);
+/* Wait for the last submission and copy its n results. */
+s2_status s2_batch_results(s2_batch *b, s2_result *out, uint32_t n);
+s2_status s2_batch_mem_usage(const s2_batch *b, size_t *bytes);
+/* Record the next submission's launches into a CUDA graph and replay it for
+ * later submissions with identical shapes (1 = on). */
+s2_status s2_batch_set_graphs(s2_batch *b, int32_t enable);
+
+/* ---- kernel timing (no reference counterpart; the reference has commented-
+ * out cuProfilerStart/Stop calls, ssimulacra2-cuda/src/lib.rs:311,963) ----
+ * When enabled, CUDA events bracket the three launches of every submission;
+ * `ms` receives the device time of the pyramid, fused and finalize kernels of
+ * the last one. */
+s2_status s2_profile_enable(s2_ctx *ctx, int32_t enable);
+s2_status s2_profile_last(s2_ctx *ctx, float ms[3]);
+s2_status s2_batch_set_profiling(s2_batch *b, int32_t enable);
+s2_status s2_batch_last_timings(s2_batch *b, float ms[3]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

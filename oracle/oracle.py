@@ -1,0 +1,177 @@
+"""ctypes wrapper of the CPU oracle (oracle/ssim2_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: the parity tests, __graft_entry__.smoke() and the
+CPU-baseline leg of bench.py use it as the checker.  The product path never
+imports it.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_build", "libssim2_oracle.so")
+
+MODE = {"fp64": 0, "cuda32": 1, "cpu32": 2, "fir32": 3}
+RULE = {"cpu": 0, "min8": 1, "all6": 2}
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB
+
+
+if not os.path.exists(LIB):
+    build()
+_lib = ctypes.CDLL(LIB)
+_P = ctypes.POINTER
+_F = _P(ctypes.c_float)
+_D = _P(ctypes.c_double)
+_U8 = _P(ctypes.c_uint8)
+_U16 = _P(ctypes.c_uint16)
+_lib.or_score_from_stats.restype = ctypes.c_double
+_lib.or_ssim2_linear.restype = ctypes.c_int
+_lib.or_ssim2_linear_f64.restype = ctypes.c_int
+_lib.or_num_scales.restype = ctypes.c_int
+_lib.or_blur_constants.restype = ctypes.c_int
+
+
+def _f(a):
+    return a.ctypes.data_as(_F)
+
+
+def _d(a):
+    return a.ctypes.data_as(_D)
+
+
+def srgb8_lut():
+    a = np.zeros(256, np.float32)
+    _lib.or_srgb8_lut(_f(a))
+    return a
+
+
+def weights():
+    w = np.zeros(108)
+    _lib.or_weights(_d(w))
+    return w
+
+
+def blur_constants():
+    arrs = [np.zeros(3, np.float32) for _ in range(5)]
+    taps = np.zeros(5)
+    radius = _lib.or_blur_constants(*[_f(a) for a in arrs], _d(taps))
+    names = ["mul_in", "mul_prev", "mul_prev2", "vert_mul_in", "vert_mul_prev"]
+    out = dict(zip(names, arrs))
+    out["radius"] = radius
+    out["fir_taps"] = taps
+    return out
+
+
+def num_scales(w, h, rule="cpu"):
+    return _lib.or_num_scales(w, h, RULE[rule])
+
+
+def score_from_stats(stats):
+    s = np.ascontiguousarray(stats, np.float64)
+    return _lib.or_score_from_stats(_d(s))
+
+
+def srgb8_to_linear(img, f64=False):
+    a = np.ascontiguousarray(img, np.uint8)
+    if f64:
+        out = np.empty(a.shape, np.float64)
+        _lib.or_srgb8_to_linear_f64(a.ctypes.data_as(_U8), ctypes.c_size_t(a.size), _d(out))
+    else:
+        out = np.empty(a.shape, np.float32)
+        _lib.or_srgb8_to_linear(a.ctypes.data_as(_U8), ctypes.c_size_t(a.size), _f(out))
+    return out
+
+
+def nv12_to_linear(y, uv, f64=False):
+    y = np.ascontiguousarray(y, np.uint8)
+    uv = np.ascontiguousarray(uv, np.uint8)
+    h, w = y.shape
+    assert uv.shape == (h // 2, w)
+    if f64:
+        out = np.empty((h, w, 3), np.float64)
+        _lib.or_nv12_to_linear_f64(y.ctypes.data_as(_U8), uv.ctypes.data_as(_U8), ctypes.c_size_t(w), w, h, _d(out))
+    else:
+        out = np.empty((h, w, 3), np.float32)
+        _lib.or_nv12_to_linear(y.ctypes.data_as(_U8), uv.ctypes.data_as(_U8), ctypes.c_size_t(w), w, h, _f(out))
+    return out
+
+
+def rgb16_to_linear(img, bits=10, f64=False):
+    a = np.ascontiguousarray(img, np.uint16)
+    n = a.size // 3
+    if f64:
+        out = np.empty(a.shape, np.float64)
+        _lib.or_rgb16_bt2020_to_linear_f64(a.ctypes.data_as(_U16), ctypes.c_size_t(n), bits, _d(out))
+    else:
+        out = np.empty(a.shape, np.float32)
+        _lib.or_rgb16_bt2020_to_linear(a.ctypes.data_as(_U16), ctypes.c_size_t(n), bits, _f(out))
+    return out
+
+
+def downscale(lin):
+    a = np.ascontiguousarray(lin, np.float32)
+    h, w, _ = a.shape
+    out = np.empty(((h + 1) // 2, (w + 1) // 2, 3), np.float32)
+    _lib.or_downscale_f32(_f(a), w, h, _f(out))
+    return out
+
+
+def linear_to_xyb(lin):
+    a = np.ascontiguousarray(lin, np.float32)
+    out = np.empty_like(a)
+    _lib.or_linear_to_xyb_f32(_f(a), ctypes.c_size_t(a.size // 3), _f(out))
+    return out
+
+
+def blur_plane(plane, mode="cuda32"):
+    a = np.ascontiguousarray(plane, np.float32)
+    h, w = a.shape
+    out = np.empty_like(a)
+    _lib.or_blur_plane_f32(_f(a), w, h, MODE[mode], _f(out))
+    return out
+
+
+def blur_plane_f64(plane):
+    a = np.ascontiguousarray(plane, np.float64)
+    h, w = a.shape
+    out = np.empty_like(a)
+    _lib.or_blur_plane_f64(_d(a), w, h, _d(out))
+    return out
+
+
+class Result:
+    def __init__(self, score, stats, sums, n_scales):
+        self.score, self.stats, self.sums, self.n_scales = score, stats, sums, n_scales
+
+
+def ssim2_linear(ref, dis, mode="fp64", rule="cpu"):
+    """Full metric from linear RGB (H, W, 3).  mode: fp64 | cuda32 | cpu32 | fir32."""
+    h, w = ref.shape[:2]
+    st = np.zeros(108)
+    su = np.zeros(108)
+    sc = ctypes.c_double()
+    ns = ctypes.c_int()
+    if mode == "fp64":
+        r = np.ascontiguousarray(ref, np.float64)
+        d = np.ascontiguousarray(dis, np.float64)
+        rc = _lib.or_ssim2_linear_f64(_d(r), _d(d), w, h, RULE[rule], _d(st), _d(su), ctypes.byref(sc),
+                                      ctypes.byref(ns))
+    else:
+        r = np.ascontiguousarray(ref, np.float32)
+        d = np.ascontiguousarray(dis, np.float32)
+        rc = _lib.or_ssim2_linear(_f(r), _f(d), w, h, MODE[mode], RULE[rule], _d(st), _d(su), ctypes.byref(sc),
+                                  ctypes.byref(ns))
+    if rc != 0:
+        raise ValueError("invalid image size %dx%d" % (w, h))
+    return Result(sc.value, st, su, ns.value)
+
+
+def ssim2_srgb8(ref, dis, mode="fp64", rule="cpu"):
+    f64 = mode == "fp64"
+    return ssim2_linear(srgb8_to_linear(ref, f64), srgb8_to_linear(dis, f64), mode, rule)

@@ -1,0 +1,21 @@
+// ssim2_launch.h -- host-side entry points of the kernels in ssim2_kernels.cu.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "ssim2_device.cuh"
+
+namespace s2 {
+const double *host_weights();
+cudaError_t upload_weights();
+cudaError_t configure_kernels();
+size_t fused_smem_bytes();
+int fused_blocks_per_sm(int storage);
+cudaError_t launch_pyramid(int storage, const DevPair *pairs, int npairs, const int *blk_first,
+                           int total_blocks, const ColorConsts &cc, const float *lut, int grid,
+                           cudaStream_t st);
+cudaError_t launch_fused(int storage, const DevPair *pairs, const Seg *segs, int nseg, int total_tiles,
+                         int *counter, double *partials, const ColorConsts &cc, const float *lut,
+                         int grid, cudaStream_t st);
+cudaError_t launch_finalize(const DevPair *pairs, int npairs, const double *partials, DevResult *out,
+                            cudaStream_t st);
+}  // namespace s2

@@ -1,0 +1,292 @@
+"""`Ssimulacra2` and `Ssim2Batch`: the reference's host API over the C ABI.
+
+Reference: crates/ssimulacra2-cuda/src/lib.rs (Ssimulacra2::new :80,
+compute :421, compute_sync :409, get_score :427, compute_srgb_sync :391,
+compute_from_cpu_srgb_sync :329, set_reference_linear :440,
+compute_with_reference_linear :556, clear_reference :595, has_reference :600,
+mem_usage :207) and crates/ssim2-gpu/src/pipeline_batch.rs (Ssim2Batch).
+
+Images on the device are torch CUDA tensors:
+  linear f32   (H, W, 3) float32, rows may be padded (stride(0) >= 3W)
+  sRGB8        (H, W, 3) uint8
+  NV12         y (H, W) uint8 and uv (H/2, W) uint8, same row stride
+  RGB16        (H, W, 3) uint16
+or `(pointer, pitch_bytes)` tuples.  Host images are numpy arrays of the
+same shapes.
+"""
+import ctypes
+
+import numpy as np
+
+from . import capi
+from .capi import lib, check, NUM_STATS
+
+
+def _stream_ptr(stream):
+    if stream is None:
+        try:
+            import torch
+            if torch.cuda.is_available():
+                return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        except ImportError:
+            pass
+        return None
+    if isinstance(stream, int):
+        return ctypes.c_void_p(stream)
+    return ctypes.c_void_p(stream.cuda_stream)
+
+
+def _dev(img, elem_bytes):
+    """(pointer, pitch in bytes) of a device image."""
+    if isinstance(img, tuple):
+        return ctypes.c_void_p(img[0]), img[1]
+    if not img.is_cuda:
+        raise capi.S2Error(capi.S2_ERR_INVALID_ARG, "expected a CUDA tensor")
+    if img.stride(-1) != 1 or (img.dim() == 3 and img.stride(1) != img.shape[2]):
+        raise capi.S2Error(capi.S2_ERR_INVALID_ARG, "rows must be packed samples")
+    return ctypes.c_void_p(img.data_ptr()), img.stride(0) * elem_bytes
+
+
+def _host(img):
+    a = np.ascontiguousarray(img)
+    return a.ctypes.data_as(ctypes.c_void_p), a.strides[0], a
+
+
+class Ssimulacra2:
+    """One (reference, distorted) size; see crates/ssimulacra2-cuda/src/lib.rs:27-77.
+
+    Unlike the reference, the instance is not bound to input buffers: every
+    compute call names them.  `Ssimulacra2.new(ref, dis)` keeps the reference's
+    binding style (`compute()` then re-reads those two tensors)."""
+
+    def __init__(self, width, height, *, device=0, storage="f32", scale_rule="cpu", strip_rows=0,
+                 hbm_budget=0):
+        self.width, self.height = int(width), int(height)
+        cfg = capi.make_config(device=device, storage=storage, scale_rule=scale_rule,
+                               strip_rows=strip_rows, hbm_budget=hbm_budget)
+        h = ctypes.c_void_p()
+        check(lib.s2_create(ctypes.byref(cfg), self.width, self.height, ctypes.byref(h)), "Ssimulacra2::new")
+        self._h = h
+        self._bound = None
+        self._keep = None
+
+    @classmethod
+    def new(cls, src_ref_linear, src_dis_linear, stream=None, **kw):
+        """Ssimulacra2::new (lib.rs:80): size from the images, bound to them."""
+        if tuple(src_ref_linear.shape) != tuple(src_dis_linear.shape):
+            raise capi.DimensionMismatch(capi.S2_ERR_DIM_MISMATCH, "Ssimulacra2::new")
+        h, w = src_ref_linear.shape[:2]
+        s = cls(w, h, **kw)
+        s._bound = (src_ref_linear, src_dis_linear)
+        return s
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.s2_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- reference API ------------------------------------------------------
+    def mem_usage(self):
+        n = ctypes.c_size_t()
+        check(lib.s2_mem_usage(self._h, ctypes.byref(n)), "mem_usage")
+        return n.value
+
+    def compute(self, stream=None):
+        """Ssimulacra2::compute (lib.rs:421): enqueue on the bound images."""
+        if self._bound is None:
+            raise capi.S2Error(capi.S2_ERR_INVALID_ARG, "compute: no bound images (use compute_linear)")
+        self.compute_linear(self._bound[0], self._bound[1], stream)
+
+    def compute_sync(self, stream=None):
+        """Ssimulacra2::compute_sync (lib.rs:409)."""
+        self.compute(stream)
+        return self.get_score()
+
+    def get_score(self):
+        """Ssimulacra2::get_score (lib.rs:427); idempotent."""
+        return self.get_result()[0]
+
+    def get_result(self):
+        """(score, stats[108], sums[108]) of the last compute."""
+        sc = ctypes.c_double()
+        st = np.zeros(NUM_STATS)
+        su = np.zeros(NUM_STATS)
+        check(lib.s2_get_result(self._h, ctypes.byref(sc), st.ctypes.data_as(capi.D),
+                                su.ctypes.data_as(capi.D)), "get_score")
+        return sc.value, st, su
+
+    def compute_linear(self, ref, dis, stream=None):
+        rp, rpitch = _dev(ref, 4)
+        dp, dpitch = _dev(dis, 4)
+        self._keep = (ref, dis)
+        check(lib.s2_compute_linear_f32(self._h, rp, rpitch, dp, dpitch, _stream_ptr(stream)), "compute")
+
+    def compute_srgb(self, src_ref, src_dis, stream=None):
+        rp, rpitch = _dev(src_ref, 1)
+        dp, dpitch = _dev(src_dis, 1)
+        self._keep = (src_ref, src_dis)
+        check(lib.s2_compute_srgb8(self._h, rp, rpitch, dp, dpitch, 0, _stream_ptr(stream)), "compute_srgb")
+
+    def compute_srgb_sync(self, src_ref, src_dis, stream=None):
+        """compute_srgb_sync (lib.rs:391): device sRGB8 pair -> score."""
+        self.compute_srgb(src_ref, src_dis, stream)
+        return self.get_score()
+
+    def compute_from_cpu_srgb_sync(self, ref_bytes, dis_bytes, stream=None):
+        """compute_from_cpu_srgb_sync (lib.rs:329): host sRGB8 (H, W, 3) pair."""
+        rp, rpitch, ra = _host(ref_bytes)
+        dp, dpitch, da = _host(dis_bytes)
+        self._check_host(ra, 3)
+        self._check_host(da, 3)
+        check(lib.s2_compute_srgb8(self._h, rp, rpitch, dp, dpitch, 1, _stream_ptr(stream)), "compute_from_cpu")
+        return self.get_score()
+
+    def compute_nv12(self, ref_y, ref_uv, dis_y, dis_uv, stream=None, on_host=False):
+        if on_host:
+            ry, rpitch, a1 = _host(ref_y)
+            ru, _, a2 = _host(ref_uv)
+            dy, dpitch, a3 = _host(dis_y)
+            du, _, a4 = _host(dis_uv)
+            self._keep = (a1, a2, a3, a4)
+        else:
+            ry, rpitch = _dev(ref_y, 1)
+            ru, _ = _dev(ref_uv, 1)
+            dy, dpitch = _dev(dis_y, 1)
+            du, _ = _dev(dis_uv, 1)
+            self._keep = (ref_y, ref_uv, dis_y, dis_uv)
+        check(lib.s2_compute_nv12(self._h, ry, ru, rpitch, dy, du, dpitch, 0, 0, int(on_host),
+                                  _stream_ptr(stream)), "compute_nv12")
+
+    def compute_rgb16(self, ref, dis, bits=10, stream=None, on_host=False):
+        if on_host:
+            rp, rpitch, a1 = _host(ref)
+            dp, dpitch, a2 = _host(dis)
+            self._keep = (a1, a2)
+        else:
+            rp, rpitch = _dev(ref, 2)
+            dp, dpitch = _dev(dis, 2)
+            self._keep = (ref, dis)
+        check(lib.s2_compute_rgb16(self._h, rp, rpitch, dp, dpitch, bits, int(on_host), _stream_ptr(stream)),
+              "compute_rgb16")
+
+    # -- cached reference ----------------------------------------------------
+    def set_reference_linear(self, src_ref_linear, stream=None):
+        """set_reference_linear (lib.rs:440)."""
+        rp, rpitch = _dev(src_ref_linear, 4)
+        check(lib.s2_set_reference_linear_f32(self._h, rp, rpitch, _stream_ptr(stream)), "set_reference_linear")
+
+    def set_reference_srgb(self, ref, stream=None, on_host=False):
+        if on_host:
+            rp, rpitch, a = _host(ref)
+            self._check_host(a, 3)
+        else:
+            rp, rpitch = _dev(ref, 1)
+        check(lib.s2_set_reference_srgb8(self._h, rp, rpitch, int(on_host), _stream_ptr(stream)), "set_reference")
+
+    def compute_with_reference_linear(self, src_dis_linear, stream=None):
+        """compute_with_reference_linear (lib.rs:556); raises NoCachedReference
+        where the reference panics."""
+        dp, dpitch = _dev(src_dis_linear, 4)
+        self._keep = (src_dis_linear,)
+        check(lib.s2_compute_with_reference_linear_f32(self._h, dp, dpitch, _stream_ptr(stream)),
+              "compute_with_reference_linear")
+        return self.get_score()
+
+    def compute_with_reference_srgb(self, dis, stream=None, on_host=False):
+        if on_host:
+            dp, dpitch, a = _host(dis)
+            self._check_host(a, 3)
+        else:
+            dp, dpitch = _dev(dis, 1)
+        self._keep = (dis,)
+        check(lib.s2_compute_with_reference_srgb8(self._h, dp, dpitch, int(on_host), _stream_ptr(stream)),
+              "compute_with_reference")
+        return self.get_score()
+
+    def clear_reference(self):
+        check(lib.s2_clear_reference(self._h), "clear_reference")
+
+    def has_reference(self):
+        return bool(lib.s2_has_reference(self._h))
+
+    def _check_host(self, a, ch):
+        if a.shape[0] != self.height or a.shape[1] != self.width or (a.ndim == 3 and a.shape[2] != ch):
+            raise capi.DimensionMismatch(capi.S2_ERR_DIM_MISMATCH, "host image shape")
+
+
+class PairDesc:
+    """One pair of a batch: device tensors of any supported format."""
+
+    def __init__(self, ref, dis, fmt="srgb8", ref_uv=None, dis_uv=None, bits=10):
+        self.ref, self.dis, self.fmt, self.ref_uv, self.dis_uv, self.bits = ref, dis, fmt, ref_uv, dis_uv, bits
+
+    def to_c(self):
+        d = capi.PairDescC()
+        eb = {"linear_f32": 4, "srgb8": 1, "nv12": 1, "rgb16": 2}[self.fmt]
+        rp, rpitch = _dev(self.ref, eb)
+        dp, dpitch = _dev(self.dis, eb)
+        d.height, d.width = self.ref.shape[0], self.ref.shape[1]
+        d.format = capi.FMT[self.fmt]
+        d.bits = self.bits
+        d.ref, d.dis = rp.value, dp.value
+        d.ref_pitch, d.dis_pitch = rpitch, dpitch
+        if self.fmt == "nv12":
+            d.ref_uv = _dev(self.ref_uv, 1)[0].value
+            d.dis_uv = _dev(self.dis_uv, 1)[0].value
+        return d
+
+
+class Ssim2Batch:
+    """Many pairs of any sizes per submission (ssim2-gpu pipeline_batch.rs:120-382,
+    widened to mixed sizes and formats)."""
+
+    def __init__(self, max_pairs, max_pixels, *, device=0, storage="f32", scale_rule="cpu", strip_rows=0,
+                 hbm_budget=0):
+        cfg = capi.make_config(device=device, storage=storage, scale_rule=scale_rule, strip_rows=strip_rows,
+                               hbm_budget=hbm_budget)
+        h = ctypes.c_void_p()
+        check(lib.s2_batch_create(ctypes.byref(cfg), max_pairs, max_pixels, ctypes.byref(h)), "Ssim2Batch::new")
+        self._h = h
+        self.max_pairs = max_pairs
+        self._n = 0
+        self._keep = None
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.s2_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def submit(self, pairs, stream=None):
+        arr = (capi.PairDescC * max(len(pairs), 1))()
+        for i, p in enumerate(pairs):
+            arr[i] = p.to_c()
+        self._keep = pairs
+        check(lib.s2_batch_submit(self._h, arr, len(pairs), _stream_ptr(stream)), "compute_batch")
+        self._n = len(pairs)
+
+    def results(self):
+        out = (capi.Result * max(self._n, 1))()
+        check(lib.s2_batch_results(self._h, out, self._n), "results")
+        return [(r.score, np.array(r.stats[:]), np.array(r.sums[:]), r.n_scales, r.status)
+                for r in out[:self._n]]
+
+    def compute_batch(self, pairs, stream=None):
+        self.submit(pairs, stream)
+        return self.results()
+
+    def mem_usage(self):
+        n = ctypes.c_size_t()
+        check(lib.s2_batch_mem_usage(self._h, ctypes.byref(n)), "mem_usage")
+        return n.value
