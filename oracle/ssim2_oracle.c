@@ -229,10 +229,11 @@ static double bt709_eotf_f64(double v) {
     if (v >= thr) return pow((v + (alpha - 1.0)) / alpha, 1.0 / 0.45);
     return v / 4.5;
 }
+static inline float eng_pow_20_9(float p);
 static float bt709_eotf_f32(float v) {
     const float beta = 0.018053968510807f, alpha = 1.0f + 5.5f * beta;
     const float thr = 0.08124285829863521110029445797874f;
-    if (v >= thr) return powf((v + (alpha - 1.0f)) / alpha, 1.0f / 0.45f);
+    if (v >= thr) return eng_pow_20_9((v + (alpha - 1.0f)) / alpha);
     return v / 4.5f;
 }
 
@@ -423,15 +424,56 @@ static void downscale_f64(const double *src, int w, int h, double *dst) {
 #define XB0 0.0037930734f
 #define XB0_ROOT 0.1559542025327239180319220163705
 
+/* Cube root as the CUDA engine computes it (ssim2_device.cuh s2_cbrtf):
+ * Newton iteration on the reciprocal cube root r <- r + r (1 - x r^3) / 3
+ * from W. Kahan's exponent-thirds bit seed, then y = x r^2 and one Newton
+ * correction.  Multiplies and fmaf only, so it rounds identically on every
+ * IEEE platform; <= 1 ulp from the true cube root.  It stands in for libm's
+ * cbrtf (the reference calls libdevice cbrtf, also <= 1 ulp). */
+static inline float eng_cbrtf(float x) {
+    if (!(x > 0.0f)) return 0.0f;
+    float sc = 1.0f;
+    if (x < 0x1p-100f) {
+        x *= 0x1p102f;
+        sc = 0x1p-34f;
+    }
+    uint32_t i;
+    memcpy(&i, &x, 4);
+    i = 0x54a2fa8cu - i / 3u;
+    float r;
+    memcpy(&r, &i, 4);
+    const float third = 0x1.555556p-2f;
+    for (int k = 0; k < 3; k++) {
+        float t = x * r;
+        t = t * r;
+        t = t * r;
+        r = fmaf(r * third, 1.0f - t, r);
+    }
+    float y = x * r;
+    y = y * r;
+    const float e = fmaf(y * y, y, -x);
+    const float c = (r * r) * third;
+    y = fmaf(-e, c, y);
+    return y * sc;
+}
+
+/* p^(20/9) (= p^(1/0.45)) as p^2 (cbrt(cbrt(p)))^2, as the engine computes it. */
+static inline float eng_pow_20_9(float p) {
+    float q = eng_cbrtf(eng_cbrtf(p));
+    return (p * p) * (q * q);
+}
+
+float or_cbrtf(float x) { return eng_cbrtf(x); }
+
 static inline void xyb_f32(float r, float g, float b, float out[3]) {
     const float m01 = 1.0f - XM02 - XM00, m11 = 1.0f - XM12 - XM10, m22 = 1.0f - XM20 - XM21;
     const float root = 0.1559542025327239180319220163705f;
     float rg = fmaf(XM00, r, fmaf(m01, g, fmaf(XM02, b, XB0)));
     float gr = fmaf(XM10, r, fmaf(m11, g, fmaf(XM12, b, XB0)));
     float bb = fmaf(XM20, r, fmaf(XM21, g, fmaf(m22, b, XB0)));
-    rg = cbrtf(rg > 0.0f ? rg : 0.0f) - root;
-    gr = cbrtf(gr > 0.0f ? gr : 0.0f) - root;
-    bb = cbrtf(bb > 0.0f ? bb : 0.0f) - root;
+    rg = eng_cbrtf(rg > 0.0f ? rg : 0.0f) - root;
+    gr = eng_cbrtf(gr > 0.0f ? gr : 0.0f) - root;
+    bb = eng_cbrtf(bb > 0.0f ? bb : 0.0f) - root;
     float x = 0.5f * (rg - gr), y = 0.5f * (rg + gr);
     out[0] = fmaf(x, 14.0f, 0.42f);
     out[1] = y + 0.01f;
@@ -720,11 +762,11 @@ static float border_gain_f(int x, int n) {
     return (float)(s - S[0]);
 }
 
-#define FIR_TW 120
+#define FIR_TW 56
 #define FIR_BAND 64
 
 /* One scale in FIR32 arithmetic.  xr/xd: planar XYB (3 planes of W*H).
- * Tiles of 120 columns x 64 rows share one shift per channel: the reference
+ * Tiles of 56 columns x 64 rows share one shift per channel: the reference
  * XYB at the tile's first column and first row.  sums[c*6 + n*3 + m]. */
 static void score_scale_fir32(const float *xr, const float *xd, int W, int H, double sums[18]) {
     const int TC = FIR_TW + 8, TR = FIR_BAND + 8;
@@ -773,14 +815,14 @@ static void score_scale_fir32(const float *xr, const float *xd, int W, int H, do
                         X[(size_t)0 * TC * FIR_BAND + (size_t)r * TC + k] = P[0 * TC * TR + (size_t)(r + 4) * TC + k];
                         X[(size_t)1 * TC * FIR_BAND + (size_t)r * TC + k] = P[1 * TC * TR + (size_t)(r + 4) * TC + k];
                     }
-                /* horizontal FIR, error maps, pooled in 5-pixel f32 chunks */
+                /* horizontal FIR, error maps, pooled in 4-pixel f32 chunks */
                 for (int r = 0; r < y1 - y0; r++) {
                     int y = y0 + r;
                     float bv = border_gain_f(y, H);
-                    for (int c0 = 0; c0 < FIR_TW; c0 += 5) {
+                    for (int c0 = 0; c0 < FIR_TW; c0 += 4) {
                         if (x0 + c0 >= W) break;
                         float fs[3] = {0, 0, 0}, f4[3] = {0, 0, 0};
-                        for (int j = 0; j < 5; j++) {
+                        for (int j = 0; j < 4; j++) {
                             int xx = x0 + c0 + j;
                             if (xx >= W) break;
                             float o[5];

@@ -98,6 +98,9 @@ int or_ssim2_linear_f64(const double *ref, const double *dis, int w, int h,
                         int rule, double stats[108], double sums[108],
                         double *score, int *n_scales);
 
+/* The engine's cube root (ssim2_device.cuh s2_cbrtf), used by every f32 mode. */
+float or_cbrtf(float x);
+
 /* Final score from the 108 statistics (cpu.rs:728-871 / lib.rs:1155-1189). */
 double or_score_from_stats(const double stats[108]);
 void or_weights(double w[108]);

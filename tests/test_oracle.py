@@ -205,3 +205,19 @@ def test_conversions_agree_f32_f64(oracle):
     m = np.zeros(9)
     oracle._lib.or_bt2020_to_bt709_matrix(m.ctypes.data_as(oracle._D))
     assert np.allclose(m.reshape(3, 3).sum(1), 1.0, atol=1e-12)  # white maps to white
+
+
+def test_engine_cube_root_within_one_ulp(oracle):
+    """The cube root shared by the engine and the oracle (Newton on the
+    reciprocal cube root, Kahan's bit seed) is within 1 ulp of the correctly
+    rounded cube root over [1e-6, 8) and exact at 0."""
+    import ctypes
+    f = oracle._lib.or_cbrtf
+    f.restype = ctypes.c_float
+    f.argtypes = [ctypes.c_float]
+    xs = np.concatenate([np.geomspace(1e-6, 8.0, 20000, dtype=np.float32), np.float32([1.0, 8.0, 0.125, 27.0])])
+    got = np.array([f(float(x)) for x in xs], np.float32)
+    want = np.cbrt(xs.astype(np.float64)).astype(np.float32)
+    ulp = np.abs(got.view(np.int32).astype(np.int64) - want.view(np.int32).astype(np.int64))
+    assert ulp.max() <= 1
+    assert f(0.0) == 0.0 and f(-1.0) == 0.0

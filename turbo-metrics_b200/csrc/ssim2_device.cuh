@@ -13,12 +13,13 @@
 namespace s2 {
 
 constexpr int kScales = 6;
-constexpr int kTileW = 120;          // output columns per fused tile
+constexpr int kTileW = 56;           // output columns per fused tile
 constexpr int kCols = kTileW + 8;    // columns incl. the 4-px halo on each side
 constexpr int kBand = 64;            // rows per shift band (tiles never straddle one)
 constexpr int kRowsPerBlk = 9;       // output rows per horizontal step (= window length)
-constexpr int kSegs = 12;            // horizontal segments per row
-constexpr int kSegW = 10;            // output pixels per segment (kSegs * kSegW == kTileW)
+constexpr int kSegs = 7;             // horizontal segments per row
+constexpr int kSegW = 8;             // output pixels per segment (kSegs * kSegW == kTileW)
+constexpr int kChunk = 4;            // pixels per f32 partial sum
 constexpr int kPyrBlk = 32;          // scale-0 block edge of the pyramid kernel
 constexpr float kC2 = 0.0009f;
 
@@ -42,8 +43,8 @@ struct DevPair {
     int fmt, bits;
     int w[kScales], h[kScales];
     int nscales;             // scored scales (>= 1)
-    int lp[kScales];         // element pitch of pyramid level s (s >= 1)
-    void *lvl[2][kScales];   // planar pyramid levels 1..5 (3 planes each)
+    int lp[kScales];         // element pitch of the XYB planes of scale s
+    void *lvl[2][kScales];   // planar XYB of scales 0..nscales-1 (3 planes each)
     int tile_base[kScales];  // first global tile of each scale
     int tile_cnt[kScales];
     int blk_base;            // first pyramid block
@@ -82,6 +83,43 @@ struct DevResult {
 #define S2_B0 0.0037930734f
 #define S2_B0_ROOT 0.1559542025327239180319220163705f
 
+// Cube root of x >= 0 (0 for x <= 0 or NaN).  Newton iteration on the
+// reciprocal cube root, r <- r + r (1 - x r^3) / 3, which needs no division,
+// from the exponent-thirds bit-manipulation seed of W. Kahan ("Computing a
+// real cube root", 1991); then y = x r^2 and one Newton correction of y.
+// Only IEEE multiplies and fused multiply-adds, so every platform rounds the
+// same way.  Error <= 1 ulp over the normal range (checked in the tests).
+__device__ __forceinline__ float s2_cbrtf(float x) {
+    if (!(x > 0.0f)) return 0.0f;
+    float sc = 1.0f;
+    if (x < 0x1p-100f) {
+        x *= 0x1p102f;
+        sc = 0x1p-34f;
+    }
+    float r = __uint_as_float(0x54a2fa8cu - __float_as_uint(x) / 3u);
+    const float third = 0x1.555556p-2f;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        float t = x * r;
+        t = t * r;
+        t = t * r;
+        r = fmaf(r * third, 1.0f - t, r);
+    }
+    float y = x * r;
+    y = y * r;
+    const float e = fmaf(y * y, y, -x);
+    const float c = (r * r) * third;
+    y = fmaf(-e, c, y);
+    return y * sc;
+}
+
+// p^(20/9) for p >= 0 (the BT.709 inverse OETF exponent 1/0.45 = 20/9),
+// as p^2 * (p^(1/9))^2 with p^(1/9) = cbrt(cbrt(p)).  <= 5 ulp.
+__device__ __forceinline__ float s2_pow_20_9(float p) {
+    const float q = s2_cbrtf(s2_cbrtf(p));
+    return (p * p) * (q * q);
+}
+
 __device__ __forceinline__ float opsin_row(int g, float r, float gg, float b) {
     const float m01 = 1.0f - S2_M02 - S2_M00;
     const float m11 = 1.0f - S2_M12 - S2_M10;
@@ -93,7 +131,7 @@ __device__ __forceinline__ float opsin_row(int g, float r, float gg, float b) {
         v = fmaf(S2_M10, r, fmaf(m11, gg, fmaf(S2_M12, b, S2_B0)));
     else
         v = fmaf(S2_M20, r, fmaf(S2_M21, gg, fmaf(m22, b, S2_B0)));
-    return cbrtf(fmaxf(v, 0.0f)) - S2_B0_ROOT;
+    return s2_cbrtf(fmaxf(v, 0.0f)) - S2_B0_ROOT;
 }
 
 // XYB channel g from the three opsin cube roots (xyb.rs:42-78).
@@ -109,7 +147,7 @@ __device__ __forceinline__ float bt709_eotf(float v) {
     const float beta = 0.018053968510807f;
     const float alpha = 1.0f + 5.5f * beta;
     const float thr = 0.08124285829863521110029445797874f;
-    if (v >= thr) return powf((v + (alpha - 1.0f)) / alpha, 1.0f / 0.45f);
+    if (v >= thr) return s2_pow_20_9((v + (alpha - 1.0f)) / alpha);
     return v / 4.5f;
 }
 

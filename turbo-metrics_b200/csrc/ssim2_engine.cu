@@ -429,7 +429,7 @@ struct Engine {
                 p.w[s] = (p.w[s - 1] + 1) / 2;
                 p.h[s] = (p.h[s - 1] + 1) / 2;
             }
-            for (int s = 1; s < p.nscales; s++) {
+            for (int s = 0; s < p.nscales; s++) {
                 p.lp[s] = (int)align_up((size_t)p.w[s], 64);
                 size_t bytes = align_up((size_t)3 * p.lp[s] * p.h[s] * esize(), 256);
                 p.lvl[0][s] = (void *)lvl_off;  // offsets, rebased at upload
@@ -438,7 +438,7 @@ struct Engine {
                 lvl_off += bytes;
             }
             P.blk_first[i] = blk;
-            if (p.nscales > 1) {
+            {
                 p.blk_x = (p.w[0] + kPyrBlk - 1) / kPyrBlk;
                 p.blk_y = (p.h[0] + kPyrBlk - 1) / kPyrBlk;
                 p.blk_base = blk;
@@ -486,7 +486,7 @@ struct Engine {
         DevPair *hp = (DevPair *)h;
         for (int i = 0; i < n; i++) {
             hp[i] = P.pairs[i];
-            for (int s = 1; s < kScales; s++)
+            for (int s = 0; s < kScales; s++)
                 for (int img = 0; img < 2; img++)
                     if (s < hp[i].nscales) hp[i].lvl[img][s] = (char *)levels_d.p + (size_t)hp[i].lvl[img][s];
                     else hp[i].lvl[img][s] = nullptr;
@@ -609,7 +609,7 @@ s2_status s2_create(const s2_config *cfg_in, uint32_t width, uint32_t height, s2
         size_t free_b = 0, total_b = 0;
         if (cudaSetDevice(cfg.device) != cudaSuccess) return cuda_fail(cudaGetLastError(), "cudaSetDevice");
         if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
-            uint64_t est = (uint64_t)width * height * 32 + (64u << 20);
+            uint64_t est = (uint64_t)width * height * 40 + (64u << 20);
             if (est > free_b || (cfg.hbm_budget && est > cfg.hbm_budget)) return S2_ERR_OOM;
         }
     }
@@ -880,7 +880,7 @@ s2_status s2_batch_create(const s2_config *cfg_in, uint32_t max_pairs, uint64_t 
     st = b->eng.init(&cfg);
     if (st == S2_OK) {
         // levels: < (1/3 + padding) of the scale-0 pixels, per image
-        size_t lv = (size_t)(max_pixels * 3 * b->eng.esize() * 2) * 2 / 3 + (size_t)max_pairs * (1u << 20);
+        size_t lv = (size_t)(max_pixels * 3 * b->eng.esize() * 2) * 4 / 3 + (size_t)max_pairs * (1u << 20);
         st = b->eng.ensure(b->eng.levels_d, lv);
         if (st == S2_OK) st = b->eng.ensure(b->eng.results_d, (size_t)max_pairs * sizeof(DevResult));
     }

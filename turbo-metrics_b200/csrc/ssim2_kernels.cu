@@ -30,13 +30,12 @@
 namespace s2 {
 
 // Shared memory layout of fused_kernel (floats).
-constexpr int kSmLin = 2 * 3 * kCols;                 // pre-linear exchange
-constexpr int kSmOp = 2 * 3 * kCols;                  // opsin cube-root exchange
-constexpr int kSmVo = kRowsPerBlk * 3 * 5 * kCols;    // vertical FIR outputs
-constexpr int kSmXo = kRowsPerBlk * 3 * 2 * kCols;    // shifted raw XYB of output rows
-constexpr int kSmLut = 256;
-constexpr int kFusedSmemFloats = kSmLin + kSmOp + kSmVo + kSmXo + kSmLut;
+constexpr int kSmVo2 = kRowsPerBlk * 3 * 2 * kCols * 2;  // vertical FIR of the plane pairs (x,y), (xx,yy)
+constexpr int kSmVo1 = kRowsPerBlk * 3 * kCols;          // vertical FIR of xy
+constexpr int kSmXo = kRowsPerBlk * 3 * kCols * 2;       // shifted raw XYB (x', y') of the output rows
+constexpr int kFusedSmemFloats = kSmVo2 + kSmVo1 + kSmXo;
 constexpr int kFusedThreads = kCols * 3;
+constexpr int kTasks = kRowsPerBlk * 3 * kSegs;          // horizontal tasks per 9-row block
 
 __device__ __forceinline__ float fir9(float a0, float a1, float a2, float a3, float a4, float a5,
                                       float a6, float a7, float a8) {
@@ -47,24 +46,33 @@ __device__ __forceinline__ float fir9(float a0, float a1, float a2, float a3, fl
     return fmaf(S2_T0, a4, acc);
 }
 
-// Linear value of channel g at (x, y) of scale s (inside the image).
-template <typename ST>
-__device__ __forceinline__ float load_pre(const DevPair &P, int img, int s, int x, int y, int g,
-                                          const float *lut, const ColorConsts &cc) {
-    if (s == 0) return pre_lin0(P, img, x, y, g, lut, cc);
-    const ST *pl = (const ST *)P.lvl[img][s] + (long long)g * P.lp[s] * P.h[s];
-    return ld_store<ST>(pl + (long long)y * P.lp[s] + x);
+// The same FIR on two planes at once (sm_100 packed f32x2; each lane rounds
+// exactly as the scalar fir9).
+__device__ __forceinline__ float2 fir9x2(float2 a0, float2 a1, float2 a2, float2 a3, float2 a4, float2 a5,
+                                         float2 a6, float2 a7, float2 a8) {
+    float2 acc = __fmul2_rn(make_float2(S2_T4, S2_T4), __fadd2_rn(a0, a8));
+    acc = __ffma2_rn(make_float2(S2_T3, S2_T3), __fadd2_rn(a1, a7), acc);
+    acc = __ffma2_rn(make_float2(S2_T2, S2_T2), __fadd2_rn(a2, a6), acc);
+    acc = __ffma2_rn(make_float2(S2_T1, S2_T1), __fadd2_rn(a3, a5), acc);
+    return __ffma2_rn(make_float2(S2_T0, S2_T0), a4, acc);
 }
 
-// Full linear RGB of a pixel (used for the shift anchor).
-template <typename ST>
-__device__ void load_lin3(const DevPair &P, int img, int s, int x, int y, const float *lut,
-                          const ColorConsts &cc, float out[3]) {
-    float p0 = load_pre<ST>(P, img, s, x, y, 0, lut, cc);
-    float p1 = load_pre<ST>(P, img, s, x, y, 1, lut, cc);
-    float p2 = load_pre<ST>(P, img, s, x, y, 2, lut, cc);
-    int fmt = s == 0 ? P.fmt : FMT_LINEAR_F32;
-    for (int g = 0; g < 3; g++) out[g] = fin_lin0(fmt, g, p0, p1, p2, cc);
+// Linear RGB of a scale-0 pixel (inside the image), any input format.
+__device__ __forceinline__ void load_lin0(const DevPair &P, int img, int x, int y, const float *lut,
+                                          const ColorConsts &cc, float out[3]) {
+    const float p0 = pre_lin0(P, img, x, y, 0, lut, cc);
+    const float p1 = pre_lin0(P, img, x, y, 1, lut, cc);
+    const float p2 = pre_lin0(P, img, x, y, 2, lut, cc);
+    for (int g = 0; g < 3; g++) out[g] = fin_lin0(P.fmt, g, p0, p1, p2, cc);
+}
+
+__device__ __forceinline__ void xyb3(const float l[3], float o[3]) {
+    const float a = opsin_row(0, l[0], l[1], l[2]);
+    const float b = opsin_row(1, l[0], l[1], l[2]);
+    const float c = opsin_row(2, l[0], l[1], l[2]);
+    o[0] = xyb_from_opsin(0, a, b, c);
+    o[1] = xyb_from_opsin(1, a, b, c);
+    o[2] = xyb_from_opsin(2, a, b, c);
 }
 
 __device__ __forceinline__ int find_seg(const Seg *segs, int nseg, int tile) {
@@ -78,15 +86,25 @@ __device__ __forceinline__ int find_seg(const Seg *segs, int nseg, int tile) {
 }
 
 // ---------------------------------------------------------------------------
-// pyramid
+// prep: input -> linear -> XYB of every scale (2x2 box pyramid in linear RGB)
 // ---------------------------------------------------------------------------
 template <typename ST>
-__global__ void __launch_bounds__(256) pyramid_kernel(const DevPair *__restrict__ pairs, int npairs,
-                                                      const int *__restrict__ blk_first,
-                                                      int total_blocks, ColorConsts cc,
-                                                      const float *__restrict__ lut_g) {
-    __shared__ float l0[2][3][kPyrBlk * kPyrBlk];                  // level-0 block [img][ch][px]
-    __shared__ float pp[2][2][3][(kPyrBlk / 2) * (kPyrBlk / 2)];  // levels >= 1, ping-pong
+__device__ __forceinline__ void store_xyb(const DevPair &P, int img, int s, int x, int y, const float lin[3]) {
+    float o[3];
+    xyb3(lin, o);
+    ST *dst = (ST *)P.lvl[img][s];
+    const long long plane = (long long)P.lp[s] * P.h[s];
+    const long long off = (long long)y * P.lp[s] + x;
+#pragma unroll
+    for (int c = 0; c < 3; c++) dst[c * plane + off] = to_store<ST>(o[c]);
+}
+
+template <typename ST>
+__global__ void __launch_bounds__(256) prep_kernel(const DevPair *__restrict__ pairs, int npairs,
+                                                   const int *__restrict__ blk_first, int total_blocks,
+                                                   ColorConsts cc, const float *__restrict__ lut_g) {
+    __shared__ float l0[2][3][kPyrBlk * kPyrBlk];                  // scale-0 linear block [img][ch][px]
+    __shared__ float pp[2][2][3][(kPyrBlk / 2) * (kPyrBlk / 2)];  // scales >= 1, ping-pong
     __shared__ float lut[256];
     for (int i = threadIdx.x; i < 256; i += blockDim.x) lut[i] = lut_g[i];
     __syncthreads();
@@ -103,9 +121,13 @@ __global__ void __launch_bounds__(256) pyramid_kernel(const DevPair *__restrict_
         const int X0 = bx * kPyrBlk, Y0 = by * kPyrBlk;
         for (int i = threadIdx.x; i < kPyrBlk * kPyrBlk; i += blockDim.x) {
             const int x = X0 + i % kPyrBlk, y = Y0 + i / kPyrBlk;
+            const bool in = x < P.w[0] && y < P.h[0];
             for (int img = 0; img < 2; img++) {
                 float v[3] = {0.f, 0.f, 0.f};
-                if (x < P.w[0] && y < P.h[0]) load_lin3<ST>(P, img, 0, x, y, lut, cc, v);
+                if (in) {
+                    load_lin0(P, img, x, y, lut, cc, v);
+                    store_xyb<ST>(P, img, 0, x, y, v);
+                }
                 for (int c = 0; c < 3; c++) l0[img][c][i] = v[c];
             }
         }
@@ -124,16 +146,16 @@ __global__ void __launch_bounds__(256) pyramid_kernel(const DevPair *__restrict_
                 const int ia = (ya - py0) * pbs, ib = (yb - py0) * pbs;
                 const int ja = xa - px0, jb = xb - px0;
                 for (int img = 0; img < 2; img++) {
-                    ST *dst = (ST *)P.lvl[img][s];
+                    float v[3];
                     for (int c = 0; c < 3; c++) {
                         const float *src = s == 1 ? l0[img][c] : pp[(s - 1) & 1][img][c];
                         float sum = src[ia + ja] + src[ia + jb];
                         sum = sum + src[ib + ja];
                         sum = sum + src[ib + jb];
-                        const float v = sum * 0.25f;
-                        pp[s & 1][img][c][i] = v;
-                        dst[(long long)c * P.lp[s] * P.h[s] + (long long)oy * P.lp[s] + ox] = to_store<ST>(v);
+                        v[c] = sum * 0.25f;
+                        pp[s & 1][img][c][i] = v[c];
                     }
+                    store_xyb<ST>(P, img, s, ox, oy, v);
                 }
             }
             __syncthreads();
@@ -145,23 +167,21 @@ __global__ void __launch_bounds__(256) pyramid_kernel(const DevPair *__restrict_
 // fused per-scale tile pass
 // ---------------------------------------------------------------------------
 template <typename ST>
-__global__ void __launch_bounds__(kFusedThreads, 1)
+__global__ void __launch_bounds__(kFusedThreads, 2)
     fused_kernel(const DevPair *__restrict__ pairs, const Seg *__restrict__ segs, int nseg,
-                 int total_tiles, int *__restrict__ counter, double *__restrict__ partials,
-                 ColorConsts cc, const float *__restrict__ lut_g) {
+                 int total_tiles, int *__restrict__ counter, double *__restrict__ partials) {
     extern __shared__ float sm[];
-    float *s_lin = sm;                 // [img][g][col]
-    float *s_op = s_lin + kSmLin;      // [img][g][col]
-    float *s_vo = s_op + kSmOp;        // [row][g][plane][col]
-    float *s_xo = s_vo + kSmVo;        // [row][g][2][col]
-    float *s_lut = s_xo + kSmXo;
+    float2 *s_vo2 = (float2 *)sm;                  // [row][g][pair][col]
+    float *s_vo1 = sm + kSmVo2;                    // [row][g][col]
+    float2 *s_xo = (float2 *)(s_vo1 + kSmVo1);     // [row][g][col]
     __shared__ int s_item;
-    __shared__ float s_c[3];
-    __shared__ double s_red[4][18];
+    __shared__ double s_red[kFusedThreads][6];
 
     const int col = threadIdx.x, g = threadIdx.y;
     const int tid = g * kCols + col;
-    for (int i = tid; i < 256; i += kFusedThreads) s_lut[i] = lut_g[i];
+    // horizontal task of this thread: row, channel, segment
+    const int t_r = tid / (3 * kSegs), t_g = (tid % (3 * kSegs)) / kSegs, t_s = tid % kSegs;
+    const bool t_on = tid < kTasks;
 
     for (;;) {
         __syncthreads();
@@ -177,123 +197,127 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
         const int tx = local % sg.tiles_x, ty = local / sg.tiles_x;
         const int x0 = tx * kTileW, y0 = ty * sg.strip_rows;
         const int y1 = min(y0 + sg.strip_rows, H);
-        const int fmt = s == 0 ? P.fmt : FMT_LINEAR_F32;
-
-        if (tid < 3) {
-            // shift anchor: reference XYB at the tile's column start, band start
-            float l[3];
-            load_lin3<ST>(P, 0, s, x0, (y0 / kBand) * kBand, s_lut, cc, l);
-            float o0 = opsin_row(0, l[0], l[1], l[2]);
-            float o1 = opsin_row(1, l[0], l[1], l[2]);
-            float o2 = opsin_row(2, l[0], l[1], l[2]);
-            s_c[tid] = xyb_from_opsin(tid, o0, o1, o2);
-        }
-        // (s_c is read after the first row's barriers)
+        const long long plane = (long long)P.lp[s] * H;
+        const ST *xr = (const ST *)P.lvl[0][s] + g * plane;
+        const ST *xd = (const ST *)P.lvl[1][s] + g * plane;
+        const int lp = P.lp[s];
+        // shift: reference XYB of channel g at the tile's first column, band start
+        const float cg = ld_store<ST>(xr + (long long)((y0 / kBand) * kBand) * lp + x0);
 
         const int x = x0 - 4 + col;
         const bool colin = (x >= 0) && (x < W);
-        float wx[9], wy[9], wxx[9], wyy[9], wxy[9];
+        float2 w2a[9], w2b[9];  // windows of (x', y') and (x'^2, y'^2)
+        float w1[9];            // window of x' y'
         double acc[6] = {0, 0, 0, 0, 0, 0};
 
-        // Stage 1 for input row y: shifted XYB channel g of ref and dis plus
-        // products; returns via the five values.
-        auto stage1 = [&](int y, float &vx, float &vy, float &vxx, float &vyy, float &vxy) {
-            const bool in = colin && y >= 0 && y < H;
-            float pr = 0.f, pd = 0.f;
+        auto shifted = [&](float vr, float vd, bool in, float2 &a, float2 &b, float &c) {
             if (in) {
-                pr = load_pre<ST>(P, 0, s, x, y, g, s_lut, cc);
-                pd = load_pre<ST>(P, 1, s, x, y, g, s_lut, cc);
-            }
-            s_lin[(0 * 3 + g) * kCols + col] = pr;
-            s_lin[(1 * 3 + g) * kCols + col] = pd;
-            __syncthreads();
-            float orr = 0.f, odd = 0.f;
-            if (in) {
-                float a0 = s_lin[0 * kCols + col], a1 = s_lin[1 * kCols + col], a2 = s_lin[2 * kCols + col];
-                float b0 = s_lin[3 * kCols + col], b1 = s_lin[4 * kCols + col], b2 = s_lin[5 * kCols + col];
-                float r0 = fin_lin0(fmt, 0, a0, a1, a2, cc), r1 = fin_lin0(fmt, 1, a0, a1, a2, cc),
-                      r2 = fin_lin0(fmt, 2, a0, a1, a2, cc);
-                float d0 = fin_lin0(fmt, 0, b0, b1, b2, cc), d1 = fin_lin0(fmt, 1, b0, b1, b2, cc),
-                      d2 = fin_lin0(fmt, 2, b0, b1, b2, cc);
-                orr = opsin_row(g, r0, r1, r2);
-                odd = opsin_row(g, d0, d1, d2);
-            }
-            s_op[(0 * 3 + g) * kCols + col] = orr;
-            s_op[(1 * 3 + g) * kCols + col] = odd;
-            __syncthreads();
-            if (in) {
-                float cg = s_c[g];
-                float xr = xyb_from_opsin(g, s_op[0 * kCols + col], s_op[1 * kCols + col], s_op[2 * kCols + col]);
-                float xd = xyb_from_opsin(g, s_op[3 * kCols + col], s_op[4 * kCols + col], s_op[5 * kCols + col]);
-                vx = xr - cg;
-                vy = xd - cg;
-                vxx = vx * vx;
-                vyy = vy * vy;
-                vxy = vx * vy;
+                const float px = vr - cg, py = vd - cg;
+                a = make_float2(px, py);
+                b = __fmul2_rn(a, a);
+                c = px * py;
             } else {
-                vx = vy = vxx = vyy = vxy = 0.f;
+                a = make_float2(0.f, 0.f);
+                b = make_float2(0.f, 0.f);
+                c = 0.f;
             }
         };
 
-        // prime the windows with input rows y0-4 .. y0+3 (slots 0..7)
+        // prime with input rows y0-4 .. y0+3 (window slots 0..7)
+        {
+            float lr[8], ld[8];
 #pragma unroll
-        for (int k = 0; k < 8; k++) stage1(y0 - 4 + k, wx[k], wy[k], wxx[k], wyy[k], wxy[k]);
+            for (int k = 0; k < 8; k++) {
+                const int y = y0 - 4 + k;
+                const bool in = colin && y >= 0 && y < H;
+                lr[k] = in ? ld_store<ST>(xr + (long long)y * lp + x) : 0.f;
+                ld[k] = in ? ld_store<ST>(xd + (long long)y * lp + x) : 0.f;
+            }
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                const int y = y0 - 4 + k;
+                shifted(lr[k], ld[k], colin && y >= 0 && y < H, w2a[k], w2b[k], w1[k]);
+            }
+        }
 
         const int rows_out = y1 - y0;
         for (int r0 = 0; r0 < rows_out; r0 += kRowsPerBlk) {
             const int nr = min(kRowsPerBlk, rows_out - r0);
+            float lr[kRowsPerBlk], ld[kRowsPerBlk];
+#pragma unroll
+            for (int k = 0; k < kRowsPerBlk; k++) {
+                const int y = y0 + r0 + k + 4;
+                const bool in = k < nr && colin && y < H;
+                lr[k] = in ? ld_store<ST>(xr + (long long)y * lp + x) : 0.f;
+                ld[k] = in ? ld_store<ST>(xd + (long long)y * lp + x) : 0.f;
+            }
 #pragma unroll
             for (int k = 0; k < kRowsPerBlk; k++) {
                 if (k < nr) {
-                    const int sl = (8 + k) % 9;  // slot of the new row
-                    stage1(y0 + r0 + k + 4, wx[sl], wy[sl], wxx[sl], wyy[sl], wxy[sl]);
-                    // window slots, oldest first: (sl+1)%9 ... sl
+                    const int sl = (8 + k) % 9;
+                    const int y = y0 + r0 + k + 4;
+                    shifted(lr[k], ld[k], colin && y < H, w2a[sl], w2b[sl], w1[sl]);
 #define S2_W(a, j) a[(sl + 1 + (j)) % 9]
-#define S2_FIR(a) fir9(S2_W(a, 0), S2_W(a, 1), S2_W(a, 2), S2_W(a, 3), S2_W(a, 4), S2_W(a, 5), S2_W(a, 6), S2_W(a, 7), S2_W(a, 8))
-                    float *vo = s_vo + (k * 3 + g) * 5 * kCols + col;
-                    vo[0 * kCols] = S2_FIR(wx);
-                    vo[1 * kCols] = S2_FIR(wy);
-                    vo[2 * kCols] = S2_FIR(wxx);
-                    vo[3 * kCols] = S2_FIR(wyy);
-                    vo[4 * kCols] = S2_FIR(wxy);
-                    float *xo = s_xo + (k * 3 + g) * 2 * kCols + col;
-                    xo[0] = S2_W(wx, 4);
-                    xo[kCols] = S2_W(wy, 4);
-#undef S2_FIR
+                    const float2 va = fir9x2(S2_W(w2a, 0), S2_W(w2a, 1), S2_W(w2a, 2), S2_W(w2a, 3), S2_W(w2a, 4),
+                                             S2_W(w2a, 5), S2_W(w2a, 6), S2_W(w2a, 7), S2_W(w2a, 8));
+                    const float2 vb = fir9x2(S2_W(w2b, 0), S2_W(w2b, 1), S2_W(w2b, 2), S2_W(w2b, 3), S2_W(w2b, 4),
+                                             S2_W(w2b, 5), S2_W(w2b, 6), S2_W(w2b, 7), S2_W(w2b, 8));
+                    const float vc = fir9(S2_W(w1, 0), S2_W(w1, 1), S2_W(w1, 2), S2_W(w1, 3), S2_W(w1, 4),
+                                          S2_W(w1, 5), S2_W(w1, 6), S2_W(w1, 7), S2_W(w1, 8));
+                    const int rb = k * 3 + g;
+                    s_vo2[(rb * 2 + 0) * kCols + col] = va;
+                    s_vo2[(rb * 2 + 1) * kCols + col] = vb;
+                    s_vo1[rb * kCols + col] = vc;
+                    s_xo[rb * kCols + col] = S2_W(w2a, 4);
 #undef S2_W
                 }
             }
             __syncthreads();
-            // horizontal FIR + error maps: task = (row, channel g, segment)
-            if (col < kRowsPerBlk * kSegs) {
-                const int r = col / kSegs, sgi = col % kSegs;
-                const int y = y0 + r0 + r;
-                const int xs = sgi * kSegW;
-                if (r < nr && x0 + xs < W) {
-                    const float cv = s_c[g];
+            // horizontal FIR + error maps: task = (row, channel, 8-px segment)
+            if (t_on && t_r < nr) {
+                const int y = y0 + r0 + t_r;
+                const int xs = t_s * kSegW;
+                if (x0 + xs < W) {
+                    const int rb = t_r * 3 + t_g;
+                    const float2 *pa = s_vo2 + (rb * 2 + 0) * kCols;
+                    const float2 *pb = s_vo2 + (rb * 2 + 1) * kCols;
+                    const float *pc = s_vo1 + rb * kCols;
+                    const float2 *px = s_xo + rb * kCols;
+                    // shift of the task's channel (same anchor as the vertical pass)
+                    const float cv = ld_store<ST>((const ST *)P.lvl[0][s] + t_g * plane +
+                                                  (long long)((y0 / kBand) * kBand) * lp + x0);
                     const float bv = border_gain(y, H);
-                    const float *vo = s_vo + (r * 3 + g) * 5 * kCols;
-                    const float *xo = s_xo + (r * 3 + g) * 2 * kCols;
 #pragma unroll
-                    for (int half = 0; half < 2; half++) {
-                        const int c0 = xs + half * 5;  // first output (tile coords)
-                        float o[5][5];
+                    for (int half = 0; half < kSegW / kChunk; half++) {
+                        const int c0 = xs + half * kChunk;  // first output (tile coords)
+                        float2 ma[kChunk], mb[kChunk];
+                        float mc[kChunk];
+                        {
+                            float2 va[kChunk + 8], vb[kChunk + 8];
+                            float vc[kChunk + 8];
 #pragma unroll
-                        for (int p = 0; p < 5; p++) {
-                            float v[13];
+                            for (int j = 0; j < kChunk + 8; j++) {
+                                va[j] = pa[c0 + j];
+                                vb[j] = pb[c0 + j];
+                                vc[j] = pc[c0 + j];
+                            }
 #pragma unroll
-                            for (int j = 0; j < 13; j++) v[j] = vo[p * kCols + c0 + j];
-#pragma unroll
-                            for (int j = 0; j < 5; j++)
-                                o[p][j] = fir9(v[j], v[j + 1], v[j + 2], v[j + 3], v[j + 4], v[j + 5], v[j + 6], v[j + 7], v[j + 8]);
+                            for (int j = 0; j < kChunk; j++) {
+                                ma[j] = fir9x2(va[j], va[j + 1], va[j + 2], va[j + 3], va[j + 4], va[j + 5], va[j + 6],
+                                               va[j + 7], va[j + 8]);
+                                mb[j] = fir9x2(vb[j], vb[j + 1], vb[j + 2], vb[j + 3], vb[j + 4], vb[j + 5], vb[j + 6],
+                                               vb[j + 7], vb[j + 8]);
+                                mc[j] = fir9(vc[j], vc[j + 1], vc[j + 2], vc[j + 3], vc[j + 4], vc[j + 5], vc[j + 6],
+                                             vc[j + 7], vc[j + 8]);
+                            }
                         }
                         float fs[3] = {0.f, 0.f, 0.f}, f4[3] = {0.f, 0.f, 0.f};
 #pragma unroll
-                        for (int j = 0; j < 5; j++) {
+                        for (int j = 0; j < kChunk; j++) {
                             const int xx = x0 + c0 + j;
                             if (xx < W) {
-                                const float m1 = o[0][j], m2 = o[1][j], s11 = o[2][j], s22 = o[3][j], s12 = o[4][j];
-                                const float xp = xo[c0 + j + 4], yp = xo[kCols + c0 + j + 4];
+                                const float m1 = ma[j].x, m2 = ma[j].y, s11 = mb[j].x, s22 = mb[j].y, s12 = mc[j];
+                                const float2 xy = px[c0 + j + 4];
                                 const float bh = border_gain(xx, W);
                                 const float corr = (float)(1.0 - (double)bh * (double)bv);
                                 const float kk = cv * corr;
@@ -307,8 +331,8 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
                                 const float den = (v1 + v2) + kC2;
                                 float d = fmaf(-num_m, num_s, den) / den;
                                 d = fmaxf(d, 0.0f);
-                                const float aa = fabsf((xp - m1) + kk);
-                                const float bb = fabsf((yp - m2) + kk);
+                                const float aa = fabsf((xy.x - m1) + kk);
+                                const float bb = fabsf((xy.y - m2) + kk);
                                 const float d1 = (bb - aa) / (1.0f + aa);
                                 const float art = fmaxf(d1, 0.0f), det = fmaxf(-d1, 0.0f);
                                 float q;
@@ -328,22 +352,15 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
             __syncthreads();
         }
 
-        // tile reduction: per channel g, warps g*4 .. g*4+3
+        // tile reduction, fixed order: sum the tasks of each channel
 #pragma unroll
-        for (int m = 0; m < 6; m++) {
-            double v = acc[m];
-#pragma unroll
-            for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-            acc[m] = v;
-        }
-        const int lane = col & 31, wg = col >> 5;  // warp within channel group
-        if (lane == 0) {
-#pragma unroll
-            for (int m = 0; m < 6; m++) s_red[wg][g * 6 + m] = acc[m];
-        }
+        for (int m = 0; m < 6; m++) s_red[tid][m] = acc[m];
         __syncthreads();
         if (tid < 18) {
-            double v = ((s_red[0][tid] + s_red[1][tid]) + s_red[2][tid]) + s_red[3][tid];
+            const int rg = tid / 6, m = tid % 6;
+            double v = 0.0;
+            for (int t = 0; t < kTasks; t++)
+                if ((t % (3 * kSegs)) / kSegs == rg) v += s_red[t][m];
             partials[(long long)item * 18 + tid] = v;
         }
     }
@@ -422,6 +439,7 @@ const double *host_weights() { return kWeights; }
 cudaError_t upload_weights() { return cudaMemcpyToSymbol(c_weight, kWeights, sizeof kWeights); }
 
 size_t fused_smem_bytes() { return (size_t)kFusedSmemFloats * sizeof(float); }
+int fused_threads() { return kFusedThreads; }
 
 template <typename ST> static const void *fused_fn() { return (const void *)fused_kernel<ST>; }
 
@@ -448,27 +466,29 @@ cudaError_t launch_pyramid(int storage, const DevPair *pairs, int npairs, const 
     if (total_blocks <= 0) return cudaSuccess;
     grid = grid > total_blocks ? total_blocks : grid;
     if (storage == ST_F16)
-        pyramid_kernel<__half><<<grid, 256, 0, st>>>(pairs, npairs, blk_first, total_blocks, cc, lut);
+        prep_kernel<__half><<<grid, 256, 0, st>>>(pairs, npairs, blk_first, total_blocks, cc, lut);
     else if (storage == ST_BF16)
-        pyramid_kernel<__nv_bfloat16><<<grid, 256, 0, st>>>(pairs, npairs, blk_first, total_blocks, cc, lut);
+        prep_kernel<__nv_bfloat16><<<grid, 256, 0, st>>>(pairs, npairs, blk_first, total_blocks, cc, lut);
     else
-        pyramid_kernel<float><<<grid, 256, 0, st>>>(pairs, npairs, blk_first, total_blocks, cc, lut);
+        prep_kernel<float><<<grid, 256, 0, st>>>(pairs, npairs, blk_first, total_blocks, cc, lut);
     return cudaGetLastError();
 }
 
 cudaError_t launch_fused(int storage, const DevPair *pairs, const Seg *segs, int nseg, int total_tiles,
                          int *counter, double *partials, const ColorConsts &cc, const float *lut,
                          int grid, cudaStream_t st) {
+    (void)cc;
+    (void)lut;
     if (total_tiles <= 0) return cudaSuccess;
     grid = grid > total_tiles ? total_tiles : grid;
     dim3 block(kCols, 3);
     size_t sm = fused_smem_bytes();
     if (storage == ST_F16)
-        fused_kernel<__half><<<grid, block, sm, st>>>(pairs, segs, nseg, total_tiles, counter, partials, cc, lut);
+        fused_kernel<__half><<<grid, block, sm, st>>>(pairs, segs, nseg, total_tiles, counter, partials);
     else if (storage == ST_BF16)
-        fused_kernel<__nv_bfloat16><<<grid, block, sm, st>>>(pairs, segs, nseg, total_tiles, counter, partials, cc, lut);
+        fused_kernel<__nv_bfloat16><<<grid, block, sm, st>>>(pairs, segs, nseg, total_tiles, counter, partials);
     else
-        fused_kernel<float><<<grid, block, sm, st>>>(pairs, segs, nseg, total_tiles, counter, partials, cc, lut);
+        fused_kernel<float><<<grid, block, sm, st>>>(pairs, segs, nseg, total_tiles, counter, partials);
     return cudaGetLastError();
 }
 
