@@ -86,7 +86,7 @@ typedef struct {
     int32_t blur;          /* S2_BLUR_* */
     int32_t storage;       /* S2_STORAGE_* */
     int32_t scale_rule;    /* S2_SCALES_* */
-    int32_t strip_rows;    /* rows per fused tile: 0 = autotuned, else 16/32/64 */
+    int32_t strip_rows;    /* rows per fused tile: 0 = autotuned, else 9/21/63 */
     uint64_t hbm_budget;   /* bytes this context may allocate; 0 = no limit */
 } s2_config;
 

@@ -443,7 +443,7 @@ static inline float eng_cbrtf(float x) {
     float r;
     memcpy(&r, &i, 4);
     const float third = 0x1.555556p-2f;
-    for (int k = 0; k < 3; k++) {
+    for (int k = 0; k < 2; k++) {
         float t = x * r;
         t = t * r;
         t = t * r;
@@ -763,10 +763,10 @@ static float border_gain_f(int x, int n) {
 }
 
 #define FIR_TW 56
-#define FIR_BAND 64
+#define FIR_BAND 63
 
 /* One scale in FIR32 arithmetic.  xr/xd: planar XYB (3 planes of W*H).
- * Tiles of 56 columns x 64 rows share one shift per channel: the reference
+ * Tiles of 56 columns x 63 rows share one shift per channel: the reference
  * XYB at the tile's first column and first row.  sums[c*6 + n*3 + m]. */
 static void score_scale_fir32(const float *xr, const float *xd, int W, int H, double sums[18]) {
     const int TC = FIR_TW + 8, TR = FIR_BAND + 8;
@@ -834,7 +834,7 @@ static void score_scale_fir32(const float *xr, const float *xd, int W, int H, do
                             float xp = X[(size_t)r * TC + c0 + j + 4];
                             float yp = X[(size_t)TC * FIR_BAND + (size_t)r * TC + c0 + j + 4];
                             float bh = border_gain_f(xx, W);
-                            float corr = (float)(1.0 - (double)bh * (double)bv);
+                            float corr = (bh == 1.0f && bv == 1.0f) ? 0.0f : (float)(1.0 - (double)bh * (double)bv);
                             float kk = cv * corr;
                             float e = cv - kk;
                             float v1 = fmaf(kk, fmaf(2.0f, m1, e), fmaf(-m1, m1, s11));

@@ -221,7 +221,7 @@ def test_batch_nv12_1080p_pair(tmb, oracle, cuda):
     assert abs(out[0][0] - exact.score) < FP64_TOL, (out[0][0], exact.score)
 
 
-@pytest.mark.parametrize("storage,tol", [("f16", 0.2), ("bf16", 2.0)])
+@pytest.mark.parametrize("storage,tol", [("f16", 0.2), ("bf16", 4.0)])
 def test_reduced_precision_storage(tmb, oracle, cuda, storage, tol):
     """FP16/BF16 storage of the XYB planes (arithmetic stays f32): the error
     against FP64 is reported, not hidden; the bound is the stated one."""

@@ -245,7 +245,7 @@ struct Plan {
     int total_blocks = 0;
     int total_tiles = 0;
     size_t level_bytes = 0;  // both images, all levels, all pairs
-    int strip_rows = 64;
+    int strip_rows = 63;
 };
 
 struct Engine {
@@ -366,12 +366,12 @@ struct Engine {
     }
 
     int choose_strip_rows(const std::vector<uint64_t> &tiles_at) const {
-        if (strip_rows_cfg == 16 || strip_rows_cfg == 32 || strip_rows_cfg == 64) return strip_rows_cfg;
+        if (strip_rows_cfg == 9 || strip_rows_cfg == 21 || strip_rows_cfg == 63) return strip_rows_cfg;
         // largest strip height that still gives ~4 waves of resident tiles
         const uint64_t resident = (uint64_t)num_sms * (uint64_t)fused_bps;
-        if (tiles_at[0] >= 4 * resident) return 64;
-        if (tiles_at[1] >= 4 * resident) return 32;
-        return 16;
+        if (tiles_at[0] >= 4 * resident) return 63;
+        if (tiles_at[1] >= 4 * resident) return 21;
+        return 9;
     }
 
     // Lay out the levels and tiles of n pairs.
@@ -386,8 +386,8 @@ struct Engine {
             ns[i] = num_scales_rule(d[i].width, d[i].height, scale_rule);
             uint64_t w = d[i].width, h = d[i].height;
             for (int s = 0; s < ns[i]; s++) {
-                tiles_at[0] += ((w + kTileW - 1) / kTileW) * ((h + 63) / 64);
-                tiles_at[1] += ((w + kTileW - 1) / kTileW) * ((h + 31) / 32);
+                tiles_at[0] += ((w + kTileW - 1) / kTileW) * ((h + 62) / 63);
+                tiles_at[1] += ((w + kTileW - 1) / kTileW) * ((h + 20) / 21);
                 w = (w + 1) / 2;
                 h = (h + 1) / 2;
             }
@@ -585,7 +585,7 @@ static s2_status check_cfg(const s2_config *cfg) {
     if (cfg->blur != S2_BLUR_FIR && cfg->blur != S2_BLUR_IIR_REF) return S2_ERR_INVALID_ARG;
     if (cfg->storage < 0 || cfg->storage > 2) return S2_ERR_INVALID_ARG;
     if (cfg->scale_rule < 0 || cfg->scale_rule > 2) return S2_ERR_INVALID_ARG;
-    if (cfg->strip_rows != 0 && cfg->strip_rows != 16 && cfg->strip_rows != 32 && cfg->strip_rows != 64)
+    if (cfg->strip_rows != 0 && cfg->strip_rows != 9 && cfg->strip_rows != 21 && cfg->strip_rows != 63)
         return S2_ERR_INVALID_ARG;
     return S2_OK;
 }

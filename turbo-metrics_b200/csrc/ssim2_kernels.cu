@@ -29,13 +29,21 @@
 
 namespace s2 {
 
-// Shared memory layout of fused_kernel (floats).
-constexpr int kSmVo2 = kRowsPerBlk * 3 * 2 * kCols * 2;  // vertical FIR of the plane pairs (x,y), (xx,yy)
-constexpr int kSmVo1 = kRowsPerBlk * 3 * kCols;          // vertical FIR of xy
-constexpr int kSmXo = kRowsPerBlk * 3 * kCols * 2;       // shifted raw XYB (x', y') of the output rows
+// Shared memory layout of fused_kernel.  Rows ("rb" = output row of the
+// block x channel, 27 of them) are kRowStride elements apart: with an odd
+// stride and the horizontal tasks numbered segment-major (lane t reads row
+// t % 27, segment t / 27), the 8-byte loads of a half-warp and the 4-byte
+// loads of a warp fall in distinct banks (at most 2-way where a warp spans two
+// segments), where the plain 64-element stride gave up to 10-way conflicts.
+constexpr int kRB = kRowsPerBlk * 3;                     // rows of one block
+constexpr int kRowStride = 73;
+constexpr int kSmVo2 = 2 * kRB * kRowStride * 2;         // vertical FIR of the plane pairs (x,y), (xx,yy) [pair][rb][col]
+constexpr int kSmVo1 = kRB * kRowStride;                 // vertical FIR of xy [rb][col]
+constexpr int kSmXo = kRB * kRowStride * 2;              // shifted raw XYB (x', y') of the output rows [rb][col]
 constexpr int kFusedSmemFloats = kSmVo2 + kSmVo1 + kSmXo;
+static_assert(kSmVo2 % 2 == 0 && kSmXo % 2 == 0, "float2 arrays must stay 8-byte aligned");
 constexpr int kFusedThreads = kCols * 3;
-constexpr int kTasks = kRowsPerBlk * 3 * kSegs;          // horizontal tasks per 9-row block
+constexpr int kTasks = kRB * kSegs;                      // horizontal tasks per 9-row block
 
 __device__ __forceinline__ float fir9(float a0, float a1, float a2, float a3, float a4, float a5,
                                       float a6, float a7, float a8) {
@@ -171,16 +179,18 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
     fused_kernel(const DevPair *__restrict__ pairs, const Seg *__restrict__ segs, int nseg,
                  int total_tiles, int *__restrict__ counter, double *__restrict__ partials) {
     extern __shared__ float sm[];
-    float2 *s_vo2 = (float2 *)sm;                  // [row][g][pair][col]
-    float *s_vo1 = sm + kSmVo2;                    // [row][g][col]
-    float2 *s_xo = (float2 *)(s_vo1 + kSmVo1);     // [row][g][col]
+    // float2 arrays first: kSmVo2 and kSmXo are even, kSmVo1 (27 x 73) is odd
+    float2 *s_vo2 = (float2 *)sm;                  // [pair][rb][col]
+    float2 *s_xo = (float2 *)(sm + kSmVo2);        // [rb][col]
+    float *s_vo1 = sm + kSmVo2 + kSmXo;            // [rb][col]
     __shared__ int s_item;
     __shared__ double s_red[kFusedThreads][6];
 
     const int col = threadIdx.x, g = threadIdx.y;
     const int tid = g * kCols + col;
-    // horizontal task of this thread: row, channel, segment
-    const int t_r = tid / (3 * kSegs), t_g = (tid % (3 * kSegs)) / kSegs, t_s = tid % kSegs;
+    // horizontal task of this thread: segment-major over the 27 block rows
+    const int t_rb = tid % kRB, t_s = tid / kRB;
+    const int t_r = t_rb / 3, t_g = t_rb % 3;
     const bool t_on = tid < kTasks;
 
     for (;;) {
@@ -265,10 +275,10 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
                     const float vc = fir9(S2_W(w1, 0), S2_W(w1, 1), S2_W(w1, 2), S2_W(w1, 3), S2_W(w1, 4),
                                           S2_W(w1, 5), S2_W(w1, 6), S2_W(w1, 7), S2_W(w1, 8));
                     const int rb = k * 3 + g;
-                    s_vo2[(rb * 2 + 0) * kCols + col] = va;
-                    s_vo2[(rb * 2 + 1) * kCols + col] = vb;
-                    s_vo1[rb * kCols + col] = vc;
-                    s_xo[rb * kCols + col] = S2_W(w2a, 4);
+                    s_vo2[rb * kRowStride + col] = va;
+                    s_vo2[(kRB + rb) * kRowStride + col] = vb;
+                    s_vo1[rb * kRowStride + col] = vc;
+                    s_xo[rb * kRowStride + col] = S2_W(w2a, 4);
 #undef S2_W
                 }
             }
@@ -278,11 +288,11 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
                 const int y = y0 + r0 + t_r;
                 const int xs = t_s * kSegW;
                 if (x0 + xs < W) {
-                    const int rb = t_r * 3 + t_g;
-                    const float2 *pa = s_vo2 + (rb * 2 + 0) * kCols;
-                    const float2 *pb = s_vo2 + (rb * 2 + 1) * kCols;
-                    const float *pc = s_vo1 + rb * kCols;
-                    const float2 *px = s_xo + rb * kCols;
+                    const int rb = t_rb;
+                    const float2 *pa = s_vo2 + rb * kRowStride;
+                    const float2 *pb = s_vo2 + (kRB + rb) * kRowStride;
+                    const float *pc = s_vo1 + rb * kRowStride;
+                    const float2 *px = s_xo + rb * kRowStride;
                     // shift of the task's channel (same anchor as the vertical pass)
                     const float cv = ld_store<ST>((const ST *)P.lvl[0][s] + t_g * plane +
                                                   (long long)((y0 / kBand) * kBand) * lp + x0);
@@ -319,7 +329,8 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
                                 const float m1 = ma[j].x, m2 = ma[j].y, s11 = mb[j].x, s22 = mb[j].y, s12 = mc[j];
                                 const float2 xy = px[c0 + j + 4];
                                 const float bh = border_gain(xx, W);
-                                const float corr = (float)(1.0 - (double)bh * (double)bv);
+                                const float corr =
+                                    (bh == 1.0f && bv == 1.0f) ? 0.0f : (float)(1.0 - (double)bh * (double)bv);
                                 const float kk = cv * corr;
                                 const float e = cv - kk;
                                 const float v1 = fmaf(kk, fmaf(2.0f, m1, e), fmaf(-m1, m1, s11));
@@ -360,7 +371,7 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
             const int rg = tid / 6, m = tid % 6;
             double v = 0.0;
             for (int t = 0; t < kTasks; t++)
-                if ((t % (3 * kSegs)) / kSegs == rg) v += s_red[t][m];
+                if ((t % kRB) % 3 == rg) v += s_red[t][m];
             partials[(long long)item * 18 + tid] = v;
         }
     }

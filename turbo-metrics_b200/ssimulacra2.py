@@ -81,9 +81,9 @@ class Ssimulacra2:
         return s
 
     def close(self):
-        if getattr(self, "_h", None):
+        if getattr(self, "_h", None) and lib is not None:
             lib.s2_destroy(self._h)
-            self._h = None
+        self._h = None
 
     def __del__(self):
         self.close()
@@ -261,9 +261,9 @@ class Ssim2Batch:
         self._keep = None
 
     def close(self):
-        if getattr(self, "_h", None):
+        if getattr(self, "_h", None) and lib is not None:
             lib.s2_batch_destroy(self._h)
-            self._h = None
+        self._h = None
 
     def __del__(self):
         self.close()
