@@ -273,7 +273,8 @@ def main():
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "kernel": "fused_kernel<float>",
                 "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
-                "kernel_ms": {"pyramid": float(acc[0]), "fused": fused_ms, "finalize": float(acc[2])},
+                "kernel_ms": {"prep": float(acc[0]), "fused": fused_ms, "finalize": float(acc[2])},
+                "fused_blocks_per_sm": int(lib.s2_fused_blocks_per_sm(0)),
                 "algorithmic_bytes_per_launch": ab}
 
     # ---- plain: the drop-in, one pair at a time ----------------------------

@@ -217,6 +217,8 @@ s2_status s2_profile_enable(s2_ctx *ctx, int32_t enable);
 s2_status s2_profile_last(s2_ctx *ctx, float ms[3]);
 s2_status s2_batch_set_profiling(s2_batch *b, int32_t enable);
 s2_status s2_batch_last_timings(s2_batch *b, float ms[3]);
+/* Resident blocks per SM of the fused kernel for a storage type (0 on error). */
+int32_t s2_fused_blocks_per_sm(int32_t storage);
 
 #ifdef __cplusplus
 }

@@ -230,11 +230,14 @@ static double bt709_eotf_f64(double v) {
     return v / 4.5;
 }
 static inline float eng_pow_20_9(float p);
+/* The engine's f32 BT.709 inverse OETF: divisions by alpha and 4.5 become
+ * multiplications by their f32 reciprocals; both branches evaluated. */
 static float bt709_eotf_f32(float v) {
-    const float beta = 0.018053968510807f, alpha = 1.0f + 5.5f * beta;
+    const float alpha_m1 = 0x1.96b84p-4f, inv_alpha = 0x1.d1c096p-1f;
     const float thr = 0.08124285829863521110029445797874f;
-    if (v >= thr) return eng_pow_20_9((v + (alpha - 1.0f)) / alpha);
-    return v / 4.5f;
+    const float hi = eng_pow_20_9((v + alpha_m1) * inv_alpha);
+    const float lo = v * 0x1.c71c72p-3f;
+    return v >= thr ? hi : lo;
 }
 
 static float clamp01f(float v) { return v < 0.0f ? 0.0f : (v > 1.0f ? 1.0f : v); }
@@ -427,41 +430,85 @@ static void downscale_f64(const double *src, int w, int h, double *dst) {
 /* Cube root as the CUDA engine computes it (ssim2_device.cuh s2_cbrtf):
  * Newton iteration on the reciprocal cube root r <- r + r (1 - x r^3) / 3
  * from W. Kahan's exponent-thirds bit seed, then y = x r^2 and one Newton
- * correction.  Multiplies and fmaf only, so it rounds identically on every
- * IEEE platform; <= 1 ulp from the true cube root.  It stands in for libm's
- * cbrtf (the reference calls libdevice cbrtf, also <= 1 ulp). */
-static inline float eng_cbrtf(float x) {
-    if (!(x > 0.0f)) return 0.0f;
-    float sc = 1.0f;
-    if (x < 0x1p-100f) {
-        x *= 0x1p102f;
-        sc = 0x1p-34f;
-    }
+ * correction; selects instead of branches.  Multiplies and fmaf only, so it
+ * rounds identically on every IEEE platform; <= 1 ulp from the true cube
+ * root.  It stands in for libm's cbrtf (the reference calls libdevice cbrtf,
+ * also <= 1 ulp). */
+static inline float asf(uint32_t i) {
+    float f;
+    memcpy(&f, &i, 4);
+    return f;
+}
+static inline uint32_t asu(float f) {
     uint32_t i;
-    memcpy(&i, &x, 4);
-    i = 0x54a2fa8cu - i / 3u;
-    float r;
-    memcpy(&r, &i, 4);
+    memcpy(&i, &f, 4);
+    return i;
+}
+static inline float eng_cbrtf(float x) {
+    const int pos = x > 0.0f, tiny = x < 0x1p-100f;
+    float xs = tiny ? x * 0x1p102f : x;
+    xs = pos ? xs : 1.0f;
+    float r = asf(0x54a2fa8cu - asu(xs) / 3u);
     const float third = 0x1.555556p-2f;
     for (int k = 0; k < 2; k++) {
-        float t = x * r;
+        float t = xs * r;
         t = t * r;
         t = t * r;
         r = fmaf(r * third, 1.0f - t, r);
     }
-    float y = x * r;
+    float y = xs * r;
     y = y * r;
-    const float e = fmaf(y * y, y, -x);
+    const float e = fmaf(y * y, y, -xs);
     const float c = (r * r) * third;
     y = fmaf(-e, c, y);
-    return y * sc;
+    y = y * (tiny ? 0x1p-34f : 1.0f);
+    return pos ? y : 0.0f;
 }
 
-/* p^(20/9) (= p^(1/0.45)) as p^2 (cbrt(cbrt(p)))^2, as the engine computes it. */
-static inline float eng_pow_20_9(float p) {
-    float q = eng_cbrtf(eng_cbrtf(p));
-    return (p * p) * (q * q);
+/* a / b for b > 0 as the engine computes it (s2_div): Newton reciprocal
+ * from the bit seed 0x7EF311C3 - bits(b), three steps, then one residual
+ * correction of q = a r. */
+static inline float eng_div(float a, float b) {
+    float r = asf(0x7EF311C3u - asu(b));
+    r = fmaf(r, fmaf(-b, r, 1.0f), r);
+    r = fmaf(r, fmaf(-b, r, 1.0f), r);
+    r = fmaf(r, fmaf(-b, r, 1.0f), r);
+    const float q = a * r;
+    const float e = fmaf(-b, q, a);
+    return fmaf(e, r, q);
 }
+float or_div(float a, float b) { return eng_div(a, b); }
+
+/* p^(20/9) (= p^(1/0.45)) as the engine computes it (ssim2_device.cuh
+ * s2_pow_20_9): p = m 2^e, m^(20/9) by a degree-7 polynomial in m - 1.5
+ * (Horner, fmaf), times 2^(2e + k) 2^(r/9) with 2e = 9k + r.  <= 3.3 ulp. */
+static inline float eng_pow2_r9(int r) {
+    static const float T[9] = {0x1p+0f, 0x1.147eccp+0f, 0x1.2aa1a6p+0f, 0x1.428a3p+0f, 0x1.5c5cbcp+0f,
+                               0x1.784086p+0f, 0x1.965feap+0f, 0x1.b6e8aep+0f, 0x1.da0c4p+0f};
+    return T[r];
+}
+static inline float eng_pow_20_9(float p) {
+    const int pos = p > 0.0f;
+    const uint32_t b = asu(pos ? p : 1.0f);
+    const int e = (int)((b >> 23) & 0xffu) - 127;
+    const float t = asf((b & 0x7fffffu) | 0x3f800000u) - 1.5f;
+    float y = 0x1.1eb37ap-12f;
+    y = fmaf(y, t, -0x1.88e318p-11f);
+    y = fmaf(y, t, 0x1.2713a6p-9f);
+    y = fmaf(y, t, -0x1.37717ep-7f);
+    y = fmaf(y, t, 0x1.2c9724p-4f);
+    y = fmaf(y, t, 0x1.7c6f02p+0f);
+    y = fmaf(y, t, 0x1.d2e55cp+1f);
+    y = fmaf(y, t, 0x1.3b279ep+1f);
+    const int n = 2 * e;
+    const int k = (n + 261) / 9 - 29;
+    const int r = n - 9 * k;
+    y = y * eng_pow2_r9(r);
+    y = y * asf((uint32_t)(2 * e + k + 127) << 23);
+    return pos ? y : 0.0f;
+}
+
+float or_pow_20_9(float p) { return eng_pow_20_9(p); }
 
 float or_cbrtf(float x) { return eng_cbrtf(x); }
 
@@ -844,11 +891,11 @@ static void score_scale_fir32(const float *xr, const float *xd, int W, int H, do
                             float num_m = fmaf(-md, md, 1.0f);
                             float num_s = fmaf(2.0f, cov, 0.0009f);
                             float den = (v1 + v2) + 0.0009f;
-                            float d = fmaf(-num_m, num_s, den) / den;
+                            float d = eng_div(fmaf(-num_m, num_s, den), den);
                             d = d > 0.0f ? d : 0.0f;
                             float aa = fabsf((xp - m1) + kk);
                             float bb = fabsf((yp - m2) + kk);
-                            float d1 = (bb - aa) / (1.0f + aa);
+                            float d1 = eng_div(bb - aa, 1.0f + aa);
                             float art = d1 > 0.0f ? d1 : 0.0f, det = -d1 > 0.0f ? -d1 : 0.0f;
                             float q;
                             fs[0] += d;   q = d * d;     f4[0] += q * q;

@@ -100,6 +100,10 @@ int or_ssim2_linear_f64(const double *ref, const double *dis, int w, int h,
 
 /* The engine's cube root (ssim2_device.cuh s2_cbrtf), used by every f32 mode. */
 float or_cbrtf(float x);
+/* The engine's division for b > 0 (Newton reciprocal + correction). */
+float or_div(float a, float b);
+/* The engine's p^(20/9) (BT.709 inverse OETF power). */
+float or_pow_20_9(float p);
 
 /* Final score from the 108 statistics (cpu.rs:728-871 / lib.rs:1155-1189). */
 double or_score_from_stats(const double stats[108]);

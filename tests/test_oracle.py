@@ -221,3 +221,34 @@ def test_engine_cube_root_within_one_ulp(oracle):
     ulp = np.abs(got.view(np.int32).astype(np.int64) - want.view(np.int32).astype(np.int64))
     assert ulp.max() <= 1
     assert f(0.0) == 0.0 and f(-1.0) == 0.0
+
+
+def test_engine_eotf_power_within_4_ulp(oracle):
+    """p^(20/9) of the BT.709 inverse OETF, shared by the engine and the
+    oracle (degree-7 polynomial on the mantissa, exponent table): <= 4 ulp of
+    the correctly rounded power over [0.1, 2]."""
+    import ctypes
+    f = oracle._lib.or_pow_20_9
+    f.restype = ctypes.c_float
+    f.argtypes = [ctypes.c_float]
+    ps = np.linspace(0.1, 2.0, 40001, dtype=np.float32)
+    got = np.array([f(float(p)) for p in ps], np.float32)
+    want = np.power(ps.astype(np.float64), 20.0 / 9.0)
+    ulp = np.abs(got.astype(np.float64) - want) / np.spacing(want.astype(np.float32)).astype(np.float64)
+    assert ulp.max() <= 4.0
+    assert f(1.0) == 1.0 and f(0.0) == 0.0
+
+
+def test_engine_division_matches_ieee(oracle):
+    """The engine's FMA-only division (Newton reciprocal from a bit seed plus
+    one residual correction) equals IEEE division on the operand ranges of the
+    error maps: denominators in [9e-4, 4], numerators of either sign."""
+    import ctypes
+    f = oracle._lib.or_div
+    f.restype = ctypes.c_float
+    f.argtypes = [ctypes.c_float, ctypes.c_float]
+    rng = np.random.default_rng(7)
+    b = np.exp(rng.uniform(np.log(9e-4), np.log(4.0), 20000)).astype(np.float32)
+    a = (rng.uniform(-2, 2, 20000) * b * np.exp(rng.uniform(-5, 2, 20000))).astype(np.float32)
+    got = np.array([f(float(x), float(y)) for x, y in zip(a, b)], np.float32)
+    assert np.array_equal(got, a / b)

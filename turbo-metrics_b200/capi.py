@@ -119,6 +119,7 @@ _sig = {
     "s2_profile_last": (ctypes.c_int, [P, ctypes.POINTER(ctypes.c_float)]),
     "s2_batch_set_profiling": (ctypes.c_int, [P, ctypes.c_int32]),
     "s2_batch_last_timings": (ctypes.c_int, [P, ctypes.POINTER(ctypes.c_float)]),
+    "s2_fused_blocks_per_sm": (ctypes.c_int32, [ctypes.c_int32]),
 }
 for _name, (_res, _args) in _sig.items():
     _f = getattr(lib, _name)

@@ -87,38 +87,79 @@ struct DevResult {
 // reciprocal cube root, r <- r + r (1 - x r^3) / 3, which needs no division,
 // from the exponent-thirds bit-manipulation seed of W. Kahan ("Computing a
 // real cube root", 1991); then y = x r^2 and one Newton correction of y.
-// Only IEEE multiplies and fused multiply-adds, so every platform rounds the
-// same way.  Two iterations from the ~3% seed leave ~1e-5, which the final
-// correction squares away: <= 1 ulp over [1e-30, 1e30] (checked in the tests).
+// Only IEEE multiplies and fused multiply-adds, and no branches, so every
+// platform rounds the same way.  Two iterations from the ~3% seed leave
+// ~1e-5, which the final correction squares away: <= 1 ulp over
+// [1e-30, 1e30] (checked in the tests).
 __device__ __forceinline__ float s2_cbrtf(float x) {
-    if (!(x > 0.0f)) return 0.0f;
-    float sc = 1.0f;
-    if (x < 0x1p-100f) {
-        x *= 0x1p102f;
-        sc = 0x1p-34f;
-    }
-    float r = __uint_as_float(0x54a2fa8cu - __float_as_uint(x) / 3u);
+    const bool pos = x > 0.0f, tiny = x < 0x1p-100f;
+    float xs = tiny ? x * 0x1p102f : x;
+    xs = pos ? xs : 1.0f;
+    float r = __uint_as_float(0x54a2fa8cu - __float_as_uint(xs) / 3u);
     const float third = 0x1.555556p-2f;
 #pragma unroll
     for (int k = 0; k < 2; k++) {
-        float t = x * r;
+        float t = xs * r;
         t = t * r;
         t = t * r;
         r = fmaf(r * third, 1.0f - t, r);
     }
-    float y = x * r;
+    float y = xs * r;
     y = y * r;
-    const float e = fmaf(y * y, y, -x);
+    const float e = fmaf(y * y, y, -xs);
     const float c = (r * r) * third;
     y = fmaf(-e, c, y);
-    return y * sc;
+    y = y * (tiny ? 0x1p-34f : 1.0f);
+    return pos ? y : 0.0f;
 }
 
-// p^(20/9) for p >= 0 (the BT.709 inverse OETF exponent 1/0.45 = 20/9),
-// as p^2 * (p^(1/9))^2 with p^(1/9) = cbrt(cbrt(p)).  <= 5 ulp.
+// a / b for b > 0 normal, without a division instruction: Newton iteration
+// on 1/b from the bit-pattern seed 0x7EF311C3 - bits(b) (three steps of
+// r <- r + r (1 - b r)), then one residual correction of q = a r.  FMA and
+// multiply only, no branches; identical to IEEE division on 5e7 samples of
+// the ranges used here (checked in the tests).
+__device__ __forceinline__ float s2_div(float a, float b) {
+    float r = __uint_as_float(0x7EF311C3u - __float_as_uint(b));
+    r = fmaf(r, fmaf(-b, r, 1.0f), r);
+    r = fmaf(r, fmaf(-b, r, 1.0f), r);
+    r = fmaf(r, fmaf(-b, r, 1.0f), r);
+    const float q = a * r;
+    const float e = fmaf(-b, q, a);
+    return fmaf(e, r, q);
+}
+
+// 2^(r/9), r = 0..8, rounded to f32
+__device__ __forceinline__ float s2_pow2_r9(int r) {
+    const float lo = r < 2 ? (r == 0 ? 0x1p+0f : 0x1.147eccp+0f) : (r == 2 ? 0x1.2aa1a6p+0f : 0x1.428a3p+0f);
+    const float mid = r < 6 ? (r == 4 ? 0x1.5c5cbcp+0f : 0x1.784086p+0f) : (r == 6 ? 0x1.965feap+0f : 0x1.b6e8aep+0f);
+    return r < 4 ? lo : (r < 8 ? mid : 0x1.da0c4p+0f);
+}
+
+// p^(20/9) for normal p > 0 (the BT.709 inverse OETF exponent 1/0.45 =
+// 20/9), 0 for p <= 0.  With p = m 2^e, m in [1, 2): m^(20/9) is a degree-7
+// polynomial in t = m - 1.5 (Chebyshev interpolation at 8 nodes, converted
+// to monomials and rounded to f32; Horner with fmaf), times 2^(20e/9) =
+// 2^(2e + k) 2^(r/9) with 2e = 9k + r, 0 <= r < 9.  Branch-free; <= 3.3 ulp
+// on [0.1, 2].
 __device__ __forceinline__ float s2_pow_20_9(float p) {
-    const float q = s2_cbrtf(s2_cbrtf(p));
-    return (p * p) * (q * q);
+    const bool pos = p > 0.0f;
+    const unsigned b = __float_as_uint(pos ? p : 1.0f);
+    const int e = (int)((b >> 23) & 0xffu) - 127;
+    const float t = __uint_as_float((b & 0x7fffffu) | 0x3f800000u) - 1.5f;
+    float y = 0x1.1eb37ap-12f;
+    y = fmaf(y, t, -0x1.88e318p-11f);
+    y = fmaf(y, t, 0x1.2713a6p-9f);
+    y = fmaf(y, t, -0x1.37717ep-7f);
+    y = fmaf(y, t, 0x1.2c9724p-4f);
+    y = fmaf(y, t, 0x1.7c6f02p+0f);
+    y = fmaf(y, t, 0x1.d2e55cp+1f);
+    y = fmaf(y, t, 0x1.3b279ep+1f);
+    const int n = 2 * e;
+    const int k = (n + 261) / 9 - 29;  // floor(n / 9) for n >= -261
+    const int r = n - 9 * k;
+    y = y * s2_pow2_r9(r);
+    y = y * __uint_as_float((unsigned)(2 * e + k + 127) << 23);
+    return pos ? y : 0.0f;
 }
 
 __device__ __forceinline__ float opsin_row(int g, float r, float gg, float b) {
@@ -143,13 +184,17 @@ __device__ __forceinline__ float xyb_from_opsin(int g, float rg, float gr, float
     return (bb - y) + 0.55f;
 }
 
-// BT.709 inverse OETF (crates/cuda-colorspace-kernel/src/lib.rs:223-238).
+// BT.709 inverse OETF (crates/cuda-colorspace-kernel/src/lib.rs:223-238):
+// ((v + (alpha - 1)) / alpha)^(1/0.45) above the threshold, v / 4.5 below.
+// The two divisions are multiplications by the f32 reciprocals 1/alpha and
+// 2/9 (<= 1 ulp from dividing); both branches are evaluated and selected.
 __device__ __forceinline__ float bt709_eotf(float v) {
-    const float beta = 0.018053968510807f;
-    const float alpha = 1.0f + 5.5f * beta;
+    const float alpha_m1 = 0x1.96b84p-4f;    // alpha - 1, alpha = 1 + 5.5 * 0.018053968510807
+    const float inv_alpha = 0x1.d1c096p-1f;  // 1 / alpha in f32
     const float thr = 0.08124285829863521110029445797874f;
-    if (v >= thr) return s2_pow_20_9((v + (alpha - 1.0f)) / alpha);
-    return v / 4.5f;
+    const float hi = s2_pow_20_9((v + alpha_m1) * inv_alpha);
+    const float lo = v * 0x1.c71c72p-3f;     // v / 4.5
+    return v >= thr ? hi : lo;
 }
 
 struct ColorConsts {
@@ -172,43 +217,45 @@ template <> __device__ __forceinline__ __nv_bfloat16 to_store<__nv_bfloat16>(flo
     return __float2bfloat16_rn(v);
 }
 
-// "Pre-linear" value of channel g of image img at scale-0 pixel (x, y): the
-// final linear value for every format except RGB16, where it is the EOTF of
-// channel g before the BT.2020 -> BT.709 matrix.  (x, y) must be inside.
-__device__ __forceinline__ float pre_lin0(const DevPair &P, int img, int x, int y, int g,
-                                          const float *lut, const ColorConsts &cc) {
+// Linear RGB of scale-0 pixel (x, y) of image img (inside the image), for
+// input format FMT.  sRGB8: the reference table; NV12: BT.709 limited range,
+// nearest 2x2 chroma (cuda-colorspace-kernel/src/biplanar.rs:8-70); RGB16:
+// BT.709/BT.2020 inverse OETF, then BT.2020 -> BT.709 primaries, clamped >= 0.
+template <int FMT>
+__device__ __forceinline__ void lin_pixel(const DevPair &P, int img, int x, int y, const float *lut,
+                                          const ColorConsts &cc, float o[3]) {
     const char *base = (const char *)P.in[img] + (long long)y * P.pitch[img];
-    switch (P.fmt) {
-    case FMT_LINEAR_F32:
-        return __ldg((const float *)base + 3 * x + g);
-    case FMT_SRGB8:
-        return lut[__ldg((const uint8_t *)base + 3 * x + g)];
-    case FMT_NV12: {
-        int Y = __ldg((const uint8_t *)base + x);
+    if (FMT == FMT_LINEAR_F32) {
+        const float *q = (const float *)base + 3 * x;
+        o[0] = __ldg(q);
+        o[1] = __ldg(q + 1);
+        o[2] = __ldg(q + 2);
+    } else if (FMT == FMT_SRGB8) {
+        const uint8_t *q = (const uint8_t *)base + 3 * x;
+        o[0] = lut[__ldg(q)];
+        o[1] = lut[__ldg(q + 1)];
+        o[2] = lut[__ldg(q + 2)];
+    } else if (FMT == FMT_NV12) {
+        const int Y = __ldg((const uint8_t *)base + x);
         const uint8_t *uv = (const uint8_t *)P.in_uv[img] + (long long)(y >> 1) * P.pitch[img] + 2 * (x >> 1);
-        float cb = (float)((int)__ldg(uv) - 128);
-        float cr = (float)((int)__ldg(uv + 1) - 128);
-        float luma = (float)(max(Y, 16) - 16) * cc.nv12[0];
-        float add;
-        if (g == 0) add = cc.nv12[1] * cr;
-        else if (g == 1) add = fmaf(cc.nv12[3], cb, cc.nv12[4] * cr);
-        else add = cc.nv12[2] * cb;
-        return fminf(fmaxf(bt709_eotf(luma + add), 0.0f), 1.0f);
+        const float cb = (float)((int)__ldg(uv) - 128);
+        const float cr = (float)((int)__ldg(uv + 1) - 128);
+        const float luma = (float)(max(Y, 16) - 16) * cc.nv12[0];
+        o[0] = fminf(fmaxf(bt709_eotf(luma + cc.nv12[1] * cr), 0.0f), 1.0f);
+        o[1] = fminf(fmaxf(bt709_eotf(luma + fmaf(cc.nv12[3], cb, cc.nv12[4] * cr)), 0.0f), 1.0f);
+        o[2] = fminf(fmaxf(bt709_eotf(luma + cc.nv12[2] * cb), 0.0f), 1.0f);
+    } else {
+        const uint16_t *q = (const uint16_t *)base + 3 * x;
+        const float inv = 1.0f / (float)((1 << P.bits) - 1);
+        const float p0 = bt709_eotf((float)__ldg(q) * inv);
+        const float p1 = bt709_eotf((float)__ldg(q + 1) * inv);
+        const float p2 = bt709_eotf((float)__ldg(q + 2) * inv);
+#pragma unroll
+        for (int g = 0; g < 3; g++) {
+            const float *m = cc.m2020 + 3 * g;
+            o[g] = fmaxf(fmaf(m[0], p0, fmaf(m[1], p1, m[2] * p2)), 0.0f);
+        }
     }
-    default: { // FMT_RGB16
-        float inv = 1.0f / (float)((1 << P.bits) - 1);
-        return bt709_eotf((float)__ldg((const uint16_t *)base + 3 * x + g) * inv);
-    }
-    }
-}
-
-// Final linear channel g from the three pre-linear values.
-__device__ __forceinline__ float fin_lin0(int fmt, int g, float p0, float p1, float p2,
-                                          const ColorConsts &cc) {
-    if (fmt != FMT_RGB16) return g == 0 ? p0 : (g == 1 ? p1 : p2);
-    const float *m = cc.m2020 + 3 * g;
-    float v = fmaf(m[0], p0, fmaf(m[1], p1, m[2] * p2));
-    return fmaxf(v, 0.0f);
 }
 
 // Sum of the exact-form FIR taps over the valid positions around x in

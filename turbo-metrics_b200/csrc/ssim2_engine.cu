@@ -949,6 +949,8 @@ s2_status s2_profile_last(s2_ctx *ctx, float ms[3]) {
     return ctx->eng.timings(ms);
 }
 
+int32_t s2_fused_blocks_per_sm(int32_t storage) { return global_init() == S2_OK ? fused_blocks_per_sm(storage) : 0; }
+
 s2_status s2_batch_set_graphs(s2_batch *b, int32_t enable) {
     if (!b) return S2_ERR_INVALID_ARG;
     (void)enable;

@@ -65,15 +65,6 @@ __device__ __forceinline__ float2 fir9x2(float2 a0, float2 a1, float2 a2, float2
     return __ffma2_rn(make_float2(S2_T0, S2_T0), a4, acc);
 }
 
-// Linear RGB of a scale-0 pixel (inside the image), any input format.
-__device__ __forceinline__ void load_lin0(const DevPair &P, int img, int x, int y, const float *lut,
-                                          const ColorConsts &cc, float out[3]) {
-    const float p0 = pre_lin0(P, img, x, y, 0, lut, cc);
-    const float p1 = pre_lin0(P, img, x, y, 1, lut, cc);
-    const float p2 = pre_lin0(P, img, x, y, 2, lut, cc);
-    for (int g = 0; g < 3; g++) out[g] = fin_lin0(P.fmt, g, p0, p1, p2, cc);
-}
-
 __device__ __forceinline__ void xyb3(const float l[3], float o[3]) {
     const float a = opsin_row(0, l[0], l[1], l[2]);
     const float b = opsin_row(1, l[0], l[1], l[2]);
@@ -107,6 +98,26 @@ __device__ __forceinline__ void store_xyb(const DevPair &P, int img, int s, int 
     for (int c = 0; c < 3; c++) dst[c * plane + off] = to_store<ST>(o[c]);
 }
 
+// Scale 0 of one 32x32 block: linear RGB into shared memory, XYB to HBM.
+template <int FMT, typename ST>
+__device__ __forceinline__ void prep_level0(const DevPair &P, int X0, int Y0, const float *lut, const ColorConsts &cc,
+                                            float (*l0)[3][kPyrBlk * kPyrBlk]) {
+    for (int i = threadIdx.x; i < kPyrBlk * kPyrBlk; i += blockDim.x) {
+        const int x = X0 + i % kPyrBlk, y = Y0 + i / kPyrBlk;
+        const bool in = x < P.w[0] && y < P.h[0];
+#pragma unroll
+        for (int img = 0; img < 2; img++) {
+            float v[3] = {0.f, 0.f, 0.f};
+            if (in) {
+                lin_pixel<FMT>(P, img, x, y, lut, cc, v);
+                store_xyb<ST>(P, img, 0, x, y, v);
+            }
+#pragma unroll
+            for (int c = 0; c < 3; c++) l0[img][c][i] = v[c];
+        }
+    }
+}
+
 template <typename ST>
 __global__ void __launch_bounds__(256) prep_kernel(const DevPair *__restrict__ pairs, int npairs,
                                                    const int *__restrict__ blk_first, int total_blocks,
@@ -123,21 +134,15 @@ __global__ void __launch_bounds__(256) prep_kernel(const DevPair *__restrict__ p
             if (blk_first[mid] <= item) lo = mid;
             else hi = mid - 1;
         }
-        const DevPair &P = pairs[lo];
+        const DevPair P = pairs[lo];  // local copy: the level stores cannot alias it
         const int b = item - blk_first[lo];
         const int bx = b % P.blk_x, by = b / P.blk_x;
         const int X0 = bx * kPyrBlk, Y0 = by * kPyrBlk;
-        for (int i = threadIdx.x; i < kPyrBlk * kPyrBlk; i += blockDim.x) {
-            const int x = X0 + i % kPyrBlk, y = Y0 + i / kPyrBlk;
-            const bool in = x < P.w[0] && y < P.h[0];
-            for (int img = 0; img < 2; img++) {
-                float v[3] = {0.f, 0.f, 0.f};
-                if (in) {
-                    load_lin0(P, img, x, y, lut, cc, v);
-                    store_xyb<ST>(P, img, 0, x, y, v);
-                }
-                for (int c = 0; c < 3; c++) l0[img][c][i] = v[c];
-            }
+        switch (P.fmt) {
+        case FMT_LINEAR_F32: prep_level0<FMT_LINEAR_F32, ST>(P, X0, Y0, lut, cc, l0); break;
+        case FMT_SRGB8: prep_level0<FMT_SRGB8, ST>(P, X0, Y0, lut, cc, l0); break;
+        case FMT_NV12: prep_level0<FMT_NV12, ST>(P, X0, Y0, lut, cc, l0); break;
+        default: prep_level0<FMT_RGB16, ST>(P, X0, Y0, lut, cc, l0); break;
         }
         __syncthreads();
         for (int s = 1; s < P.nscales; s++) {
@@ -175,7 +180,7 @@ __global__ void __launch_bounds__(256) prep_kernel(const DevPair *__restrict__ p
 // fused per-scale tile pass
 // ---------------------------------------------------------------------------
 template <typename ST>
-__global__ void __launch_bounds__(kFusedThreads, 2)
+__global__ void __maxnreg__(96)
     fused_kernel(const DevPair *__restrict__ pairs, const Seg *__restrict__ segs, int nseg,
                  int total_tiles, int *__restrict__ counter, double *__restrict__ partials) {
     extern __shared__ float sm[];
@@ -218,7 +223,8 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
         const bool colin = (x >= 0) && (x < W);
         float2 w2a[9], w2b[9];  // windows of (x', y') and (x'^2, y'^2)
         float w1[9];            // window of x' y'
-        double acc[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+        for (int m = 0; m < 6; m++) s_red[tid][m] = 0.0;
 
         auto shifted = [&](float vr, float vd, bool in, float2 &a, float2 &b, float &c) {
             if (in) {
@@ -297,7 +303,7 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
                     const float cv = ld_store<ST>((const ST *)P.lvl[0][s] + t_g * plane +
                                                   (long long)((y0 / kBand) * kBand) * lp + x0);
                     const float bv = border_gain(y, H);
-#pragma unroll
+#pragma unroll 1
                     for (int half = 0; half < kSegW / kChunk; half++) {
                         const int c0 = xs + half * kChunk;  // first output (tile coords)
                         float2 ma[kChunk], mb[kChunk];
@@ -340,11 +346,11 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
                                 const float num_m = fmaf(-md, md, 1.0f);
                                 const float num_s = fmaf(2.0f, cov, kC2);
                                 const float den = (v1 + v2) + kC2;
-                                float d = fmaf(-num_m, num_s, den) / den;
+                                float d = s2_div(fmaf(-num_m, num_s, den), den);
                                 d = fmaxf(d, 0.0f);
                                 const float aa = fabsf((xy.x - m1) + kk);
                                 const float bb = fabsf((xy.y - m2) + kk);
-                                const float d1 = (bb - aa) / (1.0f + aa);
+                                const float d1 = s2_div(bb - aa, 1.0f + aa);
                                 const float art = fmaxf(d1, 0.0f), det = fmaxf(-d1, 0.0f);
                                 float q;
                                 fs[0] += d;   q = d * d;     f4[0] += q * q;
@@ -354,8 +360,8 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
                         }
 #pragma unroll
                         for (int m = 0; m < 3; m++) {
-                            acc[m] += (double)fs[m];
-                            acc[3 + m] += (double)f4[m];
+                            s_red[tid][m] += (double)fs[m];
+                            s_red[tid][3 + m] += (double)f4[m];
                         }
                     }
                 }
@@ -364,8 +370,6 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
         }
 
         // tile reduction, fixed order: sum the tasks of each channel
-#pragma unroll
-        for (int m = 0; m < 6; m++) s_red[tid][m] = acc[m];
         __syncthreads();
         if (tid < 18) {
             const int rg = tid / 6, m = tid % 6;
@@ -456,6 +460,14 @@ template <typename ST> static const void *fused_fn() { return (const void *)fuse
 
 cudaError_t configure_kernels() {
     cudaError_t e;
+    // the fused pass is limited by registers and shared memory together: ask
+    // for the largest shared-memory carveout so that 3 blocks fit per SM
+    e = cudaFuncSetAttribute(fused_kernel<float>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(fused_kernel<__half>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(fused_kernel<__nv_bfloat16>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(fused_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fused_smem_bytes());
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(fused_kernel<__half>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fused_smem_bytes());
