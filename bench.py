@@ -168,17 +168,24 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def algorithmic_bytes_fused(storage_bytes=4):
-    """Declared I/O of one fused launch over the 64 pairs: scale-0 NV12 of both
-    frames (1.5 B/px each) + pyramid levels 1..5 of both frames (3 planes)."""
-    w, h = W, H
-    n0 = w * h
-    lv = 0
-    for _ in range(5):
+def sum_pixels(w=W, h=H, scales=6):
+    n = 0
+    for _ in range(scales):
+        n += w * h
         w, h = (w + 1) // 2, (h + 1) // 2
-        lv += w * h
-    per_pair = 2 * 1.5 * n0 + 2 * 3 * storage_bytes * lv
-    return per_pair * N_PAIRS
+    return n
+
+
+def algorithmic_bytes_fused(storage_bytes=4):
+    """Declared I/O of one fused launch over the 64 pairs: it reads the XYB
+    planes of both frames at every scale (3 planes x storage bytes x sum of
+    the scale sizes) and writes 18 doubles per tile (negligible)."""
+    return N_PAIRS * 2 * 3 * storage_bytes * sum_pixels()
+
+
+def algorithmic_bytes_prep(storage_bytes=4):
+    """prep: reads the NV12 frames (1.5 B/px each), writes the XYB planes."""
+    return N_PAIRS * (2 * 1.5 * W * H + 2 * 3 * storage_bytes * sum_pixels())
 
 
 def main():
@@ -275,7 +282,8 @@ def main():
                 "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                 "kernel_ms": {"prep": float(acc[0]), "fused": fused_ms, "finalize": float(acc[2])},
                 "fused_blocks_per_sm": int(lib.s2_fused_blocks_per_sm(0)),
-                "algorithmic_bytes_per_launch": ab}
+                "algorithmic_bytes_per_launch": ab,
+                "prep_gbs": algorithmic_bytes_prep() / (float(acc[0]) / 1e3) / 1e9}
 
     # ---- plain: the drop-in, one pair at a time ----------------------------
     ctx = tmb.Ssimulacra2(W, H)
