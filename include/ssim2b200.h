@@ -208,6 +208,25 @@ s2_status s2_batch_mem_usage(const s2_batch *b, size_t *bytes);
  * later submissions with identical shapes (1 = on). */
 s2_status s2_batch_set_graphs(s2_batch *b, int32_t enable);
 
+/* ---- scoring one pair without allocating device memory --------------------
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc
+ * (a host framework that owns all device memory through its own pool, a
+ * plug-in that must not grow the process's footprint after start-up, code
+ * that must not block on the allocator): every intermediate lives in one
+ * 16 MiB array inside the library, reserved at load time on every GPU that
+ * loads it.  sRGB8 pair on the device, default configuration (FIR blur, f32,
+ * CPU-crate scale rule); the result is written to `out_device`, a device
+ * buffer of one s2_result that the caller owns (read it after the stream
+ * completes).  A pair whose layout does not fit the array returns
+ * S2_ERR_INVALID_SIZE: any pair whose width and height are both at most 512
+ * fits, larger ones are checked exactly.  All calls share the array, so calls
+ * whose GPU work overlaps race: serialise them.  The first call on a device
+ * sets the array up with that device current; make it before any stream
+ * capture.  Allocates nothing. */
+s2_status s2_compute_srgb8_noalloc(const uint8_t *ref, size_t ref_pitch, const uint8_t *dis,
+                                   size_t dis_pitch, uint32_t width, uint32_t height,
+                                   s2_result *out_device, void *stream);
+
 /* ---- kernel timing (no reference counterpart; the reference has commented-
  * out cuProfilerStart/Stop calls, ssimulacra2-cuda/src/lib.rs:311,963) ----
  * When enabled, CUDA events bracket the three launches of every submission;

@@ -21,6 +21,7 @@ UNITS = [
     ("ssim2_kernels.cu", ["-fmad=false"]),
     ("ssim2_iir.cu", ["-fmad=false"]),
     ("ssim2_engine.cu", []),
+    ("ssim2_noalloc.cu", []),
     ("ssim2_server.cu", []),
 ]
 

@@ -120,6 +120,8 @@ _sig = {
     "s2_batch_set_profiling": (ctypes.c_int, [P, ctypes.c_int32]),
     "s2_batch_last_timings": (ctypes.c_int, [P, ctypes.POINTER(ctypes.c_float)]),
     "s2_fused_blocks_per_sm": (ctypes.c_int32, [ctypes.c_int32]),
+    "s2_compute_srgb8_noalloc": (ctypes.c_int, [P, ctypes.c_size_t, P, ctypes.c_size_t, ctypes.c_uint32,
+                                                ctypes.c_uint32, P, P]),
 }
 for _name, (_res, _args) in _sig.items():
     _f = getattr(lib, _name)
