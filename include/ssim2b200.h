@@ -208,6 +208,59 @@ s2_status s2_batch_mem_usage(const s2_batch *b, size_t *bytes);
  * later submissions with identical shapes (1 = on). */
 s2_status s2_batch_set_graphs(s2_batch *b, int32_t enable);
 
+/* ---- serving: continuous batching of jobs (reference + k candidates) -----
+ * No single counterpart in the reference: it combines the cached-reference
+ * path (ssimulacra2-cuda/src/lib.rs:440-860) with ssim2-gpu's batch
+ * (pipeline_batch.rs:247-382) behind a worker thread.  Jobs of any size arrive
+ * at any time; they are admitted in arrival order while their device bytes
+ * fit the HBM budget, their images are uploaded on a copy stream, and every
+ * round scores the pending work of all admitted jobs in one submission.  A
+ * job's reference pyramid is built once and shared by its candidates.  A job
+ * scores bit-identically alone and mixed with others.  Host images must stay
+ * valid until s2_server_wait returns for the job. */
+typedef struct {
+    uint32_t struct_size;      /* sizeof(s2_server_config) */
+    int32_t device;
+    uint32_t max_batch_pairs;  /* candidates + reference builds per round */
+    uint64_t max_batch_pixels; /* scale-0 pixels per round */
+    uint64_t hbm_budget;       /* device bytes for admitted jobs + workspaces; 0 = no limit */
+    uint32_t max_queued_jobs;  /* submit returns S2_ERR_BUSY beyond this */
+} s2_server_config;
+
+typedef struct {
+    uint32_t width, height;
+    int32_t format;                  /* S2_FMT_SRGB8 */
+    const void *ref;                 /* host image */
+    size_t ref_pitch;
+    uint32_t n_candidates;
+    const void *const *candidates;   /* host images */
+    size_t cand_pitch;
+} s2_job_desc;
+
+typedef struct {
+    uint64_t jobs_done, pairs_done, rounds, queued_jobs, hbm_in_use;
+    double p50_ms, p99_ms, max_ms;   /* arrival -> completion of finished jobs */
+    double uptime_s;
+} s2_server_report;
+
+typedef struct s2_server s2_server;
+
+void s2_server_config_default(s2_server_config *cfg);
+s2_status s2_server_create(const s2_server_config *cfg, s2_server **out);
+/* Stops accepting work, finishes admitted jobs, frees everything. */
+void s2_server_destroy(s2_server *sv);
+/* S2_ERR_OOM if the job alone exceeds the budget, S2_ERR_BUSY if the queue is full. */
+s2_status s2_server_submit(s2_server *sv, const s2_job_desc *job, uint64_t *job_id);
+/* Waits up to timeout_ms for the job; S2_ERR_TIMEOUT if it is not done.  On
+ * completion copies the n scores and per-candidate statuses and releases the
+ * job; returns S2_ERR_CANCELLED for a cancelled job. */
+s2_status s2_server_wait(s2_server *sv, uint64_t job_id, uint32_t timeout_ms, double *scores,
+                         int32_t *statuses, double *latency_ms);
+/* Candidates not yet on the GPU are dropped; in-flight ones finish. */
+s2_status s2_server_cancel(s2_server *sv, uint64_t job_id);
+s2_status s2_server_stats(s2_server *sv, s2_server_report *out);
+s2_status s2_server_reset_stats(s2_server *sv);
+
 /* ---- scoring one pair without allocating device memory --------------------
  * No counterpart in the reference.  For callers that cannot call cudaMalloc
  * (a host framework that owns all device memory through its own pool, a

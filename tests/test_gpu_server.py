@@ -1,0 +1,79 @@
+"""GPU tests of the continuous-batching server (s2_server_*): results equal
+the single-pair context's, a job scores bit-identically alone and mixed with
+other jobs, admission under the HBM budget, cancellation, bounded waits, and
+the latency statistics."""
+import numpy as np
+import pytest
+
+import synth
+
+pytestmark = pytest.mark.gpu
+
+
+def job_images(w, h, seed, k):
+    ref, _ = synth.srgb_pair(w, h, seed)
+    cands = [synth.srgb_pair(w, h, seed, step)[1] for step in (2.0, 6.0, 12.0, 24.0, 40.0)[:k]]
+    return ref, cands
+
+
+def test_server_matches_single_context(tmb, cuda):
+    ref, cands = job_images(300, 200, synth.pair_seed(4, 1), 4)
+    sv = tmb.Ssim2Server()
+    jid = sv.submit(ref, cands)
+    scores, st, lat = sv.wait(jid)
+    assert list(st) == [0] * 4 and lat > 0
+    ctx = tmb.Ssimulacra2(300, 200)
+    for c, s in zip(cands, scores):
+        assert abs(ctx.compute_from_cpu_srgb_sync(ref, c) - s) < 1e-12
+    sv.close()
+
+
+def test_server_alone_equals_mixed_bitwise(tmb, cuda):
+    ref, cands = job_images(257, 131, synth.pair_seed(4, 2), 5)
+    sv = tmb.Ssim2Server(max_batch_pairs=7, max_batch_pixels=1 << 20)
+    alone, _, _ = sv.wait(sv.submit(ref, cands))
+    others = []
+    for i, (w, h) in enumerate([(128, 128), (640, 360), (97, 333), (1024, 576), (200, 150), (333, 97)]):
+        r, c = job_images(w, h, synth.pair_seed(4, 10 + i), 3)
+        others.append(sv.submit(r, c))
+        if i == 2:
+            mid = sv.submit(ref, cands)
+    mixed, _, _ = sv.wait(mid)
+    for o in others:
+        sv.wait(o)
+    assert np.array_equal(alone, mixed)
+    rep = sv.stats()
+    assert rep["jobs_done"] == 8 and rep["pairs_done"] == 5 + 5 + 6 * 3
+    assert rep["rounds"] > 1 and 0 < rep["p50_ms"] <= rep["p99_ms"] <= rep["max_ms"]
+    sv.close()
+
+
+def test_server_budget_admits_in_order(tmb, cuda):
+    # a budget that holds about one job at a time: all still complete, in order
+    ref, cands = job_images(512, 512, synth.pair_seed(4, 3), 3)
+    sv = tmb.Ssim2Server(hbm_budget=160 << 20)
+    ids = [sv.submit(ref, cands) for _ in range(4)]
+    res = [sv.wait(i) for i in ids]
+    for r in res[1:]:
+        assert np.array_equal(r[0], res[0][0])
+    with pytest.raises(tmb.OutOfMemory):
+        big = np.zeros((4096, 4096, 3), np.uint8)
+        sv.submit(big, [big] * 4)
+    sv.close()
+
+
+def test_server_cancel_and_timeout(tmb, cuda):
+    ref, cands = job_images(1280, 720, synth.pair_seed(4, 4), 5)
+    sv = tmb.Ssim2Server(max_batch_pairs=2, hbm_budget=120 << 20)
+    ids = [sv.submit(ref, cands) for _ in range(3)]
+    sv.cancel(ids[2])  # still queued behind the budget
+    with pytest.raises(tmb.S2Error) as e:
+        sv.wait(ids[2])
+    assert e.value.status == 10  # S2_ERR_CANCELLED
+    with pytest.raises(tmb.S2Error) as e:
+        sv.wait(ids[1], timeout_ms=0)
+    assert e.value.status in (6,)  # S2_ERR_TIMEOUT (not done yet)
+    a, _, _ = sv.wait(ids[0])
+    b, _, _ = sv.wait(ids[1])
+    assert np.array_equal(a, b)
+    sv.close()

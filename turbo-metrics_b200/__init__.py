@@ -22,3 +22,4 @@ from .capi import (  # noqa: F401
     version,
 )
 from .ssimulacra2 import Ssimulacra2, Ssim2Batch, PairDesc  # noqa: F401
+from .server import Ssim2Server  # noqa: F401

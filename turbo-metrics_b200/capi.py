@@ -83,6 +83,24 @@ class PairDescC(ctypes.Structure):
                 ("dis_pitch", ctypes.c_size_t)]
 
 
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("struct_size", ctypes.c_uint32), ("device", ctypes.c_int32), ("max_batch_pairs", ctypes.c_uint32),
+                ("max_batch_pixels", ctypes.c_uint64), ("hbm_budget", ctypes.c_uint64),
+                ("max_queued_jobs", ctypes.c_uint32)]
+
+
+class JobDesc(ctypes.Structure):
+    _fields_ = [("width", ctypes.c_uint32), ("height", ctypes.c_uint32), ("format", ctypes.c_int32),
+                ("ref", ctypes.c_void_p), ("ref_pitch", ctypes.c_size_t), ("n_candidates", ctypes.c_uint32),
+                ("candidates", ctypes.POINTER(ctypes.c_void_p)), ("cand_pitch", ctypes.c_size_t)]
+
+
+class ServerReport(ctypes.Structure):
+    _fields_ = [("jobs_done", ctypes.c_uint64), ("pairs_done", ctypes.c_uint64), ("rounds", ctypes.c_uint64),
+                ("queued_jobs", ctypes.c_uint64), ("hbm_in_use", ctypes.c_uint64), ("p50_ms", ctypes.c_double),
+                ("p99_ms", ctypes.c_double), ("max_ms", ctypes.c_double), ("uptime_s", ctypes.c_double)]
+
+
 P = ctypes.c_void_p
 D = ctypes.POINTER(ctypes.c_double)
 _sig = {
@@ -120,6 +138,14 @@ _sig = {
     "s2_batch_set_profiling": (ctypes.c_int, [P, ctypes.c_int32]),
     "s2_batch_last_timings": (ctypes.c_int, [P, ctypes.POINTER(ctypes.c_float)]),
     "s2_fused_blocks_per_sm": (ctypes.c_int32, [ctypes.c_int32]),
+    "s2_server_config_default": (None, [ctypes.POINTER(ServerConfig)]),
+    "s2_server_create": (ctypes.c_int, [ctypes.POINTER(ServerConfig), ctypes.POINTER(P)]),
+    "s2_server_destroy": (None, [P]),
+    "s2_server_submit": (ctypes.c_int, [P, ctypes.POINTER(JobDesc), ctypes.POINTER(ctypes.c_uint64)]),
+    "s2_server_wait": (ctypes.c_int, [P, ctypes.c_uint64, ctypes.c_uint32, D, ctypes.POINTER(ctypes.c_int32), D]),
+    "s2_server_cancel": (ctypes.c_int, [P, ctypes.c_uint64]),
+    "s2_server_stats": (ctypes.c_int, [P, ctypes.POINTER(ServerReport)]),
+    "s2_server_reset_stats": (ctypes.c_int, [P]),
     "s2_compute_srgb8_noalloc": (ctypes.c_int, [P, ctypes.c_size_t, P, ctypes.c_size_t, ctypes.c_uint32,
                                                 ctypes.c_uint32, P, P]),
 }

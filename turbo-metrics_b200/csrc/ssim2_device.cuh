@@ -50,6 +50,8 @@ struct DevPair {
     int blk_base;            // first pyramid block
     int blk_x, blk_y;        // pyramid blocks of this pair
     int status;
+    int prep_mask;           // images the prep pass converts: bit 0 reference, bit 1 distorted
+    int lvl_ext;             // images whose XYB planes live outside the submission (bit per image)
 };
 
 // A run of tiles of one (pair, scale); tiles are numbered across segments.

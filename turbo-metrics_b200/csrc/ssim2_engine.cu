@@ -20,7 +20,7 @@
 #include <vector>
 
 #include "../../include/ssim2b200.h"
-#include "ssim2_launch.h"
+#include "ssim2_engine_internal.h"
 
 using namespace s2;
 
@@ -29,17 +29,13 @@ using namespace s2;
 // ---------------------------------------------------------------------------
 static thread_local std::string g_last_error;
 
-static s2_status cuda_fail(cudaError_t e, const char *what) {
+s2_status s2_cuda_fail(cudaError_t e, const char *what) {
     char buf[256];
     snprintf(buf, sizeof buf, "%s: %s (%d)", what, cudaGetErrorString(e), (int)e);
     g_last_error = buf;
     return e == cudaErrorMemoryAllocation ? S2_ERR_OOM : S2_ERR_CUDA;
 }
-#define S2_CUDA(call)                                    \
-    do {                                                 \
-        cudaError_t e_ = (call);                         \
-        if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
-    } while (0)
+void s2_set_last_error(const char *msg) { g_last_error = msg; }
 
 // ---------------------------------------------------------------------------
 // constants shared by all engines
@@ -48,7 +44,7 @@ static s2_status cuda_fail(cudaError_t e, const char *what) {
 // The entries follow the gamma-2.4 sRGB curve with a linear toe but were
 // printed with 6-9 decimal digits; the table, not the formula, defines the
 // reference's conversion, so the same numbers are used (hex-float spelling).
-static const float kSrgb8Lut[256] = {
+const float s2_srgb8_lut[256] = {
 #include "srgb8_lut.inc"
 };
 
@@ -114,7 +110,7 @@ static void inv3(const double m[9], double o[9]) {
     o[8] = (m[0] * m[4] - m[1] * m[3]) / d;
 }
 
-static ColorConsts make_color_consts() {
+ColorConsts s2_make_color_consts() {
     static const double BT709[8] = {0.640, 0.330, 0.300, 0.600, 0.150, 0.060, 0.3127, 0.3290};
     static const double BT2020[8] = {0.708, 0.292, 0.170, 0.797, 0.131, 0.046, 0.3127, 0.3290};
     ColorConsts cc;
@@ -188,7 +184,7 @@ static bool check_taps() {
 static std::once_flag g_init_once;
 static s2_status g_init_status = S2_OK;
 
-static s2_status global_init() {
+s2_status s2_global_init() {
     std::call_once(g_init_once, [] {
         if (!check_taps()) {
             g_last_error = "FIR taps compiled into the kernels do not match the derivation";
@@ -197,331 +193,11 @@ static s2_status global_init() {
         }
         cudaError_t e = configure_kernels();
         if (e == cudaSuccess) e = upload_weights();
-        if (e != cudaSuccess) g_init_status = cuda_fail(e, "kernel set-up");
+        if (e != cudaSuccess) g_init_status = s2_cuda_fail(e, "kernel set-up");
     });
     return g_init_status;
 }
 
-// ---------------------------------------------------------------------------
-// device buffers
-// ---------------------------------------------------------------------------
-struct DevBuf {
-    void *p = nullptr;
-    size_t n = 0;
-};
-
-static size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
-
-static int num_scales_rule(uint32_t w, uint32_t h, int rule) {
-    if (w < 1 || h < 1) return 0;
-    if (rule == S2_SCALES_ALL6) return kScales;
-    if (w < 8 || h < 8) return 0;
-    int n = 0;
-    uint64_t cw = w, ch = h;
-    if (rule == S2_SCALES_MIN8) {
-        while (n < kScales && cw >= 8 && ch >= 8) {
-            n++;
-            cw = (cw + 1) / 2;
-            ch = (ch + 1) / 2;
-        }
-        return n;
-    }
-    // CPU crate: scale s > 0 is produced when scale s-1 is at least 8x8
-    n = 1;
-    for (int s = 1; s < kScales; s++) {
-        if (cw < 8 || ch < 8) break;
-        n++;
-        cw = (cw + 1) / 2;
-        ch = (ch + 1) / 2;
-    }
-    return n;
-}
-
-// One planned submission.
-struct Plan {
-    std::vector<DevPair> pairs;
-    std::vector<int> blk_first;
-    std::vector<Seg> segs;
-    int total_blocks = 0;
-    int total_tiles = 0;
-    size_t level_bytes = 0;  // both images, all levels, all pairs
-    int strip_rows = 63;
-};
-
-struct Engine {
-    int device = 0;
-    int storage = ST_F32;
-    int scale_rule = S2_SCALES_CPU;
-    int strip_rows_cfg = 0;
-    int blur = S2_BLUR_FIR;
-    uint64_t budget = 0;
-    size_t allocated = 0;
-    int num_sms = 148;
-    int fused_bps = 1;
-    ColorConsts cc;
-
-    DevBuf pairs_d, blk_d, segs_d, counter_d, partials_d, results_d, levels_d, lut_d;
-    void *pinned = nullptr;  // staging: pairs | blk_first | segs
-    size_t pinned_n = 0;
-    DevResult *results_h = nullptr;
-    size_t results_cap = 0;
-    cudaEvent_t done = nullptr;
-    int last_n = -1;
-    bool pending = false;
-    bool profiling = false;
-    cudaEvent_t prof[4] = {nullptr, nullptr, nullptr, nullptr};
-
-    size_t esize() const { return storage == ST_F32 ? 4 : 2; }
-
-    s2_status init(const s2_config *cfg) {
-        s2_status st = global_init();
-        if (st != S2_OK) return st;
-        device = cfg->device;
-        storage = cfg->storage;
-        scale_rule = cfg->scale_rule;
-        strip_rows_cfg = cfg->strip_rows;
-        blur = cfg->blur;
-        budget = cfg->hbm_budget;
-        S2_CUDA(cudaSetDevice(device));
-        S2_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device));
-        fused_bps = fused_blocks_per_sm(storage);
-        cc = make_color_consts();
-        S2_CUDA(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
-        st = ensure(lut_d, sizeof kSrgb8Lut);
-        if (st != S2_OK) return st;
-        S2_CUDA(cudaMemcpy(lut_d.p, kSrgb8Lut, sizeof kSrgb8Lut, cudaMemcpyHostToDevice));
-        st = ensure(counter_d, 256);
-        return st;
-    }
-
-    s2_status set_profiling(bool on) {
-        if (on && !prof[0])
-            for (cudaEvent_t &e : prof) S2_CUDA(cudaEventCreate(&e));
-        profiling = on;
-        return S2_OK;
-    }
-
-    s2_status timings(float ms[3]) {
-        if (!profiling || last_n < 0) return S2_ERR_NOT_READY;
-        S2_CUDA(cudaEventSynchronize(prof[3]));
-        for (int i = 0; i < 3; i++) S2_CUDA(cudaEventElapsedTime(&ms[i], prof[i], prof[i + 1]));
-        return S2_OK;
-    }
-
-    void release() {
-        if (device >= 0) cudaSetDevice(device);
-        if (done) cudaEventSynchronize(done);
-        for (cudaEvent_t &e : prof)
-            if (e) cudaEventDestroy(e), e = nullptr;
-        for (DevBuf *b : {&pairs_d, &blk_d, &segs_d, &counter_d, &partials_d, &results_d, &levels_d, &lut_d})
-            if (b->p) cudaFree(b->p), b->p = nullptr, b->n = 0;
-        if (pinned) cudaFreeHost(pinned), pinned = nullptr;
-        if (results_h) cudaFreeHost(results_h), results_h = nullptr;
-        if (done) cudaEventDestroy(done), done = nullptr;
-        allocated = 0;
-    }
-
-    // Grow-only device allocation, checked against the budget.
-    s2_status ensure(DevBuf &b, size_t bytes) {
-        if (b.n >= bytes) return S2_OK;
-        bytes = align_up(bytes, 4096);
-        if (budget && allocated - b.n + bytes > budget) {
-            g_last_error = "allocation over the HBM budget";
-            return S2_ERR_OOM;
-        }
-        if (b.p) {
-            if (done) cudaEventSynchronize(done);
-            cudaFree(b.p);
-            allocated -= b.n;
-            b.p = nullptr;
-            b.n = 0;
-        }
-        S2_CUDA(cudaMalloc(&b.p, bytes));
-        b.n = bytes;
-        allocated += bytes;
-        return S2_OK;
-    }
-
-    s2_status ensure_pinned(size_t bytes, size_t nres) {
-        if (pinned_n < bytes) {
-            if (pinned) {
-                if (done) cudaEventSynchronize(done);
-                cudaFreeHost(pinned);
-            }
-            pinned = nullptr;
-            bytes = align_up(bytes, 4096);
-            S2_CUDA(cudaMallocHost(&pinned, bytes));
-            pinned_n = bytes;
-        }
-        if (results_cap < nres) {
-            if (results_h) {
-                if (done) cudaEventSynchronize(done);
-                cudaFreeHost(results_h);
-            }
-            results_h = nullptr;
-            S2_CUDA(cudaMallocHost((void **)&results_h, nres * sizeof(DevResult)));
-            results_cap = nres;
-        }
-        return S2_OK;
-    }
-
-    int choose_strip_rows(const std::vector<uint64_t> &tiles_at) const {
-        if (strip_rows_cfg == 9 || strip_rows_cfg == 21 || strip_rows_cfg == 63) return strip_rows_cfg;
-        // largest strip height that still gives ~4 waves of resident tiles
-        const uint64_t resident = (uint64_t)num_sms * (uint64_t)fused_bps;
-        if (tiles_at[0] >= 4 * resident) return 63;
-        if (tiles_at[1] >= 4 * resident) return 21;
-        return 9;
-    }
-
-    // Lay out the levels and tiles of n pairs.
-    s2_status plan(const s2_pair_desc *d, int n, Plan &P) {
-        P = Plan();
-        P.pairs.resize(n);
-        P.blk_first.resize(n);
-        // tile counts at strip heights 64/32 for the strip choice
-        std::vector<uint64_t> tiles_at(2, 0);
-        std::vector<int> ns(n);
-        for (int i = 0; i < n; i++) {
-            ns[i] = num_scales_rule(d[i].width, d[i].height, scale_rule);
-            uint64_t w = d[i].width, h = d[i].height;
-            for (int s = 0; s < ns[i]; s++) {
-                tiles_at[0] += ((w + kTileW - 1) / kTileW) * ((h + 62) / 63);
-                tiles_at[1] += ((w + kTileW - 1) / kTileW) * ((h + 20) / 21);
-                w = (w + 1) / 2;
-                h = (h + 1) / 2;
-            }
-        }
-        P.strip_rows = choose_strip_rows(tiles_at);
-        size_t lvl_off = 0;
-        int blk = 0;
-        for (int i = 0; i < n; i++) {
-            DevPair &p = P.pairs[i];
-            memset(&p, 0, sizeof p);
-            const s2_pair_desc &q = d[i];
-            p.in[0] = q.ref;
-            p.in[1] = q.dis;
-            p.in_uv[0] = q.ref_uv;
-            p.in_uv[1] = q.dis_uv;
-            p.pitch[0] = (long long)q.ref_pitch;
-            p.pitch[1] = (long long)q.dis_pitch;
-            p.fmt = q.format;
-            p.bits = q.bits;
-            p.nscales = ns[i];
-            p.status = S2_OK;
-            if (ns[i] == 0 || q.width > (1u << 16) || q.height > (1u << 16)) {
-                p.status = S2_ERR_INVALID_SIZE;
-                p.nscales = 0;
-                P.blk_first[i] = blk;
-                continue;
-            }
-            if (q.format < 0 || q.format > 3 || !q.ref || !q.dis ||
-                (q.format == S2_FMT_NV12 && (!q.ref_uv || !q.dis_uv || (q.width & 1) || (q.height & 1))) ||
-                (q.format == S2_FMT_RGB16 && (q.bits < 8 || q.bits > 16))) {
-                p.status = S2_ERR_INVALID_ARG;
-                p.nscales = 0;
-                P.blk_first[i] = blk;
-                continue;
-            }
-            p.w[0] = (int)q.width;
-            p.h[0] = (int)q.height;
-            for (int s = 1; s < kScales; s++) {
-                p.w[s] = (p.w[s - 1] + 1) / 2;
-                p.h[s] = (p.h[s - 1] + 1) / 2;
-            }
-            for (int s = 0; s < p.nscales; s++) {
-                p.lp[s] = (int)align_up((size_t)p.w[s], 64);
-                size_t bytes = align_up((size_t)3 * p.lp[s] * p.h[s] * esize(), 256);
-                p.lvl[0][s] = (void *)lvl_off;  // offsets, rebased at upload
-                lvl_off += bytes;
-                p.lvl[1][s] = (void *)lvl_off;
-                lvl_off += bytes;
-            }
-            P.blk_first[i] = blk;
-            {
-                p.blk_x = (p.w[0] + kPyrBlk - 1) / kPyrBlk;
-                p.blk_y = (p.h[0] + kPyrBlk - 1) / kPyrBlk;
-                p.blk_base = blk;
-                blk += p.blk_x * p.blk_y;
-            }
-        }
-        P.total_blocks = blk;
-        P.level_bytes = lvl_off;
-        // tiles: all pairs' scale 0 first, then scale 1, ... (largest work first)
-        int tile = 0;
-        for (int s = 0; s < kScales; s++) {
-            for (int i = 0; i < n; i++) {
-                DevPair &p = P.pairs[i];
-                if (p.status != S2_OK || s >= p.nscales) continue;
-                Seg sg;
-                sg.first_tile = tile;
-                sg.pair = i;
-                sg.scale = s;
-                sg.tiles_x = (p.w[s] + kTileW - 1) / kTileW;
-                sg.strip_rows = P.strip_rows;
-                int ty = (p.h[s] + P.strip_rows - 1) / P.strip_rows;
-                p.tile_base[s] = tile;
-                p.tile_cnt[s] = sg.tiles_x * ty;
-                tile += p.tile_cnt[s];
-                P.segs.push_back(sg);
-            }
-        }
-        P.total_tiles = tile;
-        return S2_OK;
-    }
-
-    s2_status enqueue(Plan &P, cudaStream_t st) {
-        const int n = (int)P.pairs.size();
-        s2_status r;
-        if ((r = ensure(levels_d, std::max<size_t>(P.level_bytes, 256))) != S2_OK) return r;
-        if ((r = ensure(partials_d, std::max<size_t>((size_t)P.total_tiles * 18 * sizeof(double), 256))) != S2_OK) return r;
-        if ((r = ensure(results_d, (size_t)n * sizeof(DevResult))) != S2_OK) return r;
-        const size_t pb = align_up(n * sizeof(DevPair), 256), bb = align_up(n * sizeof(int), 256),
-                     sb = align_up(std::max<size_t>(P.segs.size(), 1) * sizeof(Seg), 256);
-        if ((r = ensure(pairs_d, pb + bb + sb)) != S2_OK) return r;
-        if ((r = ensure_pinned(pb + bb + sb, n)) != S2_OK) return r;
-        // the previous submission may still read the pinned staging
-        if (pending) S2_CUDA(cudaEventSynchronize(done));
-        char *h = (char *)pinned;
-        DevPair *hp = (DevPair *)h;
-        for (int i = 0; i < n; i++) {
-            hp[i] = P.pairs[i];
-            for (int s = 0; s < kScales; s++)
-                for (int img = 0; img < 2; img++)
-                    if (s < hp[i].nscales) hp[i].lvl[img][s] = (char *)levels_d.p + (size_t)hp[i].lvl[img][s];
-                    else hp[i].lvl[img][s] = nullptr;
-        }
-        memcpy(h + pb, P.blk_first.data(), n * sizeof(int));
-        if (!P.segs.empty()) memcpy(h + pb + bb, P.segs.data(), P.segs.size() * sizeof(Seg));
-        char *dbase = (char *)pairs_d.p;
-        const DevPair *dpairs = (const DevPair *)dbase;
-        const int *dblk = (const int *)(dbase + pb);
-        const Seg *dsegs = (const Seg *)(dbase + pb + bb);
-        S2_CUDA(cudaMemcpyAsync(dbase, h, pb + bb + sb, cudaMemcpyHostToDevice, st));
-        S2_CUDA(cudaMemsetAsync(counter_d.p, 0, sizeof(int), st));
-        if (profiling) S2_CUDA(cudaEventRecord(prof[0], st));
-        S2_CUDA(launch_pyramid(storage, dpairs, n, dblk, P.total_blocks, cc, (const float *)lut_d.p,
-                               num_sms * 8, st));
-        if (profiling) S2_CUDA(cudaEventRecord(prof[1], st));
-        S2_CUDA(launch_fused(storage, dpairs, dsegs, (int)P.segs.size(), P.total_tiles, (int *)counter_d.p,
-                             (double *)partials_d.p, cc, (const float *)lut_d.p, num_sms * fused_bps, st));
-        if (profiling) S2_CUDA(cudaEventRecord(prof[2], st));
-        S2_CUDA(launch_finalize(dpairs, n, (const double *)partials_d.p, (DevResult *)results_d.p, st));
-        if (profiling) S2_CUDA(cudaEventRecord(prof[3], st));
-        S2_CUDA(cudaMemcpyAsync(results_h, results_d.p, n * sizeof(DevResult), cudaMemcpyDeviceToHost, st));
-        S2_CUDA(cudaEventRecord(done, st));
-        last_n = n;
-        pending = true;
-        return S2_OK;
-    }
-
-    s2_status wait() {
-        if (last_n < 0) return S2_ERR_NOT_READY;
-        S2_CUDA(cudaEventSynchronize(done));
-        pending = false;
-        return S2_OK;
-    }
-};
 
 // ---------------------------------------------------------------------------
 // single-pair context
@@ -529,10 +205,11 @@ struct Engine {
 struct s2_ctx {
     Engine eng;
     uint32_t w = 0, h = 0;
-    DevBuf stage[4];  // host-input staging: ref, dis (+ uv planes)
+    DevBuf stage[4];     // host-input staging: ref, dis (+ uv planes)
     bool has_ref = false;
-    DevBuf ref_copy;  // cached reference input (packed, device)
-    s2_pair_desc ref_desc;
+    bool last_was_ref_build = false;
+    DevBuf ref_levels;   // the cached reference's XYB planes, every scored scale
+    PairExtra ref_extra; // points the pairs of compute_with_reference at them
     Plan plan;
 };
 
@@ -578,7 +255,7 @@ void s2_config_default(s2_config *cfg) {
     cfg->hbm_budget = 0;
 }
 
-int s2_num_scales(uint32_t w, uint32_t h, int32_t rule) { return num_scales_rule(w, h, rule); }
+int s2_num_scales(uint32_t w, uint32_t h, int32_t rule) { return s2_num_scales_rule(w, h, rule); }
 
 static s2_status check_cfg(const s2_config *cfg) {
     if (!cfg || cfg->struct_size != sizeof(s2_config)) return S2_ERR_INVALID_ARG;
@@ -598,7 +275,7 @@ s2_status s2_create(const s2_config *cfg_in, uint32_t width, uint32_t height, s2
     else s2_config_default(&cfg);
     s2_status st = check_cfg(&cfg);
     if (st != S2_OK) return st;
-    if (num_scales_rule(width, height, cfg.scale_rule) == 0 || width > 65536 || height > 65536)
+    if (s2_num_scales_rule(width, height, cfg.scale_rule) == 0 || width > 65536 || height > 65536)
         return S2_ERR_INVALID_SIZE;
     if (cfg.blur != S2_BLUR_FIR) {
         g_last_error = "S2_BLUR_IIR_REF is served by s2_iir_* entry points only";
@@ -607,7 +284,7 @@ s2_status s2_create(const s2_config *cfg_in, uint32_t width, uint32_t height, s2
     // pre-flight: levels (2 images, ~1/3 of scale 0) + partials + staging
     {
         size_t free_b = 0, total_b = 0;
-        if (cudaSetDevice(cfg.device) != cudaSuccess) return cuda_fail(cudaGetLastError(), "cudaSetDevice");
+        if (cudaSetDevice(cfg.device) != cudaSuccess) return s2_cuda_fail(cudaGetLastError(), "cudaSetDevice");
         if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
             uint64_t est = (uint64_t)width * height * 40 + (64u << 20);
             if (est > free_b || (cfg.hbm_budget && est > cfg.hbm_budget)) return S2_ERR_OOM;
@@ -645,14 +322,14 @@ void s2_destroy(s2_ctx *ctx) {
     if (!ctx) return;
     for (DevBuf &b : ctx->stage)
         if (b.p) cudaFree(b.p);
-    if (ctx->ref_copy.p) cudaFree(ctx->ref_copy.p);
+    if (ctx->ref_levels.p) cudaFree(ctx->ref_levels.p);
     ctx->eng.release();
     delete ctx;
 }
 
 s2_status s2_mem_usage(const s2_ctx *ctx, size_t *bytes) {
     if (!ctx || !bytes) return S2_ERR_INVALID_ARG;
-    size_t n = ctx->eng.allocated + ctx->ref_copy.n;
+    size_t n = ctx->eng.allocated + ctx->ref_levels.n;
     for (const DevBuf &b : ctx->stage) n += b.n;
     *bytes = n;
     return S2_OK;
@@ -665,10 +342,11 @@ s2_status s2_dimensions(const s2_ctx *ctx, uint32_t *w, uint32_t *h) {
     return S2_OK;
 }
 
-static s2_status ctx_run(s2_ctx *ctx, const s2_pair_desc &d, void *stream) {
-    s2_status st = ctx->eng.plan(&d, 1, ctx->plan);
+static s2_status ctx_run(s2_ctx *ctx, const s2_pair_desc &d, void *stream, const PairExtra *ex = nullptr) {
+    s2_status st = ctx->eng.plan(&d, 1, ctx->plan, ex);
     if (st != S2_OK) return st;
     if (ctx->plan.pairs[0].status != S2_OK) return (s2_status)ctx->plan.pairs[0].status;
+    ctx->last_was_ref_build = ex && !ex->score;
     return ctx->eng.enqueue(ctx->plan, (cudaStream_t)stream);
 }
 
@@ -772,6 +450,7 @@ s2_status s2_compute_rgb16(s2_ctx *ctx, const uint16_t *ref, size_t ref_pitch, c
 
 s2_status s2_get_result(s2_ctx *ctx, double *score, double stats[S2_NUM_STATS], double sums[S2_NUM_STATS]) {
     if (!ctx) return S2_ERR_INVALID_ARG;
+    if (ctx->last_was_ref_build) return S2_ERR_NOT_READY;
     s2_status st = ctx->eng.wait();
     if (st != S2_OK) return st;
     const DevResult &r = ctx->eng.results_h[0];
@@ -790,25 +469,43 @@ s2_status s2_compute_sync_linear_f32(s2_ctx *ctx, const float *ref, size_t ref_p
 }
 
 // ---- cached reference ----------------------------------------------------
-// The context keeps a device copy of the reference input; candidates are
-// scored against it without the caller re-supplying it.
-static s2_status set_ref(s2_ctx *ctx, int fmt, const void *src, size_t pitch, size_t row, int32_t on_host,
-                         void *stream) {
-    DevBuf &b = ctx->ref_copy;
-    size_t need = row * ctx->h;
-    if (b.n < need) {
-        if (b.p) {
-            cudaStreamSynchronize((cudaStream_t)stream);
-            cudaFree(b.p);
+// set_reference converts the reference once and keeps its XYB planes of every
+// scale on the device (set_reference_linear, ssimulacra2-cuda/src/lib.rs:440-546,
+// caches the same ref-side state); compute_with_reference converts only the
+// distorted image and reads the cached planes.  Scores equal the direct path's
+// (same XYB values, same tiles).  Like the reference, set_reference returns
+// after the device work is done.
+static s2_status set_ref(s2_ctx *ctx, const s2_pair_desc &d, void *stream) {
+    size_t off[kScales];
+    const int ns = s2_num_scales_rule(ctx->w, ctx->h, ctx->eng.scale_rule);
+    const size_t bytes = s2_image_levels_layout(ctx->w, ctx->h, ns, ctx->eng.esize(), off);
+    if (ctx->ref_levels.n < bytes) {
+        if (ctx->ref_levels.p) {
+            S2_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+            cudaFree(ctx->ref_levels.p);
         }
-        b.p = nullptr;
-        b.n = 0;
-        S2_CUDA(cudaMalloc(&b.p, need));
-        b.n = need;
+        ctx->ref_levels.p = nullptr;
+        ctx->ref_levels.n = 0;
+        if (ctx->eng.budget && ctx->eng.allocated + bytes > ctx->eng.budget) {
+            g_last_error = "reference cache over the HBM budget";
+            return S2_ERR_OOM;
+        }
+        S2_CUDA(cudaMalloc(&ctx->ref_levels.p, bytes));
+        ctx->ref_levels.n = bytes;
     }
-    S2_CUDA(cudaMemcpy2DAsync(b.p, row, src, pitch, row, ctx->h,
-                              on_host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
-    ctx->ref_desc = make_desc(ctx->w, ctx->h, fmt, b.p, row, nullptr, 0);
+    PairExtra build;
+    build.prep_mask = 1;
+    build.score = false;
+    for (int s = 0; s < kScales; s++)
+        build.ref_levels[s] = s < ns ? (char *)ctx->ref_levels.p + off[s] : nullptr;
+    ctx->has_ref = false;
+    s2_status st = ctx_run(ctx, d, stream, &build);
+    if (st != S2_OK) return st;
+    S2_CUDA(cudaEventSynchronize(ctx->eng.done));
+    ctx->eng.pending = false;
+    ctx->ref_extra = build;
+    ctx->ref_extra.prep_mask = 2;
+    ctx->ref_extra.score = true;
     ctx->has_ref = true;
     return S2_OK;
 }
@@ -816,31 +513,34 @@ static s2_status set_ref(s2_ctx *ctx, int fmt, const void *src, size_t pitch, si
 s2_status s2_set_reference_linear_f32(s2_ctx *ctx, const float *ref, size_t pitch, void *stream) {
     if (!ctx || !ref) return S2_ERR_INVALID_ARG;
     if (pitch < (size_t)ctx->w * 12) return S2_ERR_DIM_MISMATCH;
-    return set_ref(ctx, S2_FMT_LINEAR_F32, ref, pitch, (size_t)ctx->w * 12, 0, stream);
+    return set_ref(ctx, make_desc(ctx->w, ctx->h, S2_FMT_LINEAR_F32, ref, pitch, nullptr, 0), stream);
 }
 
 s2_status s2_set_reference_srgb8(s2_ctx *ctx, const uint8_t *ref, size_t pitch, int32_t on_host, void *stream) {
     if (!ctx || !ref) return S2_ERR_INVALID_ARG;
-    if (pitch < (size_t)ctx->w * 3) return S2_ERR_DIM_MISMATCH;
-    return set_ref(ctx, S2_FMT_SRGB8, ref, pitch, (size_t)ctx->w * 3, on_host, stream);
+    const size_t row = (size_t)ctx->w * 3;
+    if (pitch < row) return S2_ERR_DIM_MISMATCH;
+    const void *r = ref;
+    size_t rp = pitch;
+    if (on_host) {
+        s2_status st = stage_host(ctx, 0, ref, pitch, row, ctx->h, stream, &r, &rp);
+        if (st != S2_OK) return st;
+    }
+    return set_ref(ctx, make_desc(ctx->w, ctx->h, S2_FMT_SRGB8, r, rp, nullptr, 0), stream);
 }
 
 s2_status s2_compute_with_reference_linear_f32(s2_ctx *ctx, const float *dis, size_t pitch, void *stream) {
     if (!ctx || !dis) return S2_ERR_INVALID_ARG;
     if (!ctx->has_ref) return S2_ERR_NO_REFERENCE;
-    if (ctx->ref_desc.format != S2_FMT_LINEAR_F32) return S2_ERR_DIM_MISMATCH;
     if (pitch < (size_t)ctx->w * 12) return S2_ERR_DIM_MISMATCH;
-    s2_pair_desc d = ctx->ref_desc;
-    d.dis = dis;
-    d.dis_pitch = pitch;
-    return ctx_run(ctx, d, stream);
+    return ctx_run(ctx, make_desc(ctx->w, ctx->h, S2_FMT_LINEAR_F32, nullptr, 0, dis, pitch), stream,
+                   &ctx->ref_extra);
 }
 
 s2_status s2_compute_with_reference_srgb8(s2_ctx *ctx, const uint8_t *dis, size_t pitch, int32_t on_host,
                                           void *stream) {
     if (!ctx || !dis) return S2_ERR_INVALID_ARG;
     if (!ctx->has_ref) return S2_ERR_NO_REFERENCE;
-    if (ctx->ref_desc.format != S2_FMT_SRGB8) return S2_ERR_DIM_MISMATCH;
     const size_t row = (size_t)ctx->w * 3;
     if (pitch < row) return S2_ERR_DIM_MISMATCH;
     const void *d = dis;
@@ -849,10 +549,7 @@ s2_status s2_compute_with_reference_srgb8(s2_ctx *ctx, const uint8_t *dis, size_
         s2_status st = stage_host(ctx, 1, dis, pitch, row, ctx->h, stream, &d, &dp);
         if (st != S2_OK) return st;
     }
-    s2_pair_desc desc = ctx->ref_desc;
-    desc.dis = d;
-    desc.dis_pitch = dp;
-    return ctx_run(ctx, desc, stream);
+    return ctx_run(ctx, make_desc(ctx->w, ctx->h, S2_FMT_SRGB8, nullptr, 0, d, dp), stream, &ctx->ref_extra);
 }
 
 s2_status s2_clear_reference(s2_ctx *ctx) {
@@ -949,7 +646,7 @@ s2_status s2_profile_last(s2_ctx *ctx, float ms[3]) {
     return ctx->eng.timings(ms);
 }
 
-int32_t s2_fused_blocks_per_sm(int32_t storage) { return global_init() == S2_OK ? fused_blocks_per_sm(storage) : 0; }
+int32_t s2_fused_blocks_per_sm(int32_t storage) { return s2_global_init() == S2_OK ? fused_blocks_per_sm(storage) : 0; }
 
 s2_status s2_batch_set_graphs(s2_batch *b, int32_t enable) {
     if (!b) return S2_ERR_INVALID_ARG;

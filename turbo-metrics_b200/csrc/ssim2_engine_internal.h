@@ -1,0 +1,383 @@
+// ssim2_engine_internal.h -- engine internals shared by the C-ABI units
+// (ssim2_engine.cu, ssim2_server.cu): device buffers, submission plans and the
+// Engine that lays pairs out into prep blocks and fused tiles and launches them.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/ssim2b200.h"
+#include "ssim2_launch.h"
+
+using namespace s2;
+
+s2_status s2_cuda_fail(cudaError_t e, const char *what);
+void s2_set_last_error(const char *msg);
+s2_status s2_global_init();
+ColorConsts s2_make_color_consts();
+extern const float s2_srgb8_lut[256];
+
+#define S2_CUDA(call)                                          \
+    do {                                                       \
+        cudaError_t e_ = (call);                               \
+        if (e_ != cudaSuccess) return s2_cuda_fail(e_, #call); \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// device buffers
+// ---------------------------------------------------------------------------
+struct DevBuf {
+    void *p = nullptr;
+    size_t n = 0;
+};
+
+inline size_t s2_align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+inline int s2_num_scales_rule(uint32_t w, uint32_t h, int rule) {
+    if (w < 1 || h < 1) return 0;
+    if (rule == S2_SCALES_ALL6) return kScales;
+    if (w < 8 || h < 8) return 0;
+    int n = 0;
+    uint64_t cw = w, ch = h;
+    if (rule == S2_SCALES_MIN8) {
+        while (n < kScales && cw >= 8 && ch >= 8) {
+            n++;
+            cw = (cw + 1) / 2;
+            ch = (ch + 1) / 2;
+        }
+        return n;
+    }
+    // CPU crate: scale s > 0 is produced when scale s-1 is at least 8x8
+    n = 1;
+    for (int s = 1; s < kScales; s++) {
+        if (cw < 8 || ch < 8) break;
+        n++;
+        cw = (cw + 1) / 2;
+        ch = (ch + 1) / 2;
+    }
+    return n;
+}
+
+// Per-pair options of a submission beyond s2_pair_desc: which images the
+// prep pass converts, whether the pair is scored (tiles + result), and the
+// reference's XYB planes when they were built earlier (a cached reference).
+struct PairExtra {
+    int prep_mask = 3;
+    bool score = true;
+    void *ref_levels[kScales] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+};
+
+// Byte layout of one image's XYB planes (all scored scales), as the plan lays
+// them out: plane pitch rounded up to 64 elements, 256-byte aligned scales.
+inline size_t s2_image_levels_layout(uint32_t w, uint32_t h, int ns, size_t esize, size_t off[kScales]) {
+    size_t o = 0;
+    uint64_t cw = w, ch = h;
+    for (int s = 0; s < ns; s++) {
+        off[s] = o;
+        o += s2_align_up((size_t)3 * s2_align_up((size_t)cw, 64) * ch * esize, 256);
+        cw = (cw + 1) / 2;
+        ch = (ch + 1) / 2;
+    }
+    return o;
+}
+
+// One planned submission.
+struct Plan {
+    std::vector<DevPair> pairs;
+    std::vector<int> blk_first;
+    std::vector<Seg> segs;
+    int total_blocks = 0;
+    int total_tiles = 0;
+    size_t level_bytes = 0;  // both images, all levels, all pairs
+    int strip_rows = 63;
+};
+
+struct Engine {
+    int device = 0;
+    int storage = ST_F32;
+    int scale_rule = S2_SCALES_CPU;
+    int strip_rows_cfg = 0;
+    int blur = S2_BLUR_FIR;
+    uint64_t budget = 0;
+    size_t allocated = 0;
+    int num_sms = 148;
+    int fused_bps = 1;
+    ColorConsts cc;
+
+    DevBuf pairs_d, blk_d, segs_d, counter_d, partials_d, results_d, levels_d, lut_d;
+    void *pinned = nullptr;  // staging: pairs | blk_first | segs
+    size_t pinned_n = 0;
+    DevResult *results_h = nullptr;
+    size_t results_cap = 0;
+    cudaEvent_t done = nullptr;
+    int last_n = -1;
+    bool pending = false;
+    Plan plan_storage;  // a submission's plan, owned by whoever drives this engine
+    bool profiling = false;
+    cudaEvent_t prof[4] = {nullptr, nullptr, nullptr, nullptr};
+
+    size_t esize() const { return storage == ST_F32 ? 4 : 2; }
+
+    s2_status init(const s2_config *cfg) {
+        s2_status st = s2_global_init();
+        if (st != S2_OK) return st;
+        device = cfg->device;
+        storage = cfg->storage;
+        scale_rule = cfg->scale_rule;
+        strip_rows_cfg = cfg->strip_rows;
+        blur = cfg->blur;
+        budget = cfg->hbm_budget;
+        S2_CUDA(cudaSetDevice(device));
+        S2_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device));
+        fused_bps = fused_blocks_per_sm(storage);
+        cc = s2_make_color_consts();
+        S2_CUDA(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+        st = ensure(lut_d, sizeof s2_srgb8_lut);
+        if (st != S2_OK) return st;
+        S2_CUDA(cudaMemcpy(lut_d.p, s2_srgb8_lut, sizeof s2_srgb8_lut, cudaMemcpyHostToDevice));
+        st = ensure(counter_d, 256);
+        return st;
+    }
+
+    s2_status set_profiling(bool on) {
+        if (on && !prof[0])
+            for (cudaEvent_t &e : prof) S2_CUDA(cudaEventCreate(&e));
+        profiling = on;
+        return S2_OK;
+    }
+
+    s2_status timings(float ms[3]) {
+        if (!profiling || last_n < 0) return S2_ERR_NOT_READY;
+        S2_CUDA(cudaEventSynchronize(prof[3]));
+        for (int i = 0; i < 3; i++) S2_CUDA(cudaEventElapsedTime(&ms[i], prof[i], prof[i + 1]));
+        return S2_OK;
+    }
+
+    void release() {
+        if (device >= 0) cudaSetDevice(device);
+        if (done) cudaEventSynchronize(done);
+        for (cudaEvent_t &e : prof)
+            if (e) cudaEventDestroy(e), e = nullptr;
+        for (DevBuf *b : {&pairs_d, &blk_d, &segs_d, &counter_d, &partials_d, &results_d, &levels_d, &lut_d})
+            if (b->p) cudaFree(b->p), b->p = nullptr, b->n = 0;
+        if (pinned) cudaFreeHost(pinned), pinned = nullptr;
+        if (results_h) cudaFreeHost(results_h), results_h = nullptr;
+        if (done) cudaEventDestroy(done), done = nullptr;
+        allocated = 0;
+    }
+
+    // Grow-only device allocation, checked against the budget.
+    s2_status ensure(DevBuf &b, size_t bytes) {
+        if (b.n >= bytes) return S2_OK;
+        bytes = s2_align_up(bytes, 4096);
+        if (budget && allocated - b.n + bytes > budget) {
+            s2_set_last_error("allocation over the HBM budget");
+            return S2_ERR_OOM;
+        }
+        if (b.p) {
+            if (done) cudaEventSynchronize(done);
+            cudaFree(b.p);
+            allocated -= b.n;
+            b.p = nullptr;
+            b.n = 0;
+        }
+        S2_CUDA(cudaMalloc(&b.p, bytes));
+        b.n = bytes;
+        allocated += bytes;
+        return S2_OK;
+    }
+
+    s2_status ensure_pinned(size_t bytes, size_t nres) {
+        if (pinned_n < bytes) {
+            if (pinned) {
+                if (done) cudaEventSynchronize(done);
+                cudaFreeHost(pinned);
+            }
+            pinned = nullptr;
+            bytes = s2_align_up(bytes, 4096);
+            S2_CUDA(cudaMallocHost(&pinned, bytes));
+            pinned_n = bytes;
+        }
+        if (results_cap < nres) {
+            if (results_h) {
+                if (done) cudaEventSynchronize(done);
+                cudaFreeHost(results_h);
+            }
+            results_h = nullptr;
+            S2_CUDA(cudaMallocHost((void **)&results_h, nres * sizeof(DevResult)));
+            results_cap = nres;
+        }
+        return S2_OK;
+    }
+
+    int choose_strip_rows(const std::vector<uint64_t> &tiles_at) const {
+        if (strip_rows_cfg == 9 || strip_rows_cfg == 21 || strip_rows_cfg == 63) return strip_rows_cfg;
+        // largest strip height that still gives ~4 waves of resident tiles
+        const uint64_t resident = (uint64_t)num_sms * (uint64_t)fused_bps;
+        if (tiles_at[0] >= 4 * resident) return 63;
+        if (tiles_at[1] >= 4 * resident) return 21;
+        return 9;
+    }
+
+    // Lay out the levels and tiles of n pairs.
+    s2_status plan(const s2_pair_desc *d, int n, Plan &P, const PairExtra *ex = nullptr) {
+        P = Plan();
+        P.pairs.resize(n);
+        P.blk_first.resize(n);
+        // tile counts at strip heights 64/32 for the strip choice
+        std::vector<uint64_t> tiles_at(2, 0);
+        std::vector<int> ns(n);
+        for (int i = 0; i < n; i++) {
+            ns[i] = s2_num_scales_rule(d[i].width, d[i].height, scale_rule);
+            uint64_t w = d[i].width, h = d[i].height;
+            for (int s = 0; s < ns[i]; s++) {
+                tiles_at[0] += ((w + kTileW - 1) / kTileW) * ((h + 62) / 63);
+                tiles_at[1] += ((w + kTileW - 1) / kTileW) * ((h + 20) / 21);
+                w = (w + 1) / 2;
+                h = (h + 1) / 2;
+            }
+        }
+        P.strip_rows = choose_strip_rows(tiles_at);
+        size_t lvl_off = 0;
+        int blk = 0;
+        for (int i = 0; i < n; i++) {
+            DevPair &p = P.pairs[i];
+            memset(&p, 0, sizeof p);
+            const s2_pair_desc &q = d[i];
+            p.in[0] = q.ref;
+            p.in[1] = q.dis;
+            p.in_uv[0] = q.ref_uv;
+            p.in_uv[1] = q.dis_uv;
+            p.pitch[0] = (long long)q.ref_pitch;
+            p.pitch[1] = (long long)q.dis_pitch;
+            p.fmt = q.format;
+            p.bits = q.bits;
+            p.nscales = ns[i];
+            p.status = S2_OK;
+            p.prep_mask = ex ? ex[i].prep_mask : 3;
+            const bool need_ref_in = (p.prep_mask & 1) != 0;
+            const bool need_dis_in = (p.prep_mask & 2) != 0;
+            if (ns[i] == 0 || q.width > (1u << 16) || q.height > (1u << 16)) {
+                p.status = S2_ERR_INVALID_SIZE;
+                p.nscales = 0;
+                P.blk_first[i] = blk;
+                continue;
+            }
+            if (q.format < 0 || q.format > 3 || (need_ref_in && !q.ref) || (need_dis_in && !q.dis) ||
+                (q.format == S2_FMT_NV12 && ((need_ref_in && !q.ref_uv) || (need_dis_in && !q.dis_uv) ||
+                                             (q.width & 1) || (q.height & 1))) ||
+                (q.format == S2_FMT_RGB16 && (q.bits < 8 || q.bits > 16))) {
+                p.status = S2_ERR_INVALID_ARG;
+                p.nscales = 0;
+                P.blk_first[i] = blk;
+                continue;
+            }
+            p.w[0] = (int)q.width;
+            p.h[0] = (int)q.height;
+            for (int s = 1; s < kScales; s++) {
+                p.w[s] = (p.w[s - 1] + 1) / 2;
+                p.h[s] = (p.h[s - 1] + 1) / 2;
+            }
+            const bool ref_ext = ex && ex[i].ref_levels[0] != nullptr;
+            p.lvl_ext = ref_ext ? 1 : 0;
+            for (int s = 0; s < p.nscales; s++) {
+                p.lp[s] = (int)s2_align_up((size_t)p.w[s], 64);
+                size_t bytes = s2_align_up((size_t)3 * p.lp[s] * p.h[s] * esize(), 256);
+                if (ref_ext) {
+                    p.lvl[0][s] = ex[i].ref_levels[s];
+                } else {
+                    p.lvl[0][s] = (void *)lvl_off;  // offsets, rebased at upload
+                    lvl_off += bytes;
+                }
+                p.lvl[1][s] = (void *)lvl_off;
+                lvl_off += bytes;
+            }
+            P.blk_first[i] = blk;
+            {
+                p.blk_x = (p.w[0] + kPyrBlk - 1) / kPyrBlk;
+                p.blk_y = (p.h[0] + kPyrBlk - 1) / kPyrBlk;
+                p.blk_base = blk;
+                blk += p.blk_x * p.blk_y;
+            }
+        }
+        P.total_blocks = blk;
+        P.level_bytes = lvl_off;
+        // tiles: all pairs' scale 0 first, then scale 1, ... (largest work first)
+        int tile = 0;
+        for (int s = 0; s < kScales; s++) {
+            for (int i = 0; i < n; i++) {
+                DevPair &p = P.pairs[i];
+                if (p.status != S2_OK || s >= p.nscales || (ex && !ex[i].score)) continue;
+                Seg sg;
+                sg.first_tile = tile;
+                sg.pair = i;
+                sg.scale = s;
+                sg.tiles_x = (p.w[s] + kTileW - 1) / kTileW;
+                sg.strip_rows = P.strip_rows;
+                int ty = (p.h[s] + P.strip_rows - 1) / P.strip_rows;
+                p.tile_base[s] = tile;
+                p.tile_cnt[s] = sg.tiles_x * ty;
+                tile += p.tile_cnt[s];
+                P.segs.push_back(sg);
+            }
+        }
+        P.total_tiles = tile;
+        return S2_OK;
+    }
+
+    s2_status enqueue(Plan &P, cudaStream_t st) {
+        const int n = (int)P.pairs.size();
+        s2_status r;
+        if ((r = ensure(levels_d, std::max<size_t>(P.level_bytes, 256))) != S2_OK) return r;
+        if ((r = ensure(partials_d, std::max<size_t>((size_t)P.total_tiles * 18 * sizeof(double), 256))) != S2_OK) return r;
+        if ((r = ensure(results_d, (size_t)n * sizeof(DevResult))) != S2_OK) return r;
+        const size_t pb = s2_align_up(n * sizeof(DevPair), 256), bb = s2_align_up(n * sizeof(int), 256),
+                     sb = s2_align_up(std::max<size_t>(P.segs.size(), 1) * sizeof(Seg), 256);
+        if ((r = ensure(pairs_d, pb + bb + sb)) != S2_OK) return r;
+        if ((r = ensure_pinned(pb + bb + sb, n)) != S2_OK) return r;
+        // the previous submission may still read the pinned staging
+        if (pending) S2_CUDA(cudaEventSynchronize(done));
+        char *h = (char *)pinned;
+        DevPair *hp = (DevPair *)h;
+        for (int i = 0; i < n; i++) {
+            hp[i] = P.pairs[i];
+            for (int s = 0; s < kScales; s++)
+                for (int img = 0; img < 2; img++)
+                    if (s >= hp[i].nscales) hp[i].lvl[img][s] = nullptr;
+                    else if (!((hp[i].lvl_ext >> img) & 1))
+                        hp[i].lvl[img][s] = (char *)levels_d.p + (size_t)hp[i].lvl[img][s];
+        }
+        memcpy(h + pb, P.blk_first.data(), n * sizeof(int));
+        if (!P.segs.empty()) memcpy(h + pb + bb, P.segs.data(), P.segs.size() * sizeof(Seg));
+        char *dbase = (char *)pairs_d.p;
+        const DevPair *dpairs = (const DevPair *)dbase;
+        const int *dblk = (const int *)(dbase + pb);
+        const Seg *dsegs = (const Seg *)(dbase + pb + bb);
+        S2_CUDA(cudaMemcpyAsync(dbase, h, pb + bb + sb, cudaMemcpyHostToDevice, st));
+        S2_CUDA(cudaMemsetAsync(counter_d.p, 0, sizeof(int), st));
+        if (profiling) S2_CUDA(cudaEventRecord(prof[0], st));
+        S2_CUDA(launch_pyramid(storage, dpairs, n, dblk, P.total_blocks, cc, (const float *)lut_d.p,
+                               num_sms * 8, st));
+        if (profiling) S2_CUDA(cudaEventRecord(prof[1], st));
+        S2_CUDA(launch_fused(storage, dpairs, dsegs, (int)P.segs.size(), P.total_tiles, (int *)counter_d.p,
+                             (double *)partials_d.p, cc, (const float *)lut_d.p, num_sms * fused_bps, st));
+        if (profiling) S2_CUDA(cudaEventRecord(prof[2], st));
+        S2_CUDA(launch_finalize(dpairs, n, (const double *)partials_d.p, (DevResult *)results_d.p, st));
+        if (profiling) S2_CUDA(cudaEventRecord(prof[3], st));
+        S2_CUDA(cudaMemcpyAsync(results_h, results_d.p, n * sizeof(DevResult), cudaMemcpyDeviceToHost, st));
+        S2_CUDA(cudaEventRecord(done, st));
+        last_n = n;
+        pending = true;
+        return S2_OK;
+    }
+
+    s2_status wait() {
+        if (last_n < 0) return S2_ERR_NOT_READY;
+        S2_CUDA(cudaEventSynchronize(done));
+        pending = false;
+        return S2_OK;
+    }
+};

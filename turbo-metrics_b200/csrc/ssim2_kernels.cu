@@ -108,7 +108,7 @@ __device__ __forceinline__ void prep_level0(const DevPair &P, int X0, int Y0, co
 #pragma unroll
         for (int img = 0; img < 2; img++) {
             float v[3] = {0.f, 0.f, 0.f};
-            if (in) {
+            if (in && ((P.prep_mask >> img) & 1)) {
                 lin_pixel<FMT>(P, img, x, y, lut, cc, v);
                 store_xyb<ST>(P, img, 0, x, y, v);
             }
@@ -159,6 +159,7 @@ __global__ void __launch_bounds__(256) prep_kernel(const DevPair *__restrict__ p
                 const int ia = (ya - py0) * pbs, ib = (yb - py0) * pbs;
                 const int ja = xa - px0, jb = xb - px0;
                 for (int img = 0; img < 2; img++) {
+                    if (!((P.prep_mask >> img) & 1)) continue;
                     float v[3];
                     for (int c = 0; c < 3; c++) {
                         const float *src = s == 1 ? l0[img][c] : pp[(s - 1) & 1][img][c];
