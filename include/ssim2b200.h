@@ -241,6 +241,10 @@ typedef struct {
     uint64_t jobs_done, pairs_done, rounds, queued_jobs, hbm_in_use;
     double p50_ms, p99_ms, max_ms;   /* arrival -> completion of finished jobs */
     double uptime_s;
+    double gpu_busy_s;               /* device time of the rounds' kernels */
+    double worker_wait_s;            /* worker time blocked on finished rounds */
+    double worker_upload_s;          /* worker time issuing uploads */
+    double worker_submit_s;          /* worker time planning and enqueueing rounds */
 } s2_server_report;
 
 typedef struct s2_server s2_server;

@@ -98,7 +98,9 @@ class JobDesc(ctypes.Structure):
 class ServerReport(ctypes.Structure):
     _fields_ = [("jobs_done", ctypes.c_uint64), ("pairs_done", ctypes.c_uint64), ("rounds", ctypes.c_uint64),
                 ("queued_jobs", ctypes.c_uint64), ("hbm_in_use", ctypes.c_uint64), ("p50_ms", ctypes.c_double),
-                ("p99_ms", ctypes.c_double), ("max_ms", ctypes.c_double), ("uptime_s", ctypes.c_double)]
+                ("p99_ms", ctypes.c_double), ("max_ms", ctypes.c_double), ("uptime_s", ctypes.c_double),
+                ("gpu_busy_s", ctypes.c_double), ("worker_wait_s", ctypes.c_double),
+                ("worker_upload_s", ctypes.c_double), ("worker_submit_s", ctypes.c_double)]
 
 
 P = ctypes.c_void_p

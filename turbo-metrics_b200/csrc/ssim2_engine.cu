@@ -576,10 +576,7 @@ s2_status s2_batch_create(const s2_config *cfg_in, uint32_t max_pairs, uint64_t 
     b->max_pixels = max_pixels;
     st = b->eng.init(&cfg);
     if (st == S2_OK) {
-        // levels: < (1/3 + padding) of the scale-0 pixels, per image
-        size_t lv = (size_t)(max_pixels * 3 * b->eng.esize() * 2) * 4 / 3 + (size_t)max_pairs * (1u << 20);
-        st = b->eng.ensure(b->eng.levels_d, lv);
-        if (st == S2_OK) st = b->eng.ensure(b->eng.results_d, (size_t)max_pairs * sizeof(DevResult));
+        st = b->eng.reserve(max_pairs, max_pixels, false);
     }
     if (st != S2_OK) {
         b->eng.release();

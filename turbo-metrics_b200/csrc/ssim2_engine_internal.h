@@ -190,6 +190,24 @@ struct Engine {
         return S2_OK;
     }
 
+    // Size every buffer for submissions of up to `pairs` pairs and `pixels`
+    // scale-0 pixels, so that later submissions never reallocate (a cudaFree
+    // synchronises the whole device, other streams' queued work included).
+    s2_status reserve(size_t pairs, uint64_t pixels, bool one_image) {
+        const size_t imgs = one_image ? 1 : 2;
+        // XYB planes: 3 planes x esize x (4/3 of the pixels), plus row padding
+        const size_t lv = imgs * (3 * esize() * (size_t)(pixels * 4 / 3) + pairs * (size_t(1) << 20));
+        const size_t tiles = (size_t)(pixels * 3 / 2) / (kTileW * 9) + pairs * 256;
+        s2_status r;
+        if ((r = ensure(levels_d, lv)) != S2_OK) return r;
+        if ((r = ensure(partials_d, tiles * 18 * sizeof(double))) != S2_OK) return r;
+        if ((r = ensure(results_d, pairs * sizeof(DevResult))) != S2_OK) return r;
+        const size_t desc = s2_align_up(pairs * sizeof(DevPair), 256) + s2_align_up(pairs * sizeof(int), 256) +
+                            s2_align_up(pairs * kScales * sizeof(Seg), 256);
+        if ((r = ensure(pairs_d, desc)) != S2_OK) return r;
+        return ensure_pinned(desc, pairs);
+    }
+
     s2_status ensure_pinned(size_t bytes, size_t nres) {
         if (pinned_n < bytes) {
             if (pinned) {

@@ -59,7 +59,7 @@ struct Job {
     size_t lvl_off[s2::kScales] = {0, 0, 0, 0, 0, 0};
     int ns = 0;
     cudaEvent_t uploaded = nullptr;
-    bool admitted = false, ref_scheduled = false, cancelled = false, finished = false;
+    bool admitted = false, uploading = false, ref_scheduled = false, cancelled = false, finished = false;
     int next_cand = 0, inflight = 0, harvested = 0;
     std::vector<double> scores;
     std::vector<int32_t> status;
@@ -90,6 +90,8 @@ struct s2_server {
     // statistics
     std::vector<double> latencies_ms;
     uint64_t pairs_done = 0, jobs_done = 0, rounds = 0;
+    double gpu_ms = 0.0;  // device time of the rounds' kernels (CUDA events)
+    double t_wait = 0.0, t_upload = 0.0, t_submit = 0.0;  // worker time: GPU waits, upload issue, plan+enqueue
     Clock::time_point t0;
 
     std::vector<RoundEntry> round[2];
@@ -107,22 +109,43 @@ struct s2_server {
         return off;
     }
 
-    // Admit from the head of the queue while the budget allows (caller holds mu).
-    void admit_locked() {
+    // Admit from the head of the queue while the budget allows (caller holds
+    // mu); the uploads are issued by upload() after the lock is released.
+    void admit_locked(std::vector<Job *> &fresh) {
         for (Job *j : queue) {
             if (j->admitted || j->cancelled) continue;
             if (cfg.hbm_budget && bytes_in_use + j->bytes + workspace_bytes() > cfg.hbm_budget) break;
             if (cudaMallocFromPoolAsync((void **)&j->dev, j->bytes, pool, copy) != cudaSuccess) break;
-            const size_t img = (size_t)j->w * 3 * j->h, row = (size_t)j->w * 3;
-            cudaMemcpy2DAsync(j->dev, row, j->ref_host, j->ref_pitch, row, j->h, cudaMemcpyHostToDevice, copy);
-            for (size_t c = 0; c < j->cand_host.size(); c++)
-                cudaMemcpy2DAsync(j->dev + img * (1 + c), row, j->cand_host[c], j->cand_pitch, row, j->h,
-                                  cudaMemcpyHostToDevice, copy);
-            cudaEventCreateWithFlags(&j->uploaded, cudaEventDisableTiming);
-            cudaEventRecord(j->uploaded, copy);
             j->admitted = true;
+            j->uploading = true;
             bytes_in_use += j->bytes;
+            fresh.push_back(j);
         }
+    }
+
+    // Copy admitted jobs' host images up on the copy stream (worker thread,
+    // no lock held: a copy from pageable memory blocks until staged).
+    // One image host -> device: a single linear copy when the rows are packed
+    // (a 2-D copy of short rows moves a fraction of the link bandwidth).
+    cudaError_t copy_image(unsigned char *dst, const uint8_t *src, size_t pitch, size_t row, uint32_t rows) {
+        if (pitch == row) return cudaMemcpyAsync(dst, src, row * rows, cudaMemcpyHostToDevice, copy);
+        return cudaMemcpy2DAsync(dst, row, src, pitch, row, rows, cudaMemcpyHostToDevice, copy);
+    }
+
+    s2_status upload(const std::vector<Job *> &fresh) {
+        for (Job *j : fresh) {
+            const size_t img = (size_t)j->w * 3 * j->h, row = (size_t)j->w * 3;
+            if (copy_image(j->dev, j->ref_host, j->ref_pitch, row, j->h) != cudaSuccess) return S2_ERR_CUDA;
+            for (size_t c = 0; c < j->cand_host.size(); c++)
+                if (copy_image(j->dev + img * (1 + c), j->cand_host[c], j->cand_pitch, row, j->h) != cudaSuccess)
+                    return S2_ERR_CUDA;
+            if (cudaEventCreateWithFlags(&j->uploaded, cudaEventDisableTiming) != cudaSuccess ||
+                cudaEventRecord(j->uploaded, copy) != cudaSuccess)
+                return S2_ERR_CUDA;
+        }
+        std::lock_guard<std::mutex> lock(mu);
+        for (Job *j : fresh) j->uploading = false;
+        return S2_OK;
     }
 
     // Build the next round from admitted jobs, in arrival order (caller holds mu).
@@ -130,7 +153,7 @@ struct s2_server {
         r.clear();
         uint64_t pixels = 0;
         for (Job *j : queue) {
-            if (!j->admitted) break;  // FIFO: later jobs are not admitted either
+            if (!j->admitted || j->uploading) break;  // FIFO: later jobs wait too
             if (j->cancelled) continue;
             const uint64_t px = (uint64_t)j->w * j->h;
             if (!j->ref_scheduled) {
@@ -188,9 +211,12 @@ struct s2_server {
     // Wait for round k and hand its results to the jobs (caller holds no lock).
     void harvest_round(int k) {
         eng[k].wait();
+        float ms[3] = {0.f, 0.f, 0.f};
+        const bool timed = eng[k].timings(ms) == S2_OK;
         std::vector<Job *> completed;
         {
             std::lock_guard<std::mutex> lock(mu);
+            if (timed) gpu_ms += (double)ms[0] + ms[1] + ms[2];
             const s2::DevResult *res = eng[k].results_h;
             for (size_t i = 0; i < round[k].size(); i++) {
                 const RoundEntry &e = round[k][i];
@@ -232,10 +258,25 @@ struct s2_server {
 
     void run() {
         int cur = 0;
+        std::vector<Job *> fresh;
         for (;;) {
+            fresh.clear();
+            {
+                std::lock_guard<std::mutex> lock(mu);
+                admit_locked(fresh);
+            }
+            const auto ta = Clock::now();
+            const s2_status up = fresh.empty() ? S2_OK : upload(fresh);
+            t_upload += std::chrono::duration<double>(Clock::now() - ta).count();
+            if (up != S2_OK) {
+                std::lock_guard<std::mutex> lock(mu);
+                fatal = S2_ERR_CUDA;
+                stop = true;
+                cv_done.notify_all();
+                break;
+            }
             {
                 std::unique_lock<std::mutex> lock(mu);
-                admit_locked();
                 build_round_locked(round[cur]);
                 if (round[cur].empty() && !inflight[cur ^ 1]) {
                     if (stop) break;
@@ -244,7 +285,9 @@ struct s2_server {
                 }
             }
             if (!round[cur].empty()) {
+                const auto tb = Clock::now();
                 s2_status st = submit_round(cur);
+                t_submit += std::chrono::duration<double>(Clock::now() - tb).count();
                 if (st != S2_OK) {
                     std::lock_guard<std::mutex> lock(mu);
                     fatal = st;
@@ -256,7 +299,11 @@ struct s2_server {
                 inflight[cur] = true;
                 rounds++;
             }
-            if (inflight[cur ^ 1]) harvest_round(cur ^ 1);
+            if (inflight[cur ^ 1]) {
+                const auto tc = Clock::now();
+                harvest_round(cur ^ 1);
+                t_wait += std::chrono::duration<double>(Clock::now() - tc).count();
+            }
             cur ^= 1;
         }
         for (int k = 0; k < 2; k++)
@@ -294,6 +341,8 @@ s2_status s2_server_create(const s2_server_config *cfg_in, s2_server **out) {
     ec.strip_rows = 21;  // fixed tile geometry: a job scores the same alone and mixed
     s2_status st = S2_OK;
     for (int k = 0; k < 2 && st == S2_OK; k++) st = sv->eng[k].init(&ec);
+    for (int k = 0; k < 2 && st == S2_OK; k++) st = sv->eng[k].set_profiling(true);
+    for (int k = 0; k < 2 && st == S2_OK; k++) st = sv->eng[k].reserve(cfg.max_batch_pairs, cfg.max_batch_pixels, true);
     cudaMemPoolProps props;
     memset(&props, 0, sizeof props);
     props.allocType = cudaMemAllocationTypePinned;
@@ -445,6 +494,10 @@ s2_status s2_server_stats(s2_server *sv, s2_server_report *out) {
         out->max_ms = l.back();
     }
     out->uptime_s = std::chrono::duration<double>(Clock::now() - sv->t0).count();
+    out->gpu_busy_s = sv->gpu_ms / 1e3;
+    out->worker_wait_s = sv->t_wait;
+    out->worker_upload_s = sv->t_upload;
+    out->worker_submit_s = sv->t_submit;
     return S2_OK;
 }
 
@@ -453,6 +506,8 @@ s2_status s2_server_reset_stats(s2_server *sv) {
     std::lock_guard<std::mutex> lock(sv->mu);
     sv->latencies_ms.clear();
     sv->pairs_done = sv->jobs_done = sv->rounds = 0;
+    sv->gpu_ms = 0.0;
+    sv->t_wait = sv->t_upload = sv->t_submit = 0.0;
     sv->t0 = Clock::now();
     return S2_OK;
 }
