@@ -48,10 +48,35 @@ def test_server_alone_equals_mixed_bitwise(tmb, cuda):
     sv.close()
 
 
+SMALL = dict(max_batch_pairs=8, max_batch_pixels=1 << 21)
+
+
+def job_bytes(w, h, k):
+    """Device bytes the server admits a job with: inputs + reference XYB pyramid."""
+    up = lambda v, a: (v + a - 1) // a * a
+    total = up(w * h * 3 * (1 + k), 256)
+    for _ in range(tmb_num_scales(w, h)):
+        total += up(3 * up(w, 64) * h * 4, 256)
+        w, h = (w + 1) // 2, (h + 1) // 2
+    return total
+
+
+def tmb_num_scales(w, h):
+    import conftest
+    return conftest.load_package().num_scales(w, h)
+
+
+def workspace(tmb):
+    probe = tmb.Ssim2Server(**SMALL)
+    ws = probe.stats()["hbm_in_use"]
+    probe.close()
+    return ws
+
+
 def test_server_budget_admits_in_order(tmb, cuda):
     # a budget that holds about one job at a time: all still complete, in order
     ref, cands = job_images(512, 512, synth.pair_seed(4, 3), 3)
-    sv = tmb.Ssim2Server(hbm_budget=160 << 20)
+    sv = tmb.Ssim2Server(hbm_budget=workspace(tmb) + job_bytes(512, 512, 3) * 3 // 2, **SMALL)
     ids = [sv.submit(ref, cands) for _ in range(4)]
     res = [sv.wait(i) for i in ids]
     for r in res[1:]:
@@ -64,7 +89,8 @@ def test_server_budget_admits_in_order(tmb, cuda):
 
 def test_server_cancel_and_timeout(tmb, cuda):
     ref, cands = job_images(1280, 720, synth.pair_seed(4, 4), 5)
-    sv = tmb.Ssim2Server(max_batch_pairs=2, hbm_budget=120 << 20)
+    sv = tmb.Ssim2Server(hbm_budget=workspace(tmb) + job_bytes(1280, 720, 5) * 3 // 2, max_batch_pairs=2,
+                         max_batch_pixels=1 << 21)
     ids = [sv.submit(ref, cands) for _ in range(3)]
     sv.cancel(ids[2])  # still queued behind the budget
     with pytest.raises(tmb.S2Error) as e:

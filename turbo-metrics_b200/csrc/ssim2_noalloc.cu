@@ -96,6 +96,8 @@ extern "C" s2_status s2_compute_srgb8_noalloc(const uint8_t *ref, size_t ref_pit
     P.fmt = FMT_SRGB8;
     P.nscales = ns;
     P.status = S2_OK;
+    P.prep_mask = 3;  // convert both images
+    P.lvl_ext = 0;
     P.w[0] = (int)width;
     P.h[0] = (int)height;
     for (int s = 1; s < kScales; s++) {
