@@ -20,7 +20,7 @@ constexpr int kRowsPerBlk = 9;       // output rows per horizontal step (= windo
 constexpr int kSegs = 7;             // horizontal segments per row
 constexpr int kSegW = 8;             // output pixels per segment (kSegs * kSegW == kTileW)
 constexpr int kChunk = 4;            // pixels per f32 partial sum
-constexpr int kPyrBlk = 32;          // scale-0 block edge of the pyramid kernel
+constexpr int kPyrBlk = 64;          // scale-0 block edge of the prep kernel
 constexpr float kC2 = 0.0009f;
 
 enum Format { FMT_LINEAR_F32 = 0, FMT_SRGB8 = 1, FMT_NV12 = 2, FMT_RGB16 = 3 };
@@ -256,6 +256,39 @@ __device__ __forceinline__ void lin_pixel(const DevPair &P, int img, int x, int 
         for (int g = 0; g < 3; g++) {
             const float *m = cc.m2020 + 3 * g;
             o[g] = fmaxf(fmaf(m[0], p0, fmaf(m[1], p1, m[2] * p2)), 0.0f);
+        }
+    }
+}
+
+// Linear RGB of the 2x2 quad whose top-left pixel is (x, y) (inside the
+// image); px 0..3 = (x,y), (x+1,y), (x,y+1), (x+1,y+1); pixels outside the
+// image (vx / vy false) are not read.  NV12 chroma is one sample per quad.
+template <int FMT>
+__device__ __forceinline__ void lin_quad(const DevPair &P, int img, int x, int y, bool vx, bool vy,
+                                         const float *lut, const ColorConsts &cc, float o[4][3]) {
+    if (FMT == FMT_NV12) {
+        const uint8_t *yp = (const uint8_t *)P.in[img] + (long long)y * P.pitch[img] + x;
+        const uint8_t *uv = (const uint8_t *)P.in_uv[img] + (long long)(y >> 1) * P.pitch[img] + x;
+        const float cb = (float)((int)__ldg(uv) - 128);
+        const float cr = (float)((int)__ldg(uv + 1) - 128);
+        const float ar = cc.nv12[1] * cr;
+        const float ag = fmaf(cc.nv12[3], cb, cc.nv12[4] * cr);
+        const float ab = cc.nv12[2] * cb;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const bool in = (k & 1 ? vx : true) && (k & 2 ? vy : true);
+            if (!in) continue;
+            const int Y = __ldg(yp + (k & 1) + (k & 2 ? P.pitch[img] : 0));
+            const float luma = (float)(max(Y, 16) - 16) * cc.nv12[0];
+            o[k][0] = fminf(fmaxf(bt709_eotf(luma + ar), 0.0f), 1.0f);
+            o[k][1] = fminf(fmaxf(bt709_eotf(luma + ag), 0.0f), 1.0f);
+            o[k][2] = fminf(fmaxf(bt709_eotf(luma + ab), 0.0f), 1.0f);
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const bool in = (k & 1 ? vx : true) && (k & 2 ? vy : true);
+            if (in) lin_pixel<FMT>(P, img, x + (k & 1), y + (k >> 1), lut, cc, o[k]);
         }
     }
 }

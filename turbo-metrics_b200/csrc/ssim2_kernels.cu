@@ -86,6 +86,12 @@ __device__ __forceinline__ int find_seg(const Seg *segs, int nseg, int tile) {
 
 // ---------------------------------------------------------------------------
 // prep: input -> linear -> XYB of every scale (2x2 box pyramid in linear RGB)
+//
+// Block = 64x64 scale-0 pixels of one pair, 256 threads, each thread a 2x2
+// quad at a time: it converts the quad's four pixels, stores their XYB, and
+// averages them (downscale.rs:4-35, source clamped at the far edge) into the
+// scale-1 pixel, whose XYB it stores too and whose linear RGB goes to shared
+// memory for scales 2..5.
 // ---------------------------------------------------------------------------
 template <typename ST>
 __device__ __forceinline__ void store_xyb(const DevPair &P, int img, int s, int x, int y, const float lin[3]) {
@@ -98,32 +104,78 @@ __device__ __forceinline__ void store_xyb(const DevPair &P, int img, int s, int 
     for (int c = 0; c < 3; c++) dst[c * plane + off] = to_store<ST>(o[c]);
 }
 
-// Scale 0 of one 32x32 block: linear RGB into shared memory, XYB to HBM.
+// XYB of two horizontally adjacent pixels, stored as one 2-element write
+// (x even: the planes' pitch is a multiple of 64 elements).
+template <typename ST>
+__device__ __forceinline__ void store_xyb_pair(ST *dst, long long plane, long long off, const float a[3],
+                                               const float b[3]) {
+    float oa[3], ob[3];
+    xyb3(a, oa);
+    xyb3(b, ob);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        if constexpr (sizeof(ST) == 4) {
+            *(float2 *)(dst + c * plane + off) = make_float2(oa[c], ob[c]);
+        } else {
+            ST two[2] = {to_store<ST>(oa[c]), to_store<ST>(ob[c])};
+            *(unsigned *)(dst + c * plane + off) = *(const unsigned *)two;
+        }
+    }
+}
+
+constexpr int kLv1 = kPyrBlk / 2;  // scale-1 block edge (32)
+
 template <int FMT, typename ST>
-__device__ __forceinline__ void prep_level0(const DevPair &P, int X0, int Y0, const float *lut, const ColorConsts &cc,
-                                            float (*l0)[3][kPyrBlk * kPyrBlk]) {
-    for (int i = threadIdx.x; i < kPyrBlk * kPyrBlk; i += blockDim.x) {
-        const int x = X0 + i % kPyrBlk, y = Y0 + i / kPyrBlk;
-        const bool in = x < P.w[0] && y < P.h[0];
-#pragma unroll
+__device__ __forceinline__ void prep_quads(const DevPair &P, int X0, int Y0, const float *lut, const ColorConsts &cc,
+                                           float (*lv1)[3][kLv1 * kLv1]) {
+    const int W = P.w[0], H = P.h[0];
+    const bool scale1 = P.nscales > 1;
+    for (int q = threadIdx.x; q < kLv1 * kLv1; q += blockDim.x) {
+        const int qx = q % kLv1, qy = q / kLv1;
+        const int x = X0 + 2 * qx, y = Y0 + 2 * qy;
+        if (x >= W || y >= H) continue;
+        const bool vx = x + 1 < W, vy = y + 1 < H;
+#pragma unroll 1
         for (int img = 0; img < 2; img++) {
-            float v[3] = {0.f, 0.f, 0.f};
-            if (in && ((P.prep_mask >> img) & 1)) {
-                lin_pixel<FMT>(P, img, x, y, lut, cc, v);
-                store_xyb<ST>(P, img, 0, x, y, v);
+            if (!((P.prep_mask >> img) & 1)) continue;
+            float v[4][3];
+            lin_quad<FMT>(P, img, x, y, vx, vy, lut, cc, v);
+            ST *dst = (ST *)P.lvl[img][0];
+            const long long plane = (long long)P.lp[0] * H;
+            const long long off = (long long)y * P.lp[0] + x;
+            if (vx) store_xyb_pair<ST>(dst, plane, off, v[0], v[1]);
+            else store_xyb<ST>(P, img, 0, x, y, v[0]);
+            if (vy) {
+                if (vx) store_xyb_pair<ST>(dst, plane, off + P.lp[0], v[2], v[3]);
+                else store_xyb<ST>(P, img, 0, x, y + 1, v[2]);
             }
+            if (!scale1) continue;
+            // far-edge clamp: a missing column repeats the left pixel, a
+            // missing row the upper one
+            float l1[3];
 #pragma unroll
-            for (int c = 0; c < 3; c++) l0[img][c][i] = v[c];
+            for (int c = 0; c < 3; c++) {
+                const float a = v[0][c];
+                const float b = vx ? v[1][c] : a;
+                const float cc2 = vy ? v[2][c] : a;
+                const float d = vy ? (vx ? v[3][c] : cc2) : b;
+                float sum = a + b;
+                sum = sum + cc2;
+                sum = sum + d;
+                l1[c] = sum * 0.25f;
+                lv1[img][c][q] = l1[c];
+            }
+            store_xyb<ST>(P, img, 1, (X0 >> 1) + qx, (Y0 >> 1) + qy, l1);
         }
     }
 }
 
 template <typename ST>
-__global__ void __launch_bounds__(256) prep_kernel(const DevPair *__restrict__ pairs, int npairs,
+__global__ void __launch_bounds__(256, 3) prep_kernel(const DevPair *__restrict__ pairs, int npairs,
                                                    const int *__restrict__ blk_first, int total_blocks,
                                                    ColorConsts cc, const float *__restrict__ lut_g) {
-    __shared__ float l0[2][3][kPyrBlk * kPyrBlk];                  // scale-0 linear block [img][ch][px]
-    __shared__ float pp[2][2][3][(kPyrBlk / 2) * (kPyrBlk / 2)];  // scales >= 1, ping-pong
+    __shared__ float lv1[2][3][kLv1 * kLv1];              // scale-1 linear block [img][ch][px]
+    __shared__ float pp[2][2][3][(kLv1 / 2) * (kLv1 / 2)];  // scales >= 2, ping-pong
     __shared__ float lut[256];
     for (int i = threadIdx.x; i < 256; i += blockDim.x) lut[i] = lut_g[i];
     __syncthreads();
@@ -139,13 +191,13 @@ __global__ void __launch_bounds__(256) prep_kernel(const DevPair *__restrict__ p
         const int bx = b % P.blk_x, by = b / P.blk_x;
         const int X0 = bx * kPyrBlk, Y0 = by * kPyrBlk;
         switch (P.fmt) {
-        case FMT_LINEAR_F32: prep_level0<FMT_LINEAR_F32, ST>(P, X0, Y0, lut, cc, l0); break;
-        case FMT_SRGB8: prep_level0<FMT_SRGB8, ST>(P, X0, Y0, lut, cc, l0); break;
-        case FMT_NV12: prep_level0<FMT_NV12, ST>(P, X0, Y0, lut, cc, l0); break;
-        default: prep_level0<FMT_RGB16, ST>(P, X0, Y0, lut, cc, l0); break;
+        case FMT_LINEAR_F32: prep_quads<FMT_LINEAR_F32, ST>(P, X0, Y0, lut, cc, lv1); break;
+        case FMT_SRGB8: prep_quads<FMT_SRGB8, ST>(P, X0, Y0, lut, cc, lv1); break;
+        case FMT_NV12: prep_quads<FMT_NV12, ST>(P, X0, Y0, lut, cc, lv1); break;
+        default: prep_quads<FMT_RGB16, ST>(P, X0, Y0, lut, cc, lv1); break;
         }
         __syncthreads();
-        for (int s = 1; s < P.nscales; s++) {
+        for (int s = 2; s < P.nscales; s++) {
             const int bs = kPyrBlk >> s, pbs = kPyrBlk >> (s - 1);
             const int ox0 = X0 >> s, oy0 = Y0 >> s;
             const int px0 = X0 >> (s - 1), py0 = Y0 >> (s - 1);
@@ -162,7 +214,7 @@ __global__ void __launch_bounds__(256) prep_kernel(const DevPair *__restrict__ p
                     if (!((P.prep_mask >> img) & 1)) continue;
                     float v[3];
                     for (int c = 0; c < 3; c++) {
-                        const float *src = s == 1 ? l0[img][c] : pp[(s - 1) & 1][img][c];
+                        const float *src = s == 2 ? lv1[img][c] : pp[(s - 1) & 1][img][c];
                         float sum = src[ia + ja] + src[ia + jb];
                         sum = sum + src[ib + ja];
                         sum = sum + src[ib + jb];
