@@ -63,6 +63,16 @@ struct Seg {
     int strip_rows;
 };
 
+// A run of S2_BLUR_IIR_REF work items of one (pair, scale): columns x planes
+// for the vertical walk, rows x channels for the horizontal walk.
+struct IirSeg {
+    int first;     // first work item
+    int pair;
+    int scale;
+    int rec_base;  // first row record of this (pair, scale) in the partial sums
+    float *v;      // the 15 vertical-walk output planes of this (pair, scale)
+};
+
 struct DevResult {
     double score;
     double stats[108];

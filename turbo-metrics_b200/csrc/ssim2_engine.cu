@@ -277,10 +277,6 @@ s2_status s2_create(const s2_config *cfg_in, uint32_t width, uint32_t height, s2
     if (st != S2_OK) return st;
     if (s2_num_scales_rule(width, height, cfg.scale_rule) == 0 || width > 65536 || height > 65536)
         return S2_ERR_INVALID_SIZE;
-    if (cfg.blur != S2_BLUR_FIR) {
-        g_last_error = "S2_BLUR_IIR_REF is served by s2_iir_* entry points only";
-        return S2_ERR_INVALID_ARG;
-    }
     // pre-flight: levels (2 images, ~1/3 of scale 0) + partials + staging
     {
         size_t free_b = 0, total_b = 0;
@@ -569,7 +565,6 @@ s2_status s2_batch_create(const s2_config *cfg_in, uint32_t max_pairs, uint64_t 
     else s2_config_default(&cfg);
     s2_status st = check_cfg(&cfg);
     if (st != S2_OK) return st;
-    if (cfg.blur != S2_BLUR_FIR) return S2_ERR_INVALID_ARG;
     s2_batch *b = new (std::nothrow) s2_batch();
     if (!b) return S2_ERR_OOM;
     b->max_pairs = max_pairs;

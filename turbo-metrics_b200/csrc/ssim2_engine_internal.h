@@ -93,6 +93,10 @@ struct Plan {
     int total_tiles = 0;
     size_t level_bytes = 0;  // both images, all levels, all pairs
     int strip_rows = 63;
+    // S2_BLUR_IIR_REF: vertical / horizontal work runs, vertical output planes
+    std::vector<IirSeg> vsegs, hsegs;
+    int vtotal = 0, htotal = 0;
+    size_t v_bytes = 0;
 };
 
 struct Engine {
@@ -107,7 +111,7 @@ struct Engine {
     int fused_bps = 1;
     ColorConsts cc;
 
-    DevBuf pairs_d, blk_d, segs_d, counter_d, partials_d, results_d, levels_d, lut_d;
+    DevBuf pairs_d, blk_d, segs_d, counter_d, partials_d, results_d, levels_d, lut_d, iir_d;
     void *pinned = nullptr;  // staging: pairs | blk_first | segs
     size_t pinned_n = 0;
     DevResult *results_h = nullptr;
@@ -161,7 +165,7 @@ struct Engine {
         if (done) cudaEventSynchronize(done);
         for (cudaEvent_t &e : prof)
             if (e) cudaEventDestroy(e), e = nullptr;
-        for (DevBuf *b : {&pairs_d, &blk_d, &segs_d, &counter_d, &partials_d, &results_d, &levels_d, &lut_d})
+        for (DevBuf *b : {&pairs_d, &blk_d, &segs_d, &counter_d, &partials_d, &results_d, &levels_d, &lut_d, &iir_d})
             if (b->p) cudaFree(b->p), b->p = nullptr, b->n = 0;
         if (pinned) cudaFreeHost(pinned), pinned = nullptr;
         if (results_h) cudaFreeHost(results_h), results_h = nullptr;
@@ -323,6 +327,36 @@ struct Engine {
         }
         P.total_blocks = blk;
         P.level_bytes = lvl_off;
+        if (blur == S2_BLUR_IIR_REF) {
+            // one partial-sum record per row; vertical work items per column
+            // (groups of 32) and plane, horizontal per row and channel
+            int rec = 0;
+            for (int i = 0; i < n; i++) {
+                DevPair &p = P.pairs[i];
+                if (p.status != S2_OK || (ex && !ex[i].score)) continue;
+                for (int s = 0; s < p.nscales; s++) {
+                    const size_t vb = s2_align_up((size_t)15 * p.lp[s] * p.h[s] * sizeof(float), 256);
+                    IirSeg v;
+                    v.first = P.vtotal;
+                    v.pair = i;
+                    v.scale = s;
+                    v.rec_base = rec;
+                    v.v = (float *)P.v_bytes;  // offset, rebased at upload
+                    P.vsegs.push_back(v);
+                    P.vtotal += ((p.w[s] + 31) / 32) * 32 * 15;
+                    IirSeg h = v;
+                    h.first = P.htotal;
+                    P.hsegs.push_back(h);
+                    P.htotal += 3 * p.h[s];
+                    p.tile_base[s] = rec;
+                    p.tile_cnt[s] = p.h[s];
+                    rec += p.h[s];
+                    P.v_bytes += vb;
+                }
+            }
+            P.total_tiles = rec;
+            return S2_OK;
+        }
         // tiles: all pairs' scale 0 first, then scale 1, ... (largest work first)
         int tile = 0;
         for (int s = 0; s < kScales; s++) {
@@ -354,8 +388,11 @@ struct Engine {
         if ((r = ensure(results_d, (size_t)n * sizeof(DevResult))) != S2_OK) return r;
         const size_t pb = s2_align_up(n * sizeof(DevPair), 256), bb = s2_align_up(n * sizeof(int), 256),
                      sb = s2_align_up(std::max<size_t>(P.segs.size(), 1) * sizeof(Seg), 256);
-        if ((r = ensure(pairs_d, pb + bb + sb)) != S2_OK) return r;
-        if ((r = ensure_pinned(pb + bb + sb, n)) != S2_OK) return r;
+        const size_t vsb = s2_align_up(P.vsegs.size() * sizeof(IirSeg), 256),
+                     hsb = s2_align_up(P.hsegs.size() * sizeof(IirSeg), 256);
+        if (blur == S2_BLUR_IIR_REF && (r = ensure(iir_d, std::max<size_t>(P.v_bytes, 256))) != S2_OK) return r;
+        if ((r = ensure(pairs_d, pb + bb + sb + vsb + hsb)) != S2_OK) return r;
+        if ((r = ensure_pinned(pb + bb + sb + vsb + hsb, n)) != S2_OK) return r;
         // the previous submission may still read the pinned staging
         if (pending) S2_CUDA(cudaEventSynchronize(done));
         char *h = (char *)pinned;
@@ -370,18 +407,34 @@ struct Engine {
         }
         memcpy(h + pb, P.blk_first.data(), n * sizeof(int));
         if (!P.segs.empty()) memcpy(h + pb + bb, P.segs.data(), P.segs.size() * sizeof(Seg));
+        {
+            IirSeg *hv = (IirSeg *)(h + pb + bb + sb), *hh = (IirSeg *)(h + pb + bb + sb + vsb);
+            for (size_t k = 0; k < P.vsegs.size(); k++) {
+                hv[k] = P.vsegs[k];
+                hv[k].v = (float *)((char *)iir_d.p + (size_t)P.vsegs[k].v);
+            }
+            for (size_t k = 0; k < P.hsegs.size(); k++) {
+                hh[k] = P.hsegs[k];
+                hh[k].v = (float *)((char *)iir_d.p + (size_t)P.hsegs[k].v);
+            }
+        }
         char *dbase = (char *)pairs_d.p;
         const DevPair *dpairs = (const DevPair *)dbase;
         const int *dblk = (const int *)(dbase + pb);
         const Seg *dsegs = (const Seg *)(dbase + pb + bb);
-        S2_CUDA(cudaMemcpyAsync(dbase, h, pb + bb + sb, cudaMemcpyHostToDevice, st));
+        S2_CUDA(cudaMemcpyAsync(dbase, h, pb + bb + sb + vsb + hsb, cudaMemcpyHostToDevice, st));
         S2_CUDA(cudaMemsetAsync(counter_d.p, 0, sizeof(int), st));
         if (profiling) S2_CUDA(cudaEventRecord(prof[0], st));
         S2_CUDA(launch_pyramid(storage, dpairs, n, dblk, P.total_blocks, cc, (const float *)lut_d.p,
                                num_sms * 8, st));
         if (profiling) S2_CUDA(cudaEventRecord(prof[1], st));
-        S2_CUDA(launch_fused(storage, dpairs, dsegs, (int)P.segs.size(), P.total_tiles, (int *)counter_d.p,
-                             (double *)partials_d.p, cc, (const float *)lut_d.p, num_sms * fused_bps, st));
+        if (blur == S2_BLUR_IIR_REF)
+            S2_CUDA(launch_iir(storage, dpairs, (const IirSeg *)(dbase + pb + bb + sb), (int)P.vsegs.size(), P.vtotal,
+                               (const IirSeg *)(dbase + pb + bb + sb + vsb), (int)P.hsegs.size(), P.htotal,
+                               (double *)partials_d.p, st));
+        else
+            S2_CUDA(launch_fused(storage, dpairs, dsegs, (int)P.segs.size(), P.total_tiles, (int *)counter_d.p,
+                                 (double *)partials_d.p, cc, (const float *)lut_d.p, num_sms * fused_bps, st));
         if (profiling) S2_CUDA(cudaEventRecord(prof[2], st));
         S2_CUDA(launch_finalize(dpairs, n, (const double *)partials_d.p, (DevResult *)results_d.p, st));
         if (profiling) S2_CUDA(cudaEventRecord(prof[3], st));

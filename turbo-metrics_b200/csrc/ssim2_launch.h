@@ -16,6 +16,8 @@ cudaError_t launch_pyramid(int storage, const DevPair *pairs, int npairs, const 
 cudaError_t launch_fused(int storage, const DevPair *pairs, const Seg *segs, int nseg, int total_tiles,
                          int *counter, double *partials, const ColorConsts &cc, const float *lut,
                          int grid, cudaStream_t st);
+cudaError_t launch_iir(int storage, const DevPair *pairs, const IirSeg *vsegs, int nvseg, int vtotal,
+                       const IirSeg *hsegs, int nhseg, int htotal, double *partials, cudaStream_t st);
 cudaError_t launch_finalize(const DevPair *pairs, int npairs, const double *partials, DevResult *out,
                             cudaStream_t st);
 }  // namespace s2

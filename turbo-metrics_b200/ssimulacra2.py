@@ -60,10 +60,10 @@ class Ssimulacra2:
     binding style (`compute()` then re-reads those two tensors)."""
 
     def __init__(self, width, height, *, device=0, storage="f32", scale_rule="cpu", strip_rows=0,
-                 hbm_budget=0):
+                 hbm_budget=0, blur="fir"):
         self.width, self.height = int(width), int(height)
         cfg = capi.make_config(device=device, storage=storage, scale_rule=scale_rule,
-                               strip_rows=strip_rows, hbm_budget=hbm_budget)
+                               strip_rows=strip_rows, hbm_budget=hbm_budget, blur=blur)
         h = ctypes.c_void_p()
         check(lib.s2_create(ctypes.byref(cfg), self.width, self.height, ctypes.byref(h)), "Ssimulacra2::new")
         self._h = h
@@ -250,9 +250,9 @@ class Ssim2Batch:
     widened to mixed sizes and formats)."""
 
     def __init__(self, max_pairs, max_pixels, *, device=0, storage="f32", scale_rule="cpu", strip_rows=0,
-                 hbm_budget=0):
+                 hbm_budget=0, blur="fir"):
         cfg = capi.make_config(device=device, storage=storage, scale_rule=scale_rule, strip_rows=strip_rows,
-                               hbm_budget=hbm_budget)
+                               hbm_budget=hbm_budget, blur=blur)
         h = ctypes.c_void_p()
         check(lib.s2_batch_create(ctypes.byref(cfg), max_pairs, max_pixels, ctypes.byref(h)), "Ssim2Batch::new")
         self._h = h
