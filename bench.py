@@ -236,16 +236,16 @@ def sum_pixels(w=W, h=H, scales=6):
     return n
 
 
-def algorithmic_bytes_fused(storage_bytes=4):
-    """Declared I/O of one fused launch over the 64 pairs: it reads the XYB
+def algorithmic_bytes_fused(n_pairs, storage_bytes=4):
+    """Declared I/O of one fused launch over n_pairs pairs: it reads the XYB
     planes of both frames at every scale (3 planes x storage bytes x sum of
     the scale sizes) and writes 18 doubles per tile (negligible)."""
-    return N_PAIRS * 2 * 3 * storage_bytes * sum_pixels()
+    return n_pairs * 2 * 3 * storage_bytes * sum_pixels()
 
 
-def algorithmic_bytes_prep(storage_bytes=4):
+def algorithmic_bytes_prep(n_pairs, storage_bytes=4):
     """prep: reads the NV12 frames (1.5 B/px each), writes the XYB planes."""
-    return N_PAIRS * (2 * 1.5 * W * H + 2 * 3 * storage_bytes * sum_pixels())
+    return n_pairs * (2 * 1.5 * W * H + 2 * 3 * storage_bytes * sum_pixels())
 
 
 def main():
@@ -257,11 +257,14 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--plain-pairs", type=int, default=64)
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--pairs", type=int, default=N_PAIRS,
+                    help="pairs per step (64 is the workload; smaller only for profiler captures)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
 
+    NP = args.pairs
     if args.impl == "reference":
         return run_reference(args, rank, world)
 
@@ -274,14 +277,14 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
     tmb = import_pkg()
 
-    pairs_np = gen_pairs(N_PAIRS, offset=rank * N_PAIRS)
+    pairs_np = gen_pairs(NP, offset=rank * NP)
     dev = []
     for ry, ruv, dy, duv in pairs_np:
         dev.append(tuple(torch.from_numpy(a).cuda() for a in (ry, ruv, dy, duv)))
     descs = [tmb.PairDesc(r, d, "nv12", ru, du) for r, ru, d, du in dev]
     stream = torch.cuda.current_stream()
 
-    batch = tmb.Ssim2Batch(N_PAIRS, N_PAIRS * W * H)
+    batch = tmb.Ssim2Batch(NP, NP * W * H)
     batch.submit(descs)
     scores = [r[0] for r in batch.results()]
     lib = tmb.lib
@@ -309,7 +312,7 @@ def main():
     if dist is not None:
         dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
     ms = float(ms_t.item())
-    value = world * N_PAIRS * args.steps / (ms / 1e3)
+    value = world * NP * args.steps / (ms / 1e3)
 
     # ---- fused-kernel roofline (CUDA events around each launch) ----------
     lib.s2_batch_set_profiling(batch._h, 1)
@@ -329,7 +332,7 @@ def main():
     except (OSError, ValueError):
         pass
     peak = peaks.get("hbm_gbs", 6650.0)
-    ab = algorithmic_bytes_fused()
+    ab = algorithmic_bytes_fused(NP)
     achieved = ab / (fused_ms / 1e3) / 1e9
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "fused_traffic.json")
@@ -344,11 +347,11 @@ def main():
                 "kernel_ms": {"prep": float(acc[0]), "fused": fused_ms, "finalize": float(acc[2])},
                 "fused_blocks_per_sm": int(lib.s2_fused_blocks_per_sm(0)),
                 "algorithmic_bytes_per_launch": ab,
-                "prep_gbs": algorithmic_bytes_prep() / (float(acc[0]) / 1e3) / 1e9}
+                "prep_gbs": algorithmic_bytes_prep(NP) / (float(acc[0]) / 1e3) / 1e9}
 
     # ---- plain: the drop-in, one pair at a time ----------------------------
     ctx = tmb.Ssimulacra2(W, H)
-    npl = min(args.plain_pairs, N_PAIRS)
+    npl = min(args.plain_pairs, NP)
     for i in range(3):
         r, ru, d, du = dev[i]
         ctx.compute_nv12(r, ru, d, du)
@@ -372,7 +375,7 @@ def main():
     ddev = [tuple(torch.empty_like(a, device="cuda") for a in h) for h in host]
     ddescs = [tmb.PairDesc(r, d, "nv12", ru, du) for r, ru, d, du in ddev]
     h2d = sum(a.numel() for h in host for a in h)
-    d2h = N_PAIRS * ctypes.sizeof(tmb.capi.Result)
+    d2h = NP * ctypes.sizeof(tmb.capi.Result)
 
     def e2e_step():
         for hs, ds in zip(host, ddev):
@@ -396,7 +399,7 @@ def main():
     if dist is not None:
         dist.all_reduce(et, op=dist.ReduceOp.MAX)
     e2e_ms = float(et.item())
-    e2e = world * N_PAIRS * args.steps / (e2e_ms / 1e3)
+    e2e = world * NP * args.steps / (e2e_ms / 1e3)
     assert np.allclose([r[0] for r in res], scores, atol=1e-9)
 
     served = None
@@ -412,8 +415,8 @@ def main():
             "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "64 x 1920x1080 NV12 BT.709 limited pairs per step (batched, one submission)",
-                       "pairs_per_step": N_PAIRS, "storage": "f32", "blur": "fir (fused, shifted moments)",
+            "config": {"workload": f"{NP} x 1920x1080 NV12 BT.709 limited pairs per step (batched, one submission)",
+                       "pairs_per_step": NP, "storage": "f32", "blur": "fir (fused, shifted moments)",
                        "l2": "inputs 398 MB per step > 126 MB L2 (no flush)",
                        "parallelism": "replicas" if world > 1 else "single"},
             "plain_pairs_per_s": plain, "batched_vs_plain": value / world / plain,

@@ -30,20 +30,25 @@
 namespace s2 {
 
 // Shared memory layout of fused_kernel.  Rows ("rb" = output row of the
-// block x channel, 27 of them) are kRowStride elements apart: with an odd
-// stride and the horizontal tasks numbered segment-major (lane t reads row
-// t % 27, segment t / 27), the 8-byte loads of a half-warp and the 4-byte
-// loads of a warp fall in distinct banks (at most 2-way where a warp spans two
-// segments), where the plain 64-element stride gave up to 10-way conflicts.
+// block x channel, 27 of them) of the float2 arrays are kRowStride2 float2
+// apart and rows of the float array kRowStride1 floats apart.  The horizontal
+// tasks read them with 16-byte loads, lane t taking block row t % 27 and
+// segment t / 27: with kRowStride2 / 2 and kRowStride1 / 4 odd, the eight
+// lanes of each load phase fall in distinct 16-byte bank groups (at most
+// 2-way where a warp spans two segments).  The plain 64-element stride gave
+// up to 10-way conflicts.
 constexpr int kRB = kRowsPerBlk * 3;                     // rows of one block
-constexpr int kRowStride = 73;
-constexpr int kSmVo2 = 2 * kRB * kRowStride * 2;         // vertical FIR of the plane pairs (x,y), (xx,yy) [pair][rb][col]
-constexpr int kSmVo1 = kRB * kRowStride;                 // vertical FIR of xy [rb][col]
-constexpr int kSmXo = kRB * kRowStride * 2;              // shifted raw XYB (x', y') of the output rows [rb][col]
-constexpr int kFusedSmemFloats = kSmVo2 + kSmVo1 + kSmXo;
-static_assert(kSmVo2 % 2 == 0 && kSmXo % 2 == 0, "float2 arrays must stay 8-byte aligned");
+constexpr int kRowStride2 = 74;                          // float2 elements
+constexpr int kRowStride1 = 76;                          // float elements
+static_assert(kRowStride2 % 2 == 0 && (kRowStride2 / 2) % 2 == 1, "16-byte aligned rows, odd 16-byte stride");
+static_assert(kRowStride1 % 4 == 0 && (kRowStride1 / 4) % 2 == 1, "16-byte aligned rows, odd 16-byte stride");
+constexpr int kSmVo2 = 2 * kRB * kRowStride2 * 2;        // vertical FIR of (x,y), (xx,yy) [pair][rb][col] (floats)
+constexpr int kSmXo = kRB * kRowStride2 * 2;             // shifted raw XYB (x', y') of the output rows [rb][col]
+constexpr int kSmVo1 = kRB * kRowStride1;                // vertical FIR of xy [rb][col]
+constexpr int kFusedSmemFloats = kSmVo2 + kSmXo + kSmVo1;
 constexpr int kFusedThreads = kCols * 3;
 constexpr int kTasks = kRB * kSegs;                      // horizontal tasks per 9-row block
+static_assert(kSmVo2 % 4 == 0 && kSmXo % 4 == 0, "arrays start 16-byte aligned");
 
 __device__ __forceinline__ float fir9(float a0, float a1, float a2, float a3, float a4, float a5,
                                       float a6, float a7, float a8) {
@@ -334,10 +339,10 @@ __global__ void __maxnreg__(96)
                     const float vc = fir9(S2_W(w1, 0), S2_W(w1, 1), S2_W(w1, 2), S2_W(w1, 3), S2_W(w1, 4),
                                           S2_W(w1, 5), S2_W(w1, 6), S2_W(w1, 7), S2_W(w1, 8));
                     const int rb = k * 3 + g;
-                    s_vo2[rb * kRowStride + col] = va;
-                    s_vo2[(kRB + rb) * kRowStride + col] = vb;
-                    s_vo1[rb * kRowStride + col] = vc;
-                    s_xo[rb * kRowStride + col] = S2_W(w2a, 4);
+                    s_vo2[rb * kRowStride2 + col] = va;
+                    s_vo2[(kRB + rb) * kRowStride2 + col] = vb;
+                    s_vo1[rb * kRowStride1 + col] = vc;
+                    s_xo[rb * kRowStride2 + col] = S2_W(w2a, 4);
 #undef S2_W
                 }
             }
@@ -348,36 +353,68 @@ __global__ void __maxnreg__(96)
                 const int xs = t_s * kSegW;
                 if (x0 + xs < W) {
                     const int rb = t_rb;
-                    const float2 *pa = s_vo2 + rb * kRowStride;
-                    const float2 *pb = s_vo2 + (kRB + rb) * kRowStride;
-                    const float *pc = s_vo1 + rb * kRowStride;
-                    const float2 *px = s_xo + rb * kRowStride;
+                    const float2 *pa = s_vo2 + rb * kRowStride2;
+                    const float2 *pb = s_vo2 + (kRB + rb) * kRowStride2;
+                    const float *pc = s_vo1 + rb * kRowStride1;
+                    const float2 *px = s_xo + rb * kRowStride2;
                     // shift of the task's channel (same anchor as the vertical pass)
                     const float cv = ld_store<ST>((const ST *)P.lvl[0][s] + t_g * plane +
                                                   (long long)((y0 / kBand) * kBand) * lp + x0);
                     const float bv = border_gain(y, H);
 #pragma unroll 1
                     for (int half = 0; half < kSegW / kChunk; half++) {
-                        const int c0 = xs + half * kChunk;  // first output (tile coords)
+                        const int c0 = xs + half * kChunk;  // first output (tile coords), a multiple of 4
                         float2 ma[kChunk], mb[kChunk];
                         float mc[kChunk];
                         {
-                            float2 va[kChunk + 8], vb[kChunk + 8];
-                            float vc[kChunk + 8];
+                            float2 v[kChunk + 8];
+                            const float4 *q = (const float4 *)(pa + c0);
 #pragma unroll
-                            for (int j = 0; j < kChunk + 8; j++) {
-                                va[j] = pa[c0 + j];
-                                vb[j] = pb[c0 + j];
-                                vc[j] = pc[c0 + j];
+                            for (int j = 0; j < (kChunk + 8) / 2; j++) {
+                                const float4 t4 = q[j];
+                                v[2 * j] = make_float2(t4.x, t4.y);
+                                v[2 * j + 1] = make_float2(t4.z, t4.w);
                             }
 #pragma unroll
-                            for (int j = 0; j < kChunk; j++) {
-                                ma[j] = fir9x2(va[j], va[j + 1], va[j + 2], va[j + 3], va[j + 4], va[j + 5], va[j + 6],
-                                               va[j + 7], va[j + 8]);
-                                mb[j] = fir9x2(vb[j], vb[j + 1], vb[j + 2], vb[j + 3], vb[j + 4], vb[j + 5], vb[j + 6],
-                                               vb[j + 7], vb[j + 8]);
-                                mc[j] = fir9(vc[j], vc[j + 1], vc[j + 2], vc[j + 3], vc[j + 4], vc[j + 5], vc[j + 6],
-                                             vc[j + 7], vc[j + 8]);
+                            for (int j = 0; j < kChunk; j++)
+                                ma[j] = fir9x2(v[j], v[j + 1], v[j + 2], v[j + 3], v[j + 4], v[j + 5], v[j + 6], v[j + 7], v[j + 8]);
+                        }
+                        {
+                            float2 v[kChunk + 8];
+                            const float4 *q = (const float4 *)(pb + c0);
+#pragma unroll
+                            for (int j = 0; j < (kChunk + 8) / 2; j++) {
+                                const float4 t4 = q[j];
+                                v[2 * j] = make_float2(t4.x, t4.y);
+                                v[2 * j + 1] = make_float2(t4.z, t4.w);
+                            }
+#pragma unroll
+                            for (int j = 0; j < kChunk; j++)
+                                mb[j] = fir9x2(v[j], v[j + 1], v[j + 2], v[j + 3], v[j + 4], v[j + 5], v[j + 6], v[j + 7], v[j + 8]);
+                        }
+                        {
+                            float v[kChunk + 8];
+                            const float4 *q = (const float4 *)(pc + c0);
+#pragma unroll
+                            for (int j = 0; j < (kChunk + 8) / 4; j++) {
+                                const float4 t4 = q[j];
+                                v[4 * j] = t4.x;
+                                v[4 * j + 1] = t4.y;
+                                v[4 * j + 2] = t4.z;
+                                v[4 * j + 3] = t4.w;
+                            }
+#pragma unroll
+                            for (int j = 0; j < kChunk; j++)
+                                mc[j] = fir9(v[j], v[j + 1], v[j + 2], v[j + 3], v[j + 4], v[j + 5], v[j + 6], v[j + 7], v[j + 8]);
+                        }
+                        float2 xyv[kChunk];
+                        {
+                            const float4 *q = (const float4 *)(px + c0 + 4);
+#pragma unroll
+                            for (int j = 0; j < kChunk / 2; j++) {
+                                const float4 t4 = q[j];
+                                xyv[2 * j] = make_float2(t4.x, t4.y);
+                                xyv[2 * j + 1] = make_float2(t4.z, t4.w);
                             }
                         }
                         float fs[3] = {0.f, 0.f, 0.f}, f4[3] = {0.f, 0.f, 0.f};
@@ -386,7 +423,7 @@ __global__ void __maxnreg__(96)
                             const int xx = x0 + c0 + j;
                             if (xx < W) {
                                 const float m1 = ma[j].x, m2 = ma[j].y, s11 = mb[j].x, s22 = mb[j].y, s12 = mc[j];
-                                const float2 xy = px[c0 + j + 4];
+                                const float2 xy = xyv[j];
                                 const float bh = border_gain(xx, W);
                                 const float corr =
                                     (bh == 1.0f && bv == 1.0f) ? 0.0f : (float)(1.0 - (double)bh * (double)bv);
