@@ -465,9 +465,12 @@ static inline float eng_cbrtf(float x) {
     return pos ? y : 0.0f;
 }
 
-/* a / b for b > 0 as the engine computes it (s2_div): Newton reciprocal
- * from the bit seed 0x7EF311C3 - bits(b), three steps, then one residual
- * correction of q = a r. */
+/* a / b for b > 0 on the error maps' operand ranges, equal there to IEEE
+ * division (checked in the tests): Newton reciprocal from the bit seed
+ * 0x7EF311C3 - bits(b), three steps, then the residual correction of
+ * q = a r that the engine's s2_div also ends with (the engine starts from
+ * the hardware reciprocal approximation instead, which C cannot restate;
+ * both give the IEEE quotient outside rare near-halfway cases). */
 static inline float eng_div(float a, float b) {
     float r = asf(0x7EF311C3u - asu(b));
     r = fmaf(r, fmaf(-b, r, 1.0f), r);

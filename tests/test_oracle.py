@@ -240,9 +240,10 @@ def test_engine_eotf_power_within_4_ulp(oracle):
 
 
 def test_engine_division_matches_ieee(oracle):
-    """The engine's FMA-only division (Newton reciprocal from a bit seed plus
-    one residual correction) equals IEEE division on the operand ranges of the
-    error maps: denominators in [9e-4, 4], numerators of either sign."""
+    """The oracle's FMA-only division (Newton reciprocal from a bit seed plus
+    the residual correction the engine's division also ends with) equals IEEE
+    division on the operand ranges of the error maps: denominators in
+    [9e-4, 4], numerators of either sign."""
     import ctypes
     f = oracle._lib.or_div
     f.restype = ctypes.c_float

@@ -125,16 +125,18 @@ __device__ __forceinline__ float s2_cbrtf(float x) {
     return pos ? y : 0.0f;
 }
 
-// a / b for b > 0 normal, without a division instruction: Newton iteration
-// on 1/b from the bit-pattern seed 0x7EF311C3 - bits(b) (three steps of
-// r <- r + r (1 - b r)), then one residual correction of q = a r.  FMA and
-// multiply only, no branches; identical to IEEE division on 5e7 samples of
-// the ranges used here (checked in the tests).
+// a / b for b > 0 normal (the error-map denominators: >= 9e-4 and >= 1).
+// The reciprocal comes from the SFU approximation (PTX rcp.approx.ftz.f32,
+// at most 1 ulp from 1/b); the quotient q = a r then gets one residual
+// correction q + (a - b q) r, the final step of Markstein's division
+// (P. Markstein, "IA-64 and Elementary Functions", 2000): the residual
+// a - b q is exact under FMA, so the corrected quotient is within
+// 0.5 ulp + 2^-23 of the residual's weight -- the IEEE quotient except in
+// rare near-halfway cases.  4 instructions instead of a division's
+// multi-instruction sequence with its slow path.
 __device__ __forceinline__ float s2_div(float a, float b) {
-    float r = __uint_as_float(0x7EF311C3u - __float_as_uint(b));
-    r = fmaf(r, fmaf(-b, r, 1.0f), r);
-    r = fmaf(r, fmaf(-b, r, 1.0f), r);
-    r = fmaf(r, fmaf(-b, r, 1.0f), r);
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(b));
     const float q = a * r;
     const float e = fmaf(-b, q, a);
     return fmaf(e, r, q);
