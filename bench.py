@@ -10,9 +10,10 @@ submission of all 64 pairs (pyramid + fused tiles + finalize launches).
                  NV12 = 398 MB per step, larger than the 126 MB L2, so no flush)
   plain          the drop-in path: one context, one compute + result read per
                  pair, pairs in sequence
-  e2e            the public API with host buffers: every step copies the 64
-                 pairs from pinned host memory, scores them and reads the 64
-                 results back
+  e2e            the public API with host buffers (s2_batch_submit_host):
+                 every step uploads the 64 pairs from pinned host memory in
+                 groups that overlap the compute of earlier groups, scores
+                 them and reads the 64 results back
   roofline       fused kernel: algorithmic bytes per launch (scale-0 NV12 of
                  both frames + the pyramid levels it reads) / its CUDA-event time
   cpu_baseline   the CPU SSIMULACRA2 path the reference validates against (the
@@ -372,16 +373,13 @@ def main():
     host = []
     for ry, ruv, dy, duv in pairs_np:
         host.append(tuple(torch.from_numpy(a).pin_memory() for a in (ry, ruv, dy, duv)))
-    ddev = [tuple(torch.empty_like(a, device="cuda") for a in h) for h in host]
-    ddescs = [tmb.PairDesc(r, d, "nv12", ru, du) for r, ru, d, du in ddev]
+    hdescs = [tmb.PairDesc(r, d, "nv12", ru, du) for r, ru, d, du in host]
     h2d = sum(a.numel() for h in host for a in h)
     d2h = NP * ctypes.sizeof(tmb.capi.Result)
 
     def e2e_step():
-        for hs, ds in zip(host, ddev):
-            for a, b in zip(hs, ds):
-                b.copy_(a, non_blocking=True)
-        batch.submit(ddescs)
+        # s2_batch_submit_host: uploads in groups that overlap earlier groups' compute
+        batch.submit_host(hdescs)
         return batch.results()
 
     for _ in range(args.warmup):

@@ -201,6 +201,17 @@ void s2_batch_destroy(s2_batch *b);
 /* Enqueue n pairs on `stream` (asynchronous).  A pair below 8x8 gets
  * S2_ERR_INVALID_SIZE in its result; the others run. */
 s2_status s2_batch_submit(s2_batch *b, const s2_pair_desc *pairs, uint32_t n, void *stream);
+/* The same submission with every plane in HOST memory (the decoder's output
+ * buffers): the batch uploads the planes into its own device staging in up
+ * to 16 groups of about equal pixel count on an internal copy stream, and
+ * each group's launches on `stream` wait only for that group's planes, so the
+ * uploads of later groups overlap the compute of earlier ones (ssim2-gpu's
+ * batch takes device images only, pipeline_batch.rs:247-382; its callers
+ * upload first, then compute).  Page-locked host memory gives asynchronous
+ * uploads; pageable memory works, with each copy finishing before the call
+ * goes on.  The host planes must stay unchanged until s2_batch_results
+ * returns.  S2_ERR_DIM_MISMATCH if a pitch is below the row's bytes. */
+s2_status s2_batch_submit_host(s2_batch *b, const s2_pair_desc *pairs, uint32_t n, void *stream);
 /* Wait for the last submission and copy its n results. */
 s2_status s2_batch_results(s2_batch *b, s2_result *out, uint32_t n);
 s2_status s2_batch_mem_usage(const s2_batch *b, size_t *bytes);

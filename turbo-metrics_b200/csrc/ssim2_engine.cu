@@ -596,6 +596,20 @@ s2_status s2_batch_submit(s2_batch *b, const s2_pair_desc *pairs, uint32_t n, vo
     return b->eng.enqueue(b->plan, (cudaStream_t)stream);
 }
 
+s2_status s2_batch_submit_host(s2_batch *b, const s2_pair_desc *pairs, uint32_t n, void *stream) {
+    if (!b || (!pairs && n)) return S2_ERR_INVALID_ARG;
+    if (n > b->max_pairs) return S2_ERR_INVALID_ARG;
+    for (uint32_t i = 0; i < n; i++) {
+        const size_t row = s2_row_bytes(pairs[i]);
+        if (pairs[i].ref_pitch < row || pairs[i].dis_pitch < row) return S2_ERR_DIM_MISMATCH;
+    }
+    // S2_BLUR_IIR_REF runs its two passes over all pairs at once: one group
+    const int ng = b->eng.blur == S2_BLUR_IIR_REF ? 1 : std::min<int>(kMaxGroups, std::max<int>(1, (int)n / 4));
+    s2_status st = b->eng.plan(pairs, (int)n, b->plan, nullptr, ng);
+    if (st != S2_OK) return st;
+    return b->eng.enqueue(b->plan, (cudaStream_t)stream, pairs);
+}
+
 s2_status s2_batch_results(s2_batch *b, s2_result *out, uint32_t n) {
     if (!b || (!out && n)) return S2_ERR_INVALID_ARG;
     s2_status st = b->eng.wait();

@@ -70,6 +70,19 @@ struct PairExtra {
     void *ref_levels[kScales] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
 };
 
+// Host-side bytes of one image of a pair: its main plane (rows x row bytes)
+// and, for NV12, the interleaved chroma plane (height / 2 rows of width bytes).
+inline size_t s2_row_bytes(const s2_pair_desc &q) {
+    switch (q.format) {
+    case S2_FMT_LINEAR_F32: return (size_t)q.width * 12;
+    case S2_FMT_SRGB8: return (size_t)q.width * 3;
+    case S2_FMT_NV12: return (size_t)q.width;
+    default: return (size_t)q.width * 6;
+    }
+}
+
+constexpr int kMaxGroups = 16;  // copy/compute groups of a host-input submission
+
 // Byte layout of one image's XYB planes (all scored scales), as the plan lays
 // them out: plane pitch rounded up to 64 elements, 256-byte aligned scales.
 inline size_t s2_image_levels_layout(uint32_t w, uint32_t h, int ns, size_t esize, size_t off[kScales]) {
@@ -93,6 +106,10 @@ struct Plan {
     int total_tiles = 0;
     size_t level_bytes = 0;  // both images, all levels, all pairs
     int strip_rows = 63;
+    // groups: pairs [grp_pair[g], grp_pair[g+1]) own the tiles
+    // [grp_tile[g], grp_tile[g+1]); one group unless the inputs are uploaded
+    // from the host in pipelined groups
+    std::vector<int> grp_pair, grp_tile;
     // S2_BLUR_IIR_REF: vertical / horizontal work runs, vertical output planes
     std::vector<IirSeg> vsegs, hsegs;
     int vtotal = 0, htotal = 0;
@@ -122,6 +139,13 @@ struct Engine {
     Plan plan_storage;  // a submission's plan, owned by whoever drives this engine
     bool profiling = false;
     cudaEvent_t prof[4] = {nullptr, nullptr, nullptr, nullptr};
+    // host-input submissions: staging for the uploaded planes, the copy
+    // stream, one event per group (its planes have landed) and one for the
+    // staging being free again (the last group's prep has read it)
+    DevBuf stage_d;
+    cudaStream_t copy_st = nullptr;
+    cudaEvent_t grp_copied[kMaxGroups] = {};
+    cudaEvent_t stage_free = nullptr;
 
     size_t esize() const { return storage == ST_F32 ? 4 : 2; }
 
@@ -165,7 +189,12 @@ struct Engine {
         if (done) cudaEventSynchronize(done);
         for (cudaEvent_t &e : prof)
             if (e) cudaEventDestroy(e), e = nullptr;
-        for (DevBuf *b : {&pairs_d, &blk_d, &segs_d, &counter_d, &partials_d, &results_d, &levels_d, &lut_d, &iir_d})
+        if (copy_st) cudaStreamSynchronize(copy_st), cudaStreamDestroy(copy_st), copy_st = nullptr;
+        for (cudaEvent_t &e : grp_copied)
+            if (e) cudaEventDestroy(e), e = nullptr;
+        if (stage_free) cudaEventDestroy(stage_free), stage_free = nullptr;
+        for (DevBuf *b : {&pairs_d, &blk_d, &segs_d, &counter_d, &partials_d, &results_d, &levels_d, &lut_d, &iir_d,
+                          &stage_d})
             if (b->p) cudaFree(b->p), b->p = nullptr, b->n = 0;
         if (pinned) cudaFreeHost(pinned), pinned = nullptr;
         if (results_h) cudaFreeHost(results_h), results_h = nullptr;
@@ -245,7 +274,7 @@ struct Engine {
     }
 
     // Lay out the levels and tiles of n pairs.
-    s2_status plan(const s2_pair_desc *d, int n, Plan &P, const PairExtra *ex = nullptr) {
+    s2_status plan(const s2_pair_desc *d, int n, Plan &P, const PairExtra *ex = nullptr, int ngroups = 1) {
         P = Plan();
         P.pairs.resize(n);
         P.blk_first.resize(n);
@@ -328,6 +357,8 @@ struct Engine {
         P.total_blocks = blk;
         P.level_bytes = lvl_off;
         if (blur == S2_BLUR_IIR_REF) {
+            P.grp_pair = {0, n};
+            P.grp_tile = {0, 0};
             // one partial-sum record per row; vertical work items per column
             // (groups of 32) and plane, horizontal per row and channel
             int rec = 0;
@@ -357,10 +388,24 @@ struct Engine {
             P.total_tiles = rec;
             return S2_OK;
         }
-        // tiles: all pairs' scale 0 first, then scale 1, ... (largest work first)
+        // groups of about equal scale-0 pixels (contiguous pairs)
+        P.grp_pair.assign(1, 0);
+        if (ngroups > 1) {
+            uint64_t total = 0, acc = 0;
+            for (int i = 0; i < n; i++) total += (uint64_t)P.pairs[i].w[0] * P.pairs[i].h[0];
+            for (int i = 0; i + 1 < n && (int)P.grp_pair.size() < ngroups; i++) {
+                acc += (uint64_t)P.pairs[i].w[0] * P.pairs[i].h[0];
+                if (acc * ngroups >= total * P.grp_pair.size()) P.grp_pair.push_back(i + 1);
+            }
+        }
+        P.grp_pair.push_back(n);
+        // tiles, per group: all its pairs' scale 0 first, then scale 1, ...
+        // (largest work first)
         int tile = 0;
-        for (int s = 0; s < kScales; s++) {
-            for (int i = 0; i < n; i++) {
+        P.grp_tile.assign(1, 0);
+        for (size_t g = 0; g + 1 < P.grp_pair.size(); g++) {
+          for (int s = 0; s < kScales; s++) {
+            for (int i = P.grp_pair[g]; i < P.grp_pair[g + 1]; i++) {
                 DevPair &p = P.pairs[i];
                 if (p.status != S2_OK || s >= p.nscales || (ex && !ex[i].score)) continue;
                 Seg sg;
@@ -375,13 +420,52 @@ struct Engine {
                 tile += p.tile_cnt[s];
                 P.segs.push_back(sg);
             }
+          }
+          P.grp_tile.push_back(tile);
         }
         P.total_tiles = tile;
         return S2_OK;
     }
 
-    s2_status enqueue(Plan &P, cudaStream_t st) {
+    // Staging offsets of host-input planes: the images the prep pass reads,
+    // packed rows, 256-byte aligned planes.  Rewrites the pairs' input
+    // pointers to offsets into stage_d (rebased at upload) and returns the
+    // bytes needed.
+    static size_t plan_staging(Plan &P, const s2_pair_desc *d) {
+        size_t off = 0;
+        for (size_t i = 0; i < P.pairs.size(); i++) {
+            DevPair &p = P.pairs[i];
+            if (p.status != S2_OK) continue;
+            const size_t row = s2_row_bytes(d[i]);
+            for (int img = 0; img < 2; img++) {
+                if (!((p.prep_mask >> img) & 1)) continue;
+                p.in[img] = (const void *)off;
+                p.pitch[img] = (long long)row;
+                off += s2_align_up(row * d[i].height, 256);
+                if (d[i].format == S2_FMT_NV12) {
+                    p.in_uv[img] = (const void *)off;
+                    off += s2_align_up(row * (d[i].height / 2), 256);
+                }
+            }
+        }
+        return off;
+    }
+
+    s2_status copy_plane(void *dst, const void *src, size_t pitch, size_t row, size_t rows) {
+        if (pitch == row) S2_CUDA(cudaMemcpyAsync(dst, src, row * rows, cudaMemcpyHostToDevice, copy_st));
+        else S2_CUDA(cudaMemcpy2DAsync(dst, row, src, pitch, row, rows, cudaMemcpyHostToDevice, copy_st));
+        return S2_OK;
+    }
+
+    // Enqueue a planned submission on `st`.  With `host` (the submission's
+    // descriptors, planes in host memory), the planes are uploaded group by
+    // group on the copy stream and each group's prep + fused launches wait
+    // only for their own group's planes, so uploads overlap the compute of
+    // the groups before them.
+    s2_status enqueue(Plan &P, cudaStream_t st, const s2_pair_desc *host = nullptr) {
         const int n = (int)P.pairs.size();
+        const int ng = (int)P.grp_pair.size() - 1;
+        if (ng < 1 || ng > kMaxGroups) return S2_ERR_INVALID_ARG;
         s2_status r;
         if ((r = ensure(levels_d, std::max<size_t>(P.level_bytes, 256))) != S2_OK) return r;
         if ((r = ensure(partials_d, std::max<size_t>((size_t)P.total_tiles * 18 * sizeof(double), 256))) != S2_OK) return r;
@@ -393,6 +477,15 @@ struct Engine {
         if (blur == S2_BLUR_IIR_REF && (r = ensure(iir_d, std::max<size_t>(P.v_bytes, 256))) != S2_OK) return r;
         if ((r = ensure(pairs_d, pb + bb + sb + vsb + hsb)) != S2_OK) return r;
         if ((r = ensure_pinned(pb + bb + sb + vsb + hsb, n)) != S2_OK) return r;
+        if (host) {
+            if ((r = ensure(stage_d, std::max<size_t>(plan_staging(P, host), 256))) != S2_OK) return r;
+            if (!copy_st) {
+                S2_CUDA(cudaStreamCreateWithFlags(&copy_st, cudaStreamNonBlocking));
+                for (cudaEvent_t &e : grp_copied) S2_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+                S2_CUDA(cudaEventCreateWithFlags(&stage_free, cudaEventDisableTiming));
+                S2_CUDA(cudaEventRecord(stage_free, st));
+            }
+        }
         // the previous submission may still read the pinned staging
         if (pending) S2_CUDA(cudaEventSynchronize(done));
         char *h = (char *)pinned;
@@ -404,6 +497,13 @@ struct Engine {
                     if (s >= hp[i].nscales) hp[i].lvl[img][s] = nullptr;
                     else if (!((hp[i].lvl_ext >> img) & 1))
                         hp[i].lvl[img][s] = (char *)levels_d.p + (size_t)hp[i].lvl[img][s];
+            if (host && hp[i].status == S2_OK)
+                for (int img = 0; img < 2; img++)
+                    if ((hp[i].prep_mask >> img) & 1) {
+                        hp[i].in[img] = (const char *)stage_d.p + (size_t)hp[i].in[img];
+                        if (host[i].format == S2_FMT_NV12)
+                            hp[i].in_uv[img] = (const char *)stage_d.p + (size_t)hp[i].in_uv[img];
+                    }
         }
         memcpy(h + pb, P.blk_first.data(), n * sizeof(int));
         if (!P.segs.empty()) memcpy(h + pb + bb, P.segs.data(), P.segs.size() * sizeof(Seg));
@@ -423,18 +523,47 @@ struct Engine {
         const int *dblk = (const int *)(dbase + pb);
         const Seg *dsegs = (const Seg *)(dbase + pb + bb);
         S2_CUDA(cudaMemcpyAsync(dbase, h, pb + bb + sb + vsb + hsb, cudaMemcpyHostToDevice, st));
-        S2_CUDA(cudaMemsetAsync(counter_d.p, 0, sizeof(int), st));
+        S2_CUDA(cudaMemsetAsync(counter_d.p, 0, ng * sizeof(int), st));
+        // uploads wait until the previous host submission's prep has read the staging
+        if (host) S2_CUDA(cudaStreamWaitEvent(copy_st, stage_free, 0));
         if (profiling) S2_CUDA(cudaEventRecord(prof[0], st));
-        S2_CUDA(launch_pyramid(storage, dpairs, n, dblk, P.total_blocks, cc, (const float *)lut_d.p,
-                               num_sms * 8, st));
-        if (profiling) S2_CUDA(cudaEventRecord(prof[1], st));
-        if (blur == S2_BLUR_IIR_REF)
-            S2_CUDA(launch_iir(storage, dpairs, (const IirSeg *)(dbase + pb + bb + sb), (int)P.vsegs.size(), P.vtotal,
-                               (const IirSeg *)(dbase + pb + bb + sb + vsb), (int)P.hsegs.size(), P.htotal,
-                               (double *)partials_d.p, st));
-        else
-            S2_CUDA(launch_fused(storage, dpairs, dsegs, (int)P.segs.size(), P.total_tiles, (int *)counter_d.p,
-                                 (double *)partials_d.p, cc, (const float *)lut_d.p, num_sms * fused_bps, st));
+        for (int g = 0; g < ng; g++) {
+            const int pa = P.grp_pair[g], pe = P.grp_pair[g + 1];
+            if (host) {
+                for (int i = pa; i < pe; i++) {
+                    const DevPair &q = hp[i];
+                    if (q.status != S2_OK) continue;
+                    const size_t row = s2_row_bytes(host[i]);
+                    const size_t hgt = host[i].height;
+                    for (int img = 0; img < 2; img++) {
+                        if (!((q.prep_mask >> img) & 1)) continue;
+                        const void *src = img ? host[i].dis : host[i].ref;
+                        const size_t sp = img ? host[i].dis_pitch : host[i].ref_pitch;
+                        if ((r = copy_plane((void *)q.in[img], src, sp, row, hgt)) != S2_OK) return r;
+                        if (host[i].format == S2_FMT_NV12 &&
+                            (r = copy_plane((void *)q.in_uv[img], img ? host[i].dis_uv : host[i].ref_uv, sp, row,
+                                            hgt / 2)) != S2_OK)
+                            return r;
+                    }
+                }
+                S2_CUDA(cudaEventRecord(grp_copied[g], copy_st));
+                S2_CUDA(cudaStreamWaitEvent(st, grp_copied[g], 0));
+            }
+            const int b0 = pa < n ? P.blk_first[pa] : P.total_blocks;
+            const int b1 = pe < n ? P.blk_first[pe] : P.total_blocks;
+            S2_CUDA(launch_pyramid(storage, dpairs, n, dblk, b0, b1, cc, (const float *)lut_d.p, num_sms * 8, st));
+            if (host && g + 1 == ng) S2_CUDA(cudaEventRecord(stage_free, st));
+            if (profiling && ng == 1) S2_CUDA(cudaEventRecord(prof[1], st));
+            if (blur == S2_BLUR_IIR_REF)
+                S2_CUDA(launch_iir(storage, dpairs, (const IirSeg *)(dbase + pb + bb + sb), (int)P.vsegs.size(),
+                                   P.vtotal, (const IirSeg *)(dbase + pb + bb + sb + vsb), (int)P.hsegs.size(),
+                                   P.htotal, (double *)partials_d.p, st));
+            else
+                S2_CUDA(launch_fused(storage, dpairs, dsegs, (int)P.segs.size(), P.grp_tile[g], P.grp_tile[g + 1],
+                                     (int *)counter_d.p + g, (double *)partials_d.p, num_sms * fused_bps, st));
+        }
+        // several groups interleave prep and fused: the fused slot then holds both
+        if (profiling && ng > 1) S2_CUDA(cudaEventRecord(prof[1], st));
         if (profiling) S2_CUDA(cudaEventRecord(prof[2], st));
         S2_CUDA(launch_finalize(dpairs, n, (const double *)partials_d.p, (DevResult *)results_d.p, st));
         if (profiling) S2_CUDA(cudaEventRecord(prof[3], st));

@@ -177,14 +177,15 @@ __device__ __forceinline__ void prep_quads(const DevPair &P, int X0, int Y0, con
 
 template <typename ST>
 __global__ void __launch_bounds__(256, 3) prep_kernel(const DevPair *__restrict__ pairs, int npairs,
-                                                   const int *__restrict__ blk_first, int total_blocks,
+                                                   const int *__restrict__ blk_first, int first_block,
+                                                   int end_block,
                                                    ColorConsts cc, const float *__restrict__ lut_g) {
     __shared__ float lv1[2][3][kLv1 * kLv1];              // scale-1 linear block [img][ch][px]
     __shared__ float pp[2][2][3][(kLv1 / 2) * (kLv1 / 2)];  // scales >= 2, ping-pong
     __shared__ float lut[256];
     for (int i = threadIdx.x; i < 256; i += blockDim.x) lut[i] = lut_g[i];
     __syncthreads();
-    for (int item = blockIdx.x; item < total_blocks; item += gridDim.x) {
+    for (int item = first_block + blockIdx.x; item < end_block; item += gridDim.x) {
         int lo = 0, hi = npairs - 1;
         while (lo < hi) {
             int mid = (lo + hi + 1) >> 1;
@@ -240,7 +241,7 @@ __global__ void __launch_bounds__(256, 3) prep_kernel(const DevPair *__restrict_
 template <typename ST>
 __global__ void __maxnreg__(96)
     fused_kernel(const DevPair *__restrict__ pairs, const Seg *__restrict__ segs, int nseg,
-                 int total_tiles, int *__restrict__ counter, double *__restrict__ partials) {
+                 int first_tile, int end_tile, int *__restrict__ counter, double *__restrict__ partials) {
     extern __shared__ float sm[];
     // float2 arrays first: kSmVo2 and kSmXo are even, kSmVo1 (27 x 73) is odd
     float2 *s_vo2 = (float2 *)sm;                  // [pair][rb][col]
@@ -258,10 +259,10 @@ __global__ void __maxnreg__(96)
 
     for (;;) {
         __syncthreads();
-        if (tid == 0) s_item = atomicAdd(counter, 1);
+        if (tid == 0) s_item = first_tile + atomicAdd(counter, 1);
         __syncthreads();
         const int item = s_item;
-        if (item >= total_tiles) break;
+        if (item >= end_tile) break;
         const Seg sg = segs[find_seg(segs, nseg, item)];
         const DevPair &P = pairs[sg.pair];
         const int s = sg.scale;
@@ -573,35 +574,34 @@ int fused_blocks_per_sm(int storage) {
     return n > 0 ? n : 1;
 }
 
-cudaError_t launch_pyramid(int storage, const DevPair *pairs, int npairs, const int *blk_first,
-                           int total_blocks, const ColorConsts &cc, const float *lut, int grid,
-                           cudaStream_t st) {
-    if (total_blocks <= 0) return cudaSuccess;
-    grid = grid > total_blocks ? total_blocks : grid;
+cudaError_t launch_pyramid(int storage, const DevPair *pairs, int npairs, const int *blk_first, int first_block,
+                           int end_block, const ColorConsts &cc, const float *lut, int grid, cudaStream_t st) {
+    const int nb = end_block - first_block;
+    if (nb <= 0) return cudaSuccess;
+    grid = grid > nb ? nb : grid;
     if (storage == ST_F16)
-        prep_kernel<__half><<<grid, 256, 0, st>>>(pairs, npairs, blk_first, total_blocks, cc, lut);
+        prep_kernel<__half><<<grid, 256, 0, st>>>(pairs, npairs, blk_first, first_block, end_block, cc, lut);
     else if (storage == ST_BF16)
-        prep_kernel<__nv_bfloat16><<<grid, 256, 0, st>>>(pairs, npairs, blk_first, total_blocks, cc, lut);
+        prep_kernel<__nv_bfloat16><<<grid, 256, 0, st>>>(pairs, npairs, blk_first, first_block, end_block, cc, lut);
     else
-        prep_kernel<float><<<grid, 256, 0, st>>>(pairs, npairs, blk_first, total_blocks, cc, lut);
+        prep_kernel<float><<<grid, 256, 0, st>>>(pairs, npairs, blk_first, first_block, end_block, cc, lut);
     return cudaGetLastError();
 }
 
-cudaError_t launch_fused(int storage, const DevPair *pairs, const Seg *segs, int nseg, int total_tiles,
-                         int *counter, double *partials, const ColorConsts &cc, const float *lut,
-                         int grid, cudaStream_t st) {
-    (void)cc;
-    (void)lut;
-    if (total_tiles <= 0) return cudaSuccess;
-    grid = grid > total_tiles ? total_tiles : grid;
+cudaError_t launch_fused(int storage, const DevPair *pairs, const Seg *segs, int nseg, int first_tile, int end_tile,
+                         int *counter, double *partials, int grid, cudaStream_t st) {
+    const int nt = end_tile - first_tile;
+    if (nt <= 0) return cudaSuccess;
+    grid = grid > nt ? nt : grid;
     dim3 block(kCols, 3);
     size_t sm = fused_smem_bytes();
     if (storage == ST_F16)
-        fused_kernel<__half><<<grid, block, sm, st>>>(pairs, segs, nseg, total_tiles, counter, partials);
+        fused_kernel<__half><<<grid, block, sm, st>>>(pairs, segs, nseg, first_tile, end_tile, counter, partials);
     else if (storage == ST_BF16)
-        fused_kernel<__nv_bfloat16><<<grid, block, sm, st>>>(pairs, segs, nseg, total_tiles, counter, partials);
+        fused_kernel<__nv_bfloat16><<<grid, block, sm, st>>>(pairs, segs, nseg, first_tile, end_tile, counter,
+                                                             partials);
     else
-        fused_kernel<float><<<grid, block, sm, st>>>(pairs, segs, nseg, total_tiles, counter, partials);
+        fused_kernel<float><<<grid, block, sm, st>>>(pairs, segs, nseg, first_tile, end_tile, counter, partials);
     return cudaGetLastError();
 }
 

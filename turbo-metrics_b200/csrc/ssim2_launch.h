@@ -10,12 +10,13 @@ cudaError_t upload_weights();
 cudaError_t configure_kernels();
 size_t fused_smem_bytes();
 int fused_blocks_per_sm(int storage);
-cudaError_t launch_pyramid(int storage, const DevPair *pairs, int npairs, const int *blk_first,
-                           int total_blocks, const ColorConsts &cc, const float *lut, int grid,
-                           cudaStream_t st);
-cudaError_t launch_fused(int storage, const DevPair *pairs, const Seg *segs, int nseg, int total_tiles,
-                         int *counter, double *partials, const ColorConsts &cc, const float *lut,
-                         int grid, cudaStream_t st);
+// prep over the pyramid blocks [first_block, end_block) (absolute numbering
+// of blk_first), fused over the tiles [first_tile, end_tile) with its own
+// zeroed work counter.
+cudaError_t launch_pyramid(int storage, const DevPair *pairs, int npairs, const int *blk_first, int first_block,
+                           int end_block, const ColorConsts &cc, const float *lut, int grid, cudaStream_t st);
+cudaError_t launch_fused(int storage, const DevPair *pairs, const Seg *segs, int nseg, int first_tile, int end_tile,
+                         int *counter, double *partials, int grid, cudaStream_t st);
 cudaError_t launch_iir(int storage, const DevPair *pairs, const IirSeg *vsegs, int nvseg, int vtotal,
                        const IirSeg *hsegs, int nhseg, int htotal, double *partials, cudaStream_t st);
 cudaError_t launch_finalize(const DevPair *pairs, int npairs, const double *partials, DevResult *out,

@@ -167,10 +167,10 @@ extern "C" s2_status s2_compute_srgb8_noalloc(const uint8_t *ref, size_t ref_pit
     int sms = 148, bps = fused_blocks_per_sm(ST_F32), dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (launch_pyramid(ST_F32, dp, 1, (const int *)(base + off_blk), P.blk_x * P.blk_y, cc, lut, sms * 8, cs) !=
+    if (launch_pyramid(ST_F32, dp, 1, (const int *)(base + off_blk), 0, P.blk_x * P.blk_y, cc, lut, sms * 8, cs) !=
             cudaSuccess ||
-        launch_fused(ST_F32, dp, (const Seg *)(base + off_seg), nseg, tiles, (int *)(base + kOffCounter),
-                     (double *)(base + off_part), cc, lut, sms * bps, cs) != cudaSuccess ||
+        launch_fused(ST_F32, dp, (const Seg *)(base + off_seg), nseg, 0, tiles, (int *)(base + kOffCounter),
+                     (double *)(base + off_part), sms * bps, cs) != cudaSuccess ||
         launch_finalize(dp, 1, (const double *)(base + off_part), (DevResult *)out_device, cs) != cudaSuccess)
         return fail("kernel launch");
     return S2_OK;

@@ -47,6 +47,22 @@ def _dev(img, elem_bytes):
     return ctypes.c_void_p(img.data_ptr()), img.stride(0) * elem_bytes
 
 
+def _host_ptr(img, elem_bytes):
+    """(pointer, pitch in bytes) of a host image: a CPU torch tensor (pinned
+    for asynchronous uploads) or a numpy array with packed rows."""
+    if isinstance(img, tuple):
+        return ctypes.c_void_p(img[0]), img[1]
+    if isinstance(img, np.ndarray):
+        if img.strides[-1] != img.itemsize or (img.ndim == 3 and img.strides[1] != img.shape[2] * img.itemsize):
+            raise capi.S2Error(capi.S2_ERR_INVALID_ARG, "rows must be packed samples")
+        return ctypes.c_void_p(img.ctypes.data), img.strides[0]
+    if img.is_cuda:
+        raise capi.S2Error(capi.S2_ERR_INVALID_ARG, "expected a host (CPU) tensor")
+    if img.stride(-1) != 1 or (img.dim() == 3 and img.stride(1) != img.shape[2]):
+        raise capi.S2Error(capi.S2_ERR_INVALID_ARG, "rows must be packed samples")
+    return ctypes.c_void_p(img.data_ptr()), img.stride(0) * elem_bytes
+
+
 def _host(img):
     a = np.ascontiguousarray(img)
     return a.ctypes.data_as(ctypes.c_void_p), a.strides[0], a
@@ -224,24 +240,26 @@ class Ssimulacra2:
 
 
 class PairDesc:
-    """One pair of a batch: device tensors of any supported format."""
+    """One pair of a batch: device tensors of any supported format (host arrays
+    for `Ssim2Batch.submit_host`)."""
 
     def __init__(self, ref, dis, fmt="srgb8", ref_uv=None, dis_uv=None, bits=10):
         self.ref, self.dis, self.fmt, self.ref_uv, self.dis_uv, self.bits = ref, dis, fmt, ref_uv, dis_uv, bits
 
-    def to_c(self):
+    def to_c(self, host=False):
         d = capi.PairDescC()
         eb = {"linear_f32": 4, "srgb8": 1, "nv12": 1, "rgb16": 2}[self.fmt]
-        rp, rpitch = _dev(self.ref, eb)
-        dp, dpitch = _dev(self.dis, eb)
+        ptr = _host_ptr if host else _dev
+        rp, rpitch = ptr(self.ref, eb)
+        dp, dpitch = ptr(self.dis, eb)
         d.height, d.width = self.ref.shape[0], self.ref.shape[1]
         d.format = capi.FMT[self.fmt]
         d.bits = self.bits
         d.ref, d.dis = rp.value, dp.value
         d.ref_pitch, d.dis_pitch = rpitch, dpitch
         if self.fmt == "nv12":
-            d.ref_uv = _dev(self.ref_uv, 1)[0].value
-            d.dis_uv = _dev(self.dis_uv, 1)[0].value
+            d.ref_uv = ptr(self.ref_uv, 1)[0].value
+            d.dis_uv = ptr(self.dis_uv, 1)[0].value
         return d
 
 
@@ -274,6 +292,18 @@ class Ssim2Batch:
             arr[i] = p.to_c()
         self._keep = pairs
         check(lib.s2_batch_submit(self._h, arr, len(pairs), _stream_ptr(stream)), "compute_batch")
+        self._n = len(pairs)
+
+    def submit_host(self, pairs, stream=None):
+        """Pairs whose planes are in host memory (CPU tensors, pinned for
+        overlap, or numpy arrays): uploaded in groups that overlap the compute
+        of earlier groups.  Keep the arrays alive and unchanged until
+        `results()` returns."""
+        arr = (capi.PairDescC * max(len(pairs), 1))()
+        for i, p in enumerate(pairs):
+            arr[i] = p.to_c(host=True)
+        self._keep = pairs
+        check(lib.s2_batch_submit_host(self._h, arr, len(pairs), _stream_ptr(stream)), "compute_batch_host")
         self._n = len(pairs)
 
     def results(self):
