@@ -140,12 +140,15 @@ struct Engine {
     bool profiling = false;
     cudaEvent_t prof[4] = {nullptr, nullptr, nullptr, nullptr};
     // host-input submissions: staging for the uploaded planes, the copy
-    // stream, one event per group (its planes have landed) and one for the
-    // staging being free again (the last group's prep has read it)
+    // stream and the prep stream (a group's prep runs beside the previous
+    // group's tile launch, filling the SMs its last wave leaves idle), one
+    // event per group for its planes having landed and one for its prep being
+    // done, the submission's start, and the staging being free again (the
+    // last group's prep has read it)
     DevBuf stage_d;
-    cudaStream_t copy_st = nullptr;
-    cudaEvent_t grp_copied[kMaxGroups] = {};
-    cudaEvent_t stage_free = nullptr;
+    cudaStream_t copy_st = nullptr, prep_st = nullptr;
+    cudaEvent_t grp_copied[kMaxGroups] = {}, grp_prepped[kMaxGroups] = {};
+    cudaEvent_t sub_start = nullptr, stage_free = nullptr;
 
     size_t esize() const { return storage == ST_F32 ? 4 : 2; }
 
@@ -190,8 +193,12 @@ struct Engine {
         for (cudaEvent_t &e : prof)
             if (e) cudaEventDestroy(e), e = nullptr;
         if (copy_st) cudaStreamSynchronize(copy_st), cudaStreamDestroy(copy_st), copy_st = nullptr;
+        if (prep_st) cudaStreamSynchronize(prep_st), cudaStreamDestroy(prep_st), prep_st = nullptr;
         for (cudaEvent_t &e : grp_copied)
             if (e) cudaEventDestroy(e), e = nullptr;
+        for (cudaEvent_t &e : grp_prepped)
+            if (e) cudaEventDestroy(e), e = nullptr;
+        if (sub_start) cudaEventDestroy(sub_start), sub_start = nullptr;
         if (stage_free) cudaEventDestroy(stage_free), stage_free = nullptr;
         for (DevBuf *b : {&pairs_d, &blk_d, &segs_d, &counter_d, &partials_d, &results_d, &levels_d, &lut_d, &iir_d,
                           &stage_d})
@@ -388,14 +395,17 @@ struct Engine {
             P.total_tiles = rec;
             return S2_OK;
         }
-        // groups of about equal scale-0 pixels (contiguous pairs)
+        // groups of contiguous pairs, about equal scale-0 pixels except the
+        // first, which gets half a share (its upload is the one that nothing
+        // overlaps): group g ends where the running pixel count reaches
+        // (g + 1/2) / (ngroups - 1/2) of the total
         P.grp_pair.assign(1, 0);
         if (ngroups > 1) {
             uint64_t total = 0, acc = 0;
             for (int i = 0; i < n; i++) total += (uint64_t)P.pairs[i].w[0] * P.pairs[i].h[0];
             for (int i = 0; i + 1 < n && (int)P.grp_pair.size() < ngroups; i++) {
                 acc += (uint64_t)P.pairs[i].w[0] * P.pairs[i].h[0];
-                if (acc * ngroups >= total * P.grp_pair.size()) P.grp_pair.push_back(i + 1);
+                if (acc * (2 * ngroups - 1) >= total * (2 * P.grp_pair.size() - 1)) P.grp_pair.push_back(i + 1);
             }
         }
         P.grp_pair.push_back(n);
@@ -481,7 +491,10 @@ struct Engine {
             if ((r = ensure(stage_d, std::max<size_t>(plan_staging(P, host), 256))) != S2_OK) return r;
             if (!copy_st) {
                 S2_CUDA(cudaStreamCreateWithFlags(&copy_st, cudaStreamNonBlocking));
+                S2_CUDA(cudaStreamCreateWithFlags(&prep_st, cudaStreamNonBlocking));
                 for (cudaEvent_t &e : grp_copied) S2_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+                for (cudaEvent_t &e : grp_prepped) S2_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+                S2_CUDA(cudaEventCreateWithFlags(&sub_start, cudaEventDisableTiming));
                 S2_CUDA(cudaEventCreateWithFlags(&stage_free, cudaEventDisableTiming));
                 S2_CUDA(cudaEventRecord(stage_free, st));
             }
@@ -524,9 +537,16 @@ struct Engine {
         const Seg *dsegs = (const Seg *)(dbase + pb + bb);
         S2_CUDA(cudaMemcpyAsync(dbase, h, pb + bb + sb + vsb + hsb, cudaMemcpyHostToDevice, st));
         S2_CUDA(cudaMemsetAsync(counter_d.p, 0, ng * sizeof(int), st));
-        // uploads wait until the previous host submission's prep has read the staging
-        if (host) S2_CUDA(cudaStreamWaitEvent(copy_st, stage_free, 0));
         if (profiling) S2_CUDA(cudaEventRecord(prof[0], st));
+        // uploads wait until the previous host submission's prep has read the
+        // staging; preps wait for this submission's descriptors
+        const bool split = host && blur != S2_BLUR_IIR_REF;
+        if (host) S2_CUDA(cudaStreamWaitEvent(copy_st, stage_free, 0));
+        if (split) {
+            S2_CUDA(cudaEventRecord(sub_start, st));
+            S2_CUDA(cudaStreamWaitEvent(prep_st, sub_start, 0));
+        }
+        cudaStream_t pst = split ? prep_st : st;
         for (int g = 0; g < ng; g++) {
             const int pa = P.grp_pair[g], pe = P.grp_pair[g + 1];
             if (host) {
@@ -547,12 +567,16 @@ struct Engine {
                     }
                 }
                 S2_CUDA(cudaEventRecord(grp_copied[g], copy_st));
-                S2_CUDA(cudaStreamWaitEvent(st, grp_copied[g], 0));
+                S2_CUDA(cudaStreamWaitEvent(pst, grp_copied[g], 0));
             }
             const int b0 = pa < n ? P.blk_first[pa] : P.total_blocks;
             const int b1 = pe < n ? P.blk_first[pe] : P.total_blocks;
-            S2_CUDA(launch_pyramid(storage, dpairs, n, dblk, b0, b1, cc, (const float *)lut_d.p, num_sms * 8, st));
-            if (host && g + 1 == ng) S2_CUDA(cudaEventRecord(stage_free, st));
+            S2_CUDA(launch_pyramid(storage, dpairs, n, dblk, b0, b1, cc, (const float *)lut_d.p, num_sms * 8, pst));
+            if (host && g + 1 == ng) S2_CUDA(cudaEventRecord(stage_free, pst));
+            if (split) {
+                S2_CUDA(cudaEventRecord(grp_prepped[g], prep_st));
+                S2_CUDA(cudaStreamWaitEvent(st, grp_prepped[g], 0));
+            }
             if (profiling && ng == 1) S2_CUDA(cudaEventRecord(prof[1], st));
             if (blur == S2_BLUR_IIR_REF)
                 S2_CUDA(launch_iir(storage, dpairs, (const IirSeg *)(dbase + pb + bb + sb), (int)P.vsegs.size(),
