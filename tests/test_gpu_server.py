@@ -66,8 +66,8 @@ def tmb_num_scales(w, h):
     return conftest.load_package().num_scales(w, h)
 
 
-def workspace(tmb):
-    probe = tmb.Ssim2Server(**SMALL)
+def workspace(tmb, **cfg):
+    probe = tmb.Ssim2Server(**(cfg or SMALL))
     ws = probe.stats()["hbm_in_use"]
     probe.close()
     return ws
@@ -88,17 +88,20 @@ def test_server_budget_admits_in_order(tmb, cuda):
 
 
 def test_server_cancel_and_timeout(tmb, cuda):
-    ref, cands = job_images(1280, 720, synth.pair_seed(4, 4), 5)
-    sv = tmb.Ssim2Server(hbm_budget=workspace(tmb) + job_bytes(1280, 720, 5) * 3 // 2, max_batch_pairs=2,
-                         max_batch_pixels=1 << 21)
+    # 1440p jobs, admitted one at a time by the budget: the second job cannot
+    # have finished right after the third is submitted (the first one's
+    # uploads alone take longer than the calls in between)
+    ref, cands = job_images(2560, 1440, synth.pair_seed(4, 4), 5)
+    cfg = dict(max_batch_pairs=2, max_batch_pixels=1 << 22)
+    sv = tmb.Ssim2Server(hbm_budget=workspace(tmb, **cfg) + job_bytes(2560, 1440, 5) * 3 // 2, **cfg)
     ids = [sv.submit(ref, cands) for _ in range(3)]
+    with pytest.raises(tmb.S2Error) as e:
+        sv.wait(ids[1], timeout_ms=0)
+    assert e.value.status in (6,)  # S2_ERR_TIMEOUT (not done yet)
     sv.cancel(ids[2])  # still queued behind the budget
     with pytest.raises(tmb.S2Error) as e:
         sv.wait(ids[2])
     assert e.value.status == 10  # S2_ERR_CANCELLED
-    with pytest.raises(tmb.S2Error) as e:
-        sv.wait(ids[1], timeout_ms=0)
-    assert e.value.status in (6,)  # S2_ERR_TIMEOUT (not done yet)
     a, _, _ = sv.wait(ids[0])
     b, _, _ = sv.wait(ids[1])
     assert np.array_equal(a, b)

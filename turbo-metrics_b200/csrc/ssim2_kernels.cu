@@ -419,6 +419,42 @@ __global__ void __maxnreg__(96)
                             }
                         }
                         float fs[3] = {0.f, 0.f, 0.f}, f4[3] = {0.f, 0.f, 0.f};
+                        const int xc = x0 + c0;
+                        if (bv == 1.0f && xc >= 4 && xc + kChunk + 4 <= W) {
+                            // every pixel of the chunk is interior: border gain
+                            // 1, so the correction term kk of the general form
+                            // below is zero and drops out; all pixels inside
+                            // the image.  The (mu1, mu2) and (art, det) pairs
+                            // go through f32x2 operations (each lane rounds as
+                            // the scalar operation).
+                            float2 fs12 = make_float2(0.f, 0.f), f412 = make_float2(0.f, 0.f);
+#pragma unroll
+                            for (int j = 0; j < kChunk; j++) {
+                                const float2 mu = ma[j];
+                                const float2 nmu = make_float2(-mu.x, -mu.y);
+                                const float2 var = __ffma2_rn(nmu, mu, mb[j]);  // (sigma11 - mu1^2, sigma22 - mu2^2)
+                                const float cov = fmaf(nmu.x, mu.y, mc[j]);
+                                const float md = mu.x - mu.y;
+                                const float num_m = fmaf(-md, md, 1.0f);
+                                const float num_s = fmaf(2.0f, cov, kC2);
+                                const float den = (var.x + var.y) + kC2;
+                                const float d = fmaxf(s2_div(fmaf(-num_m, num_s, den), den), 0.0f);
+                                const float2 t = __fadd2_rn(xyv[j], nmu);
+                                const float aa = fabsf(t.x), bb = fabsf(t.y);
+                                const float d1 = s2_div(bb - aa, 1.0f + aa);
+                                const float2 ad = make_float2(fmaxf(d1, 0.0f), fmaxf(-d1, 0.0f));
+                                const float q = d * d;
+                                fs[0] += d;
+                                f4[0] += q * q;
+                                const float2 q2 = __fmul2_rn(ad, ad);
+                                fs12 = __fadd2_rn(fs12, ad);
+                                f412 = __fadd2_rn(f412, __fmul2_rn(q2, q2));
+                            }
+                            fs[1] = fs12.x;
+                            fs[2] = fs12.y;
+                            f4[1] = f412.x;
+                            f4[2] = f412.y;
+                        } else {
 #pragma unroll
                         for (int j = 0; j < kChunk; j++) {
                             const int xx = x0 + c0 + j;
@@ -448,6 +484,7 @@ __global__ void __maxnreg__(96)
                                 fs[1] += art; q = art * art; f4[1] += q * q;
                                 fs[2] += det; q = det * det; f4[2] += q * q;
                             }
+                        }
                         }
 #pragma unroll
                         for (int m = 0; m < 3; m++) {
