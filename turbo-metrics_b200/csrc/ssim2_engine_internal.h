@@ -273,10 +273,11 @@ struct Engine {
 
     int choose_strip_rows(const std::vector<uint64_t> &tiles_at) const {
         if (strip_rows_cfg == 9 || strip_rows_cfg == 21 || strip_rows_cfg == 63) return strip_rows_cfg;
-        // largest strip height that still gives ~4 waves of resident tiles
+        // largest strip height that still gives ~4 waves of resident work
+        // items (three per tile: one per channel)
         const uint64_t resident = (uint64_t)num_sms * (uint64_t)fused_bps;
-        if (tiles_at[0] >= 4 * resident) return 63;
-        if (tiles_at[1] >= 4 * resident) return 21;
+        if (3 * tiles_at[0] >= 4 * resident) return 63;
+        if (3 * tiles_at[1] >= 4 * resident) return 21;
         return 9;
     }
 

@@ -29,15 +29,15 @@
 
 namespace s2 {
 
-// Shared memory layout of fused_kernel.  Rows ("rb" = output row of the
-// block x channel, 27 of them) of the float2 arrays are kRowStride2 float2
-// apart and rows of the float array kRowStride1 floats apart.  The horizontal
-// tasks read them with 16-byte loads, lane t taking block row t % 27 and
-// segment t / 27: with kRowStride2 / 2 and kRowStride1 / 4 odd, the eight
-// lanes of each load phase fall in distinct 16-byte bank groups (at most
-// 2-way where a warp spans two segments).  The plain 64-element stride gave
-// up to 10-way conflicts.
-constexpr int kRB = kRowsPerBlk * 3;                     // rows of one block
+// Shared memory layout of fused_kernel (one CTA = one channel of a tile).
+// Rows ("rb" = output row of the 9-row block) of the float2 arrays are
+// kRowStride2 float2 apart and rows of the float array kRowStride1 floats
+// apart.  The horizontal tasks read them with 16-byte loads, lane t taking
+// block row t % 9 and segment t / 9: with kRowStride2 / 2 and
+// kRowStride1 / 4 odd, consecutive rows fall in distinct 16-byte bank groups
+// (at most 2-way where a load phase spans two segments).  The plain
+// 64-element stride gave up to 10-way conflicts.
+constexpr int kRB = kRowsPerBlk;                         // rows of one block
 constexpr int kRowStride2 = 74;                          // float2 elements
 constexpr int kRowStride1 = 76;                          // float elements
 static_assert(kRowStride2 % 2 == 0 && (kRowStride2 / 2) % 2 == 1, "16-byte aligned rows, odd 16-byte stride");
@@ -46,7 +46,7 @@ constexpr int kSmVo2 = 2 * kRB * kRowStride2 * 2;        // vertical FIR of (x,y
 constexpr int kSmXo = kRB * kRowStride2 * 2;             // shifted raw XYB (x', y') of the output rows [rb][col]
 constexpr int kSmVo1 = kRB * kRowStride1;                // vertical FIR of xy [rb][col]
 constexpr int kFusedSmemFloats = kSmVo2 + kSmXo + kSmVo1;
-constexpr int kFusedThreads = kCols * 3;
+constexpr int kFusedThreads = kCols;
 constexpr int kTasks = kRB * kSegs;                      // horizontal tasks per 9-row block
 static_assert(kSmVo2 % 4 == 0 && kSmXo % 4 == 0, "arrays start 16-byte aligned");
 
@@ -238,36 +238,41 @@ __global__ void __launch_bounds__(256, 3) prep_kernel(const DevPair *__restrict_
 // ---------------------------------------------------------------------------
 // fused per-scale tile pass
 // ---------------------------------------------------------------------------
+//
+// Work item = (tile, channel): item = 3 * tile + channel, 64 threads (two
+// warps) per CTA, so that a block barrier waits for two warps only and up to
+// ten CTAs share an SM.  A tile's three items write the tile's 18 partial
+// sums (channel-major) and are summed in the same order as one CTA per tile
+// over all channels would.
 template <typename ST>
 __global__ void __maxnreg__(96)
     fused_kernel(const DevPair *__restrict__ pairs, const Seg *__restrict__ segs, int nseg,
-                 int first_tile, int end_tile, int *__restrict__ counter, double *__restrict__ partials) {
+                 int first_item, int end_item, int *__restrict__ counter, double *__restrict__ partials) {
     extern __shared__ float sm[];
-    // float2 arrays first: kSmVo2 and kSmXo are even, kSmVo1 (27 x 73) is odd
     float2 *s_vo2 = (float2 *)sm;                  // [pair][rb][col]
     float2 *s_xo = (float2 *)(sm + kSmVo2);        // [rb][col]
     float *s_vo1 = sm + kSmVo2 + kSmXo;            // [rb][col]
     __shared__ int s_item;
     __shared__ double s_red[kFusedThreads][6];
 
-    const int col = threadIdx.x, g = threadIdx.y;
-    const int tid = g * kCols + col;
-    // horizontal task of this thread: segment-major over the 27 block rows
-    const int t_rb = tid % kRB, t_s = tid / kRB;
-    const int t_r = t_rb / 3, t_g = t_rb % 3;
+    const int col = threadIdx.x;
+    const int tid = col;
+    // horizontal task of this thread: segment-major over the 9 block rows
+    const int t_r = tid % kRB, t_s = tid / kRB;
     const bool t_on = tid < kTasks;
 
     for (;;) {
         __syncthreads();
-        if (tid == 0) s_item = first_tile + atomicAdd(counter, 1);
+        if (tid == 0) s_item = first_item + atomicAdd(counter, 1);
         __syncthreads();
         const int item = s_item;
-        if (item >= end_tile) break;
-        const Seg sg = segs[find_seg(segs, nseg, item)];
+        if (item >= end_item) break;
+        const int tile = item / 3, g = item - 3 * tile;
+        const Seg sg = segs[find_seg(segs, nseg, tile)];
         const DevPair &P = pairs[sg.pair];
         const int s = sg.scale;
         const int W = P.w[s], H = P.h[s];
-        const int local = item - sg.first_tile;
+        const int local = tile - sg.first_tile;
         const int tx = local % sg.tiles_x, ty = local / sg.tiles_x;
         const int x0 = tx * kTileW, y0 = ty * sg.strip_rows;
         const int y1 = min(y0 + sg.strip_rows, H);
@@ -339,7 +344,7 @@ __global__ void __maxnreg__(96)
                                              S2_W(w2b, 5), S2_W(w2b, 6), S2_W(w2b, 7), S2_W(w2b, 8));
                     const float vc = fir9(S2_W(w1, 0), S2_W(w1, 1), S2_W(w1, 2), S2_W(w1, 3), S2_W(w1, 4),
                                           S2_W(w1, 5), S2_W(w1, 6), S2_W(w1, 7), S2_W(w1, 8));
-                    const int rb = k * 3 + g;
+                    const int rb = k;
                     s_vo2[rb * kRowStride2 + col] = va;
                     s_vo2[(kRB + rb) * kRowStride2 + col] = vb;
                     s_vo1[rb * kRowStride1 + col] = vc;
@@ -353,13 +358,13 @@ __global__ void __maxnreg__(96)
                 const int y = y0 + r0 + t_r;
                 const int xs = t_s * kSegW;
                 if (x0 + xs < W) {
-                    const int rb = t_rb;
+                    const int rb = t_r;
                     const float2 *pa = s_vo2 + rb * kRowStride2;
                     const float2 *pb = s_vo2 + (kRB + rb) * kRowStride2;
                     const float *pc = s_vo1 + rb * kRowStride1;
                     const float2 *px = s_xo + rb * kRowStride2;
                     // shift of the task's channel (same anchor as the vertical pass)
-                    const float cv = ld_store<ST>((const ST *)P.lvl[0][s] + t_g * plane +
+                    const float cv = ld_store<ST>((const ST *)P.lvl[0][s] + g * plane +
                                                   (long long)((y0 / kBand) * kBand) * lp + x0);
                     const float bv = border_gain(y, H);
 #pragma unroll 1
@@ -497,14 +502,12 @@ __global__ void __maxnreg__(96)
             __syncthreads();
         }
 
-        // tile reduction, fixed order: sum the tasks of each channel
+        // channel reduction, fixed order: the tasks segment-major
         __syncthreads();
-        if (tid < 18) {
-            const int rg = tid / 6, m = tid % 6;
+        if (tid < 6) {
             double v = 0.0;
-            for (int t = 0; t < kTasks; t++)
-                if ((t % kRB) % 3 == rg) v += s_red[t][m];
-            partials[(long long)item * 18 + tid] = v;
+            for (int t = 0; t < kTasks; t++) v += s_red[t][tid];
+            partials[(long long)item * 6 + tid] = v;  // = tile * 18 + channel * 6 + m
         }
     }
 }
@@ -627,18 +630,18 @@ cudaError_t launch_pyramid(int storage, const DevPair *pairs, int npairs, const 
 
 cudaError_t launch_fused(int storage, const DevPair *pairs, const Seg *segs, int nseg, int first_tile, int end_tile,
                          int *counter, double *partials, int grid, cudaStream_t st) {
-    const int nt = end_tile - first_tile;
+    const int fi = 3 * first_tile, ei = 3 * end_tile;  // work items: (tile, channel)
+    const int nt = ei - fi;
     if (nt <= 0) return cudaSuccess;
     grid = grid > nt ? nt : grid;
-    dim3 block(kCols, 3);
+    dim3 block(kFusedThreads);
     size_t sm = fused_smem_bytes();
     if (storage == ST_F16)
-        fused_kernel<__half><<<grid, block, sm, st>>>(pairs, segs, nseg, first_tile, end_tile, counter, partials);
+        fused_kernel<__half><<<grid, block, sm, st>>>(pairs, segs, nseg, fi, ei, counter, partials);
     else if (storage == ST_BF16)
-        fused_kernel<__nv_bfloat16><<<grid, block, sm, st>>>(pairs, segs, nseg, first_tile, end_tile, counter,
-                                                             partials);
+        fused_kernel<__nv_bfloat16><<<grid, block, sm, st>>>(pairs, segs, nseg, fi, ei, counter, partials);
     else
-        fused_kernel<float><<<grid, block, sm, st>>>(pairs, segs, nseg, first_tile, end_tile, counter, partials);
+        fused_kernel<float><<<grid, block, sm, st>>>(pairs, segs, nseg, fi, ei, counter, partials);
     return cudaGetLastError();
 }
 
