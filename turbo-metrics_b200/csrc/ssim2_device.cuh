@@ -125,6 +125,26 @@ __device__ __forceinline__ float s2_cbrtf(float x) {
     return pos ? y : 0.0f;
 }
 
+// s2_cbrtf for x in [2^-100, 2^100] (the opsin values of non-negative
+// linear RGB, which are >= the bias 0.0038): the same operations without the
+// scaling of tiny and the zero of non-positive arguments, so the same result.
+__device__ __forceinline__ float s2_cbrtf_unit(float x) {
+    float r = __uint_as_float(0x54a2fa8cu - __float_as_uint(x) / 3u);
+    const float third = 0x1.555556p-2f;
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+        float t = x * r;
+        t = t * r;
+        t = t * r;
+        r = fmaf(r * third, 1.0f - t, r);
+    }
+    float y = x * r;
+    y = y * r;
+    const float e = fmaf(y * y, y, -x);
+    const float c = (r * r) * third;
+    return fmaf(-e, c, y);
+}
+
 // a / b for b > 0 normal (the error-map denominators: >= 9e-4 and >= 1).
 // The reciprocal comes from the SFU approximation (PTX rcp.approx.ftz.f32,
 // at most 1 ulp from 1/b); the quotient q = a r then gets one residual
@@ -176,6 +196,29 @@ __device__ __forceinline__ float s2_pow_20_9(float p) {
     return pos ? y : 0.0f;
 }
 
+// s2_pow_20_9 for p in [1/8, 2): there the exponent e is -3..0 and the
+// product of 2^(r/9) and 2^(2e + k) is one f32 constant 2^(20e/9) (a power
+// of two times the rounded 2^(r/9), so multiplying by it rounds exactly as
+// the two multiplications do): the same result from 4 selects instead of
+// the exponent arithmetic.
+__device__ __forceinline__ float s2_pow_20_9_unit(float p) {
+    const unsigned b = __float_as_uint(p);
+    const int e = (int)(b >> 23) - 127;
+    const float t = __uint_as_float((b & 0x7fffffu) | 0x3f800000u) - 1.5f;
+    float y = 0x1.1eb37ap-12f;
+    y = fmaf(y, t, -0x1.88e318p-11f);
+    y = fmaf(y, t, 0x1.2713a6p-9f);
+    y = fmaf(y, t, -0x1.37717ep-7f);
+    y = fmaf(y, t, 0x1.2c9724p-4f);
+    y = fmaf(y, t, 0x1.7c6f02p+0f);
+    y = fmaf(y, t, 0x1.d2e55cp+1f);
+    y = fmaf(y, t, 0x1.3b279ep+1f);
+    const float s = e == 0 ? 1.0f : (e == -1 ? 0x1.b6e8aep-3f : (e == -2 ? 0x1.784086p-5f : 0x1.428a3p-7f));
+    return y * s;
+}
+
+// KUNIT: the argument is known >= 0.0038 (non-negative linear RGB).
+template <bool KUNIT>
 __device__ __forceinline__ float opsin_row(int g, float r, float gg, float b) {
     const float m01 = 1.0f - S2_M02 - S2_M00;
     const float m11 = 1.0f - S2_M12 - S2_M10;
@@ -187,6 +230,7 @@ __device__ __forceinline__ float opsin_row(int g, float r, float gg, float b) {
         v = fmaf(S2_M10, r, fmaf(m11, gg, fmaf(S2_M12, b, S2_B0)));
     else
         v = fmaf(S2_M20, r, fmaf(S2_M21, gg, fmaf(m22, b, S2_B0)));
+    if (KUNIT) return s2_cbrtf_unit(v) - S2_B0_ROOT;
     return s2_cbrtf(fmaxf(v, 0.0f)) - S2_B0_ROOT;
 }
 
@@ -202,11 +246,14 @@ __device__ __forceinline__ float xyb_from_opsin(int g, float rg, float gr, float
 // ((v + (alpha - 1)) / alpha)^(1/0.45) above the threshold, v / 4.5 below.
 // The two divisions are multiplications by the f32 reciprocals 1/alpha and
 // 2/9 (<= 1 ulp from dividing); both branches are evaluated and selected.
+// The power's base is clamped to [1/8, 1.5]: the selected branch has
+// base >= 0.164, and a base above 1.5 (v > 1.55, possible only for NV12,
+// whose caller clamps the result to 1) gives a result above 1 either way.
 __device__ __forceinline__ float bt709_eotf(float v) {
     const float alpha_m1 = 0x1.96b84p-4f;    // alpha - 1, alpha = 1 + 5.5 * 0.018053968510807
     const float inv_alpha = 0x1.d1c096p-1f;  // 1 / alpha in f32
     const float thr = 0.08124285829863521110029445797874f;
-    const float hi = s2_pow_20_9((v + alpha_m1) * inv_alpha);
+    const float hi = s2_pow_20_9_unit(fminf(fmaxf((v + alpha_m1) * inv_alpha, 0.125f), 1.5f));
     const float lo = v * 0x1.c71c72p-3f;     // v / 4.5
     return v >= thr ? hi : lo;
 }

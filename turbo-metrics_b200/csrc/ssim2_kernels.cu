@@ -2,26 +2,27 @@
 //
 // One pair (or a batch of pairs of any sizes) is scored by three launches:
 //
-//   pyramid_kernel   reads each pair's scale-0 input once (any input format,
-//                    converted to linear RGB on the fly) and writes the 2x2
-//                    box pyramid levels 1..5 (planar, f32/f16/bf16).
-//                    (ssimulacra2-cuda-kernel/src/downscale.rs:4-35)
-//   fused_kernel     persistent; each work item is a tile of 120 columns x
-//                    `strip_rows` rows at one scale of one pair.  Walking down
-//                    the tile it converts to XYB, forms the five blurred
-//                    inputs of each channel on block-shifted values, runs the
-//                    vertical 9-tap FIR in registers, then every 9 rows the
-//                    horizontal FIR, the SSIM / artifact / detail-loss maps and
-//                    their L1/L4 sums from shared memory.  Only the 18 pooled
-//                    sums of the tile leave the SM.
-//                    (srgb.rs, xyb.rs, blur.rs, error_maps.rs, lib.rs:862-1016)
+//   prep_kernel      reads each pair's scale-0 input once (any input format,
+//                    converted to linear RGB on the fly), builds the 2x2 box
+//                    pyramid in linear RGB and writes the XYB planes of all
+//                    six scales (planar, f32/f16/bf16).
+//                    (ssimulacra2-cuda-kernel/src/downscale.rs:4-35, srgb.rs,
+//                    xyb.rs)
+//   fused_kernel     persistent; each work item is one channel of a tile of
+//                    56 columns x `strip_rows` rows at one scale of one pair.
+//                    Walking down the tile it forms the five blurred inputs on
+//                    band-shifted values, runs the vertical 9-tap FIR in
+//                    registers, then every 9 rows the horizontal FIR, the
+//                    SSIM / artifact / detail-loss maps and their L1/L4 sums
+//                    from shared memory.  Only 6 pooled sums per item leave
+//                    the SM.  (blur.rs, error_maps.rs, lib.rs:862-1016)
 //   finalize_kernel  per pair: fixed-order f64 reduction of the tile sums,
 //                    the 108 statistics and the score (lib.rs:1018-1192).
 //
 // The blur is the exact closed form of the reference's recursive Gaussian:
 // the truncated-cosine recursion of blur.rs equals, in exact arithmetic, a
 // symmetric 9-tap FIR with zero padding.  Moments are taken of values shifted
-// by one reference XYB sample per (120-column, 64-row) block, which removes
+// by one reference XYB sample per (56-column tile, 63-row band), which removes
 // most of the f32 cancellation in sigma - mu^2; the shift is undone
 // algebraically (including at image borders, where the blur of a constant is
 // not the constant).
@@ -70,10 +71,11 @@ __device__ __forceinline__ float2 fir9x2(float2 a0, float2 a1, float2 a2, float2
     return __ffma2_rn(make_float2(S2_T0, S2_T0), a4, acc);
 }
 
+template <bool KUNIT>
 __device__ __forceinline__ void xyb3(const float l[3], float o[3]) {
-    const float a = opsin_row(0, l[0], l[1], l[2]);
-    const float b = opsin_row(1, l[0], l[1], l[2]);
-    const float c = opsin_row(2, l[0], l[1], l[2]);
+    const float a = opsin_row<KUNIT>(0, l[0], l[1], l[2]);
+    const float b = opsin_row<KUNIT>(1, l[0], l[1], l[2]);
+    const float c = opsin_row<KUNIT>(2, l[0], l[1], l[2]);
     o[0] = xyb_from_opsin(0, a, b, c);
     o[1] = xyb_from_opsin(1, a, b, c);
     o[2] = xyb_from_opsin(2, a, b, c);
@@ -98,10 +100,11 @@ __device__ __forceinline__ int find_seg(const Seg *segs, int nseg, int tile) {
 // scale-1 pixel, whose XYB it stores too and whose linear RGB goes to shared
 // memory for scales 2..5.
 // ---------------------------------------------------------------------------
-template <typename ST>
+// KUNIT: linear RGB known non-negative (every input format but linear f32).
+template <typename ST, bool KUNIT>
 __device__ __forceinline__ void store_xyb(const DevPair &P, int img, int s, int x, int y, const float lin[3]) {
     float o[3];
-    xyb3(lin, o);
+    xyb3<KUNIT>(lin, o);
     ST *dst = (ST *)P.lvl[img][s];
     const long long plane = (long long)P.lp[s] * P.h[s];
     const long long off = (long long)y * P.lp[s] + x;
@@ -111,12 +114,12 @@ __device__ __forceinline__ void store_xyb(const DevPair &P, int img, int s, int 
 
 // XYB of two horizontally adjacent pixels, stored as one 2-element write
 // (x even: the planes' pitch is a multiple of 64 elements).
-template <typename ST>
+template <typename ST, bool KUNIT>
 __device__ __forceinline__ void store_xyb_pair(ST *dst, long long plane, long long off, const float a[3],
                                                const float b[3]) {
     float oa[3], ob[3];
-    xyb3(a, oa);
-    xyb3(b, ob);
+    xyb3<KUNIT>(a, oa);
+    xyb3<KUNIT>(b, ob);
 #pragma unroll
     for (int c = 0; c < 3; c++) {
         if constexpr (sizeof(ST) == 4) {
@@ -133,6 +136,7 @@ constexpr int kLv1 = kPyrBlk / 2;  // scale-1 block edge (32)
 template <int FMT, typename ST>
 __device__ __forceinline__ void prep_quads(const DevPair &P, int X0, int Y0, const float *lut, const ColorConsts &cc,
                                            float (*lv1)[3][kLv1 * kLv1]) {
+    constexpr bool KU = FMT != FMT_LINEAR_F32;
     const int W = P.w[0], H = P.h[0];
     const bool scale1 = P.nscales > 1;
     for (int q = threadIdx.x; q < kLv1 * kLv1; q += blockDim.x) {
@@ -148,11 +152,11 @@ __device__ __forceinline__ void prep_quads(const DevPair &P, int X0, int Y0, con
             ST *dst = (ST *)P.lvl[img][0];
             const long long plane = (long long)P.lp[0] * H;
             const long long off = (long long)y * P.lp[0] + x;
-            if (vx) store_xyb_pair<ST>(dst, plane, off, v[0], v[1]);
-            else store_xyb<ST>(P, img, 0, x, y, v[0]);
+            if (vx) store_xyb_pair<ST, KU>(dst, plane, off, v[0], v[1]);
+            else store_xyb<ST, KU>(P, img, 0, x, y, v[0]);
             if (vy) {
-                if (vx) store_xyb_pair<ST>(dst, plane, off + P.lp[0], v[2], v[3]);
-                else store_xyb<ST>(P, img, 0, x, y + 1, v[2]);
+                if (vx) store_xyb_pair<ST, KU>(dst, plane, off + P.lp[0], v[2], v[3]);
+                else store_xyb<ST, KU>(P, img, 0, x, y + 1, v[2]);
             }
             if (!scale1) continue;
             // far-edge clamp: a missing column repeats the left pixel, a
@@ -170,7 +174,7 @@ __device__ __forceinline__ void prep_quads(const DevPair &P, int X0, int Y0, con
                 l1[c] = sum * 0.25f;
                 lv1[img][c][q] = l1[c];
             }
-            store_xyb<ST>(P, img, 1, (X0 >> 1) + qx, (Y0 >> 1) + qy, l1);
+            store_xyb<ST, KU>(P, img, 1, (X0 >> 1) + qx, (Y0 >> 1) + qy, l1);
         }
     }
 }
@@ -227,7 +231,8 @@ __global__ void __launch_bounds__(256, 3) prep_kernel(const DevPair *__restrict_
                         v[c] = sum * 0.25f;
                         pp[s & 1][img][c][i] = v[c];
                     }
-                    store_xyb<ST>(P, img, s, ox, oy, v);
+                    if (P.fmt == FMT_LINEAR_F32) store_xyb<ST, false>(P, img, s, ox, oy, v);
+                    else store_xyb<ST, true>(P, img, s, ox, oy, v);
                 }
             }
             __syncthreads();
@@ -517,20 +522,40 @@ __global__ void __maxnreg__(96)
 // ---------------------------------------------------------------------------
 __constant__ double c_weight[108];
 
-__global__ void __launch_bounds__(128) finalize_kernel(const DevPair *__restrict__ pairs, int npairs,
-                                                       const double *__restrict__ partials,
-                                                       DevResult *__restrict__ out) {
+// The tile records of a scale are contiguous ([tile_base, tile_base + cnt),
+// 18 doubles each).  They are staged in shared memory kFinChunk at a time by
+// coalesced loads of the whole block; then the 18 threads of that scale add
+// their column in tile order (the fixed order that makes a pair's result
+// independent of the rest of the batch).
+constexpr int kFinThreads = 256, kFinChunk = 128;
+
+__global__ void __launch_bounds__(kFinThreads) finalize_kernel(const DevPair *__restrict__ pairs, int npairs,
+                                                               const double *__restrict__ partials,
+                                                               DevResult *__restrict__ out) {
     __shared__ double st[108];
+    __shared__ double rec[kFinChunk * 18];
     const int p = blockIdx.x;
     const DevPair &P = pairs[p];
     const int t = threadIdx.x;
+    const int c = t / 36, sc_t = (t % 36) / 6, k = t % 6;
+    double sum = 0.0;
+    const int ns = P.status == 0 ? P.nscales : 0;
+    for (int s = 0; s < ns; s++) {
+        const int base = P.tile_base[s], cnt = P.tile_cnt[s];
+        for (int i0 = 0; i0 < cnt; i0 += kFinChunk) {
+            const int n = min(kFinChunk, cnt - i0);
+            const double *src = partials + (long long)(base + i0) * 18;
+            for (int j = t; j < n * 18; j += kFinThreads) rec[j] = src[j];
+            __syncthreads();
+            if (t < 108 && sc_t == s)
+                for (int i = 0; i < n; i++) sum += rec[i * 18 + c * 6 + k];
+            __syncthreads();
+        }
+    }
     if (t < 108) {
-        const int c = t / 36, s = (t % 36) / 6, k = t % 6;
-        double sum = 0.0, v = 0.0;
-        if (P.status == 0 && s < P.nscales) {
-            const int base = P.tile_base[s], cnt = P.tile_cnt[s];
-            for (int i = 0; i < cnt; i++) sum += partials[(long long)(base + i) * 18 + c * 6 + k];
-            const double inv = 1.0 / ((double)P.w[s] * (double)P.h[s]);
+        double v = 0.0;
+        if (sc_t < ns) {
+            const double inv = 1.0 / ((double)P.w[sc_t] * (double)P.h[sc_t]);
             v = k < 3 ? sum * inv : sqrt(sqrt(sum * inv));
         }
         st[t] = v;
@@ -648,7 +673,7 @@ cudaError_t launch_fused(int storage, const DevPair *pairs, const Seg *segs, int
 cudaError_t launch_finalize(const DevPair *pairs, int npairs, const double *partials, DevResult *out,
                             cudaStream_t st) {
     if (npairs <= 0) return cudaSuccess;
-    finalize_kernel<<<npairs, 128, 0, st>>>(pairs, npairs, partials, out);
+    finalize_kernel<<<npairs, kFinThreads, 0, st>>>(pairs, npairs, partials, out);
     return cudaGetLastError();
 }
 
