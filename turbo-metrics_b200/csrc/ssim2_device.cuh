@@ -258,6 +258,93 @@ __device__ __forceinline__ float bt709_eotf(float v) {
     return v >= thr ? hi : lo;
 }
 
+// ---- two pixels at once (sm_100 f32x2 operations; each lane rounds exactly
+// as the scalar operation, so these return the scalar functions' results) --
+__device__ __forceinline__ float2 s2_f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 s2_neg2(float2 a) { return make_float2(-a.x, -a.y); }
+
+__device__ __forceinline__ float s2_pow_scale_unit(unsigned b) {
+    const int e = (int)(b >> 23) - 127;
+    return e == 0 ? 1.0f : (e == -1 ? 0x1.b6e8aep-3f : (e == -2 ? 0x1.784086p-5f : 0x1.428a3p-7f));
+}
+
+// Packed f32x2 arithmetic (__fmul2_rn, __fadd2_rn, __ffma2_rn): each lane
+// rounds as the scalar operation, but the compiler contracts a packed
+// multiply whose result feeds a packed add into one fused multiply-add (one
+// rounding instead of two), even in a -fmad=false build (measured on sm_100a
+// with CUDA 12.9).  So no packed product here feeds a packed sum: products
+// that are summed are formed by scalar multiplies (never contracted under
+// -fmad=false), or the sum is the addend of a packed FMA, or the product is
+// exact (a multiplication by 0.5).
+__device__ __forceinline__ float2 s2_mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 s2_add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 s2_mul2s(float2 a, float2 b) { return make_float2(a.x * b.x, a.y * b.y); }
+
+// s2_pow_20_9_unit of both lanes
+__device__ __forceinline__ float2 s2_pow_20_9_unit2(float2 p) {
+    const unsigned bx = __float_as_uint(p.x), by = __float_as_uint(p.y);
+    const float2 m = make_float2(__uint_as_float((bx & 0x7fffffu) | 0x3f800000u),
+                                 __uint_as_float((by & 0x7fffffu) | 0x3f800000u));
+    const float2 t = s2_add2(m, s2_f2(-1.5f));
+    float2 y = __ffma2_rn(s2_f2(0x1.1eb37ap-12f), t, s2_f2(-0x1.88e318p-11f));
+    y = __ffma2_rn(y, t, s2_f2(0x1.2713a6p-9f));
+    y = __ffma2_rn(y, t, s2_f2(-0x1.37717ep-7f));
+    y = __ffma2_rn(y, t, s2_f2(0x1.2c9724p-4f));
+    y = __ffma2_rn(y, t, s2_f2(0x1.7c6f02p+0f));
+    y = __ffma2_rn(y, t, s2_f2(0x1.d2e55cp+1f));
+    y = __ffma2_rn(y, t, s2_f2(0x1.3b279ep+1f));
+    return s2_mul2(y, make_float2(s2_pow_scale_unit(bx), s2_pow_scale_unit(by)));
+}
+
+// bt709_eotf of both lanes
+__device__ __forceinline__ float2 bt709_eotf2(float2 v) {
+    const float thr = 0.08124285829863521110029445797874f;
+    const float2 q = s2_mul2(s2_add2(v, s2_f2(0x1.96b84p-4f)), s2_f2(0x1.d1c096p-1f));
+    const float2 hi = s2_pow_20_9_unit2(make_float2(fminf(fmaxf(q.x, 0.125f), 1.5f), fminf(fmaxf(q.y, 0.125f), 1.5f)));
+    const float2 lo = s2_mul2(v, s2_f2(0x1.c71c72p-3f));
+    return make_float2(v.x >= thr ? hi.x : lo.x, v.y >= thr ? hi.y : lo.y);
+}
+
+// s2_cbrtf_unit of both lanes
+__device__ __forceinline__ float2 s2_cbrtf_unit2(float2 x) {
+    float2 r = make_float2(__uint_as_float(0x54a2fa8cu - __float_as_uint(x.x) / 3u),
+                           __uint_as_float(0x54a2fa8cu - __float_as_uint(x.y) / 3u));
+    const float2 third = s2_f2(0x1.555556p-2f);
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+        float2 t = s2_mul2(x, r);
+        t = s2_mul2(t, r);
+        t = s2_mul2(t, r);
+        // 1 - t as fma(t, -1, 1): same rounding, and t (a product) is not
+        // fed to a packed add
+        r = __ffma2_rn(s2_mul2(r, third), __ffma2_rn(t, s2_f2(-1.0f), s2_f2(1.0f)), r);
+    }
+    float2 y = s2_mul2(x, r);
+    y = s2_mul2(y, r);
+    const float2 e = __ffma2_rn(s2_mul2(y, y), y, s2_neg2(x));
+    const float2 c = s2_mul2(s2_mul2(r, r), third);
+    return __ffma2_rn(s2_neg2(e), c, y);
+}
+
+// XYB of two pixels of non-negative linear RGB (opsin_row<true> and
+// xyb_from_opsin per lane): out[c] = (pixel a, pixel b) of channel c.
+__device__ __forceinline__ void xyb_pair_unit(float2 r, float2 g, float2 b, float2 out[3]) {
+    const float m01 = 1.0f - S2_M02 - S2_M00;
+    const float m11 = 1.0f - S2_M12 - S2_M10;
+    const float m22 = 1.0f - S2_M20 - S2_M21;
+    const float2 v0 = __ffma2_rn(s2_f2(S2_M00), r, __ffma2_rn(s2_f2(m01), g, __ffma2_rn(s2_f2(S2_M02), b, s2_f2(S2_B0))));
+    const float2 v1 = __ffma2_rn(s2_f2(S2_M10), r, __ffma2_rn(s2_f2(m11), g, __ffma2_rn(s2_f2(S2_M12), b, s2_f2(S2_B0))));
+    const float2 v2 = __ffma2_rn(s2_f2(S2_M20), r, __ffma2_rn(s2_f2(S2_M21), g, __ffma2_rn(s2_f2(m22), b, s2_f2(S2_B0))));
+    const float2 nroot = s2_f2(-S2_B0_ROOT);
+    const float2 rg = s2_add2(s2_cbrtf_unit2(v0), nroot);
+    const float2 gr = s2_add2(s2_cbrtf_unit2(v1), nroot);
+    const float2 bb = s2_add2(s2_cbrtf_unit2(v2), nroot);
+    const float2 y = s2_mul2(s2_f2(0.5f), s2_add2(rg, gr));
+    out[0] = __ffma2_rn(s2_mul2(s2_f2(0.5f), s2_add2(rg, s2_neg2(gr))), s2_f2(14.0f), s2_f2(0.42f));
+    out[1] = s2_add2(y, s2_f2(0.01f));
+    out[2] = s2_add2(s2_add2(bb, s2_neg2(y)), s2_f2(0.55f));
+}
+
 struct ColorConsts {
     // NV12 BT.709 limited range: y_coeff, r_coeff, b_coeff, g_coeff1, g_coeff2
     float nv12[5];
@@ -333,15 +420,26 @@ __device__ __forceinline__ void lin_quad(const DevPair &P, int img, int x, int y
         const float ar = cc.nv12[1] * cr;
         const float ag = fmaf(cc.nv12[3], cb, cc.nv12[4] * cr);
         const float ab = cc.nv12[2] * cb;
+        // pixels (0, 1) and (2, 3) as f32x2 lanes; a pixel outside the image
+        // repeats its row's first pixel (computed, never stored)
 #pragma unroll
-        for (int k = 0; k < 4; k++) {
-            const bool in = (k & 1 ? vx : true) && (k & 2 ? vy : true);
-            if (!in) continue;
-            const int Y = __ldg(yp + (k & 1) + (k & 2 ? P.pitch[img] : 0));
-            const float luma = (float)(max(Y, 16) - 16) * cc.nv12[0];
-            o[k][0] = fminf(fmaxf(bt709_eotf(luma + ar), 0.0f), 1.0f);
-            o[k][1] = fminf(fmaxf(bt709_eotf(luma + ag), 0.0f), 1.0f);
-            o[k][2] = fminf(fmaxf(bt709_eotf(luma + ab), 0.0f), 1.0f);
+        for (int row = 0; row < 2; row++) {
+            if (row == 1 && !vy) break;
+            const uint8_t *yr = yp + (row ? P.pitch[img] : 0);
+            const int Y0 = __ldg(yr), Y1 = vx ? __ldg(yr + 1) : Y0;
+            // scalar products: luma is summed with the chroma terms below
+            const float2 luma = make_float2((float)(max(Y0, 16) - 16) * cc.nv12[0],
+                                            (float)(max(Y1, 16) - 16) * cc.nv12[0]);
+            const float2 r = bt709_eotf2(s2_add2(luma, s2_f2(ar)));
+            const float2 g = bt709_eotf2(s2_add2(luma, s2_f2(ag)));
+            const float2 b = bt709_eotf2(s2_add2(luma, s2_f2(ab)));
+            float *p0 = o[2 * row], *p1 = o[2 * row + 1];
+            p0[0] = fminf(fmaxf(r.x, 0.0f), 1.0f);
+            p0[1] = fminf(fmaxf(g.x, 0.0f), 1.0f);
+            p0[2] = fminf(fmaxf(b.x, 0.0f), 1.0f);
+            p1[0] = fminf(fmaxf(r.y, 0.0f), 1.0f);
+            p1[1] = fminf(fmaxf(g.y, 0.0f), 1.0f);
+            p1[2] = fminf(fmaxf(b.y, 0.0f), 1.0f);
         }
     } else {
 #pragma unroll

@@ -64,10 +64,10 @@ __device__ __forceinline__ float fir9(float a0, float a1, float a2, float a3, fl
 // exactly as the scalar fir9).
 __device__ __forceinline__ float2 fir9x2(float2 a0, float2 a1, float2 a2, float2 a3, float2 a4, float2 a5,
                                          float2 a6, float2 a7, float2 a8) {
-    float2 acc = __fmul2_rn(make_float2(S2_T4, S2_T4), __fadd2_rn(a0, a8));
-    acc = __ffma2_rn(make_float2(S2_T3, S2_T3), __fadd2_rn(a1, a7), acc);
-    acc = __ffma2_rn(make_float2(S2_T2, S2_T2), __fadd2_rn(a2, a6), acc);
-    acc = __ffma2_rn(make_float2(S2_T1, S2_T1), __fadd2_rn(a3, a5), acc);
+    float2 acc = s2_mul2(make_float2(S2_T4, S2_T4), s2_add2(a0, a8));
+    acc = __ffma2_rn(make_float2(S2_T3, S2_T3), s2_add2(a1, a7), acc);
+    acc = __ffma2_rn(make_float2(S2_T2, S2_T2), s2_add2(a2, a6), acc);
+    acc = __ffma2_rn(make_float2(S2_T1, S2_T1), s2_add2(a3, a5), acc);
     return __ffma2_rn(make_float2(S2_T0, S2_T0), a4, acc);
 }
 
@@ -117,15 +117,22 @@ __device__ __forceinline__ void store_xyb(const DevPair &P, int img, int s, int 
 template <typename ST, bool KUNIT>
 __device__ __forceinline__ void store_xyb_pair(ST *dst, long long plane, long long off, const float a[3],
                                                const float b[3]) {
-    float oa[3], ob[3];
-    xyb3<KUNIT>(a, oa);
-    xyb3<KUNIT>(b, ob);
+    float2 o[3];
+    if (KUNIT) {
+        xyb_pair_unit(make_float2(a[0], b[0]), make_float2(a[1], b[1]), make_float2(a[2], b[2]), o);
+    } else {
+        float oa[3], ob[3];
+        xyb3<KUNIT>(a, oa);
+        xyb3<KUNIT>(b, ob);
+#pragma unroll
+        for (int c = 0; c < 3; c++) o[c] = make_float2(oa[c], ob[c]);
+    }
 #pragma unroll
     for (int c = 0; c < 3; c++) {
         if constexpr (sizeof(ST) == 4) {
-            *(float2 *)(dst + c * plane + off) = make_float2(oa[c], ob[c]);
+            *(float2 *)(dst + c * plane + off) = o[c];
         } else {
-            ST two[2] = {to_store<ST>(oa[c]), to_store<ST>(ob[c])};
+            ST two[2] = {to_store<ST>(o[c].x), to_store<ST>(o[c].y)};
             *(unsigned *)(dst + c * plane + off) = *(const unsigned *)two;
         }
     }
@@ -299,7 +306,7 @@ __global__ void __maxnreg__(96)
             if (in) {
                 const float px = vr - cg, py = vd - cg;
                 a = make_float2(px, py);
-                b = __fmul2_rn(a, a);
+                b = s2_mul2s(a, a);  // scalar squares: the FIR sums them
                 c = px * py;
             } else {
                 a = make_float2(0.f, 0.f);
@@ -449,16 +456,16 @@ __global__ void __maxnreg__(96)
                                 const float num_s = fmaf(2.0f, cov, kC2);
                                 const float den = (var.x + var.y) + kC2;
                                 const float d = fmaxf(s2_div(fmaf(-num_m, num_s, den), den), 0.0f);
-                                const float2 t = __fadd2_rn(xyv[j], nmu);
+                                const float2 t = s2_add2(xyv[j], nmu);
                                 const float aa = fabsf(t.x), bb = fabsf(t.y);
                                 const float d1 = s2_div(bb - aa, 1.0f + aa);
                                 const float2 ad = make_float2(fmaxf(d1, 0.0f), fmaxf(-d1, 0.0f));
                                 const float q = d * d;
                                 fs[0] += d;
                                 f4[0] += q * q;
-                                const float2 q2 = __fmul2_rn(ad, ad);
-                                fs12 = __fadd2_rn(fs12, ad);
-                                f412 = __fadd2_rn(f412, __fmul2_rn(q2, q2));
+                                const float2 q2 = s2_mul2(ad, ad);
+                                fs12 = s2_add2(fs12, ad);
+                                f412 = s2_add2(f412, s2_mul2s(q2, q2));  // scalar: summed
                             }
                             fs[1] = fs12.x;
                             fs[2] = fs12.y;
