@@ -406,6 +406,56 @@ __device__ __forceinline__ void lin_pixel(const DevPair &P, int img, int x, int 
     }
 }
 
+// The six samples of an NV12 quad (x, y even): luma of rows y and y + 1 and
+// the shared CbCr pair, read as 16-bit words when the plane base and pitch
+// are even (always for the engine's own staging), else as bytes.
+struct Nv12Quad {
+    unsigned y0, y1, uv;  // low byte = left / Cb, high byte = right / Cr
+};
+__device__ __forceinline__ Nv12Quad nv12_load_quad(const DevPair &P, int img, int x, int y) {
+    const uint8_t *yp = (const uint8_t *)P.in[img] + (long long)y * P.pitch[img] + x;
+    const uint8_t *uv = (const uint8_t *)P.in_uv[img] + (long long)(y >> 1) * P.pitch[img] + x;
+    Nv12Quad q;
+    if ((((unsigned long long)P.in[img] | (unsigned long long)P.in_uv[img] | (unsigned long long)P.pitch[img]) & 1) == 0) {
+        q.y0 = __ldg((const unsigned short *)yp);
+        q.y1 = __ldg((const unsigned short *)(yp + P.pitch[img]));
+        q.uv = __ldg((const unsigned short *)uv);
+    } else {
+        q.y0 = __ldg(yp) | ((unsigned)__ldg(yp + 1) << 8);
+        q.y1 = __ldg(yp + P.pitch[img]) | ((unsigned)__ldg(yp + P.pitch[img] + 1) << 8);
+        q.uv = __ldg(uv) | ((unsigned)__ldg(uv + 1) << 8);
+    }
+    return q;
+}
+
+// BT.709 limited range (cuda-colorspace-kernel/src/biplanar.rs:8-70, nearest
+// chroma) of a loaded quad: pixels (0, 1) and (2, 3) as f32x2 lanes.
+__device__ __forceinline__ void nv12_quad_linear(const Nv12Quad &q, const ColorConsts &cc, float o[4][3]) {
+    const float cb = (float)((int)(q.uv & 0xffu) - 128);
+    const float cr = (float)((int)(q.uv >> 8) - 128);
+    const float ar = cc.nv12[1] * cr;
+    const float ag = fmaf(cc.nv12[3], cb, cc.nv12[4] * cr);
+    const float ab = cc.nv12[2] * cb;
+#pragma unroll
+    for (int row = 0; row < 2; row++) {
+        const unsigned w = row ? q.y1 : q.y0;
+        const int Y0 = (int)(w & 0xffu), Y1 = (int)(w >> 8);
+        // scalar products: luma is summed with the chroma terms below
+        const float2 luma = make_float2((float)(max(Y0, 16) - 16) * cc.nv12[0],
+                                        (float)(max(Y1, 16) - 16) * cc.nv12[0]);
+        const float2 r = bt709_eotf2(s2_add2(luma, s2_f2(ar)));
+        const float2 g = bt709_eotf2(s2_add2(luma, s2_f2(ag)));
+        const float2 b = bt709_eotf2(s2_add2(luma, s2_f2(ab)));
+        float *p0 = o[2 * row], *p1 = o[2 * row + 1];
+        p0[0] = fminf(fmaxf(r.x, 0.0f), 1.0f);
+        p0[1] = fminf(fmaxf(g.x, 0.0f), 1.0f);
+        p0[2] = fminf(fmaxf(b.x, 0.0f), 1.0f);
+        p1[0] = fminf(fmaxf(r.y, 0.0f), 1.0f);
+        p1[1] = fminf(fmaxf(g.y, 0.0f), 1.0f);
+        p1[2] = fminf(fmaxf(b.y, 0.0f), 1.0f);
+    }
+}
+
 // Linear RGB of the 2x2 quad whose top-left pixel is (x, y) (inside the
 // image); px 0..3 = (x,y), (x+1,y), (x,y+1), (x+1,y+1); pixels outside the
 // image (vx / vy false) are not read.  NV12 chroma is one sample per quad.
@@ -413,34 +463,9 @@ template <int FMT>
 __device__ __forceinline__ void lin_quad(const DevPair &P, int img, int x, int y, bool vx, bool vy,
                                          const float *lut, const ColorConsts &cc, float o[4][3]) {
     if (FMT == FMT_NV12) {
-        const uint8_t *yp = (const uint8_t *)P.in[img] + (long long)y * P.pitch[img] + x;
-        const uint8_t *uv = (const uint8_t *)P.in_uv[img] + (long long)(y >> 1) * P.pitch[img] + x;
-        const float cb = (float)((int)__ldg(uv) - 128);
-        const float cr = (float)((int)__ldg(uv + 1) - 128);
-        const float ar = cc.nv12[1] * cr;
-        const float ag = fmaf(cc.nv12[3], cb, cc.nv12[4] * cr);
-        const float ab = cc.nv12[2] * cb;
-        // pixels (0, 1) and (2, 3) as f32x2 lanes; a pixel outside the image
-        // repeats its row's first pixel (computed, never stored)
-#pragma unroll
-        for (int row = 0; row < 2; row++) {
-            if (row == 1 && !vy) break;
-            const uint8_t *yr = yp + (row ? P.pitch[img] : 0);
-            const int Y0 = __ldg(yr), Y1 = vx ? __ldg(yr + 1) : Y0;
-            // scalar products: luma is summed with the chroma terms below
-            const float2 luma = make_float2((float)(max(Y0, 16) - 16) * cc.nv12[0],
-                                            (float)(max(Y1, 16) - 16) * cc.nv12[0]);
-            const float2 r = bt709_eotf2(s2_add2(luma, s2_f2(ar)));
-            const float2 g = bt709_eotf2(s2_add2(luma, s2_f2(ag)));
-            const float2 b = bt709_eotf2(s2_add2(luma, s2_f2(ab)));
-            float *p0 = o[2 * row], *p1 = o[2 * row + 1];
-            p0[0] = fminf(fmaxf(r.x, 0.0f), 1.0f);
-            p0[1] = fminf(fmaxf(g.x, 0.0f), 1.0f);
-            p0[2] = fminf(fmaxf(b.x, 0.0f), 1.0f);
-            p1[0] = fminf(fmaxf(r.y, 0.0f), 1.0f);
-            p1[1] = fminf(fmaxf(g.y, 0.0f), 1.0f);
-            p1[2] = fminf(fmaxf(b.y, 0.0f), 1.0f);
-        }
+        // NV12 has even width and height: the quad is complete
+        const Nv12Quad q = nv12_load_quad(P, img, x, y);
+        nv12_quad_linear(q, cc, o);
     } else {
 #pragma unroll
         for (int k = 0; k < 4; k++) {

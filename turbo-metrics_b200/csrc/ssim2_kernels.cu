@@ -151,11 +151,18 @@ __device__ __forceinline__ void prep_quads(const DevPair &P, int X0, int Y0, con
         const int x = X0 + 2 * qx, y = Y0 + 2 * qy;
         if (x >= W || y >= H) continue;
         const bool vx = x + 1 < W, vy = y + 1 < H;
+        // NV12: both images' samples are loaded before either is converted
+        Nv12Quad nq0{}, nq1{};
+        if (FMT == FMT_NV12) {
+            if (P.prep_mask & 1) nq0 = nv12_load_quad(P, 0, x, y);
+            if (P.prep_mask & 2) nq1 = nv12_load_quad(P, 1, x, y);
+        }
 #pragma unroll 1
         for (int img = 0; img < 2; img++) {
             if (!((P.prep_mask >> img) & 1)) continue;
             float v[4][3];
-            lin_quad<FMT>(P, img, x, y, vx, vy, lut, cc, v);
+            if (FMT == FMT_NV12) nv12_quad_linear(img ? nq1 : nq0, cc, v);
+            else lin_quad<FMT>(P, img, x, y, vx, vy, lut, cc, v);
             ST *dst = (ST *)P.lvl[img][0];
             const long long plane = (long long)P.lp[0] * H;
             const long long off = (long long)y * P.lp[0] + x;
@@ -194,8 +201,11 @@ __global__ void __launch_bounds__(256, 3) prep_kernel(const DevPair *__restrict_
     __shared__ float lv1[2][3][kLv1 * kLv1];              // scale-1 linear block [img][ch][px]
     __shared__ float pp[2][2][3][(kLv1 / 2) * (kLv1 / 2)];  // scales >= 2, ping-pong
     __shared__ float lut[256];
+    // the block's pair descriptor: in shared memory, so the level stores
+    // (global) cannot alias it and its fields need no per-thread copy
+    __shared__ DevPair sP;
+    static_assert(sizeof(DevPair) % 8 == 0, "DevPair copied as 8-byte words");
     for (int i = threadIdx.x; i < 256; i += blockDim.x) lut[i] = lut_g[i];
-    __syncthreads();
     for (int item = first_block + blockIdx.x; item < end_block; item += gridDim.x) {
         int lo = 0, hi = npairs - 1;
         while (lo < hi) {
@@ -203,7 +213,11 @@ __global__ void __launch_bounds__(256, 3) prep_kernel(const DevPair *__restrict_
             if (blk_first[mid] <= item) lo = mid;
             else hi = mid - 1;
         }
-        const DevPair P = pairs[lo];  // local copy: the level stores cannot alias it
+        __syncthreads();  // the previous item's readers of sP are done
+        for (int i = threadIdx.x; i < (int)(sizeof(DevPair) / 8); i += blockDim.x)
+            ((long long *)&sP)[i] = __ldg((const long long *)(pairs + lo) + i);
+        __syncthreads();
+        const DevPair &P = sP;
         const int b = item - blk_first[lo];
         const int bx = b % P.blk_x, by = b / P.blk_x;
         const int X0 = bx * kPyrBlk, Y0 = by * kPyrBlk;
