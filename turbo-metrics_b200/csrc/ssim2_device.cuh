@@ -352,6 +352,18 @@ struct ColorConsts {
     float m2020[9];
 };
 
+__device__ __forceinline__ void rgb16_linear(unsigned r, unsigned g, unsigned b, float inv, const ColorConsts &cc,
+                                             float o[3]) {
+    const float p0 = bt709_eotf((float)r * inv);
+    const float p1 = bt709_eotf((float)g * inv);
+    const float p2 = bt709_eotf((float)b * inv);
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const float *m = cc.m2020 + 3 * k;
+        o[k] = fmaxf(fmaf(m[0], p0, fmaf(m[1], p1, m[2] * p2)), 0.0f);
+    }
+}
+
 template <typename T> __device__ __forceinline__ float ld_store(const T *p);
 template <> __device__ __forceinline__ float ld_store<float>(const float *p) { return __ldg(p); }
 template <> __device__ __forceinline__ float ld_store<__half>(const __half *p) { return __half2float(*p); }
@@ -364,6 +376,12 @@ template <> __device__ __forceinline__ __half to_store<__half>(float v) { return
 template <> __device__ __forceinline__ __nv_bfloat16 to_store<__nv_bfloat16>(float v) {
     return __float2bfloat16_rn(v);
 }
+
+// RGB16: samples of `bits` bits, BT.709/BT.2020 inverse OETF, then BT.2020 ->
+// BT.709 primaries, clamped >= 0.  inv = 1 / (2^bits - 1) in f32.
+struct ColorConsts;
+__device__ __forceinline__ void rgb16_linear(unsigned r, unsigned g, unsigned b, float inv, const ColorConsts &cc,
+                                             float o[3]);
 
 // Linear RGB of scale-0 pixel (x, y) of image img (inside the image), for
 // input format FMT.  sRGB8: the reference table; NV12: BT.709 limited range,
@@ -394,15 +412,7 @@ __device__ __forceinline__ void lin_pixel(const DevPair &P, int img, int x, int 
         o[2] = fminf(fmaxf(bt709_eotf(luma + cc.nv12[2] * cb), 0.0f), 1.0f);
     } else {
         const uint16_t *q = (const uint16_t *)base + 3 * x;
-        const float inv = 1.0f / (float)((1 << P.bits) - 1);
-        const float p0 = bt709_eotf((float)__ldg(q) * inv);
-        const float p1 = bt709_eotf((float)__ldg(q + 1) * inv);
-        const float p2 = bt709_eotf((float)__ldg(q + 2) * inv);
-#pragma unroll
-        for (int g = 0; g < 3; g++) {
-            const float *m = cc.m2020 + 3 * g;
-            o[g] = fmaxf(fmaf(m[0], p0, fmaf(m[1], p1, m[2] * p2)), 0.0f);
-        }
+        rgb16_linear(__ldg(q), __ldg(q + 1), __ldg(q + 2), 1.0f / (float)((1 << P.bits) - 1), cc, o);
     }
 }
 
@@ -467,10 +477,47 @@ __device__ __forceinline__ void lin_quad(const DevPair &P, int img, int x, int y
         const Nv12Quad q = nv12_load_quad(P, img, x, y);
         nv12_quad_linear(q, cc, o);
     } else {
+        // a complete quad whose rows are aligned for the format's word size is
+        // read as three words per row: sRGB8 16-bit, RGB16 32-bit, linear f32
+        // 64-bit (x is even: the row pair starts 6, 12 or 24 bytes x/2 in)
+        constexpr int kAlign = FMT == FMT_SRGB8 ? 2 : (FMT == FMT_RGB16 ? 4 : 8);
+        if (vx && vy && ((((unsigned long long)P.in[img]) | (unsigned long long)P.pitch[img]) & (kAlign - 1)) == 0) {
+            const float inv = FMT == FMT_RGB16 ? 1.0f / (float)((1 << P.bits) - 1) : 0.0f;
 #pragma unroll
-        for (int k = 0; k < 4; k++) {
-            const bool in = (k & 1 ? vx : true) && (k & 2 ? vy : true);
-            if (in) lin_pixel<FMT>(P, img, x + (k & 1), y + (k >> 1), lut, cc, o[k]);
+            for (int row = 0; row < 2; row++) {
+                const char *rp = (const char *)P.in[img] + (long long)(y + row) * P.pitch[img];
+                float *p0 = o[2 * row], *p1 = o[2 * row + 1];
+                if (FMT == FMT_SRGB8) {
+                    const unsigned short *q = (const unsigned short *)(rp + 3 * x);
+                    const unsigned w0 = __ldg(q), w1 = __ldg(q + 1), w2 = __ldg(q + 2);
+                    p0[0] = lut[w0 & 0xffu];
+                    p0[1] = lut[w0 >> 8];
+                    p0[2] = lut[w1 & 0xffu];
+                    p1[0] = lut[w1 >> 8];
+                    p1[1] = lut[w2 & 0xffu];
+                    p1[2] = lut[w2 >> 8];
+                } else if (FMT == FMT_RGB16) {
+                    const unsigned *q = (const unsigned *)(rp + 6 * x);
+                    const unsigned w0 = __ldg(q), w1 = __ldg(q + 1), w2 = __ldg(q + 2);
+                    rgb16_linear(w0 & 0xffffu, w0 >> 16, w1 & 0xffffu, inv, cc, p0);
+                    rgb16_linear(w1 >> 16, w2 & 0xffffu, w2 >> 16, inv, cc, p1);
+                } else {
+                    const float2 *q = (const float2 *)(rp + 12 * x);
+                    const float2 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2);
+                    p0[0] = a.x;
+                    p0[1] = a.y;
+                    p0[2] = b.x;
+                    p1[0] = b.y;
+                    p1[1] = c.x;
+                    p1[2] = c.y;
+                }
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const bool in = (k & 1 ? vx : true) && (k & 2 ? vy : true);
+                if (in) lin_pixel<FMT>(P, img, x + (k & 1), y + (k >> 1), lut, cc, o[k]);
+            }
         }
     }
 }
