@@ -58,6 +58,25 @@ def gen_pair(i):
     return ry, ruv, dy, duv
 
 
+def replica_offset(rank, n_pairs):
+    """First pair index of a replica: every rank scores its own n_pairs pairs."""
+    return rank * n_pairs
+
+
+def max_over_ranks(x, dist, device):
+    """The slowest rank's time (the whole job ends with it); x itself on one rank."""
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world, n_pairs, steps, ms):
+    """Pairs per second of all replicas together over the max-over-ranks time."""
+    return world * n_pairs * steps / (ms / 1e3)
+
+
 def gen_pairs(n, offset=0):
     import multiprocessing as mp
     ctx = mp.get_context("spawn")
@@ -278,7 +297,7 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
     tmb = import_pkg()
 
-    pairs_np = gen_pairs(NP, offset=rank * NP)
+    pairs_np = gen_pairs(NP, offset=replica_offset(rank, NP))
     dev = []
     for ry, ruv, dy, duv in pairs_np:
         dev.append(tuple(torch.from_numpy(a).cuda() for a in (ry, ruv, dy, duv)))
@@ -308,12 +327,8 @@ def main():
         ev1.record(stream)
         torch.cuda.synchronize()
     barrier()
-    ms = ev0.elapsed_time(ev1)
-    ms_t = torch.tensor([ms], device="cuda")
-    if dist is not None:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms = float(ms_t.item())
-    value = world * NP * args.steps / (ms / 1e3)
+    ms = max_over_ranks(ev0.elapsed_time(ev1), dist, "cuda")
+    value = whole_job_rate(world, NP, args.steps, ms)
 
     # ---- fused-kernel roofline (CUDA events around each launch) ----------
     lib.s2_batch_set_profiling(batch._h, 1)
@@ -392,12 +407,8 @@ def main():
         res = e2e_step()
     e1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
-    et = torch.tensor([e2e_ms], device="cuda")
-    if dist is not None:
-        dist.all_reduce(et, op=dist.ReduceOp.MAX)
-    e2e_ms = float(et.item())
-    e2e = world * NP * args.steps / (e2e_ms / 1e3)
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), dist, "cuda")
+    e2e = whole_job_rate(world, NP, args.steps, e2e_ms)
     assert np.allclose([r[0] for r in res], scores, atol=1e-9)
 
     served = None
