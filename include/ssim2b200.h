@@ -86,7 +86,10 @@ typedef struct {
     int32_t blur;          /* S2_BLUR_* */
     int32_t storage;       /* S2_STORAGE_* */
     int32_t scale_rule;    /* S2_SCALES_* */
-    int32_t strip_rows;    /* rows per fused tile: 0 = autotuned, else 9/21/63 */
+    int32_t strip_rows;    /* rows per fused tile: 9/21/63, or 0 = autotuned: the first
+                              submission of a workload class (work items in half-octave
+                              buckets) times the tile pass at each height and the
+                              fastest is kept for the class (process-wide) */
     uint64_t hbm_budget;   /* bytes this context may allocate; 0 = no limit */
 } s2_config;
 
@@ -215,9 +218,17 @@ s2_status s2_batch_submit_host(s2_batch *b, const s2_pair_desc *pairs, uint32_t 
 /* Wait for the last submission and copy its n results. */
 s2_status s2_batch_results(s2_batch *b, s2_result *out, uint32_t n);
 s2_status s2_batch_mem_usage(const s2_batch *b, size_t *bytes);
-/* Record the next submission's launches into a CUDA graph and replay it for
- * later submissions with identical shapes (1 = on). */
+/* CUDA graphs (1 = on, the default): the operations of a device-input
+ * submission (descriptor upload, counter reset, prep, tile pass, finalize,
+ * result download) are recorded once per plan shape (pair count and block,
+ * tile and segment counts) and replayed for later submissions of that shape,
+ * like the reference's graph per bound pair (ssimulacra2-cuda/src/lib.rs:
+ * 409-424); pointers and sizes of the pairs travel in the uploaded
+ * descriptors, so one graph serves any pairs of the shape.  Host-input
+ * submissions and profiled submissions launch directly. */
 s2_status s2_batch_set_graphs(s2_batch *b, int32_t enable);
+/* The same switch for a single-pair context (default on). */
+s2_status s2_set_graphs(s2_ctx *ctx, int32_t enable);
 
 /* ---- serving: continuous batching of jobs (reference + k candidates) -----
  * No single counterpart in the reference: it combines the cached-reference

@@ -17,6 +17,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/ssim2b200.h"
@@ -200,6 +201,34 @@ s2_status s2_global_init() {
 
 
 // ---------------------------------------------------------------------------
+// tile-height autotuner cache
+// ---------------------------------------------------------------------------
+static std::mutex g_tune_mu;
+static std::unordered_map<uint64_t, int> g_tune;
+
+uint64_t s2_tune_signature(uint64_t items63, int storage, int num_sms, int bps) {
+    // half-octave bucket of the work-item count
+    int b = 0;
+    if (items63 > 0) {
+        const double l = std::log2((double)items63);
+        b = (int)std::floor(2.0 * l);
+    }
+    return ((uint64_t)(b & 0xff) << 32) | ((uint64_t)(storage & 0xf) << 24) | ((uint64_t)(num_sms & 0xfff) << 8) |
+           (uint64_t)(bps & 0xff);
+}
+
+int s2_tuned_strip(uint64_t sig) {
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    auto it = g_tune.find(sig);
+    return it == g_tune.end() ? 0 : it->second;
+}
+
+void s2_set_tuned_strip(uint64_t sig, int strip) {
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    g_tune[sig] = strip;
+}
+
+// ---------------------------------------------------------------------------
 // single-pair context
 // ---------------------------------------------------------------------------
 struct s2_ctx {
@@ -291,6 +320,7 @@ s2_status s2_create(const s2_config *cfg_in, uint32_t width, uint32_t height, s2
     c->w = width;
     c->h = height;
     st = c->eng.init(&cfg);
+    c->eng.graphs = true;
     if (st == S2_OK) {
         // allocate the steady-state buffers now (like the reference's new)
         s2_pair_desc d;
@@ -340,6 +370,8 @@ s2_status s2_dimensions(const s2_ctx *ctx, uint32_t *w, uint32_t *h) {
 
 static s2_status ctx_run(s2_ctx *ctx, const s2_pair_desc &d, void *stream, const PairExtra *ex = nullptr) {
     s2_status st = ctx->eng.plan(&d, 1, ctx->plan, ex);
+    if (st == S2_OK && ctx->plan.pairs[0].status == S2_OK && (!ex || ex->score))
+        st = ctx->eng.tune(&d, 1, ctx->plan, ex, (cudaStream_t)stream);
     if (st != S2_OK) return st;
     if (ctx->plan.pairs[0].status != S2_OK) return (s2_status)ctx->plan.pairs[0].status;
     ctx->last_was_ref_build = ex && !ex->score;
@@ -570,6 +602,7 @@ s2_status s2_batch_create(const s2_config *cfg_in, uint32_t max_pairs, uint64_t 
     b->max_pairs = max_pairs;
     b->max_pixels = max_pixels;
     st = b->eng.init(&cfg);
+    b->eng.graphs = true;
     if (st == S2_OK) {
         st = b->eng.reserve(max_pairs, max_pixels, false);
     }
@@ -592,6 +625,7 @@ s2_status s2_batch_submit(s2_batch *b, const s2_pair_desc *pairs, uint32_t n, vo
     if (!b || (!pairs && n)) return S2_ERR_INVALID_ARG;
     if (n > b->max_pairs) return S2_ERR_INVALID_ARG;
     s2_status st = b->eng.plan(pairs, (int)n, b->plan);
+    if (st == S2_OK) st = b->eng.tune(pairs, (int)n, b->plan, nullptr, (cudaStream_t)stream);
     if (st != S2_OK) return st;
     return b->eng.enqueue(b->plan, (cudaStream_t)stream);
 }
@@ -656,7 +690,15 @@ int32_t s2_fused_blocks_per_sm(int32_t storage) { return s2_global_init() == S2_
 
 s2_status s2_batch_set_graphs(s2_batch *b, int32_t enable) {
     if (!b) return S2_ERR_INVALID_ARG;
-    (void)enable;
+    b->eng.graphs = enable != 0;
+    if (!b->eng.graphs) b->eng.drop_graphs();
+    return S2_OK;
+}
+
+s2_status s2_set_graphs(s2_ctx *ctx, int32_t enable) {
+    if (!ctx) return S2_ERR_INVALID_ARG;
+    ctx->eng.graphs = enable != 0;
+    if (!ctx->eng.graphs) ctx->eng.drop_graphs();
     return S2_OK;
 }
 

@@ -20,6 +20,13 @@ s2_status s2_global_init();
 ColorConsts s2_make_color_consts();
 extern const float s2_srgb8_lut[256];
 
+// Tile-height autotuner cache (process-wide, thread-safe; ssim2_engine.cu).
+// A workload class is the number of fused work items at the tallest strip,
+// in half-octave buckets, with the storage type and the resident-CTA count.
+uint64_t s2_tune_signature(uint64_t items63, int storage, int num_sms, int bps);
+int s2_tuned_strip(uint64_t sig);  // 0 if not measured yet
+void s2_set_tuned_strip(uint64_t sig, int strip);
+
 #define S2_CUDA(call)                                          \
     do {                                                       \
         cudaError_t e_ = (call);                               \
@@ -106,6 +113,10 @@ struct Plan {
     int total_tiles = 0;
     size_t level_bytes = 0;  // both images, all levels, all pairs
     int strip_rows = 63;
+    // autotuning: the workload class of this plan, and whether the tile
+    // height for it still has to be measured
+    uint64_t tune_sig = 0;
+    bool needs_tune = false;
     // groups: pairs [grp_pair[g], grp_pair[g+1]) own the tiles
     // [grp_tile[g], grp_tile[g+1]); one group unless the inputs are uploaded
     // from the host in pipelined groups
@@ -145,6 +156,18 @@ struct Engine {
     // event per group for its planes having landed and one for its prep being
     // done, the submission's start, and the staging being free again (the
     // last group's prep has read it)
+    // CUDA graphs of single-group device-input submissions, keyed by the
+    // plan's shape (pair count, block / tile / segment counts); the buffers
+    // the graph's nodes point at are fixed until a reallocation, which drops
+    // every graph.  Captured on an engine-owned stream, launched on the
+    // caller's.
+    bool graphs = false;
+    struct GraphEntry {
+        uint64_t key[7];
+        cudaGraphExec_t exec;
+    };
+    std::vector<GraphEntry> gcache;
+    cudaStream_t cap_st = nullptr;
     DevBuf stage_d;
     cudaStream_t copy_st = nullptr, prep_st = nullptr;
     cudaEvent_t grp_copied[kMaxGroups] = {}, grp_prepped[kMaxGroups] = {};
@@ -192,6 +215,8 @@ struct Engine {
         if (done) cudaEventSynchronize(done);
         for (cudaEvent_t &e : prof)
             if (e) cudaEventDestroy(e), e = nullptr;
+        drop_graphs();
+        if (cap_st) cudaStreamDestroy(cap_st), cap_st = nullptr;
         if (copy_st) cudaStreamSynchronize(copy_st), cudaStreamDestroy(copy_st), copy_st = nullptr;
         if (prep_st) cudaStreamSynchronize(prep_st), cudaStreamDestroy(prep_st), prep_st = nullptr;
         for (cudaEvent_t &e : grp_copied)
@@ -209,9 +234,15 @@ struct Engine {
         allocated = 0;
     }
 
+    void drop_graphs() {
+        for (GraphEntry &g : gcache) cudaGraphExecDestroy(g.exec);
+        gcache.clear();
+    }
+
     // Grow-only device allocation, checked against the budget.
     s2_status ensure(DevBuf &b, size_t bytes) {
         if (b.n >= bytes) return S2_OK;
+        drop_graphs();
         bytes = s2_align_up(bytes, 4096);
         if (budget && allocated - b.n + bytes > budget) {
             s2_set_last_error("allocation over the HBM budget");
@@ -249,6 +280,7 @@ struct Engine {
     }
 
     s2_status ensure_pinned(size_t bytes, size_t nres) {
+        if (pinned_n < bytes || results_cap < nres) drop_graphs();
         if (pinned_n < bytes) {
             if (pinned) {
                 if (done) cudaEventSynchronize(done);
@@ -271,11 +303,23 @@ struct Engine {
         return S2_OK;
     }
 
-    int choose_strip_rows(const std::vector<uint64_t> &tiles_at) const {
+    int force_strip = 0;  // a tuning trial's tile height (0 = none)
+
+    // The fused pass's tile height (rows per strip): configured (9/21/63), a
+    // tuning trial's, the autotuner's measured choice for this workload class,
+    // or, until that is measured, the largest height that still gives ~4
+    // waves of resident work items (three per tile: one per channel).
+    int choose_strip_rows(const std::vector<uint64_t> &tiles_at, Plan &P) const {
+        P.needs_tune = false;
+        if (force_strip) return force_strip;
         if (strip_rows_cfg == 9 || strip_rows_cfg == 21 || strip_rows_cfg == 63) return strip_rows_cfg;
-        // largest strip height that still gives ~4 waves of resident work
-        // items (three per tile: one per channel)
         const uint64_t resident = (uint64_t)num_sms * (uint64_t)fused_bps;
+        if (blur == S2_BLUR_FIR) {
+            P.tune_sig = s2_tune_signature(3 * tiles_at[0], storage, num_sms, fused_bps);
+            const int tuned = s2_tuned_strip(P.tune_sig);
+            if (tuned) return tuned;
+            P.needs_tune = true;
+        }
         if (3 * tiles_at[0] >= 4 * resident) return 63;
         if (3 * tiles_at[1] >= 4 * resident) return 21;
         return 9;
@@ -299,7 +343,7 @@ struct Engine {
                 h = (h + 1) / 2;
             }
         }
-        P.strip_rows = choose_strip_rows(tiles_at);
+        P.strip_rows = choose_strip_rows(tiles_at, P);
         size_t lvl_off = 0;
         int blk = 0;
         for (int i = 0; i < n; i++) {
@@ -536,6 +580,22 @@ struct Engine {
         const DevPair *dpairs = (const DevPair *)dbase;
         const int *dblk = (const int *)(dbase + pb);
         const Seg *dsegs = (const Seg *)(dbase + pb + bb);
+        if (graphs && !host && !profiling && ng == 1) {
+            const uint64_t key[7] = {(uint64_t)n, (uint64_t)P.total_blocks, (uint64_t)P.total_tiles, P.segs.size(),
+                                     P.vsegs.size(), P.hsegs.size(),
+                                     ((uint64_t)(uint32_t)P.vtotal << 32) | (uint32_t)P.htotal};
+            cudaGraphExec_t ex = nullptr;
+            for (const GraphEntry &g : gcache)
+                if (!memcmp(g.key, key, sizeof key)) ex = g.exec;
+            if (!ex) ex = capture(P, key, pb + bb + sb + vsb + hsb);
+            if (ex) {
+                S2_CUDA(cudaGraphLaunch(ex, st));
+                S2_CUDA(cudaEventRecord(done, st));
+                last_n = n;
+                pending = true;
+                return S2_OK;
+            }
+        }
         S2_CUDA(cudaMemcpyAsync(dbase, h, pb + bb + sb + vsb + hsb, cudaMemcpyHostToDevice, st));
         S2_CUDA(cudaMemsetAsync(counter_d.p, 0, ng * sizeof(int), st));
         if (profiling) S2_CUDA(cudaEventRecord(prof[0], st));
@@ -599,10 +659,102 @@ struct Engine {
         return S2_OK;
     }
 
+    // Record a single-group device-input submission of plan P (its
+    // descriptors already in the pinned staging) as a graph: descriptor
+    // upload, counter reset, prep, fused (or the two IIR passes), finalize,
+    // result download.  nullptr if capture is not possible here (graphs are
+    // then switched off for this engine and the launches go directly).
+    cudaGraphExec_t capture(const Plan &P, const uint64_t key[7], size_t desc_bytes) {
+        const int n = (int)P.pairs.size();
+        const size_t pb = s2_align_up(n * sizeof(DevPair), 256), bb = s2_align_up(n * sizeof(int), 256),
+                     sb = s2_align_up(std::max<size_t>(P.segs.size(), 1) * sizeof(Seg), 256),
+                     vsb = s2_align_up(P.vsegs.size() * sizeof(IirSeg), 256);
+        char *dbase = (char *)pairs_d.p;
+        const DevPair *dpairs = (const DevPair *)dbase;
+        if (!cap_st && cudaStreamCreateWithFlags(&cap_st, cudaStreamNonBlocking) != cudaSuccess) {
+            graphs = false;
+            return nullptr;
+        }
+        if (cudaStreamBeginCapture(cap_st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            graphs = false;
+            return nullptr;
+        }
+        cudaError_t e = cudaMemcpyAsync(dbase, pinned, desc_bytes, cudaMemcpyHostToDevice, cap_st);
+        if (e == cudaSuccess) e = cudaMemsetAsync(counter_d.p, 0, sizeof(int), cap_st);
+        if (e == cudaSuccess)
+            e = launch_pyramid(storage, dpairs, n, (const int *)(dbase + pb), 0, P.total_blocks, cc,
+                               (const float *)lut_d.p, num_sms * 8, cap_st);
+        if (e == cudaSuccess) {
+            if (blur == S2_BLUR_IIR_REF)
+                e = launch_iir(storage, dpairs, (const IirSeg *)(dbase + pb + bb + sb), (int)P.vsegs.size(), P.vtotal,
+                               (const IirSeg *)(dbase + pb + bb + sb + vsb), (int)P.hsegs.size(), P.htotal,
+                               (double *)partials_d.p, cap_st);
+            else
+                e = launch_fused(storage, dpairs, (const Seg *)(dbase + pb + bb), (int)P.segs.size(), 0,
+                                 P.total_tiles, (int *)counter_d.p, (double *)partials_d.p, num_sms * fused_bps,
+                                 cap_st);
+        }
+        if (e == cudaSuccess)
+            e = launch_finalize(dpairs, n, (const double *)partials_d.p, (DevResult *)results_d.p, cap_st);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(results_h, results_d.p, n * sizeof(DevResult), cudaMemcpyDeviceToHost, cap_st);
+        cudaGraph_t graph = nullptr;
+        const cudaError_t ee = cudaStreamEndCapture(cap_st, &graph);
+        cudaGraphExec_t exec = nullptr;
+        if (e == cudaSuccess && ee == cudaSuccess && graph &&
+            cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess) {
+            if (gcache.size() >= 8) {
+                cudaGraphExecDestroy(gcache.front().exec);
+                gcache.erase(gcache.begin());
+            }
+            GraphEntry g;
+            memcpy(g.key, key, sizeof g.key);
+            g.exec = exec;
+            gcache.push_back(g);
+        } else {
+            graphs = false;
+            exec = nullptr;
+            cudaGetLastError();  // clear a capture error; the direct path follows
+        }
+        if (graph) cudaGraphDestroy(graph);
+        return exec;
+    }
+
     s2_status wait() {
         if (last_n < 0) return S2_ERR_NOT_READY;
         S2_CUDA(cudaEventSynchronize(done));
         pending = false;
         return S2_OK;
+    }
+
+    // The autotuner: the first submission of a workload class runs once per
+    // candidate tile height (9, 21, 63 rows) with the fused launch timed by
+    // CUDA events, records the fastest for the class, and re-plans P with it.
+    // The trials score the same pairs, so they need no inputs of their own;
+    // later submissions of the class use the recorded height directly.
+    s2_status tune(const s2_pair_desc *d, int n, Plan &P, const PairExtra *ex, cudaStream_t st) {
+        if (!P.needs_tune) return S2_OK;
+        const bool prof_was = profiling;
+        s2_status r = set_profiling(true);
+        if (r != S2_OK) return r;
+        static const int cand[3] = {9, 21, 63};
+        float best_ms = 0.0f;
+        int best = 0;
+        Plan T;
+        for (int c : cand) {
+            force_strip = c;
+            r = plan(d, n, T, ex);
+            if (r == S2_OK) r = enqueue(T, st);
+            if (r == S2_OK) r = wait();
+            float ms[3] = {0, 0, 0};
+            if (r == S2_OK) r = timings(ms);
+            if (r != S2_OK) break;
+            if (!best || ms[1] < best_ms) best_ms = ms[1], best = c;
+        }
+        force_strip = 0;
+        profiling = prof_was;
+        if (r != S2_OK) return r;
+        s2_set_tuned_strip(P.tune_sig, best);
+        return plan(d, n, P, ex);
     }
 };

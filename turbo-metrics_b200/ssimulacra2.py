@@ -96,6 +96,10 @@ class Ssimulacra2:
         s._bound = (src_ref_linear, src_dis_linear)
         return s
 
+    def set_graphs(self, enable=True):
+        """Replay computes of a seen shape as CUDA graphs (default on)."""
+        check(lib.s2_set_graphs(self._h, 1 if enable else 0), "set_graphs")
+
     def close(self):
         if getattr(self, "_h", None) and lib is not None:
             lib.s2_destroy(self._h)
@@ -293,6 +297,10 @@ class Ssim2Batch:
         self._keep = pairs
         check(lib.s2_batch_submit(self._h, arr, len(pairs), _stream_ptr(stream)), "compute_batch")
         self._n = len(pairs)
+
+    def set_graphs(self, enable=True):
+        """Replay submissions of a seen shape as CUDA graphs (default on)."""
+        check(lib.s2_batch_set_graphs(self._h, 1 if enable else 0), "set_graphs")
 
     def submit_host(self, pairs, stream=None):
         """Pairs whose planes are in host memory (CPU tensors, pinned for
