@@ -110,3 +110,31 @@ def test_host_batch_rejects_short_pitch(tmb, cuda):
     short = np.lib.stride_tricks.as_strided(r, shape=r.shape, strides=(64 * 3 - 3, 3, 1))
     with pytest.raises(tmb.DimensionMismatch):
         b.submit_host([tmb.PairDesc(short, d, "srgb8")])
+
+
+def test_two_host_submissions_in_flight(tmb, cuda):
+    """Submission k+1 enqueued before k's results are read (the uploads and
+    preps of k+1 overlap k's tile pass): results come back oldest first and
+    equal the device-input batch's; a third submission with both slots
+    pending drops the oldest one's results."""
+    a = make_pairs(9, 9500)
+    b = make_pairs(6, 9600)
+    c = make_pairs(4, 9700)
+    dev_b = tmb.Ssim2Batch(32, 8 << 20)
+    want = [dev_b.compute_batch([device_desc(tmb, cuda, p) for p in x]) for x in (a, b, c)]
+    bt = tmb.Ssim2Batch(32, 8 << 20)
+    ha, hb, hc = ([host_desc(tmb, cuda, p, True) for p in x] for x in (a, b, c))
+    bt.submit_host(ha)
+    bt.submit_host(hb)
+    got_a = bt.results()
+    bt.submit_host(hc)
+    got_b = bt.results()
+    got_c = bt.results()
+    for got, w in ((got_a, want[0]), (got_b, want[1]), (got_c, want[2])):
+        assert [g[0] for g in got] == [x[0] for x in w]
+    # three in flight: the first one's results are dropped, the other two come back in order
+    bt.submit_host(ha)
+    bt.submit_host(hb)
+    bt.submit_host(hc)
+    assert [g[0] for g in bt.results()] == [x[0] for x in want[1]]
+    assert [g[0] for g in bt.results()] == [x[0] for x in want[2]]

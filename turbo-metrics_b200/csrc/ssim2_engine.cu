@@ -15,6 +15,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <deque>
 #include <mutex>
 #include <string>
 #include <unordered_map>
@@ -242,11 +243,45 @@ struct s2_ctx {
     Plan plan;
 };
 
+// A batch has two submission slots (engines with their own workspaces), so a
+// caller may enqueue submission k+1 before reading submission k's results:
+// k+1's uploads and preps then overlap k's tile pass.  Device-input
+// submissions use slot 0; host-input submissions take a slot whose results
+// are not pending (slot 1 is allocated on first such use).  Results are read
+// oldest first.
 struct s2_batch {
-    Engine eng;
+    Engine eng[2];
+    bool ready[2] = {false, false};
+    Plan plan[2];
+    std::deque<int> unread;  // slots whose results were not read, oldest first
+    int last_slot = 0;
+    bool profiling = false, graphs = true;
+    s2_config cfg;
     uint32_t max_pairs = 0;
     uint64_t max_pixels = 0;
-    Plan plan;
+
+    s2_status open_slot(int k) {
+        if (ready[k]) return S2_OK;
+        s2_status st = eng[k].init(&cfg);
+        if (st == S2_OK) st = eng[k].reserve(max_pairs, max_pixels, false);
+        if (st == S2_OK) st = eng[k].set_profiling(profiling);
+        if (st != S2_OK) {
+            eng[k].release();
+            return st;
+        }
+        eng[k].graphs = graphs;
+        ready[k] = true;
+        return S2_OK;
+    }
+    // the slot for the next submission; a slot whose results are pending is
+    // reused only when both are (its results are then dropped)
+    int take_slot(bool host) {
+        auto pending = [&](int k) { return std::find(unread.begin(), unread.end(), k) != unread.end(); };
+        int k = 0;
+        if (host && pending(0)) k = pending(1) ? unread.front() : 1;
+        unread.erase(std::remove(unread.begin(), unread.end(), k), unread.end());
+        return k;
+    }
 };
 
 extern "C" {
@@ -601,13 +636,9 @@ s2_status s2_batch_create(const s2_config *cfg_in, uint32_t max_pairs, uint64_t 
     if (!b) return S2_ERR_OOM;
     b->max_pairs = max_pairs;
     b->max_pixels = max_pixels;
-    st = b->eng.init(&cfg);
-    b->eng.graphs = true;
-    if (st == S2_OK) {
-        st = b->eng.reserve(max_pairs, max_pixels, false);
-    }
+    b->cfg = cfg;
+    st = b->open_slot(0);
     if (st != S2_OK) {
-        b->eng.release();
         delete b;
         return st;
     }
@@ -617,17 +648,23 @@ s2_status s2_batch_create(const s2_config *cfg_in, uint32_t max_pairs, uint64_t 
 
 void s2_batch_destroy(s2_batch *b) {
     if (!b) return;
-    b->eng.release();
+    for (int k = 0; k < 2; k++)
+        if (b->ready[k]) b->eng[k].release();
     delete b;
 }
 
 s2_status s2_batch_submit(s2_batch *b, const s2_pair_desc *pairs, uint32_t n, void *stream) {
     if (!b || (!pairs && n)) return S2_ERR_INVALID_ARG;
     if (n > b->max_pairs) return S2_ERR_INVALID_ARG;
-    s2_status st = b->eng.plan(pairs, (int)n, b->plan);
-    if (st == S2_OK) st = b->eng.tune(pairs, (int)n, b->plan, nullptr, (cudaStream_t)stream);
+    const int k = b->take_slot(false);
+    Engine &e = b->eng[k];
+    s2_status st = e.plan(pairs, (int)n, b->plan[k]);
+    if (st == S2_OK) st = e.tune(pairs, (int)n, b->plan[k], nullptr, (cudaStream_t)stream);
+    if (st == S2_OK) st = e.enqueue(b->plan[k], (cudaStream_t)stream);
     if (st != S2_OK) return st;
-    return b->eng.enqueue(b->plan, (cudaStream_t)stream);
+    b->unread.push_back(k);
+    b->last_slot = k;
+    return S2_OK;
 }
 
 s2_status s2_batch_submit_host(s2_batch *b, const s2_pair_desc *pairs, uint32_t n, void *stream) {
@@ -637,20 +674,33 @@ s2_status s2_batch_submit_host(s2_batch *b, const s2_pair_desc *pairs, uint32_t 
         const size_t row = s2_row_bytes(pairs[i]);
         if (pairs[i].ref_pitch < row || pairs[i].dis_pitch < row) return S2_ERR_DIM_MISMATCH;
     }
-    // S2_BLUR_IIR_REF runs its two passes over all pairs at once: one group
-    const int ng = b->eng.blur == S2_BLUR_IIR_REF ? 1 : std::min<int>(kMaxGroups, std::max<int>(1, (int)n / 4));
-    s2_status st = b->eng.plan(pairs, (int)n, b->plan, nullptr, ng);
+    const int k = b->take_slot(true);
+    s2_status st = b->open_slot(k);
     if (st != S2_OK) return st;
-    return b->eng.enqueue(b->plan, (cudaStream_t)stream, pairs);
+    Engine &e = b->eng[k];
+    // S2_BLUR_IIR_REF runs its two passes over all pairs at once: one group
+    const int ng = e.blur == S2_BLUR_IIR_REF ? 1 : std::min<int>(kMaxGroups, std::max<int>(1, (int)n / 4));
+    st = e.plan(pairs, (int)n, b->plan[k], nullptr, ng);
+    if (st == S2_OK) st = e.enqueue(b->plan[k], (cudaStream_t)stream, pairs);
+    if (st != S2_OK) return st;
+    b->unread.push_back(k);
+    b->last_slot = k;
+    return S2_OK;
 }
 
 s2_status s2_batch_results(s2_batch *b, s2_result *out, uint32_t n) {
     if (!b || (!out && n)) return S2_ERR_INVALID_ARG;
-    s2_status st = b->eng.wait();
+    int k = b->last_slot;  // no unread submission: the last one again
+    if (!b->unread.empty()) {
+        k = b->unread.front();
+        b->unread.pop_front();
+    }
+    Engine &e = b->eng[k];
+    s2_status st = e.wait();
     if (st != S2_OK) return st;
-    if ((int)n > b->eng.last_n) return S2_ERR_INVALID_ARG;
+    if ((int)n > e.last_n) return S2_ERR_INVALID_ARG;
     for (uint32_t i = 0; i < n; i++) {
-        const DevResult &r = b->eng.results_h[i];
+        const DevResult &r = e.results_h[i];
         out[i].score = r.score;
         memcpy(out[i].stats, r.stats, sizeof r.stats);
         memcpy(out[i].sums, r.sums, sizeof r.sums);
@@ -662,18 +712,24 @@ s2_status s2_batch_results(s2_batch *b, s2_result *out, uint32_t n) {
 
 s2_status s2_batch_mem_usage(const s2_batch *b, size_t *bytes) {
     if (!b || !bytes) return S2_ERR_INVALID_ARG;
-    *bytes = b->eng.allocated;
+    *bytes = b->eng[0].allocated + (b->ready[1] ? b->eng[1].allocated : 0);
     return S2_OK;
 }
 
 s2_status s2_batch_set_profiling(s2_batch *b, int32_t enable) {
     if (!b) return S2_ERR_INVALID_ARG;
-    return b->eng.set_profiling(enable != 0);
+    b->profiling = enable != 0;
+    for (int k = 0; k < 2; k++)
+        if (b->ready[k]) {
+            const s2_status st = b->eng[k].set_profiling(b->profiling);
+            if (st != S2_OK) return st;
+        }
+    return S2_OK;
 }
 
 s2_status s2_batch_last_timings(s2_batch *b, float ms[3]) {
     if (!b || !ms) return S2_ERR_INVALID_ARG;
-    return b->eng.timings(ms);
+    return b->eng[b->last_slot].timings(ms);
 }
 
 s2_status s2_profile_enable(s2_ctx *ctx, int32_t enable) {
@@ -690,8 +746,12 @@ int32_t s2_fused_blocks_per_sm(int32_t storage) { return s2_global_init() == S2_
 
 s2_status s2_batch_set_graphs(s2_batch *b, int32_t enable) {
     if (!b) return S2_ERR_INVALID_ARG;
-    b->eng.graphs = enable != 0;
-    if (!b->eng.graphs) b->eng.drop_graphs();
+    b->graphs = enable != 0;
+    for (int k = 0; k < 2; k++)
+        if (b->ready[k]) {
+            b->eng[k].graphs = b->graphs;
+            if (!b->graphs) b->eng[k].drop_graphs();
+        }
     return S2_OK;
 }
 

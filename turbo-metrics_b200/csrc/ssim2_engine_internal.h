@@ -596,17 +596,20 @@ struct Engine {
                 return S2_OK;
             }
         }
-        S2_CUDA(cudaMemcpyAsync(dbase, h, pb + bb + sb + vsb + hsb, cudaMemcpyHostToDevice, st));
-        S2_CUDA(cudaMemsetAsync(counter_d.p, 0, ng * sizeof(int), st));
-        if (profiling) S2_CUDA(cudaEventRecord(prof[0], st));
-        // uploads wait until the previous host submission's prep has read the
-        // staging; preps wait for this submission's descriptors
+        // Host submissions: the copy stream first waits until the previous
+        // host submission's prep has read the staging, then uploads the
+        // descriptors ahead of the planes, so preps (on the prep stream)
+        // depend on copies only and may run beside another submission's tile
+        // pass; the tile passes and finalize stay in order on `st`.
         const bool split = host && blur != S2_BLUR_IIR_REF;
         if (host) S2_CUDA(cudaStreamWaitEvent(copy_st, stage_free, 0));
+        S2_CUDA(cudaMemcpyAsync(dbase, h, pb + bb + sb + vsb + hsb, cudaMemcpyHostToDevice, split ? copy_st : st));
         if (split) {
-            S2_CUDA(cudaEventRecord(sub_start, st));
-            S2_CUDA(cudaStreamWaitEvent(prep_st, sub_start, 0));
+            S2_CUDA(cudaEventRecord(sub_start, copy_st));
+            S2_CUDA(cudaStreamWaitEvent(st, sub_start, 0));
         }
+        S2_CUDA(cudaMemsetAsync(counter_d.p, 0, ng * sizeof(int), st));
+        if (profiling) S2_CUDA(cudaEventRecord(prof[0], st));
         cudaStream_t pst = split ? prep_st : st;
         for (int g = 0; g < ng; g++) {
             const int pa = P.grp_pair[g], pe = P.grp_pair[g + 1];

@@ -14,6 +14,7 @@ Images on the device are torch CUDA tensors:
 or `(pointer, pitch_bytes)` tuples.  Host images are numpy arrays of the
 same shapes.
 """
+import collections
 import ctypes
 
 import numpy as np
@@ -279,8 +280,20 @@ class Ssim2Batch:
         check(lib.s2_batch_create(ctypes.byref(cfg), max_pairs, max_pixels, ctypes.byref(h)), "Ssim2Batch::new")
         self._h = h
         self.max_pairs = max_pairs
-        self._n = 0
-        self._keep = None
+        # submissions whose results were not read, oldest first: (slot, n,
+        # pairs kept alive) -- the same slot rule as s2_batch (two slots;
+        # device submissions use slot 0, host ones a slot without pending
+        # results)
+        self._unread = collections.deque()
+        self._last = (0, 0, None)
+
+    def _take_slot(self, host):
+        pending = [u[0] for u in self._unread]
+        k = 0
+        if host and 0 in pending:
+            k = self._unread[0][0] if 1 in pending else 1
+        self._unread = collections.deque(u for u in self._unread if u[0] != k)
+        return k
 
     def close(self):
         if getattr(self, "_h", None) and lib is not None:
@@ -294,9 +307,10 @@ class Ssim2Batch:
         arr = (capi.PairDescC * max(len(pairs), 1))()
         for i, p in enumerate(pairs):
             arr[i] = p.to_c()
-        self._keep = pairs
+        k = self._take_slot(False)
         check(lib.s2_batch_submit(self._h, arr, len(pairs), _stream_ptr(stream)), "compute_batch")
-        self._n = len(pairs)
+        self._last = (k, len(pairs), pairs)
+        self._unread.append(self._last)
 
     def set_graphs(self, enable=True):
         """Replay submissions of a seen shape as CUDA graphs (default on)."""
@@ -306,19 +320,24 @@ class Ssim2Batch:
         """Pairs whose planes are in host memory (CPU tensors, pinned for
         overlap, or numpy arrays): uploaded in groups that overlap the compute
         of earlier groups.  Keep the arrays alive and unchanged until
-        `results()` returns."""
+        `results()` returns.  A second host submission may be made before
+        reading the first one's results: its uploads and preps then overlap
+        the first one's tile pass (results are read oldest first)."""
         arr = (capi.PairDescC * max(len(pairs), 1))()
         for i, p in enumerate(pairs):
             arr[i] = p.to_c(host=True)
-        self._keep = pairs
+        k = self._take_slot(True)
         check(lib.s2_batch_submit_host(self._h, arr, len(pairs), _stream_ptr(stream)), "compute_batch_host")
-        self._n = len(pairs)
+        self._last = (k, len(pairs), pairs)
+        self._unread.append(self._last)
 
     def results(self):
-        out = (capi.Result * max(self._n, 1))()
-        check(lib.s2_batch_results(self._h, out, self._n), "results")
+        """Results of the oldest submission not read yet (else the last one)."""
+        _, n, _ = self._unread.popleft() if self._unread else self._last
+        out = (capi.Result * max(n, 1))()
+        check(lib.s2_batch_results(self._h, out, n), "results")
         return [(r.score, np.array(r.stats[:]), np.array(r.sums[:]), r.n_scales, r.status)
-                for r in out[:self._n]]
+                for r in out[:n]]
 
     def compute_batch(self, pairs, stream=None):
         self.submit(pairs, stream)
