@@ -215,7 +215,13 @@ s2_status s2_batch_submit(s2_batch *b, const s2_pair_desc *pairs, uint32_t n, vo
  * goes on.  The host planes must stay unchanged until s2_batch_results
  * returns.  S2_ERR_DIM_MISMATCH if a pitch is below the row's bytes. */
 s2_status s2_batch_submit_host(s2_batch *b, const s2_pair_desc *pairs, uint32_t n, void *stream);
-/* Wait for the last submission and copy its n results. */
+/* Wait for the oldest submission whose results were not read yet (else the
+ * last one again) and copy its n results.  A batch has two submission
+ * slots: device-input submissions use the first; a host-input submission
+ * takes a slot without pending results, so submission k+1 may be enqueued
+ * before submission k's results are read (its uploads and preps overlap k's
+ * tile pass).  With both slots pending, a new host submission drops the
+ * older one's results. */
 s2_status s2_batch_results(s2_batch *b, s2_result *out, uint32_t n);
 s2_status s2_batch_mem_usage(const s2_batch *b, size_t *bytes);
 /* CUDA graphs (1 = on, the default): the operations of a device-input
