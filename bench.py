@@ -146,6 +146,55 @@ def serve_bucket_images(i):
     return ref, [synth.srgb_pair(w, h, seed, st)[1] for st in steps]
 
 
+def c2_pair(i):
+    import synth
+    return synth.c2_pair(i)
+
+
+def uneven_bench(tmb, n=256, steps=3):
+    """Uneven-size batch: n sRGB8 pairs with width and height each uniform in
+    [64, 2048], scored (a) as one submission -- one prep, one persistent tile
+    launch over every (pair, scale, tile, channel), one finalize, the tile
+    height autotuned -- and (b) as a chain of one-pair submissions, the way a
+    per-size instance scores them one at a time."""
+    import multiprocessing as mp
+    import torch
+    with mp.get_context("spawn").Pool(os.cpu_count() or 1) as pool:
+        raw = pool.map(c2_pair, range(n))
+    dev = [(torch.from_numpy(r).cuda(), torch.from_numpy(d).cuda()) for r, d in raw]
+    descs = [tmb.PairDesc(r, d, "srgb8") for r, d in dev]
+    px = sum(r.shape[0] * r.shape[1] for r, _ in raw)
+    stream = torch.cuda.current_stream()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    batch = tmb.Ssim2Batch(n, px)
+    for _ in range(2):
+        batched = batch.compute_batch(descs)  # the first one also tunes the tile height
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(steps):
+        batch.submit(descs)
+        batched = batch.results()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    batched_ms = ev0.elapsed_time(ev1) / steps
+    one = tmb.Ssim2Batch(1, max(r.shape[0] * r.shape[1] for r, _ in raw))
+    chain = [one.compute_batch([d])[0] for d in descs]  # warm-up: graphs and tuning per size class
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    chain = [one.compute_batch([d])[0] for d in descs]
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    chain_ms = ev0.elapsed_time(ev1)
+    worst = max(abs(a[0] - b[0]) for a, b in zip(batched, chain))
+    assert worst < 1e-9, "batched and per-pair scores differ by %g" % worst
+    batch.close()
+    one.close()
+    return {"pairs": n, "megapixels": px / 1e6, "sizes": "W, H uniform in [64, 2048], sRGB8 (C0 content)",
+            "batched_ms": batched_ms, "batched_pairs_per_s": n / (batched_ms / 1e3),
+            "per_pair_chain_ms": chain_ms, "per_pair_chain_pairs_per_s": n / (chain_ms / 1e3),
+            "batched_vs_chain": chain_ms / batched_ms, "max_score_diff": worst}
+
+
 def serving_bench(tmb, rates=(200, 1000, 5000), jobs_per_rate=(800, 1500, 1500)):
     """Serving workload: Poisson arrivals at each offered rate, sizes
     log-uniform between 128x128 and ~3840x2160, 1..16 candidates per job,
@@ -278,6 +327,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--plain-pairs", type=int, default=64)
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--no-uneven", action="store_true", help="skip the 256-pair uneven-size batch leg")
     ap.add_argument("--pairs", type=int, default=N_PAIRS,
                     help="pairs per step (64 is the workload; smaller only for profiler captures)")
     args = ap.parse_args()
@@ -420,6 +470,9 @@ def main():
     served = None
     if not args.no_serving:
         served = serving_bench(tmb)
+    uneven = None
+    if not args.no_uneven and world == 1:
+        uneven = uneven_bench(tmb)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -441,6 +494,7 @@ def main():
             "clocks": clocks.summary(),
             "cpu_baseline": cpu,
             "served": served,
+            "uneven": uneven,
             "score_mean": float(np.mean(scores)),
         }
         print(json.dumps(line), flush=True)
