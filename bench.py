@@ -195,7 +195,7 @@ def uneven_bench(tmb, n=256, steps=3):
             "batched_vs_chain": chain_ms / batched_ms, "max_score_diff": worst}
 
 
-def serving_bench(tmb, rates=(200, 1000, 5000), jobs_per_rate=(800, 1500, 1500)):
+def serving_bench(tmb, rates=(200, 1000, 5000), jobs_per_rate=(800, 1500, 1500), server_kw=None):
     """Serving workload: Poisson arrivals at each offered rate, sizes
     log-uniform between 128x128 and ~3840x2160, 1..16 candidates per job,
     40 GB admission budget; latency = arrival -> all candidates scored."""
@@ -210,7 +210,9 @@ def serving_bench(tmb, rates=(200, 1000, 5000), jobs_per_rate=(800, 1500, 1500))
     out = {"pool": "%d sizes x (1 reference + %d candidates), pinned host memory" % (SERVE_BUCKETS, SERVE_VARIANTS)}
     for rate, n in zip(rates, jobs_per_rate):
         jobs = synth.c4_jobs(n, rate, seed_index=rate)
-        sv = tmb.Ssim2Server(hbm_budget=40 << 30)
+        kw = dict(hbm_budget=40 << 30)
+        kw.update(server_kw or {})
+        sv = tmb.Ssim2Server(**kw)
         # warm-up: one job per bucket
         for ref, cands in buckets:
             sv.wait(sv.submit(ref, cands[:1]))
@@ -236,7 +238,8 @@ def serving_bench(tmb, rates=(200, 1000, 5000), jobs_per_rate=(800, 1500, 1500))
                                  "max_ms": rep["max_ms"], "rounds": rep["rounds"], "wall_s": wall,
                                  "gpu_busy_s": rep["gpu_busy_s"], "worker_wait_s": rep["worker_wait_s"],
                                  "worker_upload_s": rep["worker_upload_s"],
-                                 "worker_submit_s": rep["worker_submit_s"]}
+                                 "worker_submit_s": rep["worker_submit_s"], "copy_busy_s": rep["copy_busy_s"],
+                                 "upload_gb": rep["bytes_uploaded"] / 1e9}
     return out
 
 

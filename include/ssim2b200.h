@@ -273,6 +273,8 @@ typedef struct {
     double worker_wait_s;            /* worker time blocked on finished rounds */
     double worker_upload_s;          /* worker time issuing uploads */
     double worker_submit_s;          /* worker time planning and enqueueing rounds */
+    double copy_busy_s;              /* copy-stream time of finished jobs' uploads (CUDA events) */
+    uint64_t bytes_uploaded;         /* host -> device bytes of finished jobs */
 } s2_server_report;
 
 typedef struct s2_server s2_server;

@@ -100,7 +100,8 @@ class ServerReport(ctypes.Structure):
                 ("queued_jobs", ctypes.c_uint64), ("hbm_in_use", ctypes.c_uint64), ("p50_ms", ctypes.c_double),
                 ("p99_ms", ctypes.c_double), ("max_ms", ctypes.c_double), ("uptime_s", ctypes.c_double),
                 ("gpu_busy_s", ctypes.c_double), ("worker_wait_s", ctypes.c_double),
-                ("worker_upload_s", ctypes.c_double), ("worker_submit_s", ctypes.c_double)]
+                ("worker_upload_s", ctypes.c_double), ("worker_submit_s", ctypes.c_double),
+                ("copy_busy_s", ctypes.c_double), ("bytes_uploaded", ctypes.c_uint64)]
 
 
 P = ctypes.c_void_p

@@ -58,7 +58,7 @@ struct Job {
     size_t ref_levels_off = 0;
     size_t lvl_off[s2::kScales] = {0, 0, 0, 0, 0, 0};
     int ns = 0;
-    cudaEvent_t uploaded = nullptr;
+    cudaEvent_t uploaded = nullptr, up_start = nullptr;  // the job's uploads on the copy stream
     bool admitted = false, uploading = false, ref_scheduled = false, cancelled = false, finished = false;
     int next_cand = 0, inflight = 0, harvested = 0;
     std::vector<double> scores;
@@ -92,6 +92,8 @@ struct s2_server {
     uint64_t pairs_done = 0, jobs_done = 0, rounds = 0;
     double gpu_ms = 0.0;  // device time of the rounds' kernels (CUDA events)
     double t_wait = 0.0, t_upload = 0.0, t_submit = 0.0;  // worker time: GPU waits, upload issue, plan+enqueue
+    double copy_ms = 0.0;                                  // copy-stream time of finished jobs' uploads
+    uint64_t bytes_uploaded = 0;
     Clock::time_point t0;
 
     std::vector<RoundEntry> round[2];
@@ -135,12 +137,13 @@ struct s2_server {
     s2_status upload(const std::vector<Job *> &fresh) {
         for (Job *j : fresh) {
             const size_t img = (size_t)j->w * 3 * j->h, row = (size_t)j->w * 3;
+            if (cudaEventCreate(&j->up_start) != cudaSuccess || cudaEventRecord(j->up_start, copy) != cudaSuccess)
+                return S2_ERR_CUDA;
             if (copy_image(j->dev, j->ref_host, j->ref_pitch, row, j->h) != cudaSuccess) return S2_ERR_CUDA;
             for (size_t c = 0; c < j->cand_host.size(); c++)
                 if (copy_image(j->dev + img * (1 + c), j->cand_host[c], j->cand_pitch, row, j->h) != cudaSuccess)
                     return S2_ERR_CUDA;
-            if (cudaEventCreateWithFlags(&j->uploaded, cudaEventDisableTiming) != cudaSuccess ||
-                cudaEventRecord(j->uploaded, copy) != cudaSuccess)
+            if (cudaEventCreate(&j->uploaded) != cudaSuccess || cudaEventRecord(j->uploaded, copy) != cudaSuccess)
                 return S2_ERR_CUDA;
         }
         std::lock_guard<std::mutex> lock(mu);
@@ -245,10 +248,18 @@ struct s2_server {
             }
             for (Job *j : completed) {
                 bytes_in_use -= j->bytes;
-                cudaFreeAsync(j->dev, compute);
+                // freed on the copy stream, where later jobs' memory is
+                // allocated: the rounds that read it are complete (this
+                // harvest waited for them), so reuse needs no wait on the
+                // compute stream, whose queue already holds the next round
+                cudaFreeAsync(j->dev, copy);
                 j->dev = nullptr;
+                float ms = 0.0f;
+                if (cudaEventElapsedTime(&ms, j->up_start, j->uploaded) == cudaSuccess) copy_ms += ms;
+                bytes_uploaded += (uint64_t)j->w * 3 * j->h * (1 + j->cand_host.size());
                 cudaEventDestroy(j->uploaded);
-                j->uploaded = nullptr;
+                cudaEventDestroy(j->up_start);
+                j->uploaded = j->up_start = nullptr;
             }
         }
         round[k].clear();
@@ -355,6 +366,11 @@ s2_status s2_server_create(const s2_server_config *cfg_in, s2_server **out) {
     if (st == S2_OK) {
         uint64_t keep = cfg.hbm_budget ? cfg.hbm_budget : ~0ull;
         cudaMemPoolSetAttribute(sv->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        // Job memory is allocated and freed on the copy stream; a block is
+        // never reused through a wait on another stream (which would queue
+        // new uploads behind a round of kernels)
+        int no = 0;
+        cudaMemPoolSetAttribute(sv->pool, cudaMemPoolReuseAllowInternalDependencies, &no);
     }
     if (st != S2_OK) {
         for (int k = 0; k < 2; k++) sv->eng[k].release();
@@ -498,6 +514,8 @@ s2_status s2_server_stats(s2_server *sv, s2_server_report *out) {
     out->worker_wait_s = sv->t_wait;
     out->worker_upload_s = sv->t_upload;
     out->worker_submit_s = sv->t_submit;
+    out->copy_busy_s = sv->copy_ms / 1e3;
+    out->bytes_uploaded = sv->bytes_uploaded;
     return S2_OK;
 }
 
@@ -508,6 +526,8 @@ s2_status s2_server_reset_stats(s2_server *sv) {
     sv->pairs_done = sv->jobs_done = sv->rounds = 0;
     sv->gpu_ms = 0.0;
     sv->t_wait = sv->t_upload = sv->t_submit = 0.0;
+    sv->copy_ms = 0.0;
+    sv->bytes_uploaded = 0;
     sv->t0 = Clock::now();
     return S2_OK;
 }
