@@ -162,6 +162,12 @@ struct Engine {
     // every graph.  Captured on an engine-owned stream, launched on the
     // caller's.
     bool graphs = false;
+    // Descriptor upload by a kernel reading the page-locked staging through
+    // its device mapping instead of a copy-engine memcpy (the server: its copy
+    // stream keeps the H2D engine busy with job images, and a small memcpy on
+    // the compute stream would wait behind them).
+    bool desc_kernel = false;
+    void *pinned_dev = nullptr;  // device address of the pinned staging
     struct GraphEntry {
         uint64_t key[7];
         cudaGraphExec_t exec;
@@ -288,7 +294,8 @@ struct Engine {
             }
             pinned = nullptr;
             bytes = s2_align_up(bytes, 4096);
-            S2_CUDA(cudaMallocHost(&pinned, bytes));
+            S2_CUDA(cudaHostAlloc(&pinned, bytes, cudaHostAllocMapped));
+            S2_CUDA(cudaHostGetDevicePointer(&pinned_dev, pinned, 0));
             pinned_n = bytes;
         }
         if (results_cap < nres) {
@@ -603,7 +610,10 @@ struct Engine {
         // pass; the tile passes and finalize stay in order on `st`.
         const bool split = host && blur != S2_BLUR_IIR_REF;
         if (host) S2_CUDA(cudaStreamWaitEvent(copy_st, stage_free, 0));
-        S2_CUDA(cudaMemcpyAsync(dbase, h, pb + bb + sb + vsb + hsb, cudaMemcpyHostToDevice, split ? copy_st : st));
+        if (desc_kernel && !split)
+            S2_CUDA(launch_desc_copy(dbase, pinned_dev, pb + bb + sb + vsb + hsb, st));
+        else
+            S2_CUDA(cudaMemcpyAsync(dbase, h, pb + bb + sb + vsb + hsb, cudaMemcpyHostToDevice, split ? copy_st : st));
         if (split) {
             S2_CUDA(cudaEventRecord(sub_start, copy_st));
             S2_CUDA(cudaStreamWaitEvent(st, sub_start, 0));
@@ -682,7 +692,8 @@ struct Engine {
             graphs = false;
             return nullptr;
         }
-        cudaError_t e = cudaMemcpyAsync(dbase, pinned, desc_bytes, cudaMemcpyHostToDevice, cap_st);
+        cudaError_t e = desc_kernel ? launch_desc_copy(dbase, pinned_dev, desc_bytes, cap_st)
+                                    : cudaMemcpyAsync(dbase, pinned, desc_bytes, cudaMemcpyHostToDevice, cap_st);
         if (e == cudaSuccess) e = cudaMemsetAsync(counter_d.p, 0, sizeof(int), cap_st);
         if (e == cudaSuccess)
             e = launch_pyramid(storage, dpairs, n, (const int *)(dbase + pb), 0, P.total_blocks, cc,

@@ -691,6 +691,20 @@ cudaError_t launch_fused(int storage, const DevPair *pairs, const Seg *segs, int
     return cudaGetLastError();
 }
 
+// Device copy of the submission descriptors from page-locked host memory
+// (read through the host mapping), 16 bytes per thread.
+__global__ void __launch_bounds__(256) desc_copy_kernel(uint4 *__restrict__ dst, const uint4 *__restrict__ src, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) dst[i] = src[i];
+}
+
+cudaError_t launch_desc_copy(void *dst, const void *src_host_mapped, size_t bytes, cudaStream_t st) {
+    const int n = (int)(bytes / 16);
+    if (n <= 0) return cudaSuccess;
+    const int grid = n < 256 * 64 ? (n + 255) / 256 : 64;
+    desc_copy_kernel<<<grid, 256, 0, st>>>((uint4 *)dst, (const uint4 *)src_host_mapped, n);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_finalize(const DevPair *pairs, int npairs, const double *partials, DevResult *out,
                             cudaStream_t st) {
     if (npairs <= 0) return cudaSuccess;

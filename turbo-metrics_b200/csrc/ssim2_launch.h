@@ -19,6 +19,10 @@ cudaError_t launch_fused(int storage, const DevPair *pairs, const Seg *segs, int
                          int *counter, double *partials, int grid, cudaStream_t st);
 cudaError_t launch_iir(int storage, const DevPair *pairs, const IirSeg *vsegs, int nvseg, int vtotal,
                        const IirSeg *hsegs, int nhseg, int htotal, double *partials, cudaStream_t st);
+// Copy `bytes` (a multiple of 16, both pointers 16-byte aligned) from
+// page-locked host memory, through its device mapping, with a kernel: no copy
+// engine, so the copy is not queued behind other streams' large uploads.
+cudaError_t launch_desc_copy(void *dst, const void *src_host_mapped, size_t bytes, cudaStream_t st);
 cudaError_t launch_finalize(const DevPair *pairs, int npairs, const double *partials, DevResult *out,
                             cudaStream_t st);
 }  // namespace s2

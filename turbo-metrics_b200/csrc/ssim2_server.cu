@@ -10,8 +10,10 @@
 //   admission   jobs enter in arrival order while the device bytes they need
 //               (inputs + the reference's XYB pyramid) fit the HBM budget; the
 //               head of the queue is never overtaken (no starvation);
-//   upload      admitted jobs' host images go up on a copy stream, from a
-//               dedicated stream-ordered memory pool;
+//   upload      an uploader thread admits jobs and sends their host images up
+//               on a copy stream, into a stream-ordered memory pool grown to
+//               the budget at creation (no mapping on the serving path), so
+//               the round loop never waits for admission or upload issue;
 //   batching    each round takes, in arrival order, every admitted job's
 //               pending work -- the reference pyramid build (once per job) and
 //               candidates -- up to a pair / pixel cap, and runs it as one
@@ -78,9 +80,10 @@ struct s2_server {
     Engine eng[2];
     cudaStream_t compute = nullptr, copy = nullptr;
     cudaMemPool_t pool = nullptr;
-    std::thread worker;
+    std::thread worker, uploader;
     std::mutex mu;
-    std::condition_variable cv_work, cv_done;
+    std::condition_variable cv_work, cv_done, cv_up;
+    bool uploader_done = false;
     std::deque<Job *> queue;  // arrival order: not yet admitted, then admitted
     std::unordered_map<uint64_t, Job *> jobs;
     uint64_t next_id = 1;
@@ -132,6 +135,44 @@ struct s2_server {
     cudaError_t copy_image(unsigned char *dst, const uint8_t *src, size_t pitch, size_t row, uint32_t rows) {
         if (pitch == row) return cudaMemcpyAsync(dst, src, row * rows, cudaMemcpyHostToDevice, copy);
         return cudaMemcpy2DAsync(dst, row, src, pitch, row, rows, cudaMemcpyHostToDevice, copy);
+    }
+
+    // Uploader thread: admit in arrival order while the budget allows, send
+    // the admitted jobs' images up, hand them to the round loop.
+    void upload_loop() {
+        std::vector<Job *> fresh;
+        for (;;) {
+            fresh.clear();
+            {
+                std::unique_lock<std::mutex> lock(mu);
+                if (stop) break;
+                admit_locked(fresh);
+                if (fresh.empty()) {
+                    cv_up.wait_for(lock, std::chrono::milliseconds(1));
+                    continue;
+                }
+            }
+            const auto ta = Clock::now();
+            const s2_status up = upload(fresh);
+            {
+                std::lock_guard<std::mutex> lock(mu);
+                t_upload += std::chrono::duration<double>(Clock::now() - ta).count();
+                if (up != S2_OK) {
+                    fatal = S2_ERR_CUDA;
+                    stop = true;
+                }
+            }
+            cv_work.notify_all();
+            if (up != S2_OK) {
+                cv_done.notify_all();
+                break;
+            }
+        }
+        {
+            std::lock_guard<std::mutex> lock(mu);
+            uploader_done = true;
+        }
+        cv_work.notify_all();
     }
 
     s2_status upload(const std::vector<Job *> &fresh) {
@@ -264,33 +305,22 @@ struct s2_server {
         }
         round[k].clear();
         inflight[k] = false;
-        if (!completed.empty()) cv_done.notify_all();
+        if (!completed.empty()) {
+            cv_done.notify_all();
+            cv_up.notify_one();  // budget freed
+        }
     }
 
+    // Round loop (worker thread): build a round from uploaded jobs, enqueue
+    // it, harvest the previous one.
     void run() {
         int cur = 0;
-        std::vector<Job *> fresh;
         for (;;) {
-            fresh.clear();
-            {
-                std::lock_guard<std::mutex> lock(mu);
-                admit_locked(fresh);
-            }
-            const auto ta = Clock::now();
-            const s2_status up = fresh.empty() ? S2_OK : upload(fresh);
-            t_upload += std::chrono::duration<double>(Clock::now() - ta).count();
-            if (up != S2_OK) {
-                std::lock_guard<std::mutex> lock(mu);
-                fatal = S2_ERR_CUDA;
-                stop = true;
-                cv_done.notify_all();
-                break;
-            }
             {
                 std::unique_lock<std::mutex> lock(mu);
                 build_round_locked(round[cur]);
                 if (round[cur].empty() && !inflight[cur ^ 1]) {
-                    if (stop) break;
+                    if (stop && uploader_done) break;
                     cv_work.wait_for(lock, std::chrono::milliseconds(2));
                     continue;
                 }
@@ -300,11 +330,14 @@ struct s2_server {
                 s2_status st = submit_round(cur);
                 t_submit += std::chrono::duration<double>(Clock::now() - tb).count();
                 if (st != S2_OK) {
-                    std::lock_guard<std::mutex> lock(mu);
-                    fatal = st;
-                    for (Job *j : queue) j->job_status = st;
-                    stop = true;
+                    {
+                        std::lock_guard<std::mutex> lock(mu);
+                        fatal = st;
+                        for (Job *j : queue) j->job_status = st;
+                        stop = true;
+                    }
                     cv_done.notify_all();
+                    cv_up.notify_all();
                     break;
                 }
                 inflight[cur] = true;
@@ -353,6 +386,7 @@ s2_status s2_server_create(const s2_server_config *cfg_in, s2_server **out) {
     s2_status st = S2_OK;
     for (int k = 0; k < 2 && st == S2_OK; k++) st = sv->eng[k].init(&ec);
     for (int k = 0; k < 2 && st == S2_OK; k++) st = sv->eng[k].set_profiling(true);
+    for (int k = 0; k < 2; k++) sv->eng[k].desc_kernel = true;
     for (int k = 0; k < 2 && st == S2_OK; k++) st = sv->eng[k].reserve(cfg.max_batch_pairs, cfg.max_batch_pixels, true);
     cudaMemPoolProps props;
     memset(&props, 0, sizeof props);
@@ -371,6 +405,18 @@ s2_status s2_server_create(const s2_server_config *cfg_in, s2_server **out) {
         // new uploads behind a round of kernels)
         int no = 0;
         cudaMemPoolSetAttribute(sv->pool, cudaMemPoolReuseAllowInternalDependencies, &no);
+        // Grow the pool to the budget once, here: growing it while serving
+        // maps memory on the admission path (measured: 0.6 s of stalls while
+        // a burst of jobs was admitted).  Without a budget, or when the
+        // device cannot hold it, the pool grows on demand instead.
+        if (cfg.hbm_budget > sv->workspace_bytes()) {
+            void *p = nullptr;
+            if (cudaMallocFromPoolAsync(&p, cfg.hbm_budget - sv->workspace_bytes(), sv->pool, sv->copy) == cudaSuccess) {
+                cudaFreeAsync(p, sv->copy);
+                cudaStreamSynchronize(sv->copy);
+            }
+            cudaGetLastError();
+        }
     }
     if (st != S2_OK) {
         for (int k = 0; k < 2; k++) sv->eng[k].release();
@@ -381,6 +427,10 @@ s2_status s2_server_create(const s2_server_config *cfg_in, s2_server **out) {
     sv->worker = std::thread([sv] {
         cudaSetDevice(sv->cfg.device);
         sv->run();
+    });
+    sv->uploader = std::thread([sv] {
+        cudaSetDevice(sv->cfg.device);
+        sv->upload_loop();
     });
     *out = sv;
     return S2_OK;
@@ -395,6 +445,8 @@ void s2_server_destroy(s2_server *sv) {
             if (!j->admitted) j->cancelled = true;
     }
     sv->cv_work.notify_all();
+    sv->cv_up.notify_all();
+    if (sv->uploader.joinable()) sv->uploader.join();
     if (sv->worker.joinable()) sv->worker.join();
     cudaSetDevice(sv->cfg.device);
     cudaStreamSynchronize(sv->compute);
@@ -447,7 +499,7 @@ s2_status s2_server_submit(s2_server *sv, const s2_job_desc *jd, uint64_t *job_i
     sv->queue.push_back(j);
     sv->jobs[j->id] = j;
     *job_id = j->id;
-    sv->cv_work.notify_all();
+    sv->cv_up.notify_one();
     return S2_OK;
 }
 
