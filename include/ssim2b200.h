@@ -76,9 +76,12 @@ enum {
     S2_SCALES_ALL6 = 2  /* ssimulacra2-cuda (lib.rs:138-143): always 6 */
 };
 
-/* NV12 matrix / range selectors. */
-enum { S2_MATRIX_BT709 = 0 };
-enum { S2_RANGE_LIMITED = 0 };
+/* 4:2:0 YUV matrix / range selectors (cuda-colorspace/src/lib.rs:9-20 ColorMatrix;
+ * cuda-colorspace-kernel/src/lib.rs:46-140 Full / Limited).  The reference
+ * implements limited range only (full range is todo!()); full range here
+ * follows its Full definition (0 .. 2^N - 1, chroma neutral 2^(N-1)). */
+enum { S2_MATRIX_BT709 = 0, S2_MATRIX_BT601_525 = 1, S2_MATRIX_BT601_625 = 2 };
+enum { S2_RANGE_LIMITED = 0, S2_RANGE_FULL = 1 };
 
 typedef struct {
     uint32_t struct_size;  /* sizeof(s2_config) */
@@ -138,10 +141,18 @@ s2_status s2_compute_linear_f32(s2_ctx *ctx, const float *ref, size_t ref_pitch,
 s2_status s2_compute_srgb8(s2_ctx *ctx, const uint8_t *ref, size_t ref_pitch,
                            const uint8_t *dis, size_t dis_pitch, int32_t on_host,
                            void *stream);
-/* NV12 pair (cuda-colorspace biplanaryuv420_to_linearrgb_8_l_bt709 followed
- * by Ssimulacra2::compute; cuda-colorspace/src/lib.rs:33-51), conversion fused. */
+/* NV12 pair (cuda-colorspace biplanaryuv420_to_linearrgb_8_{l}_{bt709,
+ * bt601_525,bt601_625} followed by Ssimulacra2::compute; cuda-colorspace/src/
+ * lib.rs:33-82), conversion fused.  matrix S2_MATRIX_*, range S2_RANGE_*. */
 s2_status s2_compute_nv12(s2_ctx *ctx, const uint8_t *ref_y, const uint8_t *ref_uv,
                           size_t ref_pitch, const uint8_t *dis_y, const uint8_t *dis_uv,
+                          size_t dis_pitch, int32_t matrix, int32_t range, int32_t on_host,
+                          void *stream);
+/* P016 pair: 16-bit samples in both planes (P010 / P012 data, left-aligned,
+ * is read the same way), as biplanaryuv420_to_linearrgb_16_* (cuda-colorspace/
+ * src/lib.rs:84-131).  Pitch in bytes. */
+s2_status s2_compute_p016(s2_ctx *ctx, const uint16_t *ref_y, const uint16_t *ref_uv,
+                          size_t ref_pitch, const uint16_t *dis_y, const uint16_t *dis_uv,
                           size_t dis_pitch, int32_t matrix, int32_t range, int32_t on_host,
                           void *stream);
 /* 10/12-bit BT.2020 RGB pair (no reference counterpart: the reference has no
@@ -183,7 +194,13 @@ int32_t s2_has_reference(const s2_ctx *ctx);
  * mixed sizes: all pairs of a submission run as one pyramid launch, one
  * persistent tile launch over every (pair, scale, strip) and one finalize
  * launch.  Pairs are sRGB8 or linear f32 or NV12, on the device. */
-typedef enum { S2_FMT_LINEAR_F32 = 0, S2_FMT_SRGB8 = 1, S2_FMT_NV12 = 2, S2_FMT_RGB16 = 3 } s2_format;
+typedef enum {
+    S2_FMT_LINEAR_F32 = 0,
+    S2_FMT_SRGB8 = 1,
+    S2_FMT_NV12 = 2,  /* 4:2:0 biplanar, 8-bit samples */
+    S2_FMT_RGB16 = 3,
+    S2_FMT_P016 = 4   /* 4:2:0 biplanar, 16-bit samples */
+} s2_format;
 
 typedef struct {
     uint32_t width, height;
@@ -192,6 +209,7 @@ typedef struct {
     const void *ref, *dis;   /* packed image, or NV12 Y plane */
     const void *ref_uv, *dis_uv; /* NV12 CbCr planes */
     size_t ref_pitch, dis_pitch;
+    int32_t matrix, range;   /* NV12 / P016: S2_MATRIX_*, S2_RANGE_* (0, 0 = BT.709 limited) */
 } s2_pair_desc;
 
 typedef struct s2_batch s2_batch;

@@ -102,6 +102,29 @@ def nv12_to_linear(y, uv, f64=False):
     return out
 
 
+MATRIX = {"bt709": 0, "bt601_525": 1, "bt601_625": 2}
+
+
+def yuv420_to_linear(y, uv, matrix="bt709", full=False, f64=False):
+    """4:2:0 biplanar YUV -> linear RGB: uint8 planes (NV12) or uint16 planes
+    (P016); y (H, W), uv (H/2, W) interleaved CbCr."""
+    bits = 8 if y.dtype == np.uint8 else 16
+    y = np.ascontiguousarray(y)
+    uv = np.ascontiguousarray(uv, y.dtype)
+    h, w = y.shape
+    assert uv.shape == (h // 2, w)
+    pitch = ctypes.c_size_t(w * y.itemsize)
+    args = (y.ctypes.data_as(ctypes.c_void_p), uv.ctypes.data_as(ctypes.c_void_p), pitch, w, h, bits,
+            MATRIX[matrix], 1 if full else 0)
+    if f64:
+        out = np.empty((h, w, 3), np.float64)
+        _lib.or_yuv420_to_linear_f64(*args, _d(out))
+    else:
+        out = np.empty((h, w, 3), np.float32)
+        _lib.or_yuv420_to_linear(*args, _f(out))
+    return out
+
+
 def rgb16_to_linear(img, bits=10, f64=False):
     a = np.ascontiguousarray(img, np.uint16)
     n = a.size // 3

@@ -243,32 +243,56 @@ static float bt709_eotf_f32(float v) {
 static float clamp01f(float v) { return v < 0.0f ? 0.0f : (v > 1.0f ? 1.0f : v); }
 static double clamp01(double v) { return v < 0.0 ? 0.0 : (v > 1.0 ? 1.0 : v); }
 
-/* Coefficients of cuda-colorspace-kernel/src/lib.rs:188-203 for 8-bit limited
- * range: luma range 219, chroma range 224. */
-static void nv12_coeffs(double c[5]) {
+/* Primaries and white of the YUV matrices (cuda-colorspace-kernel/src/
+ * constants.rs): BT.709, BT.601-525 (SMPTE C), BT.601-625 (EBU), D65. */
+static const double BT601_525_PRIM[8] = {0.630, 0.340, 0.310, 0.595, 0.155, 0.070, 0.3127, 0.3290};
+static const double BT601_625_PRIM[8] = {0.640, 0.330, 0.290, 0.600, 0.150, 0.060, 0.3127, 0.3290};
+
+/* Coefficients of cuda-colorspace-kernel/src/lib.rs:188-203 for a matrix
+ * (0 BT.709, 1 BT.601-525, 2 BT.601-625), range (0 limited, 1 full) and
+ * sample depth (8 or 16 bits): luma and chroma ranges, the luma minimum and
+ * the chroma neutral value of lib.rs:46-140 (limited: 16<<(N-8), 235<<(N-8),
+ * 240<<(N-8); full: 0, 2^N - 1; neutral 2^(N-1)). */
+static void yuv_coeffs(int matrix, int full, int bits, double c[5], int *ymin, int *neutral) {
+    const double *prim = matrix == 1 ? BT601_525_PRIM : (matrix == 2 ? BT601_625_PRIM : BT709_PRIM);
     double kr, kb;
-    kr_kb_from_primaries(BT709_PRIM, &kr, &kb);
-    double kg = 1.0 - kr - kb;
-    c[0] = 1.0 / 219.0;
-    c[1] = 2.0 * (1.0 - kr) / 224.0;
-    c[2] = 2.0 * (1.0 - kb) / 224.0;
-    c[3] = -2.0 * (1.0 - kb) * kb / kg / 224.0;
-    c[4] = -2.0 * (1.0 - kr) * kr / kg / 224.0;
+    kr_kb_from_primaries(prim, &kr, &kb);
+    const double kg = 1.0 - kr - kb;
+    const int sh = bits - 8;
+    const double lrange = full ? (double)((1 << bits) - 1) : (double)((235 - 16) << sh);
+    const double crange = full ? (double)((1 << bits) - 1) : (double)((240 - 16) << sh);
+    c[0] = 1.0 / lrange;
+    c[1] = 2.0 * (1.0 - kr) / crange;
+    c[2] = 2.0 * (1.0 - kb) / crange;
+    c[3] = -2.0 * (1.0 - kb) * kb / kg / crange;
+    c[4] = -2.0 * (1.0 - kr) * kr / kg / crange;
+    *ymin = full ? 0 : (16 << sh);
+    *neutral = 1 << (bits - 1);
 }
 
-void or_nv12_to_linear(const uint8_t *yp, const uint8_t *uvp, size_t pitch, int w,
-                       int h, float *dst) {
+static inline int yuv_sample(const void *p, size_t byte_off, int bits) {
+    return bits == 8 ? ((const uint8_t *)p)[byte_off] : *(const uint16_t *)((const uint8_t *)p + byte_off);
+}
+
+/* 4:2:0 biplanar YUV (NV12 8-bit, P016 16-bit samples) -> linear RGB in the
+ * engine's f32 arithmetic (cuda-colorspace-kernel/src/biplanar.rs:8-70:
+ * nearest chroma, luma floored at the range minimum, BT.709 inverse OETF,
+ * clamp to [0, 1]).  pitch in bytes, shared by both planes. */
+void or_yuv420_to_linear(const void *yp, const void *uvp, size_t pitch, int w, int h, int bits, int matrix,
+                         int full, float *dst) {
     double cd[5];
-    nv12_coeffs(cd);
-    float yc = (float)cd[0], rc = (float)cd[1], bc = (float)cd[2], g1 = (float)cd[3],
-          g2 = (float)cd[4];
+    int ymin, neutral;
+    yuv_coeffs(matrix, full, bits, cd, &ymin, &neutral);
+    const int es = bits == 8 ? 1 : 2;
+    float yc = (float)cd[0], rc = (float)cd[1], bc = (float)cd[2], g1 = (float)cd[3], g2 = (float)cd[4];
     for (int y = 0; y < h; y++) {
         for (int x = 0; x < w; x++) {
-            const uint8_t *uv = uvp + (size_t)(y / 2) * pitch + 2 * (x / 2);
-            float cb = (float)((int)uv[0] - 128), cr = (float)((int)uv[1] - 128);
+            const size_t uvo = (size_t)(y / 2) * pitch + (size_t)es * 2 * (x / 2);
+            float cb = (float)(yuv_sample(uvp, uvo, bits) - neutral);
+            float cr = (float)(yuv_sample(uvp, uvo + es, bits) - neutral);
             float r_ = rc * cr, g_ = fmaf(g1, cb, g2 * cr), b_ = bc * cb;
-            int Y = yp[(size_t)y * pitch + x];
-            float luma = (float)((Y < 16 ? 16 : Y) - 16) * yc;
+            int Y = yuv_sample(yp, (size_t)y * pitch + (size_t)es * x, bits);
+            float luma = (float)((Y < ymin ? ymin : Y) - ymin) * yc;
             float *o = dst + ((size_t)y * w + x) * 3;
             o[0] = clamp01f(bt709_eotf_f32(luma + r_));
             o[1] = clamp01f(bt709_eotf_f32(luma + g_));
@@ -277,22 +301,33 @@ void or_nv12_to_linear(const uint8_t *yp, const uint8_t *uvp, size_t pitch, int 
     }
 }
 
-void or_nv12_to_linear_f64(const uint8_t *yp, const uint8_t *uvp, size_t pitch, int w,
-                           int h, double *dst) {
+void or_yuv420_to_linear_f64(const void *yp, const void *uvp, size_t pitch, int w, int h, int bits, int matrix,
+                             int full, double *dst) {
     double c[5];
-    nv12_coeffs(c);
+    int ymin, neutral;
+    yuv_coeffs(matrix, full, bits, c, &ymin, &neutral);
+    const int es = bits == 8 ? 1 : 2;
     for (int y = 0; y < h; y++) {
         for (int x = 0; x < w; x++) {
-            const uint8_t *uv = uvp + (size_t)(y / 2) * pitch + 2 * (x / 2);
-            double cb = (double)((int)uv[0] - 128), cr = (double)((int)uv[1] - 128);
-            int Y = yp[(size_t)y * pitch + x];
-            double luma = (double)((Y < 16 ? 16 : Y) - 16) * c[0];
+            const size_t uvo = (size_t)(y / 2) * pitch + (size_t)es * 2 * (x / 2);
+            double cb = (double)(yuv_sample(uvp, uvo, bits) - neutral);
+            double cr = (double)(yuv_sample(uvp, uvo + es, bits) - neutral);
+            int Y = yuv_sample(yp, (size_t)y * pitch + (size_t)es * x, bits);
+            double luma = (double)((Y < ymin ? ymin : Y) - ymin) * c[0];
             double *o = dst + ((size_t)y * w + x) * 3;
             o[0] = clamp01(bt709_eotf_f64(luma + c[1] * cr));
             o[1] = clamp01(bt709_eotf_f64(luma + c[3] * cb + c[4] * cr));
             o[2] = clamp01(bt709_eotf_f64(luma + c[2] * cb));
         }
     }
+}
+
+void or_nv12_to_linear(const uint8_t *yp, const uint8_t *uvp, size_t pitch, int w, int h, float *dst) {
+    or_yuv420_to_linear(yp, uvp, pitch, w, h, 8, 0, 0, dst);
+}
+
+void or_nv12_to_linear_f64(const uint8_t *yp, const uint8_t *uvp, size_t pitch, int w, int h, double *dst) {
+    or_yuv420_to_linear_f64(yp, uvp, pitch, w, h, 8, 0, 0, dst);
 }
 
 /* Linear BT.2020 RGB -> linear BT.709 RGB, derived from the published

@@ -65,6 +65,12 @@ void or_srgb8_lut(float lut[256]);
 void or_srgb8_to_linear(const uint8_t *src, size_t n_samples, float *dst);
 void or_srgb8_to_linear_f64(const uint8_t *src, size_t n_samples, double *dst);
 /* NV12, 8 bit, BT.709 matrix, limited range, nearest 2x2 chroma. */
+/* 4:2:0 biplanar YUV: bits 8 (NV12) or 16 (P016), matrix 0 BT.709 / 1 BT.601-525 /
+ * 2 BT.601-625, full 0 limited / 1 full range; pitch in bytes. */
+void or_yuv420_to_linear(const void *y, const void *uv, size_t pitch, int w, int h, int bits, int matrix,
+                         int full, float *dst);
+void or_yuv420_to_linear_f64(const void *y, const void *uv, size_t pitch, int w, int h, int bits, int matrix,
+                             int full, double *dst);
 void or_nv12_to_linear(const uint8_t *y, const uint8_t *uv, size_t pitch,
                        int w, int h, float *dst);
 void or_nv12_to_linear_f64(const uint8_t *y, const uint8_t *uv, size_t pitch,

@@ -29,7 +29,9 @@ S2_ERR_CANCELLED = 10
 BLUR = {"fir": 0, "iir_ref": 1}
 STORAGE = {"f32": 0, "f16": 1, "bf16": 2}
 SCALE_RULE = {"cpu": 0, "min8": 1, "all6": 2}
-FMT = {"linear_f32": 0, "srgb8": 1, "nv12": 2, "rgb16": 3}
+FMT = {"linear_f32": 0, "srgb8": 1, "nv12": 2, "rgb16": 3, "p016": 4}
+MATRIX = {"bt709": 0, "bt601_525": 1, "bt601_625": 2}
+RANGE = {"limited": 0, "full": 1}
 
 
 class S2Error(RuntimeError):
@@ -80,7 +82,7 @@ class PairDescC(ctypes.Structure):
     _fields_ = [("width", ctypes.c_uint32), ("height", ctypes.c_uint32), ("format", ctypes.c_int32),
                 ("bits", ctypes.c_int32), ("ref", ctypes.c_void_p), ("dis", ctypes.c_void_p),
                 ("ref_uv", ctypes.c_void_p), ("dis_uv", ctypes.c_void_p), ("ref_pitch", ctypes.c_size_t),
-                ("dis_pitch", ctypes.c_size_t)]
+                ("dis_pitch", ctypes.c_size_t), ("matrix", ctypes.c_int32), ("range", ctypes.c_int32)]
 
 
 class ServerConfig(ctypes.Structure):
@@ -119,6 +121,8 @@ _sig = {
     "s2_compute_linear_f32": (ctypes.c_int, [P, P, ctypes.c_size_t, P, ctypes.c_size_t, P]),
     "s2_compute_srgb8": (ctypes.c_int, [P, P, ctypes.c_size_t, P, ctypes.c_size_t, ctypes.c_int32, P]),
     "s2_compute_nv12": (ctypes.c_int, [P, P, P, ctypes.c_size_t, P, P, ctypes.c_size_t, ctypes.c_int32,
+                                       ctypes.c_int32, ctypes.c_int32, P]),
+    "s2_compute_p016": (ctypes.c_int, [P, P, P, ctypes.c_size_t, P, P, ctypes.c_size_t, ctypes.c_int32,
                                        ctypes.c_int32, ctypes.c_int32, P]),
     "s2_compute_rgb16": (ctypes.c_int, [P, P, ctypes.c_size_t, P, ctypes.c_size_t, ctypes.c_int32,
                                         ctypes.c_int32, P]),

@@ -5,6 +5,7 @@
 // compiled with -fmad=false, so every rounding step is the one written here
 // (the CPU restatement of the same arithmetic reproduces it).
 #pragma once
+#include <type_traits>
 
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
@@ -23,7 +24,7 @@ constexpr int kChunk = 4;            // pixels per f32 partial sum
 constexpr int kPyrBlk = 64;          // scale-0 block edge of the prep kernel
 constexpr float kC2 = 0.0009f;
 
-enum Format { FMT_LINEAR_F32 = 0, FMT_SRGB8 = 1, FMT_NV12 = 2, FMT_RGB16 = 3 };
+enum Format { FMT_LINEAR_F32 = 0, FMT_SRGB8 = 1, FMT_NV12 = 2, FMT_RGB16 = 3, FMT_P016 = 4 };
 enum Storage { ST_F32 = 0, ST_F16 = 1, ST_BF16 = 2 };
 
 // FIR taps of the exact form of the recursive Gaussian (sigma 1.5, N = 5),
@@ -51,6 +52,11 @@ struct DevPair {
     int blk_x, blk_y;        // pyramid blocks of this pair
     int status;
     int prep_mask;           // images the prep pass converts: bit 0 reference, bit 1 distorted
+    // 4:2:0 YUV (NV12 / P016): y_coeff, r_coeff, b_coeff, g_coeff1, g_coeff2
+    // of the pair's matrix, range and depth, the luma minimum and the chroma
+    // neutral value (cuda-colorspace-kernel/src/lib.rs:46-203)
+    float yuv[5];
+    int yuv_min, yuv_neutral;
     int lvl_ext;             // images whose XYB planes live outside the submission (bit per image)
 };
 
@@ -346,8 +352,6 @@ __device__ __forceinline__ void xyb_pair_unit(float2 r, float2 g, float2 b, floa
 }
 
 struct ColorConsts {
-    // NV12 BT.709 limited range: y_coeff, r_coeff, b_coeff, g_coeff1, g_coeff2
-    float nv12[5];
     // BT.2020 -> BT.709 linear matrix (row-major)
     float m2020[9];
 };
@@ -384,8 +388,8 @@ __device__ __forceinline__ void rgb16_linear(unsigned r, unsigned g, unsigned b,
                                              float o[3]);
 
 // Linear RGB of scale-0 pixel (x, y) of image img (inside the image), for
-// input format FMT.  sRGB8: the reference table; NV12: BT.709 limited range,
-// nearest 2x2 chroma (cuda-colorspace-kernel/src/biplanar.rs:8-70); RGB16:
+// input format FMT (the packed formats; 4:2:0 YUV goes by whole quads,
+// yuv_load_quad / yuv_quad_linear).  sRGB8: the reference table; RGB16:
 // BT.709/BT.2020 inverse OETF, then BT.2020 -> BT.709 primaries, clamped >= 0.
 template <int FMT>
 __device__ __forceinline__ void lin_pixel(const DevPair &P, int img, int x, int y, const float *lut,
@@ -401,58 +405,62 @@ __device__ __forceinline__ void lin_pixel(const DevPair &P, int img, int x, int 
         o[0] = lut[__ldg(q)];
         o[1] = lut[__ldg(q + 1)];
         o[2] = lut[__ldg(q + 2)];
-    } else if (FMT == FMT_NV12) {
-        const int Y = __ldg((const uint8_t *)base + x);
-        const uint8_t *uv = (const uint8_t *)P.in_uv[img] + (long long)(y >> 1) * P.pitch[img] + 2 * (x >> 1);
-        const float cb = (float)((int)__ldg(uv) - 128);
-        const float cr = (float)((int)__ldg(uv + 1) - 128);
-        const float luma = (float)(max(Y, 16) - 16) * cc.nv12[0];
-        o[0] = fminf(fmaxf(bt709_eotf(luma + cc.nv12[1] * cr), 0.0f), 1.0f);
-        o[1] = fminf(fmaxf(bt709_eotf(luma + fmaf(cc.nv12[3], cb, cc.nv12[4] * cr)), 0.0f), 1.0f);
-        o[2] = fminf(fmaxf(bt709_eotf(luma + cc.nv12[2] * cb), 0.0f), 1.0f);
     } else {
         const uint16_t *q = (const uint16_t *)base + 3 * x;
         rgb16_linear(__ldg(q), __ldg(q + 1), __ldg(q + 2), 1.0f / (float)((1 << P.bits) - 1), cc, o);
     }
 }
 
-// The six samples of an NV12 quad (x, y even): luma of rows y and y + 1 and
-// the shared CbCr pair, read as 16-bit words when the plane base and pitch
-// are even (always for the engine's own staging), else as bytes.
+// The six samples of a 4:2:0 quad (x, y even): luma of rows y and y + 1 and
+// the shared CbCr pair, two samples per word (low half = left sample / Cb).
+// ES = bytes per sample (1 NV12, 2 P016); read as one word per pair when the
+// plane bases and the pitch are aligned to it (always for the engine's own
+// staging), else sample by sample.
 struct Nv12Quad {
-    unsigned y0, y1, uv;  // low byte = left / Cb, high byte = right / Cr
+    unsigned y0, y1, uv;
 };
-__device__ __forceinline__ Nv12Quad nv12_load_quad(const DevPair &P, int img, int x, int y) {
-    const uint8_t *yp = (const uint8_t *)P.in[img] + (long long)y * P.pitch[img] + x;
-    const uint8_t *uv = (const uint8_t *)P.in_uv[img] + (long long)(y >> 1) * P.pitch[img] + x;
+template <int ES>
+__device__ __forceinline__ Nv12Quad yuv_load_quad(const DevPair &P, int img, int x, int y) {
+    using W = typename std::conditional<ES == 1, unsigned short, unsigned>::type;
+    using S = typename std::conditional<ES == 1, uint8_t, uint16_t>::type;
+    const char *yp = (const char *)P.in[img] + (long long)y * P.pitch[img] + ES * x;
+    const char *uv = (const char *)P.in_uv[img] + (long long)(y >> 1) * P.pitch[img] + ES * x;
     Nv12Quad q;
-    if ((((unsigned long long)P.in[img] | (unsigned long long)P.in_uv[img] | (unsigned long long)P.pitch[img]) & 1) == 0) {
-        q.y0 = __ldg((const unsigned short *)yp);
-        q.y1 = __ldg((const unsigned short *)(yp + P.pitch[img]));
-        q.uv = __ldg((const unsigned short *)uv);
+    if ((((unsigned long long)P.in[img] | (unsigned long long)P.in_uv[img] | (unsigned long long)P.pitch[img]) &
+         (2 * ES - 1)) == 0) {
+        q.y0 = __ldg((const W *)yp);
+        q.y1 = __ldg((const W *)(yp + P.pitch[img]));
+        q.uv = __ldg((const W *)uv);
     } else {
-        q.y0 = __ldg(yp) | ((unsigned)__ldg(yp + 1) << 8);
-        q.y1 = __ldg(yp + P.pitch[img]) | ((unsigned)__ldg(yp + P.pitch[img] + 1) << 8);
-        q.uv = __ldg(uv) | ((unsigned)__ldg(uv + 1) << 8);
+        const S *a = (const S *)yp, *b = (const S *)(yp + P.pitch[img]), *c = (const S *)uv;
+        q.y0 = (unsigned)__ldg(a) | ((unsigned)__ldg(a + 1) << (8 * ES));
+        q.y1 = (unsigned)__ldg(b) | ((unsigned)__ldg(b + 1) << (8 * ES));
+        q.uv = (unsigned)__ldg(c) | ((unsigned)__ldg(c + 1) << (8 * ES));
     }
     return q;
 }
 
-// BT.709 limited range (cuda-colorspace-kernel/src/biplanar.rs:8-70, nearest
-// chroma) of a loaded quad: pixels (0, 1) and (2, 3) as f32x2 lanes.
-__device__ __forceinline__ void nv12_quad_linear(const Nv12Quad &q, const ColorConsts &cc, float o[4][3]) {
-    const float cb = (float)((int)(q.uv & 0xffu) - 128);
-    const float cr = (float)((int)(q.uv >> 8) - 128);
-    const float ar = cc.nv12[1] * cr;
-    const float ag = fmaf(cc.nv12[3], cb, cc.nv12[4] * cr);
-    const float ab = cc.nv12[2] * cb;
+// Limited / full range YUV of the pair's matrix (cuda-colorspace-kernel/src/
+// biplanar.rs:8-70: nearest chroma, luma floored at the range minimum, BT.709
+// inverse OETF, clamp to [0, 1]) of a loaded quad: pixels (0, 1) and (2, 3)
+// as f32x2 lanes.
+template <int ES>
+__device__ __forceinline__ void yuv_quad_linear(const Nv12Quad &q, const DevPair &P, float o[4][3]) {
+    constexpr unsigned kMask = ES == 1 ? 0xffu : 0xffffu;
+    constexpr int kShift = 8 * ES;
+    const float cb = (float)((int)(q.uv & kMask) - P.yuv_neutral);
+    const float cr = (float)((int)(q.uv >> kShift) - P.yuv_neutral);
+    const float ar = P.yuv[1] * cr;
+    const float ag = fmaf(P.yuv[3], cb, P.yuv[4] * cr);
+    const float ab = P.yuv[2] * cb;
+    const int ymin = P.yuv_min;
+    const float yc = P.yuv[0];
 #pragma unroll
     for (int row = 0; row < 2; row++) {
         const unsigned w = row ? q.y1 : q.y0;
-        const int Y0 = (int)(w & 0xffu), Y1 = (int)(w >> 8);
+        const int Y0 = (int)(w & kMask), Y1 = (int)(w >> kShift);
         // scalar products: luma is summed with the chroma terms below
-        const float2 luma = make_float2((float)(max(Y0, 16) - 16) * cc.nv12[0],
-                                        (float)(max(Y1, 16) - 16) * cc.nv12[0]);
+        const float2 luma = make_float2((float)(max(Y0, ymin) - ymin) * yc, (float)(max(Y1, ymin) - ymin) * yc);
         const float2 r = bt709_eotf2(s2_add2(luma, s2_f2(ar)));
         const float2 g = bt709_eotf2(s2_add2(luma, s2_f2(ag)));
         const float2 b = bt709_eotf2(s2_add2(luma, s2_f2(ab)));
@@ -472,10 +480,10 @@ __device__ __forceinline__ void nv12_quad_linear(const Nv12Quad &q, const ColorC
 template <int FMT>
 __device__ __forceinline__ void lin_quad(const DevPair &P, int img, int x, int y, bool vx, bool vy,
                                          const float *lut, const ColorConsts &cc, float o[4][3]) {
-    if (FMT == FMT_NV12) {
-        // NV12 has even width and height: the quad is complete
-        const Nv12Quad q = nv12_load_quad(P, img, x, y);
-        nv12_quad_linear(q, cc, o);
+    if (FMT == FMT_NV12 || FMT == FMT_P016) {
+        // 4:2:0 input has even width and height: the quad is complete
+        constexpr int ES = FMT == FMT_NV12 ? 1 : 2;
+        yuv_quad_linear<ES>(yuv_load_quad<ES>(P, img, x, y), P, o);
     } else {
         // a complete quad whose rows are aligned for the format's word size is
         // read as three words per row: sRGB8 16-bit, RGB16 32-bit, linear f32

@@ -112,17 +112,32 @@ static void inv3(const double m[9], double o[9]) {
     o[8] = (m[0] * m[4] - m[1] * m[3]) / d;
 }
 
+static const double BT709[8] = {0.640, 0.330, 0.300, 0.600, 0.150, 0.060, 0.3127, 0.3290};
+static const double BT601_525[8] = {0.630, 0.340, 0.310, 0.595, 0.155, 0.070, 0.3127, 0.3290};
+static const double BT601_625[8] = {0.640, 0.330, 0.290, 0.600, 0.150, 0.060, 0.3127, 0.3290};
+
+// 4:2:0 YUV coefficients (cuda-colorspace-kernel/src/lib.rs:188-203) of a
+// matrix (primaries of constants.rs), range and sample depth, with the
+// range's luma minimum and chroma neutral value (lib.rs:46-140).
+void s2_yuv_coeffs(int matrix, int range, int bits, float out[5], int *ymin, int *neutral) {
+    const double *prim = matrix == S2_MATRIX_BT601_525 ? BT601_525 : (matrix == S2_MATRIX_BT601_625 ? BT601_625 : BT709);
+    double kr, kb;
+    kr_kb_from_primaries(prim, &kr, &kb);
+    const double kg = 1.0 - kr - kb;
+    const bool full = range == S2_RANGE_FULL;
+    const int sh = bits - 8;
+    const double lrange = full ? (double)((1 << bits) - 1) : (double)((235 - 16) << sh);
+    const double crange = full ? (double)((1 << bits) - 1) : (double)((240 - 16) << sh);
+    const double c[5] = {1.0 / lrange, 2.0 * (1.0 - kr) / crange, 2.0 * (1.0 - kb) / crange,
+                         -2.0 * (1.0 - kb) * kb / kg / crange, -2.0 * (1.0 - kr) * kr / kg / crange};
+    for (int i = 0; i < 5; i++) out[i] = (float)c[i];
+    *ymin = full ? 0 : (16 << sh);
+    *neutral = 1 << (bits - 1);
+}
+
 ColorConsts s2_make_color_consts() {
-    static const double BT709[8] = {0.640, 0.330, 0.300, 0.600, 0.150, 0.060, 0.3127, 0.3290};
     static const double BT2020[8] = {0.708, 0.292, 0.170, 0.797, 0.131, 0.046, 0.3127, 0.3290};
     ColorConsts cc;
-    double kr, kb;
-    kr_kb_from_primaries(BT709, &kr, &kb);
-    double kg = 1.0 - kr - kb;
-    // cuda-colorspace-kernel/src/lib.rs:188-203, 8-bit limited range
-    double c[5] = {1.0 / 219.0, 2.0 * (1.0 - kr) / 224.0, 2.0 * (1.0 - kb) / 224.0,
-                   -2.0 * (1.0 - kb) * kb / kg / 224.0, -2.0 * (1.0 - kr) * kr / kg / 224.0};
-    for (int i = 0; i < 5; i++) cc.nv12[i] = (float)c[i];
     double a[9], b[9], bi[9];
     rgb_to_xyz(BT2020, a);
     rgb_to_xyz(BT709, b);
@@ -471,26 +486,45 @@ s2_status s2_compute_srgb8(s2_ctx *ctx, const uint8_t *ref, size_t ref_pitch, co
     return ctx_run(ctx, make_desc(ctx->w, ctx->h, S2_FMT_SRGB8, r, rp, d, dp), stream);
 }
 
-s2_status s2_compute_nv12(s2_ctx *ctx, const uint8_t *ref_y, const uint8_t *ref_uv, size_t ref_pitch,
-                          const uint8_t *dis_y, const uint8_t *dis_uv, size_t dis_pitch, int32_t matrix,
-                          int32_t range, int32_t on_host, void *stream) {
+// 4:2:0 biplanar pair (NV12 / P016) through the single-pair context.
+static s2_status ctx_yuv420(s2_ctx *ctx, int fmt, const void *ref_y, const void *ref_uv, size_t ref_pitch,
+                            const void *dis_y, const void *dis_uv, size_t dis_pitch, int32_t matrix, int32_t range,
+                            int32_t on_host, void *stream) {
     if (!ctx || !ref_y || !ref_uv || !dis_y || !dis_uv) return S2_ERR_INVALID_ARG;
-    if (matrix != S2_MATRIX_BT709 || range != S2_RANGE_LIMITED) return S2_ERR_INVALID_ARG;
+    if (matrix < S2_MATRIX_BT709 || matrix > S2_MATRIX_BT601_625 || (range != S2_RANGE_LIMITED && range != S2_RANGE_FULL))
+        return S2_ERR_INVALID_ARG;
     if ((ctx->w & 1) || (ctx->h & 1)) return S2_ERR_INVALID_SIZE;
-    if (ref_pitch < ctx->w || dis_pitch < ctx->w) return S2_ERR_DIM_MISMATCH;
+    const size_t row = (size_t)ctx->w * (fmt == S2_FMT_P016 ? 2 : 1);
+    if (ref_pitch < row || dis_pitch < row) return S2_ERR_DIM_MISMATCH;
     const void *ry = ref_y, *ru = ref_uv, *dy = dis_y, *du = dis_uv;
     size_t rp = ref_pitch, dp = dis_pitch, tmp;
     if (on_host) {
-        s2_status st = stage_host(ctx, 0, ref_y, ref_pitch, ctx->w, ctx->h, stream, &ry, &rp);
-        if (st == S2_OK) st = stage_host(ctx, 1, dis_y, dis_pitch, ctx->w, ctx->h, stream, &dy, &dp);
-        if (st == S2_OK) st = stage_host(ctx, 2, ref_uv, ref_pitch, ctx->w, ctx->h / 2, stream, &ru, &tmp);
-        if (st == S2_OK) st = stage_host(ctx, 3, dis_uv, dis_pitch, ctx->w, ctx->h / 2, stream, &du, &tmp);
+        s2_status st = stage_host(ctx, 0, ref_y, ref_pitch, row, ctx->h, stream, &ry, &rp);
+        if (st == S2_OK) st = stage_host(ctx, 1, dis_y, dis_pitch, row, ctx->h, stream, &dy, &dp);
+        if (st == S2_OK) st = stage_host(ctx, 2, ref_uv, ref_pitch, row, ctx->h / 2, stream, &ru, &tmp);
+        if (st == S2_OK) st = stage_host(ctx, 3, dis_uv, dis_pitch, row, ctx->h / 2, stream, &du, &tmp);
         if (st != S2_OK) return st;
     }
-    s2_pair_desc d = make_desc(ctx->w, ctx->h, S2_FMT_NV12, ry, rp, dy, dp);
+    s2_pair_desc d = make_desc(ctx->w, ctx->h, fmt, ry, rp, dy, dp);
     d.ref_uv = ru;
     d.dis_uv = du;
+    d.matrix = matrix;
+    d.range = range;
     return ctx_run(ctx, d, stream);
+}
+
+s2_status s2_compute_nv12(s2_ctx *ctx, const uint8_t *ref_y, const uint8_t *ref_uv, size_t ref_pitch,
+                          const uint8_t *dis_y, const uint8_t *dis_uv, size_t dis_pitch, int32_t matrix,
+                          int32_t range, int32_t on_host, void *stream) {
+    return ctx_yuv420(ctx, S2_FMT_NV12, ref_y, ref_uv, ref_pitch, dis_y, dis_uv, dis_pitch, matrix, range, on_host,
+                      stream);
+}
+
+s2_status s2_compute_p016(s2_ctx *ctx, const uint16_t *ref_y, const uint16_t *ref_uv, size_t ref_pitch,
+                          const uint16_t *dis_y, const uint16_t *dis_uv, size_t dis_pitch, int32_t matrix,
+                          int32_t range, int32_t on_host, void *stream) {
+    return ctx_yuv420(ctx, S2_FMT_P016, ref_y, ref_uv, ref_pitch, dis_y, dis_uv, dis_pitch, matrix, range, on_host,
+                      stream);
 }
 
 s2_status s2_compute_rgb16(s2_ctx *ctx, const uint16_t *ref, size_t ref_pitch, const uint16_t *dis,

@@ -18,6 +18,7 @@ s2_status s2_cuda_fail(cudaError_t e, const char *what);
 void s2_set_last_error(const char *msg);
 s2_status s2_global_init();
 ColorConsts s2_make_color_consts();
+void s2_yuv_coeffs(int matrix, int range, int bits, float out[5], int *ymin, int *neutral);
 extern const float s2_srgb8_lut[256];
 
 // Tile-height autotuner cache (process-wide, thread-safe; ssim2_engine.cu).
@@ -79,11 +80,14 @@ struct PairExtra {
 
 // Host-side bytes of one image of a pair: its main plane (rows x row bytes)
 // and, for NV12, the interleaved chroma plane (height / 2 rows of width bytes).
+inline bool s2_is_yuv420(int format) { return format == S2_FMT_NV12 || format == S2_FMT_P016; }
+
 inline size_t s2_row_bytes(const s2_pair_desc &q) {
     switch (q.format) {
     case S2_FMT_LINEAR_F32: return (size_t)q.width * 12;
     case S2_FMT_SRGB8: return (size_t)q.width * 3;
     case S2_FMT_NV12: return (size_t)q.width;
+    case S2_FMT_P016: return (size_t)q.width * 2;
     default: return (size_t)q.width * 6;
     }
 }
@@ -376,15 +380,18 @@ struct Engine {
                 P.blk_first[i] = blk;
                 continue;
             }
-            if (q.format < 0 || q.format > 3 || (need_ref_in && !q.ref) || (need_dis_in && !q.dis) ||
-                (q.format == S2_FMT_NV12 && ((need_ref_in && !q.ref_uv) || (need_dis_in && !q.dis_uv) ||
-                                             (q.width & 1) || (q.height & 1))) ||
+            const bool yuv = q.format == S2_FMT_NV12 || q.format == S2_FMT_P016;
+            if (q.format < 0 || q.format > 4 || (need_ref_in && !q.ref) || (need_dis_in && !q.dis) ||
+                (yuv && ((need_ref_in && !q.ref_uv) || (need_dis_in && !q.dis_uv) || (q.width & 1) ||
+                         (q.height & 1) || q.matrix < S2_MATRIX_BT709 || q.matrix > S2_MATRIX_BT601_625 ||
+                         (q.range != S2_RANGE_LIMITED && q.range != S2_RANGE_FULL))) ||
                 (q.format == S2_FMT_RGB16 && (q.bits < 8 || q.bits > 16))) {
                 p.status = S2_ERR_INVALID_ARG;
                 p.nscales = 0;
                 P.blk_first[i] = blk;
                 continue;
             }
+            if (yuv) s2_yuv_coeffs(q.matrix, q.range, q.format == S2_FMT_P016 ? 16 : 8, p.yuv, &p.yuv_min, &p.yuv_neutral);
             p.w[0] = (int)q.width;
             p.h[0] = (int)q.height;
             for (int s = 1; s < kScales; s++) {
@@ -504,7 +511,7 @@ struct Engine {
                 p.in[img] = (const void *)off;
                 p.pitch[img] = (long long)row;
                 off += s2_align_up(row * d[i].height, 256);
-                if (d[i].format == S2_FMT_NV12) {
+                if (s2_is_yuv420(d[i].format)) {
                     p.in_uv[img] = (const void *)off;
                     off += s2_align_up(row * (d[i].height / 2), 256);
                 }
@@ -566,7 +573,7 @@ struct Engine {
                 for (int img = 0; img < 2; img++)
                     if ((hp[i].prep_mask >> img) & 1) {
                         hp[i].in[img] = (const char *)stage_d.p + (size_t)hp[i].in[img];
-                        if (host[i].format == S2_FMT_NV12)
+                        if (s2_is_yuv420(host[i].format))
                             hp[i].in_uv[img] = (const char *)stage_d.p + (size_t)hp[i].in_uv[img];
                     }
         }
@@ -634,7 +641,7 @@ struct Engine {
                         const void *src = img ? host[i].dis : host[i].ref;
                         const size_t sp = img ? host[i].dis_pitch : host[i].ref_pitch;
                         if ((r = copy_plane((void *)q.in[img], src, sp, row, hgt)) != S2_OK) return r;
-                        if (host[i].format == S2_FMT_NV12 &&
+                        if (s2_is_yuv420(host[i].format) &&
                             (r = copy_plane((void *)q.in_uv[img], img ? host[i].dis_uv : host[i].ref_uv, sp, row,
                                             hgt / 2)) != S2_OK)
                             return r;

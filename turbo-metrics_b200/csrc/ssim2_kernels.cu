@@ -151,17 +151,19 @@ __device__ __forceinline__ void prep_quads(const DevPair &P, int X0, int Y0, con
         const int x = X0 + 2 * qx, y = Y0 + 2 * qy;
         if (x >= W || y >= H) continue;
         const bool vx = x + 1 < W, vy = y + 1 < H;
-        // NV12: both images' samples are loaded before either is converted
+        // 4:2:0 YUV: both images' samples are loaded before either is converted
+        constexpr bool kYuv = FMT == FMT_NV12 || FMT == FMT_P016;
+        constexpr int kEs = FMT == FMT_P016 ? 2 : 1;
         Nv12Quad nq0{}, nq1{};
-        if (FMT == FMT_NV12) {
-            if (P.prep_mask & 1) nq0 = nv12_load_quad(P, 0, x, y);
-            if (P.prep_mask & 2) nq1 = nv12_load_quad(P, 1, x, y);
+        if (kYuv) {
+            if (P.prep_mask & 1) nq0 = yuv_load_quad<kEs>(P, 0, x, y);
+            if (P.prep_mask & 2) nq1 = yuv_load_quad<kEs>(P, 1, x, y);
         }
 #pragma unroll 1
         for (int img = 0; img < 2; img++) {
             if (!((P.prep_mask >> img) & 1)) continue;
             float v[4][3];
-            if (FMT == FMT_NV12) nv12_quad_linear(img ? nq1 : nq0, cc, v);
+            if (kYuv) yuv_quad_linear<kEs>(img ? nq1 : nq0, P, v);
             else lin_quad<FMT>(P, img, x, y, vx, vy, lut, cc, v);
             ST *dst = (ST *)P.lvl[img][0];
             const long long plane = (long long)P.lp[0] * H;
@@ -225,6 +227,7 @@ __global__ void __launch_bounds__(256, 3) prep_kernel(const DevPair *__restrict_
         case FMT_LINEAR_F32: prep_quads<FMT_LINEAR_F32, ST>(P, X0, Y0, lut, cc, lv1); break;
         case FMT_SRGB8: prep_quads<FMT_SRGB8, ST>(P, X0, Y0, lut, cc, lv1); break;
         case FMT_NV12: prep_quads<FMT_NV12, ST>(P, X0, Y0, lut, cc, lv1); break;
+        case FMT_P016: prep_quads<FMT_P016, ST>(P, X0, Y0, lut, cc, lv1); break;
         default: prep_quads<FMT_RGB16, ST>(P, X0, Y0, lut, cc, lv1); break;
         }
         __syncthreads();

@@ -171,7 +171,7 @@ class Ssimulacra2:
         check(lib.s2_compute_srgb8(self._h, rp, rpitch, dp, dpitch, 1, _stream_ptr(stream)), "compute_from_cpu")
         return self.get_score()
 
-    def compute_nv12(self, ref_y, ref_uv, dis_y, dis_uv, stream=None, on_host=False):
+    def _yuv420(self, fn, es, ref_y, ref_uv, dis_y, dis_uv, matrix, range_, stream, on_host):
         if on_host:
             ry, rpitch, a1 = _host(ref_y)
             ru, _, a2 = _host(ref_uv)
@@ -179,13 +179,23 @@ class Ssimulacra2:
             du, _, a4 = _host(dis_uv)
             self._keep = (a1, a2, a3, a4)
         else:
-            ry, rpitch = _dev(ref_y, 1)
-            ru, _ = _dev(ref_uv, 1)
-            dy, dpitch = _dev(dis_y, 1)
-            du, _ = _dev(dis_uv, 1)
+            ry, rpitch = _dev(ref_y, es)
+            ru, _ = _dev(ref_uv, es)
+            dy, dpitch = _dev(dis_y, es)
+            du, _ = _dev(dis_uv, es)
             self._keep = (ref_y, ref_uv, dis_y, dis_uv)
-        check(lib.s2_compute_nv12(self._h, ry, ru, rpitch, dy, du, dpitch, 0, 0, int(on_host),
-                                  _stream_ptr(stream)), "compute_nv12")
+        check(fn(self._h, ry, ru, rpitch, dy, du, dpitch, capi.MATRIX[matrix], capi.RANGE[range_], int(on_host),
+                 _stream_ptr(stream)), fn.__name__)
+
+    def compute_nv12(self, ref_y, ref_uv, dis_y, dis_uv, stream=None, on_host=False, matrix="bt709",
+                     range="limited"):
+        """8-bit 4:2:0 biplanar pair: Y (H, W) and interleaved CbCr (H/2, W) planes."""
+        self._yuv420(lib.s2_compute_nv12, 1, ref_y, ref_uv, dis_y, dis_uv, matrix, range, stream, on_host)
+
+    def compute_p016(self, ref_y, ref_uv, dis_y, dis_uv, stream=None, on_host=False, matrix="bt709",
+                     range="limited"):
+        """16-bit 4:2:0 biplanar pair (P016; P010/P012 data left-aligned): uint16 / int16 planes."""
+        self._yuv420(lib.s2_compute_p016, 2, ref_y, ref_uv, dis_y, dis_uv, matrix, range, stream, on_host)
 
     def compute_rgb16(self, ref, dis, bits=10, stream=None, on_host=False):
         if on_host:
@@ -248,12 +258,13 @@ class PairDesc:
     """One pair of a batch: device tensors of any supported format (host arrays
     for `Ssim2Batch.submit_host`)."""
 
-    def __init__(self, ref, dis, fmt="srgb8", ref_uv=None, dis_uv=None, bits=10):
+    def __init__(self, ref, dis, fmt="srgb8", ref_uv=None, dis_uv=None, bits=10, matrix="bt709", range="limited"):
         self.ref, self.dis, self.fmt, self.ref_uv, self.dis_uv, self.bits = ref, dis, fmt, ref_uv, dis_uv, bits
+        self.matrix, self.range = matrix, range
 
     def to_c(self, host=False):
         d = capi.PairDescC()
-        eb = {"linear_f32": 4, "srgb8": 1, "nv12": 1, "rgb16": 2}[self.fmt]
+        eb = {"linear_f32": 4, "srgb8": 1, "nv12": 1, "rgb16": 2, "p016": 2}[self.fmt]
         ptr = _host_ptr if host else _dev
         rp, rpitch = ptr(self.ref, eb)
         dp, dpitch = ptr(self.dis, eb)
@@ -262,9 +273,11 @@ class PairDesc:
         d.bits = self.bits
         d.ref, d.dis = rp.value, dp.value
         d.ref_pitch, d.dis_pitch = rpitch, dpitch
-        if self.fmt == "nv12":
-            d.ref_uv = ptr(self.ref_uv, 1)[0].value
-            d.dis_uv = ptr(self.dis_uv, 1)[0].value
+        if self.fmt in ("nv12", "p016"):
+            d.ref_uv = ptr(self.ref_uv, eb)[0].value
+            d.dis_uv = ptr(self.dis_uv, eb)[0].value
+            d.matrix = capi.MATRIX[self.matrix]
+            d.range = capi.RANGE[self.range]
         return d
 
 

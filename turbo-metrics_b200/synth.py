@@ -184,6 +184,22 @@ def nv12_frame_pair(w: int, h: int, seed: int):
     return pack(Y, U, V), pack(Yd, Ud, Vd)
 
 
+def p016_frame_pair(w: int, h: int, seed: int, bits: int = 10):
+    """P016 version of nv12_frame_pair: the 8-bit samples scaled to `bits`
+    bits (value * 2^(bits-8) plus seeded low-order noise), left-aligned in
+    16-bit words as P010/P016 store them.  Returns (ref, dis) of (y, uv)
+    uint16 planes."""
+    ref, dis = nv12_frame_pair(w, h, seed)
+    st = Stream(seed ^ 0x0F16)
+    sh = bits - 8
+
+    def widen(a):
+        low = (st.uniform(a.size) * (1 << sh)).astype(np.uint32).reshape(a.shape) if sh else 0
+        return (((a.astype(np.uint32) << sh) + low) << (16 - bits)).astype(np.uint16)
+
+    return tuple(widen(p) for p in ref), tuple(widen(p) for p in dis)
+
+
 def c1_pair(index: int, w: int = 1920, h: int = 1080):
     return nv12_frame_pair(w, h, pair_seed(1, index))
 
