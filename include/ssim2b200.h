@@ -189,6 +189,17 @@ s2_status s2_compute_with_reference_srgb8(s2_ctx *ctx, const uint8_t *dis, size_
 s2_status s2_clear_reference(s2_ctx *ctx);
 int32_t s2_has_reference(const s2_ctx *ctx);
 
+/* Error-map export (the reference materialises the maps per scale,
+ * ssimulacra2-cuda/src/lib.rs:965-970; the fused pass here pools them
+ * without storing): writes the last compute's SSIM error, artifact and
+ * detail-loss maps of `scale` to the device buffer `maps` as 9 float planes
+ * [channel X, Y, B][ssim, artifact, detail], each h_s rows of `pitch` bytes
+ * (w_s = ceil(w / 2^scale), h_s likewise).  Enqueued on `stream` after that
+ * compute (its planes must not have been overwritten by another compute).
+ * FIR blur only (S2_ERR_INVALID_ARG for S2_BLUR_IIR_REF); S2_ERR_NOT_READY
+ * before a scored compute. */
+s2_status s2_error_maps(s2_ctx *ctx, int32_t scale, float *maps, size_t pitch, void *stream);
+
 /* ---- batches of pairs of uneven sizes ---------------------------------- */
 /* Semantics from ssim2-gpu Ssim2Batch (pipeline_batch.rs:120-382), widened to
  * mixed sizes: all pairs of a submission run as one pyramid launch, one

@@ -23,3 +23,4 @@ from .capi import (  # noqa: F401
 )
 from .ssimulacra2 import Ssimulacra2, Ssim2Batch, PairDesc  # noqa: F401
 from .server import Ssim2Server  # noqa: F401
+from .frames import FramePairScorer, Stats, select_frames  # noqa: F401

@@ -139,6 +139,7 @@ _sig = {
     "s2_batch_submit": (ctypes.c_int, [P, ctypes.POINTER(PairDescC), ctypes.c_uint32, P]),
     "s2_batch_submit_host": (ctypes.c_int, [P, ctypes.POINTER(PairDescC), ctypes.c_uint32, P]),
     "s2_set_graphs": (ctypes.c_int, [P, ctypes.c_int32]),
+    "s2_error_maps": (ctypes.c_int, [P, ctypes.c_int32, P, ctypes.c_size_t, P]),
     "s2_batch_results": (ctypes.c_int, [P, ctypes.POINTER(Result), ctypes.c_uint32]),
     "s2_batch_mem_usage": (ctypes.c_int, [P, ctypes.POINTER(ctypes.c_size_t)]),
     "s2_batch_set_graphs": (ctypes.c_int, [P, ctypes.c_int32]),

@@ -657,6 +657,30 @@ s2_status s2_clear_reference(s2_ctx *ctx) {
 
 int32_t s2_has_reference(const s2_ctx *ctx) { return ctx && ctx->has_ref ? 1 : 0; }
 
+s2_status s2_error_maps(s2_ctx *ctx, int32_t scale, float *maps, size_t pitch, void *stream) {
+    if (!ctx || !maps) return S2_ERR_INVALID_ARG;
+    Engine &e = ctx->eng;
+    Plan &P = ctx->plan;
+    if (e.last_n != 1 || P.pairs.empty() || ctx->last_was_ref_build) return S2_ERR_NOT_READY;
+    if (e.blur != S2_BLUR_FIR) return S2_ERR_INVALID_ARG;
+    const DevPair &p = P.pairs[0];
+    if (p.status != S2_OK || scale < 0 || scale >= p.nscales) return S2_ERR_INVALID_ARG;
+    const size_t row = (size_t)p.w[scale] * sizeof(float);
+    if (pitch < row || pitch % sizeof(float)) return S2_ERR_DIM_MISMATCH;
+    // the last compute's descriptors and XYB planes are still in the
+    // workspace; re-run its tile pass over this scale with the export on
+    const int t0 = p.tile_base[scale], t1 = t0 + p.tile_cnt[scale];
+    const size_t pb = s2_align_up(sizeof(DevPair), 256), bb = s2_align_up(sizeof(int), 256);
+    char *dbase = (char *)e.pairs_d.p;
+    cudaStream_t st = (cudaStream_t)stream;
+    const long long mpitch = (long long)(pitch / sizeof(float));
+    S2_CUDA(cudaMemsetAsync(e.counter_d.p, 0, sizeof(int), st));
+    S2_CUDA(launch_fused_export(e.storage, (const DevPair *)dbase, (const Seg *)(dbase + pb + bb), (int)P.segs.size(), t0,
+                                t1, (int *)e.counter_d.p, (double *)e.partials_d.p, maps, mpitch,
+                                mpitch * p.h[scale], e.num_sms * e.fused_bps, st));
+    return S2_OK;
+}
+
 // ---- batches -----------------------------------------------------------
 s2_status s2_batch_create(const s2_config *cfg_in, uint32_t max_pairs, uint64_t max_pixels, s2_batch **out) {
     if (!out || max_pairs == 0) return S2_ERR_INVALID_ARG;

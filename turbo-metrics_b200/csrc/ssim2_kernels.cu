@@ -273,10 +273,20 @@ __global__ void __launch_bounds__(256, 3) prep_kernel(const DevPair *__restrict_
 // ten CTAs share an SM.  A tile's three items write the tile's 18 partial
 // sums (channel-major) and are summed in the same order as one CTA per tile
 // over all channels would.
-template <typename ST>
+//
+// EXPORT (error-map export, one scale of one pair): every pixel's SSIM error,
+// artifact and detail-loss values are also stored to `maps`, 9 planes
+// [channel][map] of `mpitch` floats per row and `mplane` floats per plane.
+struct MapOut {
+    float *maps;
+    long long mpitch, mplane;
+};
+
+template <typename ST, bool EXPORT = false>
 __global__ void __maxnreg__(96)
     fused_kernel(const DevPair *__restrict__ pairs, const Seg *__restrict__ segs, int nseg,
-                 int first_item, int end_item, int *__restrict__ counter, double *__restrict__ partials) {
+                 int first_item, int end_item, int *__restrict__ counter, double *__restrict__ partials,
+                 MapOut mo = MapOut{nullptr, 0, 0}) {
     extern __shared__ float sm[];
     float2 *s_vo2 = (float2 *)sm;                  // [pair][rb][col]
     float2 *s_xo = (float2 *)(sm + kSmVo2);        // [rb][col]
@@ -477,6 +487,12 @@ __global__ void __maxnreg__(96)
                                 const float aa = fabsf(t.x), bb = fabsf(t.y);
                                 const float d1 = s2_div(bb - aa, 1.0f + aa);
                                 const float2 ad = make_float2(fmaxf(d1, 0.0f), fmaxf(-d1, 0.0f));
+                                if (EXPORT) {
+                                    float *m = mo.maps + (long long)(3 * g) * mo.mplane + (long long)y * mo.mpitch + xc + j;
+                                    m[0] = d;
+                                    m[mo.mplane] = ad.x;
+                                    m[2 * mo.mplane] = ad.y;
+                                }
                                 const float q = d * d;
                                 fs[0] += d;
                                 f4[0] += q * q;
@@ -513,6 +529,12 @@ __global__ void __maxnreg__(96)
                                 const float bb = fabsf((xy.y - m2) + kk);
                                 const float d1 = s2_div(bb - aa, 1.0f + aa);
                                 const float art = fmaxf(d1, 0.0f), det = fmaxf(-d1, 0.0f);
+                                if (EXPORT) {
+                                    float *m = mo.maps + (long long)(3 * g) * mo.mplane + (long long)y * mo.mpitch + xx;
+                                    m[0] = d;
+                                    m[mo.mplane] = art;
+                                    m[2 * mo.mplane] = det;
+                                }
                                 float q;
                                 fs[0] += d;   q = d * d;     f4[0] += q * q;
                                 fs[1] += art; q = art * art; f4[1] += q * q;
@@ -691,6 +713,34 @@ cudaError_t launch_fused(int storage, const DevPair *pairs, const Seg *segs, int
         fused_kernel<__nv_bfloat16><<<grid, block, sm, st>>>(pairs, segs, nseg, fi, ei, counter, partials);
     else
         fused_kernel<float><<<grid, block, sm, st>>>(pairs, segs, nseg, fi, ei, counter, partials);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fused_export(int storage, const DevPair *pairs, const Seg *segs, int nseg, int first_tile,
+                                int end_tile, int *counter, double *partials, float *maps, long long mpitch,
+                                long long mplane, int grid, cudaStream_t st) {
+    const int fi = 3 * first_tile, ei = 3 * end_tile;
+    const int nt = ei - fi;
+    if (nt <= 0) return cudaSuccess;
+    grid = grid > nt ? nt : grid;
+    dim3 block(kFusedThreads);
+    size_t sm = fused_smem_bytes();
+    const MapOut mo{maps, mpitch, mplane};
+    cudaError_t e;
+    if (storage == ST_F16) {
+        e = cudaFuncSetAttribute(fused_kernel<__half, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e != cudaSuccess) return e;
+        fused_kernel<__half, true><<<grid, block, sm, st>>>(pairs, segs, nseg, fi, ei, counter, partials, mo);
+    } else if (storage == ST_BF16) {
+        e = cudaFuncSetAttribute(fused_kernel<__nv_bfloat16, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sm);
+        if (e != cudaSuccess) return e;
+        fused_kernel<__nv_bfloat16, true><<<grid, block, sm, st>>>(pairs, segs, nseg, fi, ei, counter, partials, mo);
+    } else {
+        e = cudaFuncSetAttribute(fused_kernel<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e != cudaSuccess) return e;
+        fused_kernel<float, true><<<grid, block, sm, st>>>(pairs, segs, nseg, fi, ei, counter, partials, mo);
+    }
     return cudaGetLastError();
 }
 

@@ -23,6 +23,13 @@ cudaError_t launch_iir(int storage, const DevPair *pairs, const IirSeg *vsegs, i
 // page-locked host memory, through its device mapping, with a kernel: no copy
 // engine, so the copy is not queued behind other streams' large uploads.
 cudaError_t launch_desc_copy(void *dst, const void *src_host_mapped, size_t bytes, cudaStream_t st);
+// The fused pass over the tiles [first_tile, end_tile) of one scale of one
+// pair, also storing each pixel's three error-map values to `maps` (9 float
+// planes [channel][ssim, artifact, detail], mpitch floats per row, mplane
+// floats per plane).
+cudaError_t launch_fused_export(int storage, const DevPair *pairs, const Seg *segs, int nseg, int first_tile,
+                                int end_tile, int *counter, double *partials, float *maps, long long mpitch,
+                                long long mplane, int grid, cudaStream_t st);
 cudaError_t launch_finalize(const DevPair *pairs, int npairs, const double *partials, DevResult *out,
                             cudaStream_t st);
 }  // namespace s2

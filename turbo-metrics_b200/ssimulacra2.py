@@ -97,6 +97,18 @@ class Ssimulacra2:
         s._bound = (src_ref_linear, src_dis_linear)
         return s
 
+    def error_maps(self, scale, stream=None):
+        """The last compute's error maps at `scale` as a (3, 3, h_s, w_s) float32
+        CUDA tensor: [channel X, Y, B][ssim, artifact, detail]."""
+        import torch
+        w, h = self.width, self.height
+        for _ in range(scale):
+            w, h = (w + 1) // 2, (h + 1) // 2
+        out = torch.empty((3, 3, h, w), dtype=torch.float32, device="cuda")
+        check(lib.s2_error_maps(self._h, int(scale), ctypes.c_void_p(out.data_ptr()), w * 4, _stream_ptr(stream)),
+              "error_maps")
+        return out
+
     def set_graphs(self, enable=True):
         """Replay computes of a seen shape as CUDA graphs (default on)."""
         check(lib.s2_set_graphs(self._h, 1 if enable else 0), "set_graphs")
