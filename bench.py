@@ -312,7 +312,7 @@ def sum_pixels(w=W, h=H, scales=6):
 def algorithmic_bytes_fused(n_pairs, storage_bytes=4):
     """Declared I/O of one fused launch over n_pairs pairs: it reads the XYB
     planes of both frames at every scale (3 planes x storage bytes x sum of
-    the scale sizes) and writes 18 doubles per tile (negligible)."""
+    the scale sizes) and writes 6 doubles per (tile, channel) (negligible)."""
     return n_pairs * 2 * 3 * storage_bytes * sum_pixels()
 
 

@@ -12,7 +12,9 @@
  *                bytes apart (the NPP C3 layout the reference binds)
  *   sRGB8        packed interleaved RGB, 3 bytes per pixel, gamma-2.4 sRGB
  *   NV12         8-bit 4:2:0, Y plane then interleaved CbCr plane (w/2 pairs
- *                per row, h/2 rows), both with the same `pitch`
+ *                per row, h/2 rows), both with the same `pitch`; BT.709 or
+ *                BT.601-525/625 matrix, limited or full range
+ *   P016         the same layout with 16-bit samples (P010/P012 left-aligned)
  *   RGB16        packed RGB uint16 code values of `bits` bits (10 or 12),
  *                BT.2020 primaries, BT.709/BT.2020 transfer
  * Device pointers must stay valid until the stream work completes.
@@ -23,7 +25,8 @@
  * error, 1 = artifact, 2 = detail loss.  Unscored scales hold 0.
  *
  * Thread safety: one context per thread, or external synchronisation.  No
- * process-global state except the no-allocation entry point's scratch.
+ * process-global state except the no-allocation entry point's scratch and
+ * the tile-height autotuner's per-class choices (mutex-protected).
  */
 #ifndef SSIM2B200_H
 #define SSIM2B200_H
@@ -204,7 +207,7 @@ s2_status s2_error_maps(s2_ctx *ctx, int32_t scale, float *maps, size_t pitch, v
 /* Semantics from ssim2-gpu Ssim2Batch (pipeline_batch.rs:120-382), widened to
  * mixed sizes: all pairs of a submission run as one pyramid launch, one
  * persistent tile launch over every (pair, scale, strip) and one finalize
- * launch.  Pairs are sRGB8 or linear f32 or NV12, on the device. */
+ * launch.  Pairs are any of the image formats above, mixed freely. */
 typedef enum {
     S2_FMT_LINEAR_F32 = 0,
     S2_FMT_SRGB8 = 1,
@@ -217,8 +220,8 @@ typedef struct {
     uint32_t width, height;
     int32_t format;          /* s2_format */
     int32_t bits;            /* RGB16 only */
-    const void *ref, *dis;   /* packed image, or NV12 Y plane */
-    const void *ref_uv, *dis_uv; /* NV12 CbCr planes */
+    const void *ref, *dis;   /* packed image, or NV12 / P016 Y plane */
+    const void *ref_uv, *dis_uv; /* NV12 / P016 CbCr planes */
     size_t ref_pitch, dis_pitch;
     int32_t matrix, range;   /* NV12 / P016: S2_MATRIX_*, S2_RANGE_* (0, 0 = BT.709 limited) */
 } s2_pair_desc;
