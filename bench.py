@@ -417,7 +417,12 @@ def main():
                 "kernel_ms": {"prep": float(acc[0]), "fused": fused_ms, "finalize": float(acc[2])},
                 "fused_blocks_per_sm": int(lib.s2_fused_blocks_per_sm(0)),
                 "algorithmic_bytes_per_launch": ab,
-                "prep_gbs": algorithmic_bytes_prep(NP) / (float(acc[0]) / 1e3) / 1e9}
+                "prep_gbs": algorithmic_bytes_prep(NP) / (float(acc[0]) / 1e3) / 1e9,
+                # every pass's declared I/O over the sum of their times (prep: NV12 in + XYB
+                # planes out; fused: XYB planes in; finalize: negligible)
+                "all_passes": {"bytes": algorithmic_bytes_prep(NP) + ab, "ms": float(acc.sum()),
+                               "gbs": (algorithmic_bytes_prep(NP) + ab) / (float(acc.sum()) / 1e3) / 1e9,
+                               "frac": (algorithmic_bytes_prep(NP) + ab) / (float(acc.sum()) / 1e3) / 1e9 / peak}}
 
     # ---- plain: the drop-in, one pair at a time ----------------------------
     ctx = tmb.Ssimulacra2(W, H)
