@@ -198,3 +198,40 @@ def ssim2_linear(ref, dis, mode="fp64", rule="cpu"):
 def ssim2_srgb8(ref, dis, mode="fp64", rule="cpu"):
     f64 = mode == "fp64"
     return ssim2_linear(srgb8_to_linear(ref, f64), srgb8_to_linear(dis, f64), mode, rule)
+
+
+# ---- DSSIM (dssim_oracle.c): crates/dssim-cuda's metric ----------------------
+DSSIM_MODE = {"fp64": 0, "cuda32": 1}
+_lib.or_dssim_linear.restype = ctypes.c_int
+
+
+class DssimResult:
+    def __init__(self, dssim, level_scores, level_means):
+        self.dssim, self.level_scores, self.level_means = dssim, level_scores, level_means
+
+
+def dssim_level_dims(w, h):
+    dw = (ctypes.c_int * 5)()
+    dh = (ctypes.c_int * 5)()
+    _lib.or_dssim_level_dims(w, h, dw, dh)
+    return list(zip(dw, dh))
+
+
+def dssim_linear(ref, dis, mode="cuda32"):
+    """DSSIM from linear RGB (H, W, 3).  mode: cuda32 (the reference GPU's
+    f32 arithmetic) | fp64."""
+    h, w = ref.shape[:2]
+    r = np.ascontiguousarray(ref, np.float32)
+    d = np.ascontiguousarray(dis, np.float32)
+    sc = np.zeros(5)
+    mn = np.zeros(5)
+    out = ctypes.c_double()
+    if _lib.or_dssim_linear(_f(r), _f(d), w, h, DSSIM_MODE[mode], _d(sc), _d(mn), ctypes.byref(out)) != 0:
+        raise ValueError("invalid image size %dx%d" % (w, h))
+    return DssimResult(out.value, sc, mn)
+
+
+def dssim_srgb8(ref, dis, mode="cuda32"):
+    """DSSIM of two sRGB8 images (H, W, 3): the reference's 256-entry LUT,
+    then dssim_linear (dssim-cuda's srgb_to_linear, srgb.rs:23-73)."""
+    return dssim_linear(srgb8_to_linear(ref), srgb8_to_linear(dis), mode)

@@ -115,6 +115,19 @@ float or_pow_20_9(float p);
 double or_score_from_stats(const double stats[108]);
 void or_weights(double w[108]);
 
+/* ---- DSSIM (dssim_oracle.c) ----------------------------------------------
+ * The sibling metric of crates/dssim-cuda: five scales of a clamped 2x2
+ * linear-RGB pyramid (sizes halved rounding up, never below 8), dssim-core's
+ * scaled Lab, two-pass 3x3 blurs, a channel-averaged SSIM map, per-scale
+ * 1 - mean |mean^(0.5^s) - ssim|, weighted, then 1/ssim - 1. */
+enum { OR_DSSIM_F64 = 0, OR_DSSIM_F32 = 1 };
+void or_dssim_level_dims(int w, int h, int dw[5], int dh[5]);
+void or_dssim_lab_f32(float r, float g, float b, float out[3]);
+/* Packed linear RGB in; per-level scores (1 - MAD) and SSIM means out.
+ * Returns 1 for images below 8x8. */
+int or_dssim_linear(const float *ref, const float *dis, int w, int h, int mode, double level_score[5],
+                    double level_mean[5], double *dssim);
+
 #ifdef __cplusplus
 }
 #endif

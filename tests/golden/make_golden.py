@@ -12,6 +12,15 @@ where the reference is absent:
   blur_consts      crates/ssimulacra2-cuda/examples/cpu.rs:931-948 (f32)
   corpus_scores    crates/ssim2-gpu/PORT_STATUS.md:28-33 -- scores of the CPU
                    crate ssimulacra2 0.5.1 on crates/dssim-cuda/test_data
+
+DSSIM (the sibling metric sharing the linear-RGB pyramid):
+
+  dssim.blur_kernel    crates/dssim-cuda-kernel/src/blur.rs:13-17 (3x3 f32)
+  dssim.lab            crates/dssim-cuda-kernel/src/lab.rs:15-34 (f32 constants)
+  dssim.c1, c2         crates/dssim-cuda-kernel/src/ssim.rs:18-19
+  dssim.scale_weights  crates/dssim-cuda/src/lib.rs:77
+  dssim.published      crates/dssim-gpu/PORT_STATUS.md:26-30 -- dssim-core 3.4
+                       (CPU) and dssim-gpu scores of the parity_lock.rs cases
 """
 import json
 import os
@@ -51,6 +60,7 @@ def main():
     corpus = {}
     for q, cpu_s in re.findall(r"^\|\s*(\d+)\s*\|\s*(-?[0-9.]+)\s*\|", status, re.M):
         corpus["q%s" % q] = float(cpu_s)
+    dssim = dssim_tables()
     assert len(lut) == 256 and len(cpu_lut) == 256 and len(weights) == 108, (len(lut), len(cpu_lut), len(weights))
     out = {
         "source": "imazen/turbo-metrics (parsed by tests/golden/make_golden.py)",
@@ -60,10 +70,35 @@ def main():
         "blur_consts": consts,
         "corpus_scores_cpu_crate": corpus,
         "corpus_decoder_note": "scores produced by the image 0.25 JPEG decoder; other decoders may differ by +-1 per sample",
+        "dssim": dssim,
     }
     with open(OUT, "w") as f:
         json.dump(out, f, indent=1)
     print("wrote", OUT, len(lut), len(weights), consts.keys(), corpus)
+
+
+def dssim_tables():
+    blur = read("crates/dssim-cuda-kernel/src/blur.rs")
+    kern = floats_between(blur, "const KERNEL")
+    lab = read("crates/dssim-cuda-kernel/src/lab.rs")
+    labc = {}
+    for name, val in re.findall(r"^const (\w+): f32 = ([-0-9.e_]+);", lab, re.M):
+        labc[name] = float(val.replace("_", ""))
+    ssim = read("crates/dssim-cuda-kernel/src/ssim.rs")
+    c = dict(re.findall(r"^const (C[12]): f32 = ([0-9.e-]+);", ssim, re.M))
+    lib = read("crates/dssim-cuda/src/lib.rs")
+    sw = floats_between(lib, "const SCALE_WEIGHTS")
+    status = read("crates/dssim-gpu/PORT_STATUS.md")
+    pub = {}
+    names = {"32×32 identical gradient": "identical_32", "64×64 black vs white": "black_white_64",
+             "64×64 noisy gradient (±8)": "noisy_gradient_64", "`dssim-cuda` corpus q70.jpg vs source.png": "q70",
+             "`dssim-cuda` corpus q90.jpg vs source.png": "q90"}
+    for label, cpu_s, gpu_s in re.findall(r"^\|\s*([^|]+?)\s*\|\s*([0-9.]+)\s*\|\s*([0-9.]+)\s*\|", status, re.M):
+        if label in names:
+            pub[names[label]] = {"dssim_core_cpu": float(cpu_s), "dssim_gpu": float(gpu_s)}
+    assert len(kern) == 9 and len(sw) == 5 and len(pub) == 5 and "M_B_Z" in labc, (kern, sw, pub, labc)
+    return {"blur_kernel": kern, "lab": labc, "c1": float(c["C1"]), "c2": float(c["C2"]), "scale_weights": sw,
+            "published": pub}
 
 
 if __name__ == "__main__":
