@@ -20,6 +20,9 @@ submission of all 64 pairs (pyramid + fused tiles + finalize launches).
   cpu_baseline   the CPU SSIMULACRA2 path the reference validates against (the
                  oracle's restatement of examples/cpu.rs), all host cores,
                  bounded sample
+  dssim          the sibling metric DSSIM (crates/dssim-cuda) on the same 64
+                 pairs: both metrics from one prep pass, and DSSIM alone,
+                 with the DSSIM passes' kernel time against their declared I/O
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 """
@@ -268,6 +271,66 @@ def cpu_baseline(seconds=15.0, threads=None):
                       % (n, one)}
 
 
+def dssim_bench(tmb, descs, n_pairs, steps, warmup, s2_value, peak):
+    """DSSIM, the sibling metric, on the same batch: both metrics from one
+    prep pass, and DSSIM alone; device-timed like the main leg, with the
+    DSSIM passes' kernel time and their declared I/O (Lab planes of both
+    images read, SSIM map written by the tile pass and read by the MAD pass:
+    32 bytes per pixel over the five levels)."""
+    import torch
+    b = tmb.Ssim2Batch(n_pairs, n_pairs * W * H)
+    out = {}
+    stream = torch.cuda.current_stream()
+    for key, metrics in (("both", ("ssimulacra2", "dssim")), ("dssim_only", "dssim")):
+        b.set_metrics(metrics)
+        for _ in range(max(warmup, 3)):
+            b.submit(descs)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            b.submit(descs)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        out[key + "_pairs_per_s"] = n_pairs * steps / (e0.elapsed_time(e1) / 1e3)
+    res = b.results()
+    out["dssim_mean"] = float(np.mean([r[5] for r in res]))
+    tmb.lib.s2_batch_set_profiling(b._h, 1)
+    kt = (ctypes.c_float * 3)()
+    dms = ctypes.c_float()
+    acc = np.zeros(4)
+    for _ in range(3):
+        b.submit(descs)
+        tmb.lib.s2_batch_last_timings(b._h, kt)
+        tmb.lib.s2_batch_last_dssim_ms(b._h, ctypes.byref(dms))
+        acc += np.array(list(kt[:]) + [dms.value])
+    tmb.lib.s2_batch_set_profiling(b._h, 0)
+    acc /= 3
+    npx = sum(max((W + (1 << s) - 1) >> s, 8) * max((H + (1 << s) - 1) >> s, 8) for s in range(5))
+    ab = 32 * npx * n_pairs
+    out["kernel_ms"] = {"prep_lab": float(acc[0]), "dssim_passes": float(acc[3])}
+    out["roofline"] = {"bound": "hbm", "achieved": ab / (acc[3] / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                       "frac": ab / (acc[3] / 1e3) / 1e9 / peak, "algorithmic_bytes_per_launch": ab,
+                       "kernel": "dssim clamp+tile+mean+mad+final"}
+    out["both_vs_ssimulacra2_only"] = out["both_pairs_per_s"] / s2_value
+    b.close()
+    return out
+
+
+def dssim_cpu_baseline():
+    """Oracle f32 mirror of dssim-cuda on one 1080p pair, single thread."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    import synth
+    (ry, ruv), (dy, duv) = synth.c1_pair(0, W, H)
+    rl, dl = oracle.nv12_to_linear(ry, ruv), oracle.nv12_to_linear(dy, duv)
+    t0 = time.time()
+    oracle.dssim_linear(rl, dl, "cuda32")
+    dt = time.time() - t0
+    return {"value": 1.0 / dt, "unit": "pairs/s", "cores": 1, "kind": "port",
+            "sample": "1 x 1920x1080 pair, oracle f32 mirror of dssim-cuda (dssim_oracle.c)"}
+
+
 def run_reference(args, rank, world):
     """--impl reference: the reference's CPU path (oracle port), all host threads."""
     if rank != 0:
@@ -331,6 +394,7 @@ def main():
     ap.add_argument("--plain-pairs", type=int, default=64)
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-uneven", action="store_true", help="skip the 256-pair uneven-size batch leg")
+    ap.add_argument("--no-dssim", action="store_true", help="skip the DSSIM (sibling metric) leg")
     ap.add_argument("--pairs", type=int, default=N_PAIRS,
                     help="pairs per step (64 is the workload; smaller only for profiler captures)")
     args = ap.parse_args()
@@ -482,9 +546,15 @@ def main():
     if not args.no_uneven and world == 1:
         uneven = uneven_bench(tmb)
 
+    dssim = None
+    if not args.no_dssim:
+        dssim = dssim_bench(tmb, descs, NP, args.steps, args.warmup, value / world, peak)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline()
+        if dssim is not None:
+            dssim["cpu_baseline"] = dssim_cpu_baseline()
 
     if rank == 0:
         line = {
@@ -503,6 +573,7 @@ def main():
             "cpu_baseline": cpu,
             "served": served,
             "uneven": uneven,
+            "dssim": dssim,
             "score_mean": float(np.mean(scores)),
         }
         print(json.dumps(line), flush=True)

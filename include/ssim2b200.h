@@ -105,6 +105,11 @@ typedef struct {
     double sums[S2_NUM_STATS]; /* raw pooled sums: sum d (L1 slots), sum d^4 (L4 slots) */
     int32_t n_scales;
     int32_t status;            /* s2_status of this pair */
+    /* DSSIM (the sibling metric of crates/dssim-cuda, scored from the same
+     * pyramid when S2_METRIC_DSSIM is on): the value and the five per-scale
+     * scores 1 - mean |mean^(0.5^s) - ssim|.  NaN when DSSIM was not scored. */
+    double dssim;
+    double dssim_scale[5];
 } s2_result;
 
 typedef struct s2_ctx s2_ctx;
@@ -268,6 +273,45 @@ s2_status s2_batch_set_graphs(s2_batch *b, int32_t enable);
 /* The same switch for a single-pair context (default on). */
 s2_status s2_set_graphs(s2_ctx *ctx, int32_t enable);
 
+/* ---- DSSIM, the sibling metric sharing the pyramid ----------------------
+ * DSSIM as crates/dssim-cuda computes it (five scales of dssim-core's scaled
+ * Lab, two-pass 3x3 blurs, a channel-averaged SSIM map, per-scale
+ * 1 - mean |mean^(0.5^s) - ssim|, weighted, 1/ssim - 1), scored from the
+ * same prep pass as SSIMULACRA2: the pass reads each input once, builds one
+ * linear-RGB pyramid and writes the XYB planes of one metric and the Lab
+ * planes of the other side by side.  Any input format of this library
+ * (the reference's DSSIM takes sRGB8 only).  Scores are in s2_result's
+ * dssim fields (s2_get_dssim for a context). */
+enum { S2_METRIC_SSIMULACRA2 = 1, S2_METRIC_DSSIM = 2 };
+/* Metrics scored by later submissions of a context or batch: a non-empty
+ * set of S2_METRIC_* bits (default S2_METRIC_SSIMULACRA2).  With DSSIM alone
+ * the SSIMULACRA2 fields of a result hold NaN / 0.  Cached-reference
+ * submissions (s2_compute_with_reference_*) score SSIMULACRA2 only. */
+s2_status s2_set_metrics(s2_ctx *ctx, int32_t metrics);
+s2_status s2_batch_set_metrics(s2_batch *b, int32_t metrics);
+/* The last submission's DSSIM and its five per-scale scores (waits for the
+ * stream work).  S2_ERR_NOT_READY when that submission did not score DSSIM. */
+s2_status s2_get_dssim(s2_ctx *ctx, double *dssim, double scale_scores[5]);
+
+/* The drop-in for dssim-cuda's `Dssim` (crates/dssim-cuda/src/lib.rs:170-467):
+ * a context of one size that scores DSSIM only. */
+typedef struct s2_dssim s2_dssim;
+/* Dssim::new (lib.rs:184-222).  S2_ERR_INVALID_SIZE below 8x8. */
+s2_status s2_dssim_create(int32_t device, uint32_t width, uint32_t height, s2_dssim **out);
+void s2_dssim_destroy(s2_dssim *d);
+/* Dssim::compute_sync (lib.rs:225-232): sRGB8 images, device memory or,
+ * with on_host, host memory; waits for the result. */
+s2_status s2_dssim_compute_srgb8(s2_dssim *d, const uint8_t *ref, size_t ref_pitch, const uint8_t *dis,
+                                 size_t dis_pitch, int32_t on_host, void *stream, double *dssim);
+/* Dssim::compute_sync_dis_only (lib.rs:245-251): scores `dis` against the
+ * reference of this context's last compute, whose Lab planes stay on the
+ * device; only the distorted image is converted.  S2_ERR_NO_REFERENCE before
+ * a first compute. */
+s2_status s2_dssim_compute_dis_only_srgb8(s2_dssim *d, const uint8_t *dis, size_t dis_pitch, int32_t on_host,
+                                          void *stream, double *dssim);
+/* Dssim::mem_usage (lib.rs:438-451): device bytes held. */
+s2_status s2_dssim_mem_usage(const s2_dssim *d, size_t *bytes);
+
 /* ---- serving: continuous batching of jobs (reference + k candidates) -----
  * No single counterpart in the reference: it combines the cached-reference
  * path (ssimulacra2-cuda/src/lib.rs:440-860) with ssim2-gpu's batch
@@ -345,6 +389,8 @@ s2_status s2_server_reset_stats(s2_server *sv);
 s2_status s2_compute_srgb8_noalloc(const uint8_t *ref, size_t ref_pitch, const uint8_t *dis,
                                    size_t dis_pitch, uint32_t width, uint32_t height,
                                    s2_result *out_device, void *stream);
+/* (The no-allocation entry point scores SSIMULACRA2 only and leaves the
+ * dssim fields of *out_device unwritten.) */
 
 /* ---- kernel timing (no reference counterpart; the reference has commented-
  * out cuProfilerStart/Stop calls, ssimulacra2-cuda/src/lib.rs:311,963) ----
@@ -355,6 +401,9 @@ s2_status s2_profile_enable(s2_ctx *ctx, int32_t enable);
 s2_status s2_profile_last(s2_ctx *ctx, float ms[3]);
 s2_status s2_batch_set_profiling(s2_batch *b, int32_t enable);
 s2_status s2_batch_last_timings(s2_batch *b, float ms[3]);
+/* Device time of the DSSIM passes (clamp, tile, mean, MAD, final) of the
+ * last profiled submission that scored DSSIM. */
+s2_status s2_batch_last_dssim_ms(s2_batch *b, float *ms);
 /* Resident blocks per SM of the fused kernel for a storage type (0 on error). */
 int32_t s2_fused_blocks_per_sm(int32_t storage);
 

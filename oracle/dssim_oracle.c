@@ -24,8 +24,11 @@
  *                  operation: fused multiply-adds exactly where lab.rs and
  *                  ssim.rs use mul_add, separate multiply and add elsewhere
  *                  (the file is compiled with -ffp-contract=off), IEEE
- *                  division, libm cbrtf; sums of the SSIM map and of
- *                  |avg - ssim| in double (NPP Sum returns f64).
+ *                  division; sums of the SSIM map and of |avg - ssim| in
+ *                  double (NPP Sum returns f64).  The cube root is
+ *                  or_cbrtf, the engine's own (Kahan seed, Newton steps,
+ *                  IEEE multiplies and FMAs only; within an ulp), where the
+ *                  reference calls its GPU math library's cbrtf.
  *   OR_DSSIM_F64   every stage in double with the same constants: the
  *                  value the f32 pipeline approximates.
  */
@@ -64,7 +67,7 @@ static inline int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ?
 static inline float lab_f32(float t) {
     const float eps = 216.0f / 24389.0f;
     const float k = 24389.0f / (27.0f * 116.0f);
-    return t > eps ? cbrtf(t) : fmaf(k, t, 16.0f / 116.0f);
+    return t > eps ? or_cbrtf(t) : fmaf(k, t, 16.0f / 116.0f);
 }
 
 void or_dssim_lab_f32(float r, float g, float b, float out[3]) {

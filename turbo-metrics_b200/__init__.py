@@ -1,4 +1,5 @@
-"""turbo-metrics B200: SSIMULACRA2 on sm_100a behind a C ABI.
+"""turbo-metrics B200: SSIMULACRA2 (and DSSIM from the same pyramid) on
+sm_100a behind a C ABI.
 
 Python host mirror of the `ssimulacra2-cuda` crate's `Ssimulacra2` type
 (crates/ssimulacra2-cuda/src/lib.rs:27-602) and of `ssim2-gpu`'s batch API
@@ -21,6 +22,6 @@ from .capi import (  # noqa: F401
     num_scales,
     version,
 )
-from .ssimulacra2 import Ssimulacra2, Ssim2Batch, PairDesc  # noqa: F401
+from .ssimulacra2 import Ssimulacra2, Ssim2Batch, PairDesc, Dssim  # noqa: F401
 from .server import Ssim2Server  # noqa: F401
 from .frames import FramePairScorer, Stats, select_frames  # noqa: F401

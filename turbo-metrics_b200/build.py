@@ -2,7 +2,7 @@
 
     python turbo-metrics_b200/build.py        # or: from build import build_library
 
-The kernels translation unit is compiled with -fmad=false: every fused
+The kernel translation units are compiled with -fmad=false: every fused
 multiply-add in it is written explicitly, so the CPU restatement of the same
 arithmetic can reproduce each rounding.
 """
@@ -20,6 +20,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
 UNITS = [
     ("ssim2_kernels.cu", ["-fmad=false"]),
     ("ssim2_iir.cu", ["-fmad=false"]),
+    ("dssim_kernels.cu", ["-fmad=false"]),
     ("ssim2_engine.cu", []),
     ("ssim2_noalloc.cu", []),
     ("ssim2_server.cu", []),

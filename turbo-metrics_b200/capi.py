@@ -75,7 +75,21 @@ class Config(ctypes.Structure):
 
 class Result(ctypes.Structure):
     _fields_ = [("score", ctypes.c_double), ("stats", ctypes.c_double * NUM_STATS),
-                ("sums", ctypes.c_double * NUM_STATS), ("n_scales", ctypes.c_int32), ("status", ctypes.c_int32)]
+                ("sums", ctypes.c_double * NUM_STATS), ("n_scales", ctypes.c_int32), ("status", ctypes.c_int32),
+                ("dssim", ctypes.c_double), ("dssim_scale", ctypes.c_double * 5)]
+
+
+METRIC = {"ssimulacra2": 1, "dssim": 2}
+
+
+def metrics_mask(metrics):
+    """'ssimulacra2', 'dssim' or an iterable of them -> S2_METRIC_* bits."""
+    if isinstance(metrics, str):
+        metrics = (metrics,)
+    m = 0
+    for name in metrics:
+        m |= METRIC[name]
+    return m
 
 
 class PairDescC(ctypes.Structure):
@@ -158,6 +172,15 @@ _sig = {
     "s2_server_reset_stats": (ctypes.c_int, [P]),
     "s2_compute_srgb8_noalloc": (ctypes.c_int, [P, ctypes.c_size_t, P, ctypes.c_size_t, ctypes.c_uint32,
                                                 ctypes.c_uint32, P, P]),
+    "s2_set_metrics": (ctypes.c_int, [P, ctypes.c_int32]),
+    "s2_batch_set_metrics": (ctypes.c_int, [P, ctypes.c_int32]),
+    "s2_get_dssim": (ctypes.c_int, [P, D, D]),
+    "s2_batch_last_dssim_ms": (ctypes.c_int, [P, ctypes.POINTER(ctypes.c_float)]),
+    "s2_dssim_create": (ctypes.c_int, [ctypes.c_int32, ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(P)]),
+    "s2_dssim_destroy": (None, [P]),
+    "s2_dssim_compute_srgb8": (ctypes.c_int, [P, P, ctypes.c_size_t, P, ctypes.c_size_t, ctypes.c_int32, P, D]),
+    "s2_dssim_compute_dis_only_srgb8": (ctypes.c_int, [P, P, ctypes.c_size_t, ctypes.c_int32, P, D]),
+    "s2_dssim_mem_usage": (ctypes.c_int, [P, ctypes.POINTER(ctypes.c_size_t)]),
 }
 for _name, (_res, _args) in _sig.items():
     _f = getattr(lib, _name)

@@ -23,6 +23,7 @@ constexpr int kSegW = 8;             // output pixels per segment (kSegs * kSegW
 constexpr int kChunk = 4;            // pixels per f32 partial sum
 constexpr int kPyrBlk = 64;          // scale-0 block edge of the prep kernel
 constexpr float kC2 = 0.0009f;
+constexpr int kDsLevels = 5;         // DSSIM scales (dssim-cuda/src/lib.rs:73)
 
 enum Format { FMT_LINEAR_F32 = 0, FMT_SRGB8 = 1, FMT_NV12 = 2, FMT_RGB16 = 3, FMT_P016 = 4 };
 enum Storage { ST_F32 = 0, ST_F16 = 1, ST_BF16 = 2 };
@@ -58,6 +59,39 @@ struct DevPair {
     float yuv[5];
     int yuv_min, yuv_neutral;
     int lvl_ext;             // images whose XYB planes live outside the submission (bit per image)
+    // DSSIM, the sibling metric sharing this pyramid: the prep pass also
+    // converts levels 0..lab_levels-1 to dssim-core's scaled Lab (3 f32
+    // planes per level, pitch lp[s]) and, when DSSIM's later levels are
+    // clamped to 8 pixels, keeps the linear RGB of level lab_levels-1 in
+    // `keep` (3 planes, pitch lp[s]) for the clamp pass.
+    float *lab[2][kDsLevels];
+    float *keep[2];
+    int lab_levels;          // 0: no Lab output
+    int prep_levels;         // levels the prep pass builds (XYB and Lab)
+};
+
+// One pair as the DSSIM kernels see it.  Level sizes follow dssim-cuda
+// (halved rounding up, never below 8: dssim-cuda/src/lib.rs:184-205).
+struct DsPair {
+    float *lab[2][kDsLevels];    // 3 planes (L, a, b) per level, `pitch` floats per row
+    float *map[kDsLevels];       // SSIM map per level, same pitch
+    float *keep[2];              // clamp pass source: linear RGB of level clamp_from - 1
+    float *scratch[2];           // clamp pass: two linear-RGB levels, 3 planes each
+    long long splane;            // floats per plane of one scratch level
+    int w[kDsLevels], h[kDsLevels], pitch[kDsLevels];
+    int tile_base[kDsLevels], tile_cnt[kDsLevels];
+    int kw, kh, kpitch;          // keep geometry
+    int clamp_from;              // first level the clamp pass builds (kDsLevels: none)
+    int prep_mask;
+    int status;
+};
+
+// A run of DSSIM tiles (32 x 32 outputs) of one (pair, level).
+struct DsSeg {
+    int first_tile;
+    int pair;
+    int level;
+    int tiles_x;
 };
 
 // A run of tiles of one (pair, scale); tiles are numbered across segments.
@@ -85,11 +119,14 @@ struct DevResult {
     double sums[108];
     int n_scales;
     int status;
+    double dssim;                // DSSIM of the pair (NaN when not scored)
+    double dssim_scale[kDsLevels];  // per-level 1 - mean |avg - ssim|
 };
 
 // ---------------------------------------------------------------------------
 // colour math
 // ---------------------------------------------------------------------------
+
 
 // Opsin absorbance (crates/ssimulacra2-cuda-kernel/src/xyb.rs:3-36).
 #define S2_M00 0.30f
@@ -149,6 +186,27 @@ __device__ __forceinline__ float s2_cbrtf_unit(float x) {
     const float e = fmaf(y * y, y, -x);
     const float c = (r * r) * third;
     return fmaf(-e, c, y);
+}
+
+// dssim-core's scaled Lab of one linear-RGB pixel, with the reference GPU's
+// f32 operations: fused multiply-adds where dssim-cuda-kernel/src/lab.rs:42-86
+// uses mul_add, IEEE divisions, a cube root above the CIE threshold and the
+// linear segment below it (lab.rs:37-44).  The cube root is s2_cbrtf (within
+// an ulp, like the math library's the reference calls), whose IEEE-only
+// operations the CPU restatement reproduces bit for bit: the SSIM map's
+// variance terms amplify ulp-level differences of the Lab values.
+__device__ __forceinline__ float ds_lab_f(float t) {
+    return t > 216.0f / 24389.0f ? s2_cbrtf(t) : fmaf(24389.0f / (27.0f * 116.0f), t, 16.0f / 116.0f);
+}
+
+__device__ __forceinline__ void ds_lab(float r, float g, float b, float o[3]) {
+    const float x = fmaf(0.4124f, r, fmaf(0.3576f, g, 0.1805f * b)) / 0.9505f;
+    const float y = fmaf(0.2126f, r, fmaf(0.7152f, g, 0.0722f * b)) / 1.0f;
+    const float z = fmaf(0.0193f, r, fmaf(0.1192f, g, 0.9505f * b)) / 1.089f;
+    const float fx = ds_lab_f(x), fy = ds_lab_f(y), fz = ds_lab_f(z);
+    o[0] = (fy - 16.0f / 116.0f) * 1.05f;
+    o[1] = fmaf(fx - fy, 500.0f / 220.0f, 86.2f / 220.0f);
+    o[2] = fmaf(fy - fz, 200.0f / 220.0f, 107.9f / 220.0f);
 }
 
 // a / b for b > 0 normal (the error-map denominators: >= 9e-4 and >= 1).

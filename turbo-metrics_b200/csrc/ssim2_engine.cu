@@ -271,6 +271,7 @@ struct s2_batch {
     std::deque<int> unread;  // slots whose results were not read, oldest first
     int last_slot = 0;
     bool profiling = false, graphs = true;
+    int metrics = S2_METRIC_SSIMULACRA2;
     s2_config cfg;
     uint32_t max_pairs = 0;
     uint64_t max_pixels = 0;
@@ -285,6 +286,7 @@ struct s2_batch {
             return st;
         }
         eng[k].graphs = graphs;
+        eng[k].metrics = metrics;
         ready[k] = true;
         return S2_OK;
     }
@@ -346,7 +348,13 @@ static s2_status check_cfg(const s2_config *cfg) {
     return S2_OK;
 }
 
+static s2_status ctx_create(const s2_config *cfg_in, uint32_t width, uint32_t height, int metrics, s2_ctx **out);
+
 s2_status s2_create(const s2_config *cfg_in, uint32_t width, uint32_t height, s2_ctx **out) {
+    return ctx_create(cfg_in, width, height, S2_METRIC_SSIMULACRA2, out);
+}
+
+static s2_status ctx_create(const s2_config *cfg_in, uint32_t width, uint32_t height, int metrics, s2_ctx **out) {
     if (!out) return S2_ERR_INVALID_ARG;
     *out = nullptr;
     s2_config cfg;
@@ -354,7 +362,8 @@ s2_status s2_create(const s2_config *cfg_in, uint32_t width, uint32_t height, s2
     else s2_config_default(&cfg);
     s2_status st = check_cfg(&cfg);
     if (st != S2_OK) return st;
-    if (s2_num_scales_rule(width, height, cfg.scale_rule) == 0 || width > 65536 || height > 65536)
+    if (((metrics & S2_METRIC_SSIMULACRA2) && s2_num_scales_rule(width, height, cfg.scale_rule) == 0) ||
+        ((metrics & S2_METRIC_DSSIM) && (width < 8 || height < 8)) || width > 65536 || height > 65536)
         return S2_ERR_INVALID_SIZE;
     // pre-flight: levels (2 images, ~1/3 of scale 0) + partials + staging
     {
@@ -371,6 +380,7 @@ s2_status s2_create(const s2_config *cfg_in, uint32_t width, uint32_t height, s2
     c->h = height;
     st = c->eng.init(&cfg);
     c->eng.graphs = true;
+    c->eng.metrics = metrics;
     if (st == S2_OK) {
         // allocate the steady-state buffers now (like the reference's new)
         s2_pair_desc d;
@@ -384,6 +394,7 @@ s2_status s2_create(const s2_config *cfg_in, uint32_t width, uint32_t height, s2
         if (st == S2_OK)
             st = c->eng.ensure(c->eng.partials_d, std::max<size_t>((size_t)c->plan.total_tiles * 18 * 8, 256));
         if (st == S2_OK) st = c->eng.ensure(c->eng.results_d, sizeof(DevResult));
+        if (st == S2_OK && (metrics & S2_METRIC_DSSIM)) st = c->eng.ensure(c->eng.ds_d, Engine::ds_bytes(c->plan));
     }
     if (st != S2_OK) {
         c->eng.release();
@@ -593,6 +604,7 @@ static s2_status set_ref(s2_ctx *ctx, const s2_pair_desc &d, void *stream) {
     PairExtra build;
     build.prep_mask = 1;
     build.score = false;
+    build.dssim = false;
     for (int s = 0; s < kScales; s++)
         build.ref_levels[s] = s < ns ? (char *)ctx->ref_levels.p + off[s] : nullptr;
     ctx->has_ref = false;
@@ -764,6 +776,9 @@ s2_status s2_batch_results(s2_batch *b, s2_result *out, uint32_t n) {
         memcpy(out[i].sums, r.sums, sizeof r.sums);
         out[i].n_scales = r.n_scales;
         out[i].status = r.status;
+        const bool ds = (b->plan[k].metrics & S2_METRIC_DSSIM) != 0;
+        out[i].dssim = ds ? r.dssim : std::nan("");
+        for (int s = 0; s < kDsLevels; s++) out[i].dssim_scale[s] = ds ? r.dssim_scale[s] : std::nan("");
     }
     return S2_OK;
 }
@@ -818,6 +833,114 @@ s2_status s2_set_graphs(s2_ctx *ctx, int32_t enable) {
     ctx->eng.graphs = enable != 0;
     if (!ctx->eng.graphs) ctx->eng.drop_graphs();
     return S2_OK;
+}
+
+// ---- DSSIM --------------------------------------------------------------
+static bool metrics_ok(int32_t m) { return m >= 1 && m <= 3; }
+
+s2_status s2_set_metrics(s2_ctx *ctx, int32_t metrics) {
+    if (!ctx || !metrics_ok(metrics)) return S2_ERR_INVALID_ARG;
+    if ((metrics & S2_METRIC_SSIMULACRA2) && s2_num_scales_rule(ctx->w, ctx->h, ctx->eng.scale_rule) == 0)
+        return S2_ERR_INVALID_SIZE;
+    if ((metrics & S2_METRIC_DSSIM) && (ctx->w < 8 || ctx->h < 8)) return S2_ERR_INVALID_SIZE;
+    ctx->eng.metrics = metrics;
+    return S2_OK;
+}
+
+s2_status s2_batch_set_metrics(s2_batch *b, int32_t metrics) {
+    if (!b || !metrics_ok(metrics)) return S2_ERR_INVALID_ARG;
+    b->metrics = metrics;
+    for (int k = 0; k < 2; k++)
+        if (b->ready[k]) b->eng[k].metrics = metrics;
+    return S2_OK;
+}
+
+s2_status s2_batch_last_dssim_ms(s2_batch *b, float *ms) {
+    if (!b || !ms) return S2_ERR_INVALID_ARG;
+    float t[3];
+    return b->eng[b->last_slot].timings(t, ms);
+}
+
+s2_status s2_get_dssim(s2_ctx *ctx, double *dssim, double scale_scores[5]) {
+    if (!ctx) return S2_ERR_INVALID_ARG;
+    if (ctx->last_was_ref_build) return S2_ERR_NOT_READY;
+    s2_status st = ctx->eng.wait();
+    if (st != S2_OK) return st;
+    const Plan &P = ctx->plan;
+    if (!(P.metrics & S2_METRIC_DSSIM) || P.ds.empty() || P.ds[0].status == -1) return S2_ERR_NOT_READY;
+    const DevResult &r = ctx->eng.results_h[0];
+    if (r.status != S2_OK) return (s2_status)r.status;
+    if (dssim) *dssim = r.dssim;
+    if (scale_scores)
+        for (int s = 0; s < kDsLevels; s++) scale_scores[s] = r.dssim_scale[s];
+    return S2_OK;
+}
+
+// s2_dssim: a context scoring DSSIM only.  A full compute leaves both
+// images' Lab planes in the context's workspace at offsets fixed by its size;
+// compute_dis_only converts the distorted image alone and reads the
+// reference's planes from there.
+struct s2_dssim {
+    s2_ctx *ctx = nullptr;
+    bool has_ref = false;
+};
+
+s2_status s2_dssim_create(int32_t device, uint32_t width, uint32_t height, s2_dssim **out) {
+    if (!out) return S2_ERR_INVALID_ARG;
+    *out = nullptr;
+    s2_config cfg;
+    s2_config_default(&cfg);
+    cfg.device = device;
+    s2_dssim *d = new (std::nothrow) s2_dssim();
+    if (!d) return S2_ERR_OOM;
+    s2_status st = ctx_create(&cfg, width, height, S2_METRIC_DSSIM, &d->ctx);
+    if (st != S2_OK) {
+        delete d;
+        return st;
+    }
+    *out = d;
+    return S2_OK;
+}
+
+void s2_dssim_destroy(s2_dssim *d) {
+    if (!d) return;
+    s2_destroy(d->ctx);
+    delete d;
+}
+
+s2_status s2_dssim_compute_srgb8(s2_dssim *d, const uint8_t *ref, size_t ref_pitch, const uint8_t *dis,
+                                 size_t dis_pitch, int32_t on_host, void *stream, double *dssim) {
+    if (!d || !dssim) return S2_ERR_INVALID_ARG;
+    d->has_ref = false;
+    s2_status st = s2_compute_srgb8(d->ctx, ref, ref_pitch, dis, dis_pitch, on_host, stream);
+    if (st == S2_OK) st = s2_get_dssim(d->ctx, dssim, nullptr);
+    if (st == S2_OK) d->has_ref = true;
+    return st;
+}
+
+s2_status s2_dssim_compute_dis_only_srgb8(s2_dssim *d, const uint8_t *dis, size_t dis_pitch, int32_t on_host,
+                                          void *stream, double *dssim) {
+    if (!d || !dis || !dssim) return S2_ERR_INVALID_ARG;
+    if (!d->has_ref) return S2_ERR_NO_REFERENCE;
+    s2_ctx *ctx = d->ctx;
+    const size_t row = (size_t)ctx->w * 3;
+    if (dis_pitch < row) return S2_ERR_DIM_MISMATCH;
+    const void *dv = dis;
+    size_t dp = dis_pitch;
+    if (on_host) {
+        s2_status st = stage_host(ctx, 1, dis, dis_pitch, row, ctx->h, stream, &dv, &dp);
+        if (st != S2_OK) return st;
+    }
+    PairExtra ex;
+    ex.prep_mask = 2;
+    s2_status st = ctx_run(ctx, make_desc(ctx->w, ctx->h, S2_FMT_SRGB8, nullptr, 0, dv, dp), stream, &ex);
+    if (st == S2_OK) st = s2_get_dssim(ctx, dssim, nullptr);
+    return st;
+}
+
+s2_status s2_dssim_mem_usage(const s2_dssim *d, size_t *bytes) {
+    if (!d) return S2_ERR_INVALID_ARG;
+    return s2_mem_usage(d->ctx, bytes);
 }
 
 }  // extern "C"

@@ -75,8 +75,20 @@ inline int s2_num_scales_rule(uint32_t w, uint32_t h, int rule) {
 struct PairExtra {
     int prep_mask = 3;
     bool score = true;
+    bool dssim = true;  // score DSSIM too when the engine's metrics include it
     void *ref_levels[kScales] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
 };
+
+// DSSIM level sizes (dssim-cuda/src/lib.rs:184-205): halved rounding up,
+// never below 8.
+inline void s2_dssim_dims(uint32_t w, uint32_t h, int dw[kDsLevels], int dh[kDsLevels]) {
+    for (int s = 0; s < kDsLevels; s++) {
+        dw[s] = (int)w;
+        dh[s] = (int)h;
+        w = std::max<uint32_t>((w + 1) / 2, 8);
+        h = std::max<uint32_t>((h + 1) / 2, 8);
+    }
+}
 
 // Host-side bytes of one image of a pair: its main plane (rows x row bytes)
 // and, for NV12, the interleaved chroma plane (height / 2 rows of width bytes).
@@ -129,6 +141,34 @@ struct Plan {
     std::vector<IirSeg> vsegs, hsegs;
     int vtotal = 0, htotal = 0;
     size_t v_bytes = 0;
+    // DSSIM (metrics include S2_METRIC_DSSIM): per-pair descriptors, tile
+    // runs, and whether any pair needs the clamp pass
+    int metrics = S2_METRIC_SSIMULACRA2;
+    std::vector<DsPair> ds;
+    std::vector<DsSeg> dsegs;
+    int ds_tiles = 0;
+    bool ds_clamp = false;
+
+    // descriptor region: pairs | blk_first | segs | IIR vsegs | hsegs | DSSIM pairs | DSSIM segs
+    struct Layout {
+        size_t pb, bb, sb, vsb, hsb, dpb, dsb;
+        size_t total() const { return pb + bb + sb + vsb + hsb + dpb + dsb; }
+        size_t ds_pairs() const { return pb + bb + sb + vsb + hsb; }
+        size_t ds_segs() const { return ds_pairs() + dpb; }
+    };
+    Layout layout() const {
+        const size_t n = pairs.size();
+        Layout L;
+        L.pb = s2_align_up(n * sizeof(DevPair), 256);
+        L.bb = s2_align_up(n * sizeof(int), 256);
+        L.sb = s2_align_up(std::max<size_t>(segs.size(), 1) * sizeof(Seg), 256);
+        L.vsb = s2_align_up(vsegs.size() * sizeof(IirSeg), 256);
+        L.hsb = s2_align_up(hsegs.size() * sizeof(IirSeg), 256);
+        const bool d = (metrics & S2_METRIC_DSSIM) != 0;
+        L.dpb = d ? s2_align_up(n * sizeof(DsPair), 256) : 0;
+        L.dsb = d ? s2_align_up(std::max<size_t>(dsegs.size(), 1) * sizeof(DsSeg), 256) : 0;
+        return L;
+    }
 };
 
 struct Engine {
@@ -137,6 +177,7 @@ struct Engine {
     int scale_rule = S2_SCALES_CPU;
     int strip_rows_cfg = 0;
     int blur = S2_BLUR_FIR;
+    int metrics = S2_METRIC_SSIMULACRA2;  // S2_METRIC_* bits scored by each submission
     uint64_t budget = 0;
     size_t allocated = 0;
     int num_sms = 148;
@@ -144,6 +185,7 @@ struct Engine {
     ColorConsts cc;
 
     DevBuf pairs_d, blk_d, segs_d, counter_d, partials_d, results_d, levels_d, lut_d, iir_d;
+    DevBuf ds_d;  // DSSIM: per-tile SSIM sums, per-tile |avg - ssim| sums, per-level avg
     void *pinned = nullptr;  // staging: pairs | blk_first | segs
     size_t pinned_n = 0;
     DevResult *results_h = nullptr;
@@ -153,7 +195,8 @@ struct Engine {
     bool pending = false;
     Plan plan_storage;  // a submission's plan, owned by whoever drives this engine
     bool profiling = false;
-    cudaEvent_t prof[4] = {nullptr, nullptr, nullptr, nullptr};
+    // start, prep done, tile pass done, finalize done, DSSIM passes done
+    cudaEvent_t prof[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     // host-input submissions: staging for the uploaded planes, the copy
     // stream and the prep stream (a group's prep runs beside the previous
     // group's tile launch, filling the SMs its last wave leaves idle), one
@@ -173,7 +216,7 @@ struct Engine {
     bool desc_kernel = false;
     void *pinned_dev = nullptr;  // device address of the pinned staging
     struct GraphEntry {
-        uint64_t key[7];
+        uint64_t key[8];
         cudaGraphExec_t exec;
     };
     std::vector<GraphEntry> gcache;
@@ -213,10 +256,11 @@ struct Engine {
         return S2_OK;
     }
 
-    s2_status timings(float ms[3]) {
+    s2_status timings(float ms[3], float *ds_ms = nullptr) {
         if (!profiling || last_n < 0) return S2_ERR_NOT_READY;
-        S2_CUDA(cudaEventSynchronize(prof[3]));
+        S2_CUDA(cudaEventSynchronize(prof[4]));
         for (int i = 0; i < 3; i++) S2_CUDA(cudaEventElapsedTime(&ms[i], prof[i], prof[i + 1]));
+        if (ds_ms) S2_CUDA(cudaEventElapsedTime(ds_ms, prof[3], prof[4]));
         return S2_OK;
     }
 
@@ -236,7 +280,7 @@ struct Engine {
         if (sub_start) cudaEventDestroy(sub_start), sub_start = nullptr;
         if (stage_free) cudaEventDestroy(stage_free), stage_free = nullptr;
         for (DevBuf *b : {&pairs_d, &blk_d, &segs_d, &counter_d, &partials_d, &results_d, &levels_d, &lut_d, &iir_d,
-                          &stage_d})
+                          &stage_d, &ds_d})
             if (b->p) cudaFree(b->p), b->p = nullptr, b->n = 0;
         if (pinned) cudaFreeHost(pinned), pinned = nullptr;
         if (results_h) cudaFreeHost(results_h), results_h = nullptr;
@@ -323,6 +367,7 @@ struct Engine {
     int choose_strip_rows(const std::vector<uint64_t> &tiles_at, Plan &P) const {
         P.needs_tune = false;
         if (force_strip) return force_strip;
+        if (tiles_at[0] == 0) return 63;  // no tile pass (DSSIM only, or no valid pair)
         if (strip_rows_cfg == 9 || strip_rows_cfg == 21 || strip_rows_cfg == 63) return strip_rows_cfg;
         const uint64_t resident = (uint64_t)num_sms * (uint64_t)fused_bps;
         if (blur == S2_BLUR_FIR) {
@@ -336,16 +381,75 @@ struct Engine {
         return 9;
     }
 
+    // DSSIM layout of one valid pair (offsets into levels_d, rebased at
+    // upload): Lab planes and SSIM map of each of the five levels; levels
+    // whose DSSIM size equals the pyramid's ceil-halved size are written by
+    // the prep pass, later ones (clamped to 8) by the clamp pass from the
+    // kept linear RGB of the last equal level.
+    static size_t plan_dssim(const s2_pair_desc &q, DevPair &p, DsPair &D, size_t off, const PairExtra *ex,
+                             bool &clamp) {
+        memset(&D, 0, sizeof D);
+        D.prep_mask = p.prep_mask;
+        D.clamp_from = kDsLevels;
+        if (ex && (!ex->dssim || !ex->score)) {  // not scored by this submission
+            D.status = -1;
+            p.lab_levels = 0;
+            p.prep_levels = p.nscales;
+            return off;
+        }
+        int dw[kDsLevels], dh[kDsLevels];
+        s2_dssim_dims(q.width, q.height, dw, dh);
+        int ll = 0;
+        while (ll < kDsLevels && dw[ll] == p.w[ll] && dh[ll] == p.h[ll]) ll++;
+        p.lab_levels = ll;
+        p.prep_levels = std::max(p.nscales, ll);
+        for (int s = 0; s < p.prep_levels; s++) p.lp[s] = (int)s2_align_up((size_t)p.w[s], 64);
+        for (int s = 0; s < kDsLevels; s++) {
+            D.w[s] = dw[s];
+            D.h[s] = dh[s];
+            D.pitch[s] = (int)s2_align_up((size_t)dw[s], 64);
+            const size_t plane = (size_t)D.pitch[s] * dh[s] * sizeof(float);
+            for (int img = 0; img < 2; img++) {
+                D.lab[img][s] = (float *)off;
+                if (s < ll) p.lab[img][s] = D.lab[img][s];
+                off += s2_align_up(3 * plane, 256);
+            }
+            D.map[s] = (float *)off;
+            off += s2_align_up(plane, 256);
+        }
+        D.clamp_from = ll;
+        if (ll < kDsLevels) {
+            clamp = true;
+            const int k = ll - 1;
+            D.kw = p.w[k];
+            D.kh = p.h[k];
+            D.kpitch = p.lp[k];
+            long long sp = 0;
+            for (int s = ll; s < kDsLevels; s++) sp = std::max<long long>(sp, (long long)D.pitch[s] * dh[s]);
+            D.splane = sp;
+            for (int img = 0; img < 2; img++) {
+                p.keep[img] = D.keep[img] = (float *)off;
+                off += s2_align_up((size_t)3 * D.kpitch * D.kh * sizeof(float), 256);
+                D.scratch[img] = (float *)off;
+                off += s2_align_up((size_t)6 * sp * sizeof(float), 256);
+            }
+        }
+        return off;
+    }
+
     // Lay out the levels and tiles of n pairs.
     s2_status plan(const s2_pair_desc *d, int n, Plan &P, const PairExtra *ex = nullptr, int ngroups = 1) {
         P = Plan();
+        P.metrics = metrics;
+        const bool m_s2 = (metrics & S2_METRIC_SSIMULACRA2) != 0, m_ds = (metrics & S2_METRIC_DSSIM) != 0;
         P.pairs.resize(n);
         P.blk_first.resize(n);
+        if (m_ds) P.ds.assign(n, DsPair());
         // tile counts at strip heights 64/32 for the strip choice
         std::vector<uint64_t> tiles_at(2, 0);
         std::vector<int> ns(n);
         for (int i = 0; i < n; i++) {
-            ns[i] = s2_num_scales_rule(d[i].width, d[i].height, scale_rule);
+            ns[i] = m_s2 ? s2_num_scales_rule(d[i].width, d[i].height, scale_rule) : 0;
             uint64_t w = d[i].width, h = d[i].height;
             for (int s = 0; s < ns[i]; s++) {
                 tiles_at[0] += ((w + kTileW - 1) / kTileW) * ((h + 62) / 63);
@@ -374,7 +478,8 @@ struct Engine {
             p.prep_mask = ex ? ex[i].prep_mask : 3;
             const bool need_ref_in = (p.prep_mask & 1) != 0;
             const bool need_dis_in = (p.prep_mask & 2) != 0;
-            if (ns[i] == 0 || q.width > (1u << 16) || q.height > (1u << 16)) {
+            if ((m_s2 && ns[i] == 0) || (m_ds && (q.width < 8 || q.height < 8)) || q.width > (1u << 16) ||
+                q.height > (1u << 16)) {
                 p.status = S2_ERR_INVALID_SIZE;
                 p.nscales = 0;
                 P.blk_first[i] = blk;
@@ -412,6 +517,7 @@ struct Engine {
                 p.lvl[1][s] = (void *)lvl_off;
                 lvl_off += bytes;
             }
+            if (m_ds) lvl_off = plan_dssim(q, p, P.ds[i], lvl_off, ex ? &ex[i] : nullptr, P.ds_clamp);
             P.blk_first[i] = blk;
             {
                 p.blk_x = (p.w[0] + kPyrBlk - 1) / kPyrBlk;
@@ -422,6 +528,27 @@ struct Engine {
         }
         P.total_blocks = blk;
         P.level_bytes = lvl_off;
+        if (m_ds) {
+            for (int i = 0; i < n; i++)
+                if (P.pairs[i].status != S2_OK) P.ds[i].status = P.pairs[i].status;
+            // DSSIM tiles: all pairs' level 0 first, then level 1, ...
+            int dt = 0;
+            for (int s = 0; s < kDsLevels; s++)
+                for (int i = 0; i < n; i++) {
+                    DsPair &D = P.ds[i];
+                    if (D.status != 0) continue;
+                    DsSeg sg;
+                    sg.first_tile = dt;
+                    sg.pair = i;
+                    sg.level = s;
+                    sg.tiles_x = (D.w[s] + 31) / 32;
+                    D.tile_base[s] = dt;
+                    D.tile_cnt[s] = sg.tiles_x * ((D.h[s] + 31) / 32);
+                    dt += D.tile_cnt[s];
+                    P.dsegs.push_back(sg);
+                }
+            P.ds_tiles = dt;
+        }
         if (blur == S2_BLUR_IIR_REF) {
             P.grp_pair = {0, n};
             P.grp_tile = {0, 0};
@@ -539,13 +666,13 @@ struct Engine {
         if ((r = ensure(levels_d, std::max<size_t>(P.level_bytes, 256))) != S2_OK) return r;
         if ((r = ensure(partials_d, std::max<size_t>((size_t)P.total_tiles * 18 * sizeof(double), 256))) != S2_OK) return r;
         if ((r = ensure(results_d, (size_t)n * sizeof(DevResult))) != S2_OK) return r;
-        const size_t pb = s2_align_up(n * sizeof(DevPair), 256), bb = s2_align_up(n * sizeof(int), 256),
-                     sb = s2_align_up(std::max<size_t>(P.segs.size(), 1) * sizeof(Seg), 256);
-        const size_t vsb = s2_align_up(P.vsegs.size() * sizeof(IirSeg), 256),
-                     hsb = s2_align_up(P.hsegs.size() * sizeof(IirSeg), 256);
+        const Plan::Layout L = P.layout();
+        const size_t pb = L.pb, bb = L.bb, sb = L.sb, vsb = L.vsb;
+        const bool m_s2 = (P.metrics & S2_METRIC_SSIMULACRA2) != 0, m_ds = (P.metrics & S2_METRIC_DSSIM) != 0;
         if (blur == S2_BLUR_IIR_REF && (r = ensure(iir_d, std::max<size_t>(P.v_bytes, 256))) != S2_OK) return r;
-        if ((r = ensure(pairs_d, pb + bb + sb + vsb + hsb)) != S2_OK) return r;
-        if ((r = ensure_pinned(pb + bb + sb + vsb + hsb, n)) != S2_OK) return r;
+        if (m_ds && (r = ensure(ds_d, ds_bytes(P))) != S2_OK) return r;
+        if ((r = ensure(pairs_d, L.total())) != S2_OK) return r;
+        if ((r = ensure_pinned(L.total(), n)) != S2_OK) return r;
         if (host) {
             if ((r = ensure(stage_d, std::max<size_t>(plan_staging(P, host), 256))) != S2_OK) return r;
             if (!copy_st) {
@@ -562,6 +689,7 @@ struct Engine {
         if (pending) S2_CUDA(cudaEventSynchronize(done));
         char *h = (char *)pinned;
         DevPair *hp = (DevPair *)h;
+        char *const lb = (char *)levels_d.p;
         for (int i = 0; i < n; i++) {
             hp[i] = P.pairs[i];
             for (int s = 0; s < kScales; s++)
@@ -569,6 +697,15 @@ struct Engine {
                     if (s >= hp[i].nscales) hp[i].lvl[img][s] = nullptr;
                     else if (!((hp[i].lvl_ext >> img) & 1))
                         hp[i].lvl[img][s] = (char *)levels_d.p + (size_t)hp[i].lvl[img][s];
+            if (m_ds && hp[i].status == S2_OK) {
+                for (int img = 0; img < 2; img++) {
+                    for (int s = 0; s < kDsLevels; s++)
+                        hp[i].lab[img][s] = s < hp[i].lab_levels ? (float *)(lb + (size_t)hp[i].lab[img][s]) : nullptr;
+                    hp[i].keep[img] = hp[i].lab_levels > 0 && hp[i].lab_levels < kDsLevels
+                                          ? (float *)(lb + (size_t)hp[i].keep[img])
+                                          : nullptr;
+                }
+            }
             if (host && hp[i].status == S2_OK)
                 for (int img = 0; img < 2; img++)
                     if ((hp[i].prep_mask >> img) & 1) {
@@ -590,18 +727,38 @@ struct Engine {
                 hh[k].v = (float *)((char *)iir_d.p + (size_t)P.hsegs[k].v);
             }
         }
+        if (m_ds) {
+            DsPair *hd = (DsPair *)(h + L.ds_pairs());
+            for (int i = 0; i < n; i++) {
+                hd[i] = P.ds[i];
+                if (hd[i].status != 0) continue;
+                for (int s = 0; s < kDsLevels; s++) {
+                    for (int img = 0; img < 2; img++) hd[i].lab[img][s] = (float *)(lb + (size_t)hd[i].lab[img][s]);
+                    hd[i].map[s] = (float *)(lb + (size_t)hd[i].map[s]);
+                }
+                for (int img = 0; img < 2; img++)
+                    if (hd[i].clamp_from < kDsLevels) {
+                        hd[i].keep[img] = (float *)(lb + (size_t)hd[i].keep[img]);
+                        hd[i].scratch[img] = (float *)(lb + (size_t)hd[i].scratch[img]);
+                    }
+            }
+            if (!P.dsegs.empty()) memcpy(h + L.ds_segs(), P.dsegs.data(), P.dsegs.size() * sizeof(DsSeg));
+        }
         char *dbase = (char *)pairs_d.p;
         const DevPair *dpairs = (const DevPair *)dbase;
         const int *dblk = (const int *)(dbase + pb);
         const Seg *dsegs = (const Seg *)(dbase + pb + bb);
+        const int pout = (m_s2 ? 1 : 0) | (m_ds ? 2 : 0);
         if (graphs && !host && !profiling && ng == 1) {
-            const uint64_t key[7] = {(uint64_t)n, (uint64_t)P.total_blocks, (uint64_t)P.total_tiles, P.segs.size(),
+            const uint64_t key[8] = {(uint64_t)n, (uint64_t)P.total_blocks, (uint64_t)P.total_tiles, P.segs.size(),
                                      P.vsegs.size(), P.hsegs.size(),
-                                     ((uint64_t)(uint32_t)P.vtotal << 32) | (uint32_t)P.htotal};
+                                     ((uint64_t)(uint32_t)P.vtotal << 32) | (uint32_t)P.htotal,
+                                     ((uint64_t)(uint32_t)P.ds_tiles << 32) | ((uint64_t)P.dsegs.size() << 3) |
+                                         ((uint64_t)P.ds_clamp << 2) | (uint64_t)P.metrics};
             cudaGraphExec_t ex = nullptr;
             for (const GraphEntry &g : gcache)
                 if (!memcmp(g.key, key, sizeof key)) ex = g.exec;
-            if (!ex) ex = capture(P, key, pb + bb + sb + vsb + hsb);
+            if (!ex) ex = capture(P, key, L.total());
             if (ex) {
                 S2_CUDA(cudaGraphLaunch(ex, st));
                 S2_CUDA(cudaEventRecord(done, st));
@@ -618,9 +775,9 @@ struct Engine {
         const bool split = host && blur != S2_BLUR_IIR_REF;
         if (host) S2_CUDA(cudaStreamWaitEvent(copy_st, stage_free, 0));
         if (desc_kernel && !split)
-            S2_CUDA(launch_desc_copy(dbase, pinned_dev, pb + bb + sb + vsb + hsb, st));
+            S2_CUDA(launch_desc_copy(dbase, pinned_dev, L.total(), st));
         else
-            S2_CUDA(cudaMemcpyAsync(dbase, h, pb + bb + sb + vsb + hsb, cudaMemcpyHostToDevice, split ? copy_st : st));
+            S2_CUDA(cudaMemcpyAsync(dbase, h, L.total(), cudaMemcpyHostToDevice, split ? copy_st : st));
         if (split) {
             S2_CUDA(cudaEventRecord(sub_start, copy_st));
             S2_CUDA(cudaStreamWaitEvent(st, sub_start, 0));
@@ -652,13 +809,15 @@ struct Engine {
             }
             const int b0 = pa < n ? P.blk_first[pa] : P.total_blocks;
             const int b1 = pe < n ? P.blk_first[pe] : P.total_blocks;
-            S2_CUDA(launch_pyramid(storage, dpairs, n, dblk, b0, b1, cc, (const float *)lut_d.p, num_sms * 8, pst));
+            S2_CUDA(launch_pyramid(storage, dpairs, n, dblk, b0, b1, cc, (const float *)lut_d.p, num_sms * 8, pst,
+                                   pout));
             if (host && g + 1 == ng) S2_CUDA(cudaEventRecord(stage_free, pst));
             if (split) {
                 S2_CUDA(cudaEventRecord(grp_prepped[g], prep_st));
                 S2_CUDA(cudaStreamWaitEvent(st, grp_prepped[g], 0));
             }
             if (profiling && ng == 1) S2_CUDA(cudaEventRecord(prof[1], st));
+            if (!m_s2) continue;
             if (blur == S2_BLUR_IIR_REF)
                 S2_CUDA(launch_iir(storage, dpairs, (const IirSeg *)(dbase + pb + bb + sb), (int)P.vsegs.size(),
                                    P.vtotal, (const IirSeg *)(dbase + pb + bb + sb + vsb), (int)P.hsegs.size(),
@@ -670,8 +829,10 @@ struct Engine {
         // several groups interleave prep and fused: the fused slot then holds both
         if (profiling && ng > 1) S2_CUDA(cudaEventRecord(prof[1], st));
         if (profiling) S2_CUDA(cudaEventRecord(prof[2], st));
-        S2_CUDA(launch_finalize(dpairs, n, (const double *)partials_d.p, (DevResult *)results_d.p, st));
+        if (m_s2) S2_CUDA(launch_finalize(dpairs, n, (const double *)partials_d.p, (DevResult *)results_d.p, st));
         if (profiling) S2_CUDA(cudaEventRecord(prof[3], st));
+        if (m_ds) S2_CUDA(launch_ds(P, dbase, st));
+        if (profiling) S2_CUDA(cudaEventRecord(prof[4], st));
         S2_CUDA(cudaMemcpyAsync(results_h, results_d.p, n * sizeof(DevResult), cudaMemcpyDeviceToHost, st));
         S2_CUDA(cudaEventRecord(done, st));
         last_n = n;
@@ -679,16 +840,32 @@ struct Engine {
         return S2_OK;
     }
 
+    // DSSIM workspace: two f64 sums per tile, one f32 avg per (pair, level).
+    static size_t ds_bytes(const Plan &P) {
+        return s2_align_up((size_t)2 * std::max(P.ds_tiles, 1) * sizeof(double), 256) +
+               P.pairs.size() * kDsLevels * sizeof(float);
+    }
+
+    cudaError_t launch_ds(const Plan &P, char *dbase, cudaStream_t st) {
+        const Plan::Layout L = P.layout();
+        const int n = (int)P.pairs.size();
+        double *part = (double *)ds_d.p;
+        float *avg = (float *)((char *)ds_d.p + s2_align_up((size_t)2 * std::max(P.ds_tiles, 1) * sizeof(double), 256));
+        return launch_dssim((const DsPair *)(dbase + L.ds_pairs()), n, (const DsSeg *)(dbase + L.ds_segs()),
+                            (int)P.dsegs.size(), P.ds_tiles, P.ds_clamp, part, avg, (DevResult *)results_d.p,
+                            (P.metrics & S2_METRIC_SSIMULACRA2) == 0, num_sms, st);
+    }
+
     // Record a single-group device-input submission of plan P (its
     // descriptors already in the pinned staging) as a graph: descriptor
     // upload, counter reset, prep, fused (or the two IIR passes), finalize,
     // result download.  nullptr if capture is not possible here (graphs are
     // then switched off for this engine and the launches go directly).
-    cudaGraphExec_t capture(const Plan &P, const uint64_t key[7], size_t desc_bytes) {
+    cudaGraphExec_t capture(const Plan &P, const uint64_t key[8], size_t desc_bytes) {
         const int n = (int)P.pairs.size();
-        const size_t pb = s2_align_up(n * sizeof(DevPair), 256), bb = s2_align_up(n * sizeof(int), 256),
-                     sb = s2_align_up(std::max<size_t>(P.segs.size(), 1) * sizeof(Seg), 256),
-                     vsb = s2_align_up(P.vsegs.size() * sizeof(IirSeg), 256);
+        const Plan::Layout L = P.layout();
+        const size_t pb = L.pb, bb = L.bb, sb = L.sb, vsb = L.vsb;
+        const bool m_s2 = (P.metrics & S2_METRIC_SSIMULACRA2) != 0, m_ds = (P.metrics & S2_METRIC_DSSIM) != 0;
         char *dbase = (char *)pairs_d.p;
         const DevPair *dpairs = (const DevPair *)dbase;
         if (!cap_st && cudaStreamCreateWithFlags(&cap_st, cudaStreamNonBlocking) != cudaSuccess) {
@@ -704,8 +881,8 @@ struct Engine {
         if (e == cudaSuccess) e = cudaMemsetAsync(counter_d.p, 0, sizeof(int), cap_st);
         if (e == cudaSuccess)
             e = launch_pyramid(storage, dpairs, n, (const int *)(dbase + pb), 0, P.total_blocks, cc,
-                               (const float *)lut_d.p, num_sms * 8, cap_st);
-        if (e == cudaSuccess) {
+                               (const float *)lut_d.p, num_sms * 8, cap_st, (m_s2 ? 1 : 0) | (m_ds ? 2 : 0));
+        if (e == cudaSuccess && m_s2) {
             if (blur == S2_BLUR_IIR_REF)
                 e = launch_iir(storage, dpairs, (const IirSeg *)(dbase + pb + bb + sb), (int)P.vsegs.size(), P.vtotal,
                                (const IirSeg *)(dbase + pb + bb + sb + vsb), (int)P.hsegs.size(), P.htotal,
@@ -715,8 +892,9 @@ struct Engine {
                                  P.total_tiles, (int *)counter_d.p, (double *)partials_d.p, num_sms * fused_bps,
                                  cap_st);
         }
-        if (e == cudaSuccess)
+        if (e == cudaSuccess && m_s2)
             e = launch_finalize(dpairs, n, (const double *)partials_d.p, (DevResult *)results_d.p, cap_st);
+        if (e == cudaSuccess && m_ds) e = launch_ds(P, dbase, cap_st);
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(results_h, results_d.p, n * sizeof(DevResult), cudaMemcpyDeviceToHost, cap_st);
         cudaGraph_t graph = nullptr;

@@ -140,12 +140,34 @@ __device__ __forceinline__ void store_xyb_pair(ST *dst, long long plane, long lo
 
 constexpr int kLv1 = kPyrBlk / 2;  // scale-1 block edge (32)
 
-template <int FMT, typename ST>
+// DSSIM outputs of one level's pixel: its Lab (levels below lab_levels) and,
+// for the clamp pass, its linear RGB (level lab_levels - 1, when kept).
+__device__ __forceinline__ void store_lab(const DevPair &P, int img, int s, int x, int y, const float lin[3]) {
+    const long long plane = (long long)P.lp[s] * P.h[s];
+    const long long off = (long long)y * P.lp[s] + x;
+    if (s < P.lab_levels) {
+        float o[3];
+        ds_lab(lin[0], lin[1], lin[2], o);
+        float *dst = P.lab[img][s];
+#pragma unroll
+        for (int c = 0; c < 3; c++) dst[c * plane + off] = o[c];
+    }
+    if (s == P.lab_levels - 1 && P.keep[img]) {
+        float *dst = P.keep[img];
+#pragma unroll
+        for (int c = 0; c < 3; c++) dst[c * plane + off] = lin[c];
+    }
+}
+
+// OUT: bit 0 SSIMULACRA2's XYB planes, bit 1 DSSIM's Lab planes (both from
+// the same linear pyramid).  OUT == 1 is the SSIMULACRA2-only pass.
+template <int FMT, typename ST, int OUT>
 __device__ __forceinline__ void prep_quads(const DevPair &P, int X0, int Y0, const float *lut, const ColorConsts &cc,
                                            float (*lv1)[3][kLv1 * kLv1]) {
     constexpr bool KU = FMT != FMT_LINEAR_F32;
+    constexpr bool kX = (OUT & 1) != 0, kL = (OUT & 2) != 0;
     const int W = P.w[0], H = P.h[0];
-    const bool scale1 = P.nscales > 1;
+    const bool scale1 = (kL ? P.prep_levels : P.nscales) > 1;
     for (int q = threadIdx.x; q < kLv1 * kLv1; q += blockDim.x) {
         const int qx = q % kLv1, qy = q / kLv1;
         const int x = X0 + 2 * qx, y = Y0 + 2 * qy;
@@ -165,14 +187,22 @@ __device__ __forceinline__ void prep_quads(const DevPair &P, int X0, int Y0, con
             float v[4][3];
             if (kYuv) yuv_quad_linear<kEs>(img ? nq1 : nq0, P, v);
             else lin_quad<FMT>(P, img, x, y, vx, vy, lut, cc, v);
-            ST *dst = (ST *)P.lvl[img][0];
-            const long long plane = (long long)P.lp[0] * H;
-            const long long off = (long long)y * P.lp[0] + x;
-            if (vx) store_xyb_pair<ST, KU>(dst, plane, off, v[0], v[1]);
-            else store_xyb<ST, KU>(P, img, 0, x, y, v[0]);
-            if (vy) {
-                if (vx) store_xyb_pair<ST, KU>(dst, plane, off + P.lp[0], v[2], v[3]);
-                else store_xyb<ST, KU>(P, img, 0, x, y + 1, v[2]);
+            if (kX && (!kL || P.nscales > 0)) {
+                ST *dst = (ST *)P.lvl[img][0];
+                const long long plane = (long long)P.lp[0] * H;
+                const long long off = (long long)y * P.lp[0] + x;
+                if (vx) store_xyb_pair<ST, KU>(dst, plane, off, v[0], v[1]);
+                else store_xyb<ST, KU>(P, img, 0, x, y, v[0]);
+                if (vy) {
+                    if (vx) store_xyb_pair<ST, KU>(dst, plane, off + P.lp[0], v[2], v[3]);
+                    else store_xyb<ST, KU>(P, img, 0, x, y + 1, v[2]);
+                }
+            }
+            if (kL) {
+                store_lab(P, img, 0, x, y, v[0]);
+                if (vx) store_lab(P, img, 0, x + 1, y, v[1]);
+                if (vy) store_lab(P, img, 0, x, y + 1, v[2]);
+                if (vx && vy) store_lab(P, img, 0, x + 1, y + 1, v[3]);
             }
             if (!scale1) continue;
             // far-edge clamp: a missing column repeats the left pixel, a
@@ -190,12 +220,13 @@ __device__ __forceinline__ void prep_quads(const DevPair &P, int X0, int Y0, con
                 l1[c] = sum * 0.25f;
                 lv1[img][c][q] = l1[c];
             }
-            store_xyb<ST, KU>(P, img, 1, (X0 >> 1) + qx, (Y0 >> 1) + qy, l1);
+            if (kX && (!kL || P.nscales > 1)) store_xyb<ST, KU>(P, img, 1, (X0 >> 1) + qx, (Y0 >> 1) + qy, l1);
+            if (kL) store_lab(P, img, 1, (X0 >> 1) + qx, (Y0 >> 1) + qy, l1);
         }
     }
 }
 
-template <typename ST>
+template <typename ST, int OUT>
 __global__ void __launch_bounds__(256, 3) prep_kernel(const DevPair *__restrict__ pairs, int npairs,
                                                    const int *__restrict__ blk_first, int first_block,
                                                    int end_block,
@@ -224,14 +255,15 @@ __global__ void __launch_bounds__(256, 3) prep_kernel(const DevPair *__restrict_
         const int bx = b % P.blk_x, by = b / P.blk_x;
         const int X0 = bx * kPyrBlk, Y0 = by * kPyrBlk;
         switch (P.fmt) {
-        case FMT_LINEAR_F32: prep_quads<FMT_LINEAR_F32, ST>(P, X0, Y0, lut, cc, lv1); break;
-        case FMT_SRGB8: prep_quads<FMT_SRGB8, ST>(P, X0, Y0, lut, cc, lv1); break;
-        case FMT_NV12: prep_quads<FMT_NV12, ST>(P, X0, Y0, lut, cc, lv1); break;
-        case FMT_P016: prep_quads<FMT_P016, ST>(P, X0, Y0, lut, cc, lv1); break;
-        default: prep_quads<FMT_RGB16, ST>(P, X0, Y0, lut, cc, lv1); break;
+        case FMT_LINEAR_F32: prep_quads<FMT_LINEAR_F32, ST, OUT>(P, X0, Y0, lut, cc, lv1); break;
+        case FMT_SRGB8: prep_quads<FMT_SRGB8, ST, OUT>(P, X0, Y0, lut, cc, lv1); break;
+        case FMT_NV12: prep_quads<FMT_NV12, ST, OUT>(P, X0, Y0, lut, cc, lv1); break;
+        case FMT_P016: prep_quads<FMT_P016, ST, OUT>(P, X0, Y0, lut, cc, lv1); break;
+        default: prep_quads<FMT_RGB16, ST, OUT>(P, X0, Y0, lut, cc, lv1); break;
         }
         __syncthreads();
-        for (int s = 2; s < P.nscales; s++) {
+        const int nlev = (OUT & 2) ? P.prep_levels : P.nscales;
+        for (int s = 2; s < nlev; s++) {
             const int bs = kPyrBlk >> s, pbs = kPyrBlk >> (s - 1);
             const int ox0 = X0 >> s, oy0 = Y0 >> s;
             const int px0 = X0 >> (s - 1), py0 = Y0 >> (s - 1);
@@ -255,8 +287,11 @@ __global__ void __launch_bounds__(256, 3) prep_kernel(const DevPair *__restrict_
                         v[c] = sum * 0.25f;
                         pp[s & 1][img][c][i] = v[c];
                     }
-                    if (P.fmt == FMT_LINEAR_F32) store_xyb<ST, false>(P, img, s, ox, oy, v);
-                    else store_xyb<ST, true>(P, img, s, ox, oy, v);
+                    if ((OUT & 1) && (!(OUT & 2) || s < P.nscales)) {
+                        if (P.fmt == FMT_LINEAR_F32) store_xyb<ST, false>(P, img, s, ox, oy, v);
+                        else store_xyb<ST, true>(P, img, s, ox, oy, v);
+                    }
+                    if (OUT & 2) store_lab(P, img, s, ox, oy, v);
                 }
             }
             __syncthreads();
@@ -685,17 +720,33 @@ int fused_blocks_per_sm(int storage) {
     return n > 0 ? n : 1;
 }
 
+template <int OUT>
+static void prep_launch(int storage, const DevPair *pairs, int npairs, const int *blk_first, int first_block,
+                        int end_block, const ColorConsts &cc, const float *lut, int grid, cudaStream_t st) {
+    // Lab planes are f32 whatever the storage type; XYB-less passes need one instance
+    if constexpr (OUT != 2) {
+        if (storage == ST_F16) {
+            prep_kernel<__half, OUT><<<grid, 256, 0, st>>>(pairs, npairs, blk_first, first_block, end_block, cc, lut);
+            return;
+        }
+        if (storage == ST_BF16) {
+            prep_kernel<__nv_bfloat16, OUT>
+                <<<grid, 256, 0, st>>>(pairs, npairs, blk_first, first_block, end_block, cc, lut);
+            return;
+        }
+    }
+    prep_kernel<float, OUT><<<grid, 256, 0, st>>>(pairs, npairs, blk_first, first_block, end_block, cc, lut);
+}
+
 cudaError_t launch_pyramid(int storage, const DevPair *pairs, int npairs, const int *blk_first, int first_block,
-                           int end_block, const ColorConsts &cc, const float *lut, int grid, cudaStream_t st) {
+                           int end_block, const ColorConsts &cc, const float *lut, int grid, cudaStream_t st,
+                           int out) {
     const int nb = end_block - first_block;
     if (nb <= 0) return cudaSuccess;
     grid = grid > nb ? nb : grid;
-    if (storage == ST_F16)
-        prep_kernel<__half><<<grid, 256, 0, st>>>(pairs, npairs, blk_first, first_block, end_block, cc, lut);
-    else if (storage == ST_BF16)
-        prep_kernel<__nv_bfloat16><<<grid, 256, 0, st>>>(pairs, npairs, blk_first, first_block, end_block, cc, lut);
-    else
-        prep_kernel<float><<<grid, 256, 0, st>>>(pairs, npairs, blk_first, first_block, end_block, cc, lut);
+    if (out == 3) prep_launch<3>(storage, pairs, npairs, blk_first, first_block, end_block, cc, lut, grid, st);
+    else if (out == 2) prep_launch<2>(storage, pairs, npairs, blk_first, first_block, end_block, cc, lut, grid, st);
+    else prep_launch<1>(storage, pairs, npairs, blk_first, first_block, end_block, cc, lut, grid, st);
     return cudaGetLastError();
 }
 

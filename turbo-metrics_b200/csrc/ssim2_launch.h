@@ -12,9 +12,11 @@ size_t fused_smem_bytes();
 int fused_blocks_per_sm(int storage);
 // prep over the pyramid blocks [first_block, end_block) (absolute numbering
 // of blk_first), fused over the tiles [first_tile, end_tile) with its own
-// zeroed work counter.
+// zeroed work counter.  out: 1 XYB planes (SSIMULACRA2), 2 Lab planes
+// (DSSIM), 3 both from one pass.
 cudaError_t launch_pyramid(int storage, const DevPair *pairs, int npairs, const int *blk_first, int first_block,
-                           int end_block, const ColorConsts &cc, const float *lut, int grid, cudaStream_t st);
+                           int end_block, const ColorConsts &cc, const float *lut, int grid, cudaStream_t st,
+                           int out = 1);
 cudaError_t launch_fused(int storage, const DevPair *pairs, const Seg *segs, int nseg, int first_tile, int end_tile,
                          int *counter, double *partials, int grid, cudaStream_t st);
 cudaError_t launch_iir(int storage, const DevPair *pairs, const IirSeg *vsegs, int nvseg, int vtotal,
@@ -32,4 +34,14 @@ cudaError_t launch_fused_export(int storage, const DevPair *pairs, const Seg *se
                                 long long mplane, int grid, cudaStream_t st);
 cudaError_t launch_finalize(const DevPair *pairs, int npairs, const double *partials, DevResult *out,
                             cudaStream_t st);
+
+// DSSIM over the Lab planes of a submission (dssim_kernels.cu): the clamp
+// pass (levels clamped to 8 pixels, pairs with clamp_from < 5), the tile
+// pass (SSIM map and per-tile sums), the per-level means, the per-tile
+// |avg - ssim| sums and the per-pair result.  `partials` holds 2 * ntiles
+// doubles, `avg` 5 floats per pair.  write_all: the submission scores DSSIM
+// only, so the final kernel also fills the SSIMULACRA2 fields of the result.
+cudaError_t launch_dssim(const DsPair *pairs, int npairs, const DsSeg *segs, int nseg, int ntiles, bool clamp,
+                         double *partials, float *avg, DevResult *out, bool write_all, int num_sms,
+                         cudaStream_t st);
 }  // namespace s2

@@ -127,6 +127,17 @@ class Ssimulacra2:
     def __exit__(self, *a):
         self.close()
 
+    def set_metrics(self, metrics):
+        """Metrics of later computes: 'ssimulacra2', 'dssim' or both."""
+        check(lib.s2_set_metrics(self._h, capi.metrics_mask(metrics)), "set_metrics")
+
+    def get_dssim(self):
+        """(dssim, per-scale scores[5]) of the last compute (DSSIM scored)."""
+        v = ctypes.c_double()
+        sc = np.zeros(5)
+        check(lib.s2_get_dssim(self._h, ctypes.byref(v), sc.ctypes.data_as(capi.D)), "get_dssim")
+        return v.value, sc
+
     # -- reference API ------------------------------------------------------
     def mem_usage(self):
         n = ctypes.c_size_t()
@@ -341,6 +352,12 @@ class Ssim2Batch:
         """Replay submissions of a seen shape as CUDA graphs (default on)."""
         check(lib.s2_batch_set_graphs(self._h, 1 if enable else 0), "set_graphs")
 
+    def set_metrics(self, metrics):
+        """Metrics of later submissions: 'ssimulacra2', 'dssim' or both (one
+        prep pass feeds both); results then carry the DSSIM value and its
+        per-scale scores (NaN when DSSIM is not scored)."""
+        check(lib.s2_batch_set_metrics(self._h, capi.metrics_mask(metrics)), "set_metrics")
+
     def submit_host(self, pairs, stream=None):
         """Pairs whose planes are in host memory (CPU tensors, pinned for
         overlap, or numpy arrays): uploaded in groups that overlap the compute
@@ -361,8 +378,8 @@ class Ssim2Batch:
         _, n, _ = self._unread.popleft() if self._unread else self._last
         out = (capi.Result * max(n, 1))()
         check(lib.s2_batch_results(self._h, out, n), "results")
-        return [(r.score, np.array(r.stats[:]), np.array(r.sums[:]), r.n_scales, r.status)
-                for r in out[:n]]
+        return [(r.score, np.array(r.stats[:]), np.array(r.sums[:]), r.n_scales, r.status, r.dssim,
+                 np.array(r.dssim_scale[:])) for r in out[:n]]
 
     def compute_batch(self, pairs, stream=None):
         self.submit(pairs, stream)
@@ -371,4 +388,57 @@ class Ssim2Batch:
     def mem_usage(self):
         n = ctypes.c_size_t()
         check(lib.s2_batch_mem_usage(self._h, ctypes.byref(n)), "mem_usage")
+        return n.value
+
+
+class Dssim:
+    """DSSIM of one size: the drop-in for dssim-cuda's `Dssim`
+    (crates/dssim-cuda/src/lib.rs:170-467).  Images are sRGB8 (H, W, 3):
+    torch CUDA tensors, or host arrays for the `*_from_cpu` calls."""
+
+    def __init__(self, width, height, *, device=0):
+        self.width, self.height = int(width), int(height)
+        h = ctypes.c_void_p()
+        check(lib.s2_dssim_create(device, self.width, self.height, ctypes.byref(h)), "Dssim::new")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None) and lib is not None:
+            lib.s2_dssim_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def compute_sync(self, ref_srgb, dis_srgb, stream=None):
+        """Dssim::compute_sync (lib.rs:225-232)."""
+        rp, rpitch = _dev(ref_srgb, 1)
+        dp, dpitch = _dev(dis_srgb, 1)
+        v = ctypes.c_double()
+        check(lib.s2_dssim_compute_srgb8(self._h, rp, rpitch, dp, dpitch, 0, _stream_ptr(stream), ctypes.byref(v)),
+              "Dssim::compute_sync")
+        return v.value
+
+    def compute_sync_dis_only(self, dis_srgb, stream=None):
+        """Dssim::compute_sync_dis_only (lib.rs:245-251): against the reference
+        of the last compute_sync."""
+        dp, dpitch = _dev(dis_srgb, 1)
+        v = ctypes.c_double()
+        check(lib.s2_dssim_compute_dis_only_srgb8(self._h, dp, dpitch, 0, _stream_ptr(stream), ctypes.byref(v)),
+              "Dssim::compute_sync_dis_only")
+        return v.value
+
+    def compute_from_cpu_sync(self, ref_bytes, dis_bytes, stream=None):
+        """Host sRGB8 (H, W, 3) pair (uploaded by the library)."""
+        rp, rpitch, _ = _host(ref_bytes)
+        dp, dpitch, _ = _host(dis_bytes)
+        v = ctypes.c_double()
+        check(lib.s2_dssim_compute_srgb8(self._h, rp, rpitch, dp, dpitch, 1, _stream_ptr(stream), ctypes.byref(v)),
+              "Dssim::compute_from_cpu_sync")
+        return v.value
+
+    def mem_usage(self):
+        """Dssim::mem_usage (lib.rs:438-451)."""
+        n = ctypes.c_size_t()
+        check(lib.s2_dssim_mem_usage(self._h, ctypes.byref(n)), "mem_usage")
         return n.value
