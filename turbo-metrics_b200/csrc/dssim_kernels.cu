@@ -33,36 +33,14 @@ namespace s2 {
 
 constexpr int kDsT = 32;             // output tile edge
 constexpr int kDsThreads = 256;
-constexpr int kDsRows = kDsThreads / kDsT;  // rows of outputs per pass (8)
 constexpr int kDsR = kDsT + 8;       // raw a/b region (halo 4)
 constexpr int kDsP = kDsT + 6;       // first a/b pre-blur (halo 3)
 constexpr int kDsX = kDsT + 4;       // blur input x, y (halo 2)
 constexpr int kDsB = kDsT + 2;       // first statistics blur (halo 1)
-static_assert(2 * kDsX * kDsX <= 2 * kDsR * kDsR && 2 * kDsP * kDsP <= 5 * kDsB * kDsB, "buffer reuse");
 
 // dssim-cuda-kernel/src/blur.rs:13-17
 __device__ __forceinline__ float ds_k(int i) {
     return (i == 4) ? 0.146293f : ((i & 1) ? 0.118095f : 0.095332f);
-}
-
-// One 3x3 tap sum centred on (ci, cj) of an m-wide buffer.  KIND 0: v * k;
-// 1: v * v * k; 2: v * u * k (blur.rs:46-54, :124-132, :160-170).
-template <int KIND>
-__device__ __forceinline__ float ds_blur_at(const float *in, const float *in2, int m, int ci, int cj) {
-    float sum = 0.0f;
-#pragma unroll
-    for (int ky = 0; ky < 3; ky++)
-#pragma unroll
-        for (int kx = 0; kx < 3; kx++) {
-            const int idx = (cj + ky - 1) * m + ci + kx - 1;
-            const float v = in[idx];
-            float t;
-            if (KIND == 0) t = v * ds_k(ky * 3 + kx);
-            else if (KIND == 1) t = v * v * ds_k(ky * 3 + kx);
-            else t = v * in2[idx] * ds_k(ky * 3 + kx);
-            sum = sum + t;
-        }
-    return sum;
 }
 
 __device__ __forceinline__ int ds_clamp(int v, int hi) { return v < 0 ? 0 : (v > hi ? hi : v); }
@@ -157,14 +135,113 @@ __global__ void __launch_bounds__(kDsThreads) dssim_clamp_kernel(const DsPair *_
 // ---------------------------------------------------------------------------
 // tile pass
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kDsThreads, 4) dssim_tile_kernel(const DsPair *__restrict__ pairs,
+//
+// Each blur stage fills an n x n buffer (n = 32 + 2 x its halo, even) from the
+// (n + 2)-wide buffer of the stage before.  A thread takes two adjacent
+// columns and kDsRun consecutive rows and slides a 3 x 4 window of the input
+// down them (two 8-byte shared loads per row).  Each tap is a scalar multiply
+// per column and one f32x2 add for both columns, in the reference's
+// row-major tap order: every lane rounds as the scalar reference does (the
+// products are scalar multiplies, which -fmad=false keeps out of any fused
+// multiply-add).  The first tap initialises the sum, which equals 0 + tap
+// for every tap but -0 (no Lab value or product of two is -0 where it
+// matters: the sign of a zero sum does not reach the SSIM).  x^2, y^2 and xy
+// are formed once per input position, so the first statistics blur is five
+// plain blurs.  The window is evaluated at every position; on tiles that
+// touch the level's edge, positions outside the level then take the value of
+// the position clamped into it (ds_fix_edges), which is what the reference's
+// next stage reads there with clamped indexes.
+constexpr int kDsRun = 4;
+
+__device__ __forceinline__ float2 ds_sum9x2(const float (&w)[3][4]) {
+    float2 sum = make_float2(w[0][0] * ds_k(0), w[0][1] * ds_k(0));
+#pragma unroll
+    for (int i = 1; i < 9; i++) {
+        const int ky = i / 3, kx = i % 3;
+        const float k = ds_k(i);
+        sum = __fadd2_rn(sum, make_float2(w[ky][kx] * k, w[ky][kx + 1] * k));
+    }
+    return sum;
+}
+
+__device__ __forceinline__ void ds_load4(float (&row)[4], const float *src) {
+    const float2 a = *(const float2 *)src, b = *(const float2 *)(src + 2);
+    row[0] = a.x, row[1] = a.y, row[2] = b.x, row[3] = b.y;
+}
+
+__device__ __forceinline__ void ds_slide(float (&w)[3][4], const float *src) {
+#pragma unroll
+    for (int kx = 0; kx < 4; kx++) w[0][kx] = w[1][kx], w[1][kx] = w[2][kx];
+    ds_load4(w[2], src);
+}
+
+// `planes` planes: out[p] (n x n) = 3x3 blur of in[p] (pitch n + 2, plane (n + 2)^2)
+__device__ __forceinline__ void ds_stage_blur(const float *in, float *out, int n, int planes) {
+    const int m = n + 2, half = n / 2, runs = (n + kDsRun - 1) / kDsRun;
+    for (int it = threadIdx.x; it < planes * half * runs; it += kDsThreads) {
+        const int p = it / (half * runs), q = it % (half * runs);
+        const int c = 2 * (q % half), j0 = (q / half) * kDsRun;
+        const float *src = in + p * m * m + c;
+        float *dst = out + p * n * n + c;
+        float w[3][4];
+        ds_load4(w[1], src + j0 * m);
+        ds_load4(w[2], src + (j0 + 1) * m);
+#pragma unroll
+        for (int r = 0; r < kDsRun; r++) {
+            if (j0 + r >= n) break;
+            ds_slide(w, src + (j0 + r + 2) * m);
+            *(float2 *)(dst + (j0 + r) * n) = ds_sum9x2(w);
+        }
+    }
+}
+
+// x^2, y^2, xy of every position of the blur input (planes 2..4 after x, y)
+__device__ __forceinline__ void ds_products(float *xy, int nn) {
+    for (int i = threadIdx.x; i < nn; i += kDsThreads) {
+        const float x = xy[i], y = xy[nn + i];
+        xy[2 * nn + i] = x * x;
+        xy[3 * nn + i] = y * y;
+        xy[4 * nn + i] = x * y;
+    }
+}
+
+// positions of an n x n stage buffer (origin X0 - h, Y0 - h) outside the
+// level take the value at the position clamped into the level
+__device__ void ds_fix_edges(float *buf, int planes, int n, int h, int X0, int Y0, int W, int H) {
+    for (int i = threadIdx.x; i < n * n; i += kDsThreads) {
+        const int x = X0 - h + i % n, y = Y0 - h + i / n;
+        if (x >= 0 && x < W && y >= 0 && y < H) continue;
+        const int src = (ds_clamp(y, H - 1) - (Y0 - h)) * n + ds_clamp(x, W - 1) - (X0 - h);
+        for (int p = 0; p < planes; p++) buf[p * n * n + i] = buf[p * n * n + src];
+    }
+}
+
+// Fixed-order block sum: each warp by shuffles, then the warps in order.
+__device__ double ds_block_reduce_w(double v, double *wsum) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double r = 0.0;
+    for (int w = 0; w < kDsThreads / 32; w++) r += wsum[w];
+    return r;
+}
+
+constexpr int kDsOutCols = kDsT / 2;             // column pairs of a tile
+constexpr int kDsOutRows = 2;                    // output rows per thread
+static_assert(kDsThreads == kDsOutCols * (kDsT / kDsOutRows), "one 2 x 2 output block per thread");
+
+__global__ void __launch_bounds__(kDsThreads, 3) dssim_tile_kernel(const DsPair *__restrict__ pairs,
                                                                    const DsSeg *__restrict__ segs, int nseg,
                                                                    int ntiles, double *__restrict__ partials) {
-    __shared__ float bufA[2 * kDsR * kDsR];  // raw a/b, then x and y of the blur input
-    __shared__ float bufB[5 * kDsB * kDsB];  // first pre-blur, then the five first blurs
-    __shared__ double red[kDsThreads];
+    __shared__ __align__(16) float bufA[5 * kDsX * kDsX];  // raw a/b; then x, y, x^2, y^2, xy (pitch 36)
+    __shared__ __align__(16) float bufB[5 * kDsB * kDsB];  // first pre-blur; then the five first blurs
+    __shared__ double wsum[kDsThreads / 32];
+    static_assert(2 * kDsR * kDsR <= 5 * kDsX * kDsX && 2 * kDsP * kDsP <= 5 * kDsB * kDsB, "buffer reuse");
     const int t = threadIdx.x;
-    const int tx = t % kDsT, ty = t / kDsT;
+    const int c0 = 2 * (t % kDsOutCols), r0 = (t / kDsOutCols) * kDsOutRows;
+    constexpr int nnX = kDsX * kDsX, nnB = kDsB * kDsB;
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const DsSeg sg = segs[ds_find_seg(segs, nseg, tile)];
         const DsPair &P = pairs[sg.pair];
@@ -173,18 +250,21 @@ __global__ void __launch_bounds__(kDsThreads, 4) dssim_tile_kernel(const DsPair 
         const long long pitch = P.pitch[s], plane = pitch * H;
         const int tl = tile - sg.first_tile;
         const int X0 = (tl % sg.tiles_x) * kDsT, Y0 = (tl / sg.tiles_x) * kDsT;
-        // per output: sums over L, a, b of mu1^2, mu2^2, mu1 mu2, blur(x^2),
-        // blur(y^2), blur(xy), added in channel order as ssim.rs:208-215 does
-        float acc[kDsT / kDsRows][6];
+        // the tile's halo reaches outside the level: stage values there are fixed up
+        const bool edge = X0 == 0 || Y0 == 0 || X0 + kDsT + 4 > W || Y0 + kDsT + 4 > H;
+        // per output (2 rows x 2 columns): sums over L, a, b of mu1^2, mu2^2,
+        // mu1 mu2, blur(x^2), blur(y^2), blur(xy), added in channel order as
+        // ssim.rs:208-215 does
+        float2 acc[kDsOutRows][6];
 #pragma unroll 1
         for (int c = 0; c < 3; c++) {
             const float *xr = P.lab[0][s] + c * plane;
             const float *yr = P.lab[1][s] + c * plane;
             __syncthreads();  // the previous channel's readers are done
             if (c == 0) {
-                // L: the blur input is the plane itself (halo 2)
-                for (int i = t; i < 2 * kDsX * kDsX; i += kDsThreads) {
-                    const int img = i / (kDsX * kDsX), r = i % (kDsX * kDsX);
+                // L: the blur input is the plane itself (halo 2, clamped loads)
+                for (int i = t; i < 2 * nnX; i += kDsThreads) {
+                    const int img = i / nnX, r = i % nnX;
                     const int gx = ds_clamp(X0 - 2 + r % kDsX, W - 1), gy = ds_clamp(Y0 - 2 + r / kDsX, H - 1);
                     bufA[i] = (img ? yr : xr)[gy * pitch + gx];
                 }
@@ -196,56 +276,58 @@ __global__ void __launch_bounds__(kDsThreads, 4) dssim_tile_kernel(const DsPair 
                     bufA[i] = (img ? yr : xr)[gy * pitch + gx];
                 }
                 __syncthreads();
-                for (int i = t; i < 2 * kDsP * kDsP; i += kDsThreads) {
-                    const int img = i / (kDsP * kDsP), r = i % (kDsP * kDsP);
-                    const int ci = ds_clamp(X0 - 3 + r % kDsP, W - 1) - (X0 - 4);
-                    const int cj = ds_clamp(Y0 - 3 + r / kDsP, H - 1) - (Y0 - 4);
-                    bufB[i] = ds_blur_at<0>(bufA + img * kDsR * kDsR, nullptr, kDsR, ci, cj);
-                }
+                ds_stage_blur(bufA, bufB, kDsP, 2);
                 __syncthreads();
-                for (int i = t; i < 2 * kDsX * kDsX; i += kDsThreads) {
-                    const int img = i / (kDsX * kDsX), r = i % (kDsX * kDsX);
-                    const int ci = ds_clamp(X0 - 2 + r % kDsX, W - 1) - (X0 - 3);
-                    const int cj = ds_clamp(Y0 - 2 + r / kDsX, H - 1) - (Y0 - 3);
-                    bufA[i] = ds_blur_at<0>(bufB + img * kDsP * kDsP, nullptr, kDsP, ci, cj);
+                if (edge) {
+                    ds_fix_edges(bufB, 2, kDsP, 3, X0, Y0, W, H);
+                    __syncthreads();
+                }
+                ds_stage_blur(bufB, bufA, kDsX, 2);
+                __syncthreads();
+                if (edge) {
+                    ds_fix_edges(bufA, 2, kDsX, 2, X0, Y0, W, H);
+                    __syncthreads();
                 }
             }
             __syncthreads();
-            // first blur of x, y, x^2, y^2, xy (halo 1)
-            for (int i = t; i < kDsB * kDsB; i += kDsThreads) {
-                const int ci = ds_clamp(X0 - 1 + i % kDsB, W - 1) - (X0 - 2);
-                const int cj = ds_clamp(Y0 - 1 + i / kDsB, H - 1) - (Y0 - 2);
-                const float *X = bufA, *Y = bufA + kDsX * kDsX;
-                bufB[i] = ds_blur_at<0>(X, nullptr, kDsX, ci, cj);
-                bufB[kDsB * kDsB + i] = ds_blur_at<0>(Y, nullptr, kDsX, ci, cj);
-                bufB[2 * kDsB * kDsB + i] = ds_blur_at<1>(X, nullptr, kDsX, ci, cj);
-                bufB[3 * kDsB * kDsB + i] = ds_blur_at<1>(Y, nullptr, kDsX, ci, cj);
-                bufB[4 * kDsB * kDsB + i] = ds_blur_at<2>(X, Y, kDsX, ci, cj);
-            }
+            ds_products(bufA, nnX);
             __syncthreads();
-            // second blur at the tile's outputs
+            ds_stage_blur(bufA, bufB, kDsB, 5);
+            __syncthreads();
+            if (edge) {
+                ds_fix_edges(bufB, 5, kDsB, 1, X0, Y0, W, H);
+                __syncthreads();
+            }
+            // second blurs at the thread's 2 x 2 outputs
+            float2 q[5][kDsOutRows];
 #pragma unroll
-            for (int k = 0; k < kDsT / kDsRows; k++) {
-                const int ci = tx + 1, cj = ty + k * kDsRows + 1;
-                const float m1 = ds_blur_at<0>(bufB, nullptr, kDsB, ci, cj);
-                const float m2 = ds_blur_at<0>(bufB + kDsB * kDsB, nullptr, kDsB, ci, cj);
-                const float s1 = ds_blur_at<0>(bufB + 2 * kDsB * kDsB, nullptr, kDsB, ci, cj);
-                const float s2 = ds_blur_at<0>(bufB + 3 * kDsB * kDsB, nullptr, kDsB, ci, cj);
-                const float s12 = ds_blur_at<0>(bufB + 4 * kDsB * kDsB, nullptr, kDsB, ci, cj);
+            for (int pl = 0; pl < 5; pl++) {
+                const float *src = bufB + pl * nnB + c0;
+                float w[3][4];
+                ds_load4(w[1], src + r0 * kDsB);
+                ds_load4(w[2], src + (r0 + 1) * kDsB);
+#pragma unroll
+                for (int r = 0; r < kDsOutRows; r++) {
+                    ds_slide(w, src + (r0 + r + 2) * kDsB);
+                    q[pl][r] = ds_sum9x2(w);
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < kDsOutRows; r++) {
+                const float2 m1 = q[0][r], m2 = q[1][r];
+                const float2 a0 = make_float2(m1.x * m1.x, m1.y * m1.y);
+                const float2 a1 = make_float2(m2.x * m2.x, m2.y * m2.y);
+                const float2 a2 = make_float2(m1.x * m2.x, m1.y * m2.y);
                 if (c == 0) {
-                    acc[k][0] = m1 * m1;
-                    acc[k][1] = m2 * m2;
-                    acc[k][2] = m1 * m2;
-                    acc[k][3] = s1;
-                    acc[k][4] = s2;
-                    acc[k][5] = s12;
+                    acc[r][0] = a0, acc[r][1] = a1, acc[r][2] = a2;
+                    acc[r][3] = q[2][r], acc[r][4] = q[3][r], acc[r][5] = q[4][r];
                 } else {
-                    acc[k][0] = acc[k][0] + m1 * m1;
-                    acc[k][1] = acc[k][1] + m2 * m2;
-                    acc[k][2] = acc[k][2] + m1 * m2;
-                    acc[k][3] = acc[k][3] + s1;
-                    acc[k][4] = acc[k][4] + s2;
-                    acc[k][5] = acc[k][5] + s12;
+                    acc[r][0] = __fadd2_rn(acc[r][0], a0);
+                    acc[r][1] = __fadd2_rn(acc[r][1], a1);
+                    acc[r][2] = __fadd2_rn(acc[r][2], a2);
+                    acc[r][3] = __fadd2_rn(acc[r][3], q[2][r]);
+                    acc[r][4] = __fadd2_rn(acc[r][4], q[3][r]);
+                    acc[r][5] = __fadd2_rn(acc[r][5], q[4][r]);
                 }
             }
         }
@@ -254,20 +336,24 @@ __global__ void __launch_bounds__(kDsThreads, 4) dssim_tile_kernel(const DsPair 
         float *map = P.map[s];
         double tsum = 0.0;
 #pragma unroll
-        for (int k = 0; k < kDsT / kDsRows; k++) {
-            const int ox = X0 + tx, oy = Y0 + ty + k * kDsRows;
-            if (ox >= W || oy >= H) continue;
-            const float mu1_sq = acc[k][0] * third, mu2_sq = acc[k][1] * third, mu1_mu2 = acc[k][2] * third;
-            const float sigma1_sq = acc[k][3] * third - mu1_sq;
-            const float sigma2_sq = acc[k][4] * third - mu2_sq;
-            const float sigma12 = acc[k][5] * third - mu1_mu2;
-            const float num = fmaf(2.0f, mu1_mu2, c1) * fmaf(2.0f, sigma12, c2);
-            const float den = (mu1_sq + mu2_sq + c1) * (sigma1_sq + sigma2_sq + c2);
-            const float v = num / den;
-            map[oy * pitch + ox] = v;
-            tsum += (double)v;
-        }
-        const double r = ds_block_reduce(tsum, red);
+        for (int r = 0; r < kDsOutRows; r++)
+#pragma unroll
+            for (int l = 0; l < 2; l++) {
+                const int ox = X0 + c0 + l, oy = Y0 + r0 + r;
+                if (ox >= W || oy >= H) continue;
+                const float *a = (const float *)acc[r];
+                const float mu1_sq = a[0 * 2 + l] * third, mu2_sq = a[1 * 2 + l] * third;
+                const float mu1_mu2 = a[2 * 2 + l] * third;
+                const float sigma1_sq = a[3 * 2 + l] * third - mu1_sq;
+                const float sigma2_sq = a[4 * 2 + l] * third - mu2_sq;
+                const float sigma12 = a[5 * 2 + l] * third - mu1_mu2;
+                const float num = fmaf(2.0f, mu1_mu2, c1) * fmaf(2.0f, sigma12, c2);
+                const float den = (mu1_sq + mu2_sq + c1) * (sigma1_sq + sigma2_sq + c2);
+                const float val = num / den;
+                map[oy * pitch + ox] = val;
+                tsum += (double)val;
+            }
+        const double r = ds_block_reduce_w(tsum, wsum);
         if (t == 0) partials[tile] = r;
     }
 }
@@ -294,7 +380,7 @@ __global__ void __launch_bounds__(kDsThreads) dssim_mad_kernel(const DsPair *__r
                                                                double *__restrict__ mad) {
     __shared__ double red[kDsThreads];
     const int t = threadIdx.x;
-    const int tx = t % kDsT, ty = t / kDsT;
+    const int tx = t % kDsT, j0 = (t / kDsT) * kDsRun;  // one column, kDsRun rows
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const DsSeg sg = segs[ds_find_seg(segs, nseg, tile)];
         const DsPair &P = pairs[sg.pair];
@@ -306,8 +392,8 @@ __global__ void __launch_bounds__(kDsThreads) dssim_mad_kernel(const DsPair *__r
         const long long pitch = P.pitch[s];
         double acc = 0.0;
 #pragma unroll
-        for (int k = 0; k < kDsT / kDsRows; k++) {
-            const int ox = X0 + tx, oy = Y0 + ty + k * kDsRows;
+        for (int k = 0; k < kDsRun; k++) {
+            const int ox = X0 + tx, oy = Y0 + j0 + k;
             if (ox < P.w[s] && oy < P.h[s]) acc += (double)fabsf(a - map[oy * pitch + ox]);
         }
         const double r = ds_block_reduce(acc, red);
@@ -359,7 +445,9 @@ cudaError_t launch_dssim(const DsPair *pairs, int npairs, const DsSeg *segs, int
     if (npairs <= 0) return cudaSuccess;
     if (clamp) dssim_clamp_kernel<<<npairs, kDsThreads, 0, st>>>(pairs);
     if (ntiles > 0) {
-        const int grid = ntiles < num_sms * 4 ? ntiles : num_sms * 4;
+        // persistent: the resident blocks of the tile kernel (3 per SM), each
+        // striding over the tiles
+        const int grid = ntiles < num_sms * 3 ? ntiles : num_sms * 3;
         dssim_tile_kernel<<<grid, kDsThreads, 0, st>>>(pairs, segs, nseg, ntiles, partials);
         dssim_mean_kernel<<<npairs * kDsLevels, kDsThreads, 0, st>>>(pairs, partials, avg);
         dssim_mad_kernel<<<grid, kDsThreads, 0, st>>>(pairs, segs, nseg, ntiles, avg, partials + ntiles);
