@@ -195,14 +195,43 @@ __device__ __forceinline__ void ds_stage_blur(const float *in, float *out, int n
     }
 }
 
-// x^2, y^2, xy of every position of the blur input (planes 2..4 after x, y)
-__device__ __forceinline__ void ds_products(float *xy, int nn) {
+// the five blur inputs x, y, x^2, y^2, xy of every position (out: 5 planes)
+__device__ __forceinline__ void ds_products(const float *X, const float *Y, float *out, int nn) {
     for (int i = threadIdx.x; i < nn; i += kDsThreads) {
-        const float x = xy[i], y = xy[nn + i];
-        xy[2 * nn + i] = x * x;
-        xy[3 * nn + i] = y * y;
-        xy[4 * nn + i] = x * y;
+        const float x = X[i], y = Y[i];
+        out[i] = x;
+        out[nn + i] = y;
+        out[2 * nn + i] = x * x;
+        out[3 * nn + i] = y * y;
+        out[4 * nn + i] = x * y;
     }
+}
+
+// Asynchronous 4-byte global -> shared copies (cp.async): the next channel's
+// raw Lab region is fetched while the current channel computes.
+__device__ __forceinline__ void ds_cp4(float *dst, const float *src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
+
+// Issue the copies of channel c's raw region of `tile` (halo 2 for L, 4 for
+// a and b; clamped into the level) into R, pitch 32 + 2 x halo, both images.
+__device__ void ds_prefetch(const DsPair *__restrict__ pairs, const DsSeg *__restrict__ segs, int nseg, int tile,
+                            int c, float *R) {
+    const DsSeg sg = segs[ds_find_seg(segs, nseg, tile)];
+    const DsPair &P = pairs[sg.pair];
+    const int s = sg.level, W = P.w[s], H = P.h[s];
+    const long long pitch = P.pitch[s], plane = pitch * H;
+    const int tl = tile - sg.first_tile;
+    const int X0 = (tl % sg.tiles_x) * kDsT, Y0 = (tl / sg.tiles_x) * kDsT;
+    const int h = c == 0 ? 2 : 4, n = kDsT + 2 * h;
+    const float *xr = P.lab[0][s] + c * plane, *yr = P.lab[1][s] + c * plane;
+    for (int i = threadIdx.x; i < 2 * n * n; i += kDsThreads) {
+        const int img = i / (n * n), r = i % (n * n);
+        const int gx = ds_clamp(X0 - h + r % n, W - 1), gy = ds_clamp(Y0 - h + r / n, H - 1);
+        ds_cp4(R + i, (img ? yr : xr) + gy * pitch + gx);
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
 }
 
 // positions of an n x n stage buffer (origin X0 - h, Y0 - h) outside the
@@ -232,22 +261,31 @@ constexpr int kDsOutCols = kDsT / 2;             // column pairs of a tile
 constexpr int kDsOutRows = 2;                    // output rows per thread
 static_assert(kDsThreads == kDsOutCols * (kDsT / kDsOutRows), "one 2 x 2 output block per thread");
 
+// dynamic shared memory: A (5 planes of 36^2: x, y, x^2, y^2, xy, and the
+// second a/b pre-blur), B (5 planes of 34^2: the first blurs, and the first
+// a/b pre-blur), R (the raw region being fetched: 2 planes of up to 40^2)
+constexpr int kDsSmemFloats = 5 * kDsX * kDsX + 5 * kDsB * kDsB + 2 * kDsR * kDsR;
+
 __global__ void __launch_bounds__(kDsThreads, 3) dssim_tile_kernel(const DsPair *__restrict__ pairs,
                                                                    const DsSeg *__restrict__ segs, int nseg,
                                                                    int ntiles, double *__restrict__ partials) {
-    __shared__ __align__(16) float bufA[5 * kDsX * kDsX];  // raw a/b; then x, y, x^2, y^2, xy (pitch 36)
-    __shared__ __align__(16) float bufB[5 * kDsB * kDsB];  // first pre-blur; then the five first blurs
+    extern __shared__ __align__(16) float ds_smem[];
+    float *const bufA = ds_smem;
+    float *const bufB = bufA + 5 * kDsX * kDsX;
+    float *const bufR = bufB + 5 * kDsB * kDsB;
     __shared__ double wsum[kDsThreads / 32];
-    static_assert(2 * kDsR * kDsR <= 5 * kDsX * kDsX && 2 * kDsP * kDsP <= 5 * kDsB * kDsB, "buffer reuse");
+    static_assert(2 * kDsX * kDsX <= 5 * kDsX * kDsX && 2 * kDsP * kDsP <= 5 * kDsB * kDsB, "buffer reuse");
+    static_assert((5 * kDsX * kDsX) % 4 == 0 && (5 * kDsB * kDsB) % 4 == 0, "16-byte aligned buffers");
     const int t = threadIdx.x;
     const int c0 = 2 * (t % kDsOutCols), r0 = (t / kDsOutCols) * kDsOutRows;
     constexpr int nnX = kDsX * kDsX, nnB = kDsB * kDsB;
+    if ((int)blockIdx.x < ntiles) ds_prefetch(pairs, segs, nseg, blockIdx.x, 0, bufR);
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const DsSeg sg = segs[ds_find_seg(segs, nseg, tile)];
         const DsPair &P = pairs[sg.pair];
         const int s = sg.level;
         const int W = P.w[s], H = P.h[s];
-        const long long pitch = P.pitch[s], plane = pitch * H;
+        const long long pitch = P.pitch[s];
         const int tl = tile - sg.first_tile;
         const int X0 = (tl % sg.tiles_x) * kDsT, Y0 = (tl / sg.tiles_x) * kDsT;
         // the tile's halo reaches outside the level: stage values there are fixed up
@@ -258,26 +296,24 @@ __global__ void __launch_bounds__(kDsThreads, 3) dssim_tile_kernel(const DsPair 
         float2 acc[kDsOutRows][6];
 #pragma unroll 1
         for (int c = 0; c < 3; c++) {
-            const float *xr = P.lab[0][s] + c * plane;
-            const float *yr = P.lab[1][s] + c * plane;
-            __syncthreads();  // the previous channel's readers are done
+            // channel c's raw region has landed in R; the previous channel's
+            // readers of A and B are done
+            asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+            __syncthreads();
             if (c == 0) {
                 // L: the blur input is the plane itself (halo 2, clamped loads)
-                for (int i = t; i < 2 * nnX; i += kDsThreads) {
-                    const int img = i / nnX, r = i % nnX;
-                    const int gx = ds_clamp(X0 - 2 + r % kDsX, W - 1), gy = ds_clamp(Y0 - 2 + r / kDsX, H - 1);
-                    bufA[i] = (img ? yr : xr)[gy * pitch + gx];
-                }
+                ds_products(bufR, bufR + nnX, bufA, nnX);
+                __syncthreads();
             } else {
                 // a, b: pre-blurred twice first (lib.rs:296-316)
-                for (int i = t; i < 2 * kDsR * kDsR; i += kDsThreads) {
-                    const int img = i / (kDsR * kDsR), r = i % (kDsR * kDsR);
-                    const int gx = ds_clamp(X0 - 4 + r % kDsR, W - 1), gy = ds_clamp(Y0 - 4 + r / kDsR, H - 1);
-                    bufA[i] = (img ? yr : xr)[gy * pitch + gx];
-                }
+                ds_stage_blur(bufR, bufB, kDsP, 2);
                 __syncthreads();
-                ds_stage_blur(bufA, bufB, kDsP, 2);
-                __syncthreads();
+            }
+            // R is free: fetch the next channel (or the next tile's L) during
+            // this channel's blurs
+            if (c < 2) ds_prefetch(pairs, segs, nseg, tile, c + 1, bufR);
+            else if (tile + (int)gridDim.x < ntiles) ds_prefetch(pairs, segs, nseg, tile + gridDim.x, 0, bufR);
+            if (c > 0) {
                 if (edge) {
                     ds_fix_edges(bufB, 2, kDsP, 3, X0, Y0, W, H);
                     __syncthreads();
@@ -288,10 +324,9 @@ __global__ void __launch_bounds__(kDsThreads, 3) dssim_tile_kernel(const DsPair 
                     ds_fix_edges(bufA, 2, kDsX, 2, X0, Y0, W, H);
                     __syncthreads();
                 }
+                ds_products(bufA, bufA + nnX, bufA, nnX);
+                __syncthreads();
             }
-            __syncthreads();
-            ds_products(bufA, nnX);
-            __syncthreads();
             ds_stage_blur(bufA, bufB, kDsB, 5);
             __syncthreads();
             if (edge) {
@@ -439,6 +474,11 @@ __global__ void __launch_bounds__(kDsThreads) dssim_final_kernel(const DsPair *_
     }
 }
 
+cudaError_t configure_dssim_kernels() {
+    return cudaFuncSetAttribute(dssim_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(kDsSmemFloats * sizeof(float)));
+}
+
 cudaError_t launch_dssim(const DsPair *pairs, int npairs, const DsSeg *segs, int nseg, int ntiles, bool clamp,
                          double *partials, float *avg, DevResult *out, bool write_all, int num_sms,
                          cudaStream_t st) {
@@ -448,7 +488,8 @@ cudaError_t launch_dssim(const DsPair *pairs, int npairs, const DsSeg *segs, int
         // persistent: the resident blocks of the tile kernel (3 per SM), each
         // striding over the tiles
         const int grid = ntiles < num_sms * 3 ? ntiles : num_sms * 3;
-        dssim_tile_kernel<<<grid, kDsThreads, 0, st>>>(pairs, segs, nseg, ntiles, partials);
+        dssim_tile_kernel<<<grid, kDsThreads, kDsSmemFloats * sizeof(float), st>>>(pairs, segs, nseg, ntiles,
+                                                                                  partials);
         dssim_mean_kernel<<<npairs * kDsLevels, kDsThreads, 0, st>>>(pairs, partials, avg);
         dssim_mad_kernel<<<grid, kDsThreads, 0, st>>>(pairs, segs, nseg, ntiles, avg, partials + ntiles);
     }

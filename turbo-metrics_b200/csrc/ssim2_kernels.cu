@@ -710,7 +710,8 @@ cudaError_t configure_kernels() {
     e = cudaFuncSetAttribute(fused_kernel<__half>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fused_smem_bytes());
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(fused_kernel<__nv_bfloat16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fused_smem_bytes());
-    return e;
+    if (e != cudaSuccess) return e;
+    return configure_dssim_kernels();
 }
 
 int fused_blocks_per_sm(int storage) {

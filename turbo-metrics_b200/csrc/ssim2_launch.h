@@ -41,6 +41,7 @@ cudaError_t launch_finalize(const DevPair *pairs, int npairs, const double *part
 // |avg - ssim| sums and the per-pair result.  `partials` holds 2 * ntiles
 // doubles, `avg` 5 floats per pair.  write_all: the submission scores DSSIM
 // only, so the final kernel also fills the SSIMULACRA2 fields of the result.
+cudaError_t configure_dssim_kernels();
 cudaError_t launch_dssim(const DsPair *pairs, int npairs, const DsSeg *segs, int nseg, int ntiles, bool clamp,
                          double *partials, float *avg, DevResult *out, bool write_all, int num_sms,
                          cudaStream_t st);
