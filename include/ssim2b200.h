@@ -2,8 +2,10 @@
  * ssim2b200.h -- C ABI of the B200-native SSIMULACRA2 engine.
  *
  * The engine is a drop-in for the `Ssimulacra2` type of the turbo-metrics
- * crate `ssimulacra2-cuda` (crates/ssimulacra2-cuda/src/lib.rs).  Every entry
- * point below names the reference interface it replaces.  Signatures use
+ * crate `ssimulacra2-cuda` (crates/ssimulacra2-cuda/src/lib.rs) and, sharing
+ * its input conversion and pyramid, for the `Dssim` type of `dssim-cuda`
+ * (crates/dssim-cuda/src/lib.rs).  Every entry point below names the
+ * reference interface it replaces.  Signatures use
  * plain pointers and sizes only; `stream` arguments are `cudaStream_t` values
  * passed as `void *` (NULL = the legacy default stream).
  *

@@ -51,3 +51,30 @@ def test_config_validation_needs_no_gpu(tmb):
     assert tmb.lib.s2_create(ctypes.byref(cfg), 7, 64, ctypes.byref(h)) == 2  # invalid size
     cfg.struct_size = 4
     assert tmb.lib.s2_create(ctypes.byref(cfg), 64, 64, ctypes.byref(h)) == 8
+
+
+def test_result_layout_and_metric_bits(tmb):
+    """s2_result: score, 108 stats, 108 sums, n_scales, status, then the DSSIM
+    value and its five per-scale scores."""
+    R = tmb.capi.Result
+    assert ctypes.sizeof(R) == 8 + 108 * 8 * 2 + 4 + 4 + 8 + 5 * 8
+    assert R.dssim.offset == 8 + 108 * 8 * 2 + 8
+    assert tmb.capi.metrics_mask("ssimulacra2") == 1
+    assert tmb.capi.metrics_mask("dssim") == 2
+    assert tmb.capi.metrics_mask(("ssimulacra2", "dssim")) == 3
+    with pytest.raises(KeyError):
+        tmb.capi.metrics_mask("butteraugli")
+
+
+def test_dssim_entry_points_validate_without_gpu(tmb):
+    """Argument and size checks come before any device call."""
+    lib = tmb.lib
+    d = ctypes.c_void_p()
+    assert lib.s2_dssim_create(0, 7, 64, ctypes.byref(d)) == 2  # below 8x8: invalid size
+    assert lib.s2_dssim_create(0, 64, 64, None) == 8
+    v = ctypes.c_double()
+    assert lib.s2_dssim_compute_srgb8(None, None, 0, None, 0, 0, None, ctypes.byref(v)) == 8
+    assert lib.s2_dssim_compute_dis_only_srgb8(None, None, 0, 0, None, ctypes.byref(v)) == 8
+    assert lib.s2_set_metrics(None, 3) == 8
+    assert lib.s2_batch_set_metrics(None, 2) == 8
+    assert lib.s2_get_dssim(None, None, None) == 8
