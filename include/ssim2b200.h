@@ -288,7 +288,8 @@ enum { S2_METRIC_SSIMULACRA2 = 1, S2_METRIC_DSSIM = 2 };
 /* Metrics scored by later submissions of a context or batch: a non-empty
  * set of S2_METRIC_* bits (default S2_METRIC_SSIMULACRA2).  With DSSIM alone
  * the SSIMULACRA2 fields of a result hold NaN / 0.  Cached-reference
- * submissions (s2_compute_with_reference_*) score SSIMULACRA2 only. */
+ * submissions (s2_set_reference_* / s2_compute_with_reference_*) score
+ * SSIMULACRA2 only (S2_ERR_INVALID_ARG on a context scoring DSSIM alone). */
 s2_status s2_set_metrics(s2_ctx *ctx, int32_t metrics);
 s2_status s2_batch_set_metrics(s2_batch *b, int32_t metrics);
 /* The last submission's DSSIM and its five per-scale scores (waits for the

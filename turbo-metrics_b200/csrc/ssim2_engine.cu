@@ -430,6 +430,8 @@ s2_status s2_dimensions(const s2_ctx *ctx, uint32_t *w, uint32_t *h) {
 }
 
 static s2_status ctx_run(s2_ctx *ctx, const s2_pair_desc &d, void *stream, const PairExtra *ex = nullptr) {
+    // the cached-reference path keeps SSIMULACRA2's XYB planes only
+    if (ex && !ex->dssim && !(ctx->eng.metrics & S2_METRIC_SSIMULACRA2)) return S2_ERR_INVALID_ARG;
     s2_status st = ctx->eng.plan(&d, 1, ctx->plan, ex);
     if (st == S2_OK && ctx->plan.pairs[0].status == S2_OK && (!ex || ex->score))
         st = ctx->eng.tune(&d, 1, ctx->plan, ex, (cudaStream_t)stream);
