@@ -1,0 +1,148 @@
+// plan_check.cu -- host-only check of the submission planner (Engine::plan in
+// turbo-metrics_b200/csrc/ssim2_engine_internal.h) over random submissions:
+// every device region a plan lays out (XYB levels, DSSIM Lab planes, SSIM
+// maps, kept linear levels, clamp-pass scratch) lies inside the plan's level
+// bytes, starts 256-byte aligned and overlaps no other; DSSIM level sizes
+// follow dssim-cuda (halved rounding up, never below 8); the levels the prep
+// pass converts and the clamp pass builds split where those sizes leave the
+// ceil-halved pyramid; DSSIM tiles cover every level of every pair once.
+// plan() makes no CUDA call, so this runs without a GPU (built and run by
+// tests/test_cpu_plan.py).
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <random>
+#include <vector>
+
+#include "../turbo-metrics_b200/csrc/ssim2_engine_internal.h"
+
+static int fails = 0;
+#define CHECK(c, ...)                              \
+    do {                                           \
+        if (!(c)) {                                \
+            if (fails++ < 20) {                    \
+                printf("FAIL %s:%d: ", __FILE__, __LINE__); \
+                printf(__VA_ARGS__);               \
+                printf("\n");                      \
+            }                                      \
+        }                                          \
+    } while (0)
+
+struct Region {
+    size_t off, bytes;
+};
+
+int main(int argc, char **argv) {
+    const int iters = argc > 1 ? atoi(argv[1]) : 400;
+    std::mt19937_64 rng(0x5EED);
+    auto dim = [&](void) -> uint32_t {
+        switch (rng() % 4) {
+        case 0: return 1 + (uint32_t)(rng() % 24);      // tiny: invalid or clamped levels
+        case 1: return 8 + (uint32_t)(rng() % 120);     // small: clamped DSSIM levels
+        case 2: return 64 + (uint32_t)(rng() % 1000);
+        default: return 500 + (uint32_t)(rng() % 3500);
+        }
+    };
+    size_t planned = 0, with_clamp = 0;
+    for (int it = 0; it < iters; it++) {
+        Engine e;  // not initialised: planning is host-only
+        e.metrics = 1 + (int)(rng() % 3);
+        e.scale_rule = (int)(rng() % 3);
+        e.storage = (int)(rng() % 3);
+        e.strip_rows_cfg = 21;
+        const int n = 1 + (int)(rng() % 12);
+        std::vector<s2_pair_desc> d(n);
+        for (auto &q : d) {
+            memset(&q, 0, sizeof q);
+            q.format = (int)(rng() % 5);
+            q.width = dim();
+            q.height = dim();
+            if (q.format == S2_FMT_NV12 || q.format == S2_FMT_P016) q.width += q.width & 1, q.height += q.height & 1;
+            q.bits = 10;
+            q.ref = q.dis = q.ref_uv = q.dis_uv = (const void *)64;
+            q.ref_pitch = q.dis_pitch = (size_t)q.width * 12;
+        }
+        Plan P;
+        const s2_status st = e.plan(d.data(), n, P);
+        CHECK(st == S2_OK, "plan status %d", (int)st);
+        const bool m_s2 = (e.metrics & S2_METRIC_SSIMULACRA2) != 0, m_ds = (e.metrics & S2_METRIC_DSSIM) != 0;
+        std::vector<Region> regs;
+        const size_t es = e.esize();
+        for (int i = 0; i < n; i++) {
+            const DevPair &p = P.pairs[i];
+            const s2_pair_desc &q = d[i];
+            const bool valid = (!m_s2 || s2_num_scales_rule(q.width, q.height, e.scale_rule) > 0) &&
+                               (!m_ds || (q.width >= 8 && q.height >= 8));
+            CHECK((p.status == S2_OK) == valid, "pair %d status %d for %ux%u metrics %d", i, p.status, q.width,
+                  q.height, e.metrics);
+            if (p.status != S2_OK) {
+                if (m_ds) CHECK(P.ds[i].status == p.status, "DSSIM status of an invalid pair");
+                continue;
+            }
+            planned++;
+            CHECK(p.nscales == (m_s2 ? s2_num_scales_rule(q.width, q.height, e.scale_rule) : 0), "nscales");
+            for (int s = 0; s < p.nscales; s++) {
+                CHECK(p.lp[s] == (int)s2_align_up((size_t)p.w[s], 64), "XYB pitch");
+                for (int img = 0; img < 2; img++)
+                    regs.push_back({(size_t)p.lvl[img][s], s2_align_up((size_t)3 * p.lp[s] * p.h[s] * es, 256)});
+            }
+            if (!m_ds) {
+                CHECK(p.lab_levels == 0, "Lab levels without DSSIM");
+                continue;
+            }
+            const DsPair &D = P.ds[i];
+            CHECK(D.status == 0, "DSSIM status %d", D.status);
+            int dw[kDsLevels], dh[kDsLevels];
+            uint32_t w = q.width, h = q.height;
+            for (int s = 0; s < kDsLevels; s++) {
+                dw[s] = (int)w, dh[s] = (int)h;
+                w = std::max<uint32_t>((w + 1) / 2, 8), h = std::max<uint32_t>((h + 1) / 2, 8);
+                CHECK(D.w[s] == dw[s] && D.h[s] == dh[s], "DSSIM size of level %d", s);
+                CHECK(D.pitch[s] >= D.w[s] && D.pitch[s] % 64 == 0, "DSSIM pitch");
+            }
+            int ll = 0;
+            while (ll < kDsLevels && dw[ll] == p.w[ll] && dh[ll] == p.h[ll]) ll++;
+            CHECK(ll >= 1 && p.lab_levels == ll && D.clamp_from == ll, "Lab levels %d / %d", p.lab_levels, ll);
+            CHECK(p.prep_levels == std::max(p.nscales, ll), "prep levels");
+            for (int s = 0; s < p.prep_levels; s++) CHECK(p.lp[s] == (int)s2_align_up((size_t)p.w[s], 64), "pitch");
+            for (int s = 0; s < kDsLevels; s++) {
+                for (int img = 0; img < 2; img++) {
+                    if (s < ll) CHECK(p.lab[img][s] == D.lab[img][s] && D.pitch[s] == p.lp[s], "prep Lab plane");
+                    regs.push_back({(size_t)D.lab[img][s],
+                                    s2_align_up((size_t)3 * D.pitch[s] * D.h[s] * sizeof(float), 256)});
+                }
+                regs.push_back({(size_t)D.map[s], s2_align_up((size_t)D.pitch[s] * D.h[s] * sizeof(float), 256)});
+                CHECK(D.tile_cnt[s] == ((D.w[s] + 31) / 32) * ((D.h[s] + 31) / 32), "tile count");
+            }
+            if (ll < kDsLevels) {
+                with_clamp++;
+                CHECK(D.kw == p.w[ll - 1] && D.kh == p.h[ll - 1] && D.kpitch == p.lp[ll - 1], "kept level");
+                for (int s = ll; s < kDsLevels; s++)
+                    CHECK(D.splane >= (long long)D.pitch[s] * D.h[s], "scratch plane of level %d", s);
+                for (int img = 0; img < 2; img++) {
+                    CHECK(p.keep[img] == D.keep[img], "keep pointer");
+                    regs.push_back({(size_t)D.keep[img], s2_align_up((size_t)3 * D.kpitch * D.kh * sizeof(float), 256)});
+                    regs.push_back({(size_t)D.scratch[img], s2_align_up((size_t)6 * D.splane * sizeof(float), 256)});
+                }
+            }
+        }
+        std::sort(regs.begin(), regs.end(), [](const Region &a, const Region &b) { return a.off < b.off; });
+        for (size_t k = 0; k < regs.size(); k++) {
+            CHECK(regs[k].off % 256 == 0, "alignment");
+            CHECK(regs[k].off + regs[k].bytes <= P.level_bytes, "region past the level bytes");
+            if (k) CHECK(regs[k - 1].off + regs[k - 1].bytes <= regs[k].off, "overlapping regions");
+        }
+        if (m_ds) {
+            int next = 0;
+            for (const DsSeg &sg : P.dsegs) {
+                CHECK(sg.first_tile == next, "DSSIM tiles not contiguous");
+                const DsPair &D = P.ds[sg.pair];
+                CHECK(D.tile_base[sg.level] == sg.first_tile && sg.tiles_x == (D.w[sg.level] + 31) / 32, "segment");
+                next += D.tile_cnt[sg.level];
+            }
+            CHECK(next == P.ds_tiles, "DSSIM tile total");
+        }
+    }
+    printf("%s fails=%d pairs=%zu clamped=%zu\n", fails ? "FAILED" : "OK", fails, planned, with_clamp);
+    return fails ? 1 : 0;
+}
