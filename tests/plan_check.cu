@@ -5,7 +5,9 @@
 // bytes, starts 256-byte aligned and overlaps no other; DSSIM level sizes
 // follow dssim-cuda (halved rounding up, never below 8); the levels the prep
 // pass converts and the clamp pass builds split where those sizes leave the
-// ceil-halved pyramid; DSSIM tiles cover every level of every pair once.
+// ceil-halved pyramid; DSSIM tiles cover every level of every pair once;
+// the copy/compute groups of host-input submissions split pairs and tiles
+// contiguously; the staging of host planes is packed, aligned and disjoint.
 // plan() makes no CUDA call, so this runs without a GPU (built and run by
 // tests/test_cpu_plan.py).
 #include <algorithm>
@@ -63,7 +65,8 @@ int main(int argc, char **argv) {
             q.ref_pitch = q.dis_pitch = (size_t)q.width * 12;
         }
         Plan P;
-        const s2_status st = e.plan(d.data(), n, P);
+        const int ngroups = 1 + (int)(rng() % 6);
+        const s2_status st = e.plan(d.data(), n, P, nullptr, e.blur == S2_BLUR_FIR ? ngroups : 1);
         CHECK(st == S2_OK, "plan status %d", (int)st);
         const bool m_s2 = (e.metrics & S2_METRIC_SSIMULACRA2) != 0, m_ds = (e.metrics & S2_METRIC_DSSIM) != 0;
         std::vector<Region> regs;
@@ -141,6 +144,39 @@ int main(int argc, char **argv) {
                 next += D.tile_cnt[sg.level];
             }
             CHECK(next == P.ds_tiles, "DSSIM tile total");
+        }
+        // groups of a host-input submission: contiguous pairs and tiles, all covered
+        const int ng = (int)P.grp_pair.size() - 1;
+        CHECK(ng >= 1 && ng <= std::min(ngroups, n) && P.grp_pair.front() == 0 && P.grp_pair.back() == n,
+              "group pairs");
+        CHECK((int)P.grp_tile.size() == ng + 1 && P.grp_tile.front() == 0 && P.grp_tile.back() == P.total_tiles,
+              "group tiles");
+        for (int g = 0; g < ng; g++) {
+            CHECK(P.grp_pair[g] < P.grp_pair[g + 1] && P.grp_tile[g] <= P.grp_tile[g + 1], "group order");
+            for (int i = P.grp_pair[g]; i < P.grp_pair[g + 1]; i++)
+                for (int sc = 0; sc < P.pairs[i].nscales && P.pairs[i].status == S2_OK; sc++)
+                    CHECK(P.pairs[i].tile_base[sc] >= P.grp_tile[g] &&
+                              P.pairs[i].tile_base[sc] + P.pairs[i].tile_cnt[sc] <= P.grp_tile[g + 1],
+                          "a pair's tiles outside its group");
+        }
+        // staging of host planes: every plane the prep pass reads, packed, aligned, disjoint
+        const size_t stage = Engine::plan_staging(P, d.data());
+        std::vector<Region> st_regs;
+        for (int i = 0; i < n; i++) {
+            const DevPair &p = P.pairs[i];
+            if (p.status != S2_OK) continue;
+            const size_t row = s2_row_bytes(d[i]);
+            for (int img = 0; img < 2; img++) {
+                CHECK(p.pitch[img] == (long long)row, "staged pitch");
+                st_regs.push_back({(size_t)p.in[img], s2_align_up(row * d[i].height, 256)});
+                if (s2_is_yuv420(d[i].format))
+                    st_regs.push_back({(size_t)p.in_uv[img], s2_align_up(row * (d[i].height / 2), 256)});
+            }
+        }
+        std::sort(st_regs.begin(), st_regs.end(), [](const Region &a, const Region &b) { return a.off < b.off; });
+        for (size_t k = 0; k < st_regs.size(); k++) {
+            CHECK(st_regs[k].off % 256 == 0 && st_regs[k].off + st_regs[k].bytes <= stage, "staging bounds");
+            if (k) CHECK(st_regs[k - 1].off + st_regs[k - 1].bytes <= st_regs[k].off, "overlapping staging");
         }
     }
     printf("%s fails=%d pairs=%zu clamped=%zu\n", fails ? "FAILED" : "OK", fails, planned, with_clamp);
