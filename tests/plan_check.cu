@@ -7,7 +7,8 @@
 // pass converts and the clamp pass builds split where those sizes leave the
 // ceil-halved pyramid; DSSIM tiles cover every level of every pair once;
 // the copy/compute groups of host-input submissions split pairs and tiles
-// contiguously; the staging of host planes is packed, aligned and disjoint.
+// contiguously; the staging of host planes is packed, aligned and disjoint;
+// the reference-IIR mode's row records and vertical-walk planes are packed.
 // plan() makes no CUDA call, so this runs without a GPU (built and run by
 // tests/test_cpu_plan.py).
 #include <algorithm>
@@ -52,6 +53,7 @@ int main(int argc, char **argv) {
         e.scale_rule = (int)(rng() % 3);
         e.storage = (int)(rng() % 3);
         e.strip_rows_cfg = 21;
+        e.blur = rng() % 4 == 0 ? S2_BLUR_IIR_REF : S2_BLUR_FIR;
         const int n = 1 + (int)(rng() % 12);
         std::vector<s2_pair_desc> d(n);
         for (auto &q : d) {
@@ -144,6 +146,24 @@ int main(int argc, char **argv) {
                 next += D.tile_cnt[sg.level];
             }
             CHECK(next == P.ds_tiles, "DSSIM tile total");
+        }
+        if (e.blur == S2_BLUR_IIR_REF) {
+            // the reference's recursion: one record per row of each scored
+            // (pair, scale), its vertical-walk planes packed back to back
+            int rec = 0;
+            size_t vb = 0;
+            CHECK(P.vsegs.size() == P.hsegs.size(), "IIR segments");
+            for (size_t k = 0; k < P.vsegs.size(); k++) {
+                const IirSeg &v = P.vsegs[k];
+                const DevPair &p = P.pairs[v.pair];
+                CHECK(v.rec_base == rec && p.tile_base[v.scale] == rec && p.tile_cnt[v.scale] == p.h[v.scale],
+                      "IIR records");
+                CHECK((size_t)v.v == vb && (size_t)P.hsegs[k].v == vb, "IIR planes");
+                rec += p.h[v.scale];
+                vb += s2_align_up((size_t)15 * p.lp[v.scale] * p.h[v.scale] * sizeof(float), 256);
+            }
+            CHECK(rec == P.total_tiles && vb == P.v_bytes, "IIR totals");
+            continue;
         }
         // groups of a host-input submission: contiguous pairs and tiles, all covered
         const int ng = (int)P.grp_pair.size() - 1;
