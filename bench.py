@@ -309,9 +309,17 @@ def dssim_bench(tmb, descs, n_pairs, steps, warmup, s2_value, peak):
     npx = sum(max((W + (1 << s) - 1) >> s, 8) * max((H + (1 << s) - 1) >> s, 8) for s in range(5))
     ab = 32 * npx * n_pairs
     out["kernel_ms"] = {"prep_lab": float(acc[0]), "dssim_passes": float(acc[3])}
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "dssim_traffic.json")) as f:
+            traffic = json.load(f).get("bytes_per_launch") * n_pairs // 64
+    except (OSError, ValueError, TypeError):
+        traffic = None
     out["roofline"] = {"bound": "hbm", "achieved": ab / (acc[3] / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
                        "frac": ab / (acc[3] / 1e3) / 1e9 / peak, "algorithmic_bytes_per_launch": ab,
-                       "kernel": "dssim clamp+tile+mean+mad+final"}
+                       "kernel": "dssim clamp+tile+mean+mad+final",
+                       # ncu DRAM bytes of the tile launch (the passes' dominant kernel), per launch
+                       "traffic_tile_kernel": traffic}
     out["both_vs_ssimulacra2_only"] = out["both_pairs_per_s"] / s2_value
     b.close()
     return out
