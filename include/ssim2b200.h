@@ -124,6 +124,15 @@ const char *s2_last_error(void);
 void s2_config_default(s2_config *cfg);
 /* Number of scales scored for a w x h pair under a rule (0 if too small). */
 int s2_num_scales(uint32_t w, uint32_t h, int32_t scale_rule);
+/* The 4:2:0 YUV conversion coefficients the engine uses for a matrix
+ * (S2_MATRIX_*), range (S2_RANGE_*) and sample depth (8 for NV12, 16 for
+ * P016): y_coeff, r_coeff, b_coeff, g_coeff1, g_coeff2 as
+ * MatrixCoefficients::coefficients computes them (cuda-colorspace-kernel/
+ * src/lib.rs:188-203, Kr / Kb from constants_from_primaries :205-221, in
+ * f32), the luma minimum and the chroma neutral value (lib.rs:46-140).
+ * Introspection for parity checks; S2_ERR_INVALID_ARG on a bad selector. */
+s2_status s2_yuv_coefficients(int32_t matrix, int32_t range, int32_t bits, float coeffs[5],
+                              int32_t *luma_min, int32_t *chroma_neutral);
 
 /* ---- single pair (the drop-in) ----------------------------------------- */
 
@@ -379,16 +388,22 @@ s2_status s2_server_reset_stats(s2_server *sv);
  * (a host framework that owns all device memory through its own pool, a
  * plug-in that must not grow the process's footprint after start-up, code
  * that must not block on the allocator): every intermediate lives in one
- * 16 MiB array inside the library, reserved at load time on every GPU that
- * loads it.  sRGB8 pair on the device, default configuration (FIR blur, f32,
+ * 16 MiB array inside the library, held on every GPU that loads the
+ * library's device code.  The driver reserves it when it loads that code:
+ * at library load with eager module loading, or -- under lazy module
+ * loading, CUDA's default since 12.2 -- during the first call on each
+ * device, which may then synchronise: make that first call at start-up.
+ * sRGB8 pair on the device, default configuration (FIR blur, f32,
  * CPU-crate scale rule); the result is written to `out_device`, a device
  * buffer of one s2_result that the caller owns (read it after the stream
  * completes).  A pair whose layout does not fit the array returns
  * S2_ERR_INVALID_SIZE: any pair whose width and height are both at most 512
  * fits, larger ones are checked exactly.  All calls share the array, so calls
  * whose GPU work overlaps race: serialise them.  The first call on a device
- * sets the array up with that device current; make it before any stream
- * capture.  Allocates nothing. */
+ * sets the array up with that device current (a synchronous copy of the sRGB
+ * table into it); make it before any stream capture.  Each call hands its
+ * pair descriptor to the GPU as kernel arguments, so nothing reads the
+ * caller's host memory after the call returns.  Allocates nothing. */
 s2_status s2_compute_srgb8_noalloc(const uint8_t *ref, size_t ref_pitch, const uint8_t *dis,
                                    size_t dis_pitch, uint32_t width, uint32_t height,
                                    s2_result *out_device, void *stream);

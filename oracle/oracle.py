@@ -125,6 +125,23 @@ def yuv420_to_linear(y, uv, matrix="bt709", full=False, f64=False):
     return out
 
 
+def yuv_coeffs_ref_f32(matrix="bt709", full=False, bits=8):
+    """The reference's f32 derivation (cuda-colorspace-kernel/src/lib.rs:188-221)
+    of y_coeff, r_coeff, b_coeff, g_coeff1, g_coeff2, with the luma minimum and
+    chroma neutral value."""
+    c = np.zeros(5, np.float32)
+    ymin, neu = ctypes.c_int(), ctypes.c_int()
+    _lib.or_yuv_coeffs_ref_f32(MATRIX[matrix], 1 if full else 0, bits, _f(c), ctypes.byref(ymin), ctypes.byref(neu))
+    return c, ymin.value, neu.value
+
+
+def bt709_eotf_consts():
+    """alpha - 1, 1 / alpha, threshold, 1 / 4.5 as the f32 conversion uses them."""
+    c = np.zeros(4, np.float32)
+    _lib.or_bt709_eotf_consts(_f(c))
+    return c
+
+
 def rgb16_to_linear(img, bits=10, f64=False):
     a = np.ascontiguousarray(img, np.uint16)
     n = a.size // 3

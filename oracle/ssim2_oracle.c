@@ -270,6 +270,54 @@ static void yuv_coeffs(int matrix, int full, int bits, double c[5], int *ymin, i
     *neutral = 1 << (bits - 1);
 }
 
+/* The reference's own f32 derivation of the same five coefficients
+ * (cuda-colorspace-kernel/src/lib.rs:188-221 with const_algebra.rs): Kr / Kb
+ * from the f32 primaries by constants_from_primaries, then
+ * MatrixCoefficients::coefficients, every operation rounded to f32 in the
+ * reference's order (this file is built with -ffp-contract=off). */
+typedef struct { float x, y, z; } or_v3f;
+static or_v3f or_xy_to_xyz(float x, float y) {
+    or_v3f r = {x / y, 1.0f, ((1.0f - x) - y) / y};
+    return r;
+}
+static float or_dot3f(or_v3f a, or_v3f b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+static or_v3f or_cross3f(or_v3f a, or_v3f b) {
+    or_v3f r = {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+    return r;
+}
+void or_yuv_coeffs_ref_f32(int matrix, int full, int bits, float c[5], int *ymin, int *neutral) {
+    static const float P709[8] = {0.640f, 0.330f, 0.300f, 0.600f, 0.150f, 0.060f, 0.3127f, 0.3290f};
+    static const float P525[8] = {0.630f, 0.340f, 0.310f, 0.595f, 0.155f, 0.070f, 0.3127f, 0.3290f};
+    static const float P625[8] = {0.640f, 0.330f, 0.290f, 0.600f, 0.150f, 0.060f, 0.3127f, 0.3290f};
+    const float *p = matrix == 1 ? P525 : (matrix == 2 ? P625 : P709);
+    or_v3f r = or_xy_to_xyz(p[0], p[1]), g = or_xy_to_xyz(p[2], p[3]), b = or_xy_to_xyz(p[4], p[5]),
+           w = or_xy_to_xyz(p[6], p[7]);
+    or_v3f xr = {r.x, g.x, b.x}, yr = {r.y, g.y, b.y}, zr = {r.z, g.z, b.z};
+    float mul = 1.0f / or_dot3f(xr, or_cross3f(yr, zr));
+    float kr = or_dot3f(w, or_cross3f(g, b)) * mul;
+    float kb = or_dot3f(w, or_cross3f(r, g)) * mul;
+    const int sh = bits - 8;
+    float lrange = (float)(full ? (1u << bits) - 1u : (235u - 16u) << sh);
+    float crange = (float)(full ? (1u << bits) - 1u : (240u - 16u) << sh);
+    float kg = 1.0f - kr - kb;
+    c[0] = 1.0f / lrange;
+    c[1] = 2.0f * (1.0f - kr) * 1.0f / crange;
+    c[2] = 2.0f * (1.0f - kb) * 1.0f / crange;
+    c[3] = -2.0f * (1.0f - kb) * kb / kg * 1.0f / crange;
+    c[4] = -2.0f * (1.0f - kr) * kr / kg * 1.0f / crange;
+    if (ymin) *ymin = full ? 0 : (16 << sh);
+    if (neutral) *neutral = 1 << (bits - 1);
+}
+
+/* The f32 constants of the BT.709 inverse OETF as the engine compiles them:
+ * alpha - 1, 1 / alpha, the threshold, 1 / 4.5 (for the parity tests). */
+void or_bt709_eotf_consts(float out[4]) {
+    out[0] = 0x1.96b84p-4f;
+    out[1] = 0x1.d1c096p-1f;
+    out[2] = 0.08124285829863521110029445797874f;
+    out[3] = 0x1.c71c72p-3f;
+}
+
 static inline int yuv_sample(const void *p, size_t byte_off, int bits) {
     return bits == 8 ? ((const uint8_t *)p)[byte_off] : *(const uint16_t *)((const uint8_t *)p + byte_off);
 }
@@ -280,11 +328,11 @@ static inline int yuv_sample(const void *p, size_t byte_off, int bits) {
  * clamp to [0, 1]).  pitch in bytes, shared by both planes. */
 void or_yuv420_to_linear(const void *yp, const void *uvp, size_t pitch, int w, int h, int bits, int matrix,
                          int full, float *dst) {
-    double cd[5];
+    float cf[5];
     int ymin, neutral;
-    yuv_coeffs(matrix, full, bits, cd, &ymin, &neutral);
+    or_yuv_coeffs_ref_f32(matrix, full, bits, cf, &ymin, &neutral);
     const int es = bits == 8 ? 1 : 2;
-    float yc = (float)cd[0], rc = (float)cd[1], bc = (float)cd[2], g1 = (float)cd[3], g2 = (float)cd[4];
+    float yc = cf[0], rc = cf[1], bc = cf[2], g1 = cf[3], g2 = cf[4];
     for (int y = 0; y < h; y++) {
         for (int x = 0; x < w; x++) {
             const size_t uvo = (size_t)(y / 2) * pitch + (size_t)es * 2 * (x / 2);

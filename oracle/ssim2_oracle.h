@@ -77,6 +77,12 @@ void or_nv12_to_linear_f64(const uint8_t *y, const uint8_t *uv, size_t pitch,
                            int w, int h, double *dst);
 /* Packed RGB, uint16 holding `bits`-bit code values, BT.2020 primaries and
  * BT.709/BT.2020 transfer, converted to linear BT.709 RGB, clamped >= 0. */
+/* The reference's f32 derivation of the 4:2:0 coefficients (y, r, b, g1, g2;
+ * cuda-colorspace-kernel/src/lib.rs:188-221), luma minimum and chroma
+ * neutral value; matrix 0 BT.709, 1 BT.601-525, 2 BT.601-625. */
+void or_yuv_coeffs_ref_f32(int matrix, int full, int bits, float c[5], int *ymin, int *neutral);
+/* alpha - 1, 1 / alpha, threshold, 1 / 4.5 of the f32 BT.709 inverse OETF. */
+void or_bt709_eotf_consts(float out[4]);
 void or_rgb16_bt2020_to_linear(const uint16_t *src, size_t n_pixels, int bits,
                                float *dst);
 void or_rgb16_bt2020_to_linear_f64(const uint16_t *src, size_t n_pixels,

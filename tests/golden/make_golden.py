@@ -27,7 +27,7 @@ import os
 import re
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("TURBO_METRICS_REF", "/root/reference")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_tables.json")
 
 

@@ -17,7 +17,7 @@ import pytest
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLD = json.load(open(os.path.join(HERE, "golden", "reference_tables.json")))["dssim"]
 PUB = GOLD["published"]
-REF_TREE = "/root/reference"
+REF_TREE = os.environ.get("TURBO_METRICS_REF", "/root/reference")
 
 
 def solid(w, h, v):

@@ -25,7 +25,10 @@ def test_noalloc_matches_allocating_entry_point(tmb, cuda):
     lib = tmb.lib
     stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
     size = ctypes.sizeof(tmb.capi.Result)
-    for (w, h, seed, step) in [(512, 384, synth.pair_seed(0, 11), 16), (317, 200, synth.pair_seed(0, 12), 8)]:
+    # 512x512 and 500x512 sit on the documented bound (width and height at most
+    # 512 always fit); 317x200 has an odd width
+    for (w, h, seed, step) in [(512, 384, synth.pair_seed(0, 11), 16), (317, 200, synth.pair_seed(0, 12), 8),
+                               (512, 512, synth.pair_seed(0, 13), 12), (500, 512, synth.pair_seed(0, 14), 24)]:
         ref, dis = synth.srgb_pair(w, h, seed, step)
         rt = torch.from_numpy(ref).cuda()
         dt = torch.from_numpy(dis).cuda()
@@ -55,4 +58,10 @@ def test_noalloc_rejects_pairs_over_its_array(tmb, cuda):
     st = tmb.lib.s2_compute_srgb8_noalloc(ctypes.c_void_p(buf.data_ptr()), w * 3, ctypes.c_void_p(buf.data_ptr()),
                                           w * 3, w, h, ctypes.c_void_p(out.data_ptr()), None)
     assert st == 2  # S2_ERR_INVALID_SIZE
+    # twice the documented bound: 1024x1024 needs about 34 MB
+    w = h = 1024
+    big = torch.zeros((h, w, 3), dtype=torch.uint8, device="cuda")
+    st = tmb.lib.s2_compute_srgb8_noalloc(ctypes.c_void_p(big.data_ptr()), w * 3, ctypes.c_void_p(big.data_ptr()),
+                                          w * 3, w, h, ctypes.c_void_p(out.data_ptr()), None)
+    assert st == 2
     assert tmb.lib.s2_compute_srgb8_noalloc(None, 0, None, 0, 64, 64, None, None) == 8  # S2_ERR_INVALID_ARG

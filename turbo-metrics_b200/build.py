@@ -16,7 +16,7 @@ OUT = os.path.join(HERE, "libssim2b200.so")
 BUILD = os.path.join(HERE, "_build")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2"]
+COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2", "-Xcompiler", "-ffp-contract=off"]
 UNITS = [
     ("ssim2_kernels.cu", ["-fmad=false"]),
     ("ssim2_iir.cu", ["-fmad=false"]),

@@ -50,27 +50,6 @@ const float s2_srgb8_lut[256] = {
 #include "srgb8_lut.inc"
 };
 
-static void kr_kb_from_primaries(const double prim[8], double *kr, double *kb) {
-    // cuda-colorspace-kernel/src/lib.rs:205-221, in double
-    double xyz[4][3];
-    for (int i = 0; i < 4; i++) {
-        double x = prim[2 * i], y = prim[2 * i + 1];
-        xyz[i][0] = x / y;
-        xyz[i][1] = 1.0;
-        xyz[i][2] = (1.0 - x - y) / y;
-    }
-    double X[3] = {xyz[0][0], xyz[1][0], xyz[2][0]};
-    double Y[3] = {xyz[0][1], xyz[1][1], xyz[2][1]};
-    double Z[3] = {xyz[0][2], xyz[1][2], xyz[2][2]};
-    double cyz[3] = {Y[1] * Z[2] - Y[2] * Z[1], Y[2] * Z[0] - Y[0] * Z[2], Y[0] * Z[1] - Y[1] * Z[0]};
-    double mul = 1.0 / (X[0] * cyz[0] + X[1] * cyz[1] + X[2] * cyz[2]);
-    const double *r = xyz[0], *g = xyz[1], *b = xyz[2], *w = xyz[3];
-    double gxb[3] = {g[1] * b[2] - g[2] * b[1], g[2] * b[0] - g[0] * b[2], g[0] * b[1] - g[1] * b[0]};
-    double rxg[3] = {r[1] * g[2] - r[2] * g[1], r[2] * g[0] - r[0] * g[2], r[0] * g[1] - r[1] * g[0]};
-    *kr = (w[0] * gxb[0] + w[1] * gxb[1] + w[2] * gxb[2]) * mul;
-    *kb = (w[0] * rxg[0] + w[1] * rxg[1] + w[2] * rxg[2]) * mul;
-}
-
 static double det3(const double m[9]) {
     return m[0] * (m[4] * m[8] - m[5] * m[7]) - m[1] * (m[3] * m[8] - m[5] * m[6]) +
            m[2] * (m[3] * m[7] - m[4] * m[6]);
@@ -113,26 +92,69 @@ static void inv3(const double m[9], double o[9]) {
 }
 
 static const double BT709[8] = {0.640, 0.330, 0.300, 0.600, 0.150, 0.060, 0.3127, 0.3290};
-static const double BT601_525[8] = {0.630, 0.340, 0.310, 0.595, 0.155, 0.070, 0.3127, 0.3290};
-static const double BT601_625[8] = {0.640, 0.330, 0.290, 0.600, 0.150, 0.060, 0.3127, 0.3290};
 
-// 4:2:0 YUV coefficients (cuda-colorspace-kernel/src/lib.rs:188-203) of a
-// matrix (primaries of constants.rs), range and sample depth, with the
-// range's luma minimum and chroma neutral value (lib.rs:46-140).
+// 4:2:0 YUV coefficients of a matrix, range and sample depth, with the
+// range's luma minimum and chroma neutral value (cuda-colorspace-kernel/src/
+// lib.rs:46-140).  Derived in f32 with the reference's operations and their
+// order, so the five values are the reference's to the bit: Kr / Kb by
+// constants_from_primaries (lib.rs:205-221; the const Vec2 / Vec3 algebra of
+// const_algebra.rs, every product and sum rounded to f32, no fused
+// multiply-adds: this unit is built with -ffp-contract=off), then
+// MatrixCoefficients::coefficients (lib.rs:188-203), e.g. r_coeff =
+// ((2 * (1 - kr)) * 1) / chroma_range.  Primaries: constants.rs.
+namespace {
+struct V2f {
+    float x, y;
+};
+struct V3f {
+    float x, y, z;
+};
+V3f xy_to_xyz(V2f p) { return V3f{p.x / p.y, 1.0f, ((1.0f - p.x) - p.y) / p.y}; }
+float dot3(V3f a, V3f b) {
+    float s = a.x * b.x;
+    s = s + a.y * b.y;
+    return s + a.z * b.z;
+}
+V3f cross3(V3f a, V3f b) {
+    return V3f{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+const float kPrim709[8] = {0.640f, 0.330f, 0.300f, 0.600f, 0.150f, 0.060f, 0.3127f, 0.3290f};
+const float kPrim601_525[8] = {0.630f, 0.340f, 0.310f, 0.595f, 0.155f, 0.070f, 0.3127f, 0.3290f};
+const float kPrim601_625[8] = {0.640f, 0.330f, 0.290f, 0.600f, 0.150f, 0.060f, 0.3127f, 0.3290f};
+}  // namespace
+
 void s2_yuv_coeffs(int matrix, int range, int bits, float out[5], int *ymin, int *neutral) {
-    const double *prim = matrix == S2_MATRIX_BT601_525 ? BT601_525 : (matrix == S2_MATRIX_BT601_625 ? BT601_625 : BT709);
-    double kr, kb;
-    kr_kb_from_primaries(prim, &kr, &kb);
-    const double kg = 1.0 - kr - kb;
+    const float *pr = matrix == S2_MATRIX_BT601_525 ? kPrim601_525 : (matrix == S2_MATRIX_BT601_625 ? kPrim601_625 : kPrim709);
+    const V3f r = xy_to_xyz({pr[0], pr[1]}), g = xy_to_xyz({pr[2], pr[3]}), b = xy_to_xyz({pr[4], pr[5]}),
+              w = xy_to_xyz({pr[6], pr[7]});
+    const V3f x_rgb{r.x, g.x, b.x}, y_rgb{r.y, g.y, b.y}, z_rgb{r.z, g.z, b.z};
+    const float mul = 1.0f / dot3(x_rgb, cross3(y_rgb, z_rgb));
+    const float kr = dot3(w, cross3(g, b)) * mul;
+    const float kb = dot3(w, cross3(r, g)) * mul;
     const bool full = range == S2_RANGE_FULL;
     const int sh = bits - 8;
-    const double lrange = full ? (double)((1 << bits) - 1) : (double)((235 - 16) << sh);
-    const double crange = full ? (double)((1 << bits) - 1) : (double)((240 - 16) << sh);
-    const double c[5] = {1.0 / lrange, 2.0 * (1.0 - kr) / crange, 2.0 * (1.0 - kb) / crange,
-                         -2.0 * (1.0 - kb) * kb / kg / crange, -2.0 * (1.0 - kr) * kr / kg / crange};
-    for (int i = 0; i < 5; i++) out[i] = (float)c[i];
+    const float lrange = (float)(full ? (1u << bits) - 1u : (235u - 16u) << sh);
+    const float crange = (float)(full ? (1u << bits) - 1u : (240u - 16u) << sh);
+    const float kg = (1.0f - kr) - kb;
+    out[0] = 1.0f / lrange;
+    out[1] = ((2.0f * (1.0f - kr)) * 1.0f) / crange;
+    out[2] = ((2.0f * (1.0f - kb)) * 1.0f) / crange;
+    out[3] = (((((-2.0f) * (1.0f - kb)) * kb) / kg) * 1.0f) / crange;
+    out[4] = (((((-2.0f) * (1.0f - kr)) * kr) / kg) * 1.0f) / crange;
     *ymin = full ? 0 : (16 << sh);
     *neutral = 1 << (bits - 1);
+}
+
+extern "C" s2_status s2_yuv_coefficients(int32_t matrix, int32_t range, int32_t bits, float coeffs[5],
+                                         int32_t *luma_min, int32_t *chroma_neutral) {
+    if (!coeffs || matrix < S2_MATRIX_BT709 || matrix > S2_MATRIX_BT601_625 ||
+        (range != S2_RANGE_LIMITED && range != S2_RANGE_FULL) || (bits != 8 && bits != 16))
+        return S2_ERR_INVALID_ARG;
+    int ymin = 0, neutral = 0;
+    s2_yuv_coeffs(matrix, range, bits, coeffs, &ymin, &neutral);
+    if (luma_min) *luma_min = ymin;
+    if (chroma_neutral) *chroma_neutral = neutral;
+    return S2_OK;
 }
 
 ColorConsts s2_make_color_consts() {

@@ -7,8 +7,12 @@
 // cudaMalloc can synchronise the device).  For them this entry point keeps
 // every intermediate of the pipeline -- the XYB planes of all scales, the tile
 // sums, the work counter, the pair descriptor and the sRGB table -- in one
-// file-scope device array of fixed size, reserved when the library is loaded
-// and held by every GPU that loads it until the process exits.
+// file-scope device array of fixed size, held by every GPU that loads the
+// library's device code until the process exits.  The driver reserves it when
+// it loads the module that holds it: at library load with eager module
+// loading, or -- under CUDA's lazy module loading, the default since CUDA
+// 12.2 -- at the first call on each device, which may then synchronise.
+// Callers that must never block make that first call at start-up.
 //
 // Limits and rules:
 //   * the array holds 16 MiB; a pair whose layout needs more is rejected with
@@ -17,8 +21,11 @@
 //   * every call shares the array, so calls whose GPU work overlaps (other
 //     streams, other host threads) race and corrupt each other; serialise them;
 //   * the first call on a device looks the array's device address up and
-//     copies the sRGB table into it; make that first call before any stream
-//     capture on that device;
+//     copies the sRGB table into it (a synchronous copy); make that first
+//     call before any stream capture on that device;
+//   * the per-call pair descriptor reaches the array through a kernel that
+//     takes it as a by-value argument, so no call reads host memory after
+//     it returns;
 //   * nothing here calls cudaMalloc, cudaFree or an allocating library
 //     routine; the caller passes the inputs and a device buffer for the result.
 #include <cuda_runtime.h>
@@ -74,6 +81,31 @@ s2_status device_base(unsigned char **out) {
     }
     *out = g_base[dev];
     return S2_OK;
+}
+
+// The descriptors of one call, passed by value to desc_kernel (kernel
+// arguments are copied when the launch is enqueued).
+struct NoallocDesc {
+    DevPair pair;
+    Seg segs[kScales];
+    int nseg;
+    int blk_first;
+    unsigned off_pair, off_blk, off_seg;
+};
+static_assert(sizeof(NoallocDesc) < 4000, "kernel argument size");
+static_assert(sizeof(DevPair) % 4 == 0 && sizeof(Seg) % 4 == 0, "copied as 32-bit words");
+
+// Writes the descriptors into the array and zeroes the work counter.
+__global__ void desc_kernel(NoallocDesc d, unsigned char *base) {
+    const int t = threadIdx.x;
+    const unsigned *pw = (const unsigned *)&d.pair;
+    for (int i = t; i < (int)(sizeof(DevPair) / 4); i += blockDim.x) ((unsigned *)(base + d.off_pair))[i] = pw[i];
+    const unsigned *sw = (const unsigned *)d.segs;
+    for (int i = t; i < (int)(d.nseg * sizeof(Seg) / 4); i += blockDim.x) ((unsigned *)(base + d.off_seg))[i] = sw[i];
+    if (t == 0) {
+        *(int *)(base + d.off_blk) = d.blk_first;
+        *(int *)(base + kOffCounter) = 0;
+    }
 }
 
 }  // namespace
@@ -152,14 +184,20 @@ extern "C" s2_status s2_compute_srgb8_noalloc(const uint8_t *ref, size_t ref_pit
     for (int s = 0; s < ns; s++)
         for (int img = 0; img < 2; img++) P.lvl[img][s] = base + lvl_off[s][img];
 
-    // Descriptors into the array: pageable host memory is staged before
-    // cudaMemcpyAsync returns, so the stack copies may go out of scope.
+    // Descriptors into the array, as kernel arguments (copied at enqueue:
+    // nothing reads this stack frame after the call returns).
     cudaStream_t cs = (cudaStream_t)stream;
-    if (cudaMemcpyAsync(base + off_pair, &P, sizeof P, cudaMemcpyHostToDevice, cs) != cudaSuccess ||
-        cudaMemcpyAsync(base + off_blk, &blk_first, sizeof blk_first, cudaMemcpyHostToDevice, cs) != cudaSuccess ||
-        cudaMemcpyAsync(base + off_seg, segs, sizeof(Seg) * nseg, cudaMemcpyHostToDevice, cs) != cudaSuccess ||
-        cudaMemsetAsync(base + kOffCounter, 0, sizeof(int), cs) != cudaSuccess)
-        return fail("staging the pair descriptor");
+    NoallocDesc nd;
+    memset(&nd, 0, sizeof nd);
+    nd.pair = P;
+    memcpy(nd.segs, segs, sizeof(Seg) * nseg);
+    nd.nseg = nseg;
+    nd.blk_first = blk_first;
+    nd.off_pair = (unsigned)off_pair;
+    nd.off_blk = (unsigned)off_blk;
+    nd.off_seg = (unsigned)off_seg;
+    desc_kernel<<<1, 64, 0, cs>>>(nd, base);
+    if (cudaGetLastError() != cudaSuccess) return fail("staging the pair descriptor");
 
     const DevPair *dp = (const DevPair *)(base + off_pair);
     const ColorConsts cc{};  // sRGB8 input uses the table, not these constants
