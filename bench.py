@@ -134,19 +134,10 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-SERVE_BUCKETS = 10      # sizes of the serving pool (log-uniform 128^2 .. ~3840x2160)
-SERVE_VARIANTS = 4      # distinct candidates per size; jobs reuse them cyclically
-
-
-def serve_bucket_images(i):
-    """Reference + SERVE_VARIANTS DCT-quantised candidates at bucket i."""
+def serve_pool_candidate(args):
     import synth
-    t = (i + 0.5) / SERVE_BUCKETS
-    w, h = int(round(128 * 30.0 ** t)), int(round(128 * 16.875 ** t))
-    seed = synth.pair_seed(4, 500 + i)
-    ref, _ = synth.srgb_pair(w, h, seed)
-    steps = [2.0 + 46.0 * (v + 0.5) / SERVE_VARIANTS for v in range(SERVE_VARIANTS)]
-    return ref, [synth.srgb_pair(w, h, seed, st)[1] for st in steps]
+    ref, i = args
+    return synth.c4_pool_candidate(ref, i)
 
 
 def c2_pair(i):
@@ -198,45 +189,59 @@ def uneven_bench(tmb, n=256, steps=3):
             "batched_vs_chain": chain_ms / batched_ms, "max_score_diff": worst}
 
 
-def serving_bench(tmb, rates=(200, 1000, 5000), jobs_per_rate=(800, 1500, 1500), server_kw=None):
-    """Serving workload: Poisson arrivals at each offered rate, sizes
-    log-uniform between 128x128 and ~3840x2160, 1..16 candidates per job,
-    40 GB admission budget; latency = arrival -> all candidates scored."""
+def serving_bench(tmb, rates=(200, 1000, 5000), jobs_per_rate=10000, server_kw=None):
+    """Serving workload: `jobs_per_rate` Poisson arrivals at each offered rate;
+    job sizes continuous log-uniform between 128x128 and 3840x2160, 1..16
+    candidates per job with DCT steps uniform in [2, 48]; 40 GB admission
+    budget; latency = arrival -> all candidates scored.  Images are crops of a
+    pregenerated 3840x2160 pool (one reference, 16 candidates whose steps are
+    the midpoints of 16 bins of [2, 48]) at a per-job offset; a job's
+    candidates are the pool candidates of its steps' bins.  They sit in pinned
+    host memory and are passed with the pool's row pitch (no copies).  Jobs
+    the server refuses (Busy: 128 unfinished jobs) are counted, not retried."""
     import multiprocessing as mp
     import synth
     import torch
-    with mp.get_context("spawn").Pool(min(8, os.cpu_count() or 1)) as pool:
-        raw = pool.map(serve_bucket_images, range(SERVE_BUCKETS))
-    # the images live in pinned host memory, as a caller feeding PCIe keeps them
-    pinned = [(torch.from_numpy(r).pin_memory(), [torch.from_numpy(c).pin_memory() for c in cs]) for r, cs in raw]
-    buckets = [(r.numpy(), [c.numpy() for c in cs]) for r, cs in pinned]
-    out = {"pool": "%d sizes x (1 reference + %d candidates), pinned host memory" % (SERVE_BUCKETS, SERVE_VARIANTS)}
-    for rate, n in zip(rates, jobs_per_rate):
-        jobs = synth.c4_jobs(n, rate, seed_index=rate)
+    ref = synth.c4_pool_reference()
+    with mp.get_context("spawn").Pool(min(16, os.cpu_count() or 1)) as pool:
+        cands = pool.map(serve_pool_candidate, [(ref, i) for i in range(synth.C4_POOL_CANDS)])
+    pinned = [torch.from_numpy(a).pin_memory() for a in [ref] + cands]
+    pool_imgs = [t.numpy() for t in pinned]
+    out = {"workload": "C4: %d Poisson jobs per rate, sizes log-uniform 128x128..3840x2160 (continuous), "
+                       "1-16 candidates, DCT step U[2,48]" % jobs_per_rate,
+           "pool": "crops of one 3840x2160 reference + %d candidates (DCT step bin midpoints), pinned host "
+                   "memory" % synth.C4_POOL_CANDS}
+    for rate in rates:
+        jobs = synth.c4_jobs(jobs_per_rate, rate, seed_index=rate)
+        crops = [synth.c4_job_crop(jb) for jb in jobs]
         kw = dict(hbm_budget=40 << 30)
         kw.update(server_kw or {})
         sv = tmb.Ssim2Server(**kw)
-        # warm-up: one job per bucket
-        for ref, cands in buckets:
-            sv.wait(sv.submit(ref, cands[:1]))
+        # warm-up: a few jobs of assorted sizes
+        for jb, (ox, oy, idx) in list(zip(jobs, crops))[:8]:
+            w, h = jb["w"], jb["h"]
+            sv.wait(sv.submit(pool_imgs[0][oy:oy + h, ox:ox + w], [pool_imgs[1 + idx[0]][oy:oy + h, ox:ox + w]]))
         sv.reset_stats()
-        ids, pairs = [], 0
+        ids, pairs, rejected = [], 0, 0
         t0 = time.perf_counter()
-        for jb in jobs:
-            b = min(int(np.log(jb["w"] / 128.0) / np.log(30.0) * SERVE_BUCKETS), SERVE_BUCKETS - 1)
-            ref, cands = buckets[b]
-            k = jb["k"]
+        for jb, (ox, oy, idx) in zip(jobs, crops):
+            w, h = jb["w"], jb["h"]
             dt = jb["t"] - (time.perf_counter() - t0)
             if dt > 0:
                 time.sleep(dt)
-            ids.append(sv.submit(ref, [cands[c % SERVE_VARIANTS] for c in range(k)]))
-            pairs += k
+            try:
+                ids.append(sv.submit(pool_imgs[0][oy:oy + h, ox:ox + w],
+                                     [pool_imgs[1 + c][oy:oy + h, ox:ox + w] for c in idx]))
+                pairs += jb["k"]
+            except tmb.Busy:
+                rejected += 1
         for i in ids:
             sv.wait(i, timeout_ms=600000)
         wall = time.perf_counter() - t0
         rep = sv.stats()
         sv.close()
-        out["rate_%d" % rate] = {"offered_jobs_per_s": rate, "jobs": n, "pairs": pairs,
+        out["rate_%d" % rate] = {"offered_jobs_per_s": rate, "jobs": jobs_per_rate, "accepted_jobs": len(ids),
+                                 "rejected_busy": rejected, "pairs": pairs,
                                  "pairs_per_s": pairs / wall, "p50_ms": rep["p50_ms"], "p99_ms": rep["p99_ms"],
                                  "max_ms": rep["max_ms"], "rounds": rep["rounds"], "wall_s": wall,
                                  "gpu_busy_s": rep["gpu_busy_s"], "worker_wait_s": rep["worker_wait_s"],
@@ -267,8 +272,8 @@ def cpu_baseline(seconds=15.0, threads=None):
     dt = time.time() - t0
     return {"value": n / dt, "unit": "pairs/s", "cores": threads, "kind": "port",
             "sample": "%d x 1920x1080 pairs (NV12 converted to linear f32 outside the timed region), "
-                      "oracle cpu32 = restatement of ssimulacra2-cuda/examples/cpu.rs; single-thread %.2f s/pair"
-                      % (n, one)}
+                      "oracle cpu32 = scalar C port of ssimulacra2-cuda/examples/cpu.rs (-O3 -march=x86-64-v3, "
+                      "one pair per thread); single-thread %.2f s/pair" % (n, one)}
 
 
 def dssim_bench(tmb, descs, n_pairs, steps, warmup, s2_value, peak):
@@ -374,9 +379,10 @@ def run_reference(args, rank, world):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "1920x1080 NV12 pairs, reference CPU path, %d pairs per step" % per_step},
             "cpu_baseline": {"value": v, "unit": "pairs/s", "cores": threads, "kind": "port",
-                             "sample": "%d steps x %d 1080p pairs; oracle cpu32 = restatement of "
-                                       "ssimulacra2-cuda/examples/cpu.rs (the reference's Rust/NPP code "
-                                       "cannot be built here)" % (steps, per_step)},
+                             "sample": "%d steps x %d 1080p pairs; oracle cpu32 = scalar C port of "
+                                       "ssimulacra2-cuda/examples/cpu.rs (-O3 -march=x86-64-v3, one pair per "
+                                       "thread; the reference's Rust/NPP code cannot be built here)"
+                                       % (steps, per_step)},
             "e2e": {"value": v, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -410,6 +416,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--plain-pairs", type=int, default=64)
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--serve-jobs", type=int, default=10000, help="jobs per offered rate of the serving leg")
     ap.add_argument("--no-uneven", action="store_true", help="skip the 256-pair uneven-size batch leg")
     ap.add_argument("--no-dssim", action="store_true", help="skip the DSSIM (sibling metric) leg")
     ap.add_argument("--pairs", type=int, default=N_PAIRS,
@@ -558,7 +565,7 @@ def main():
 
     served = None
     if not args.no_serving:
-        served = serving_bench(tmb)
+        served = serving_bench(tmb, jobs_per_rate=args.serve_jobs)
     uneven = None
     if not args.no_uneven and world == 1:
         uneven = uneven_bench(tmb)

@@ -94,7 +94,7 @@ typedef struct {
     int32_t blur;          /* S2_BLUR_* */
     int32_t storage;       /* S2_STORAGE_* */
     int32_t scale_rule;    /* S2_SCALES_* */
-    int32_t strip_rows;    /* rows per fused tile: 9/21/63, or 0 = autotuned: the first
+    int32_t strip_rows;    /* rows per fused tile: 16/32/64, or 0 = autotuned: the first
                               submission of a workload class (work items in half-octave
                               buckets) times the tile pass at each height and the
                               fastest is kept for the class (process-wide) */
@@ -340,7 +340,9 @@ typedef struct {
     uint32_t max_batch_pairs;  /* candidates + reference builds per round */
     uint64_t max_batch_pixels; /* scale-0 pixels per round */
     uint64_t hbm_budget;       /* device bytes for admitted jobs + workspaces; 0 = no limit */
-    uint32_t max_queued_jobs;  /* submit returns S2_ERR_BUSY beyond this */
+    uint32_t max_queued_jobs;  /* unfinished jobs (waiting or admitted); submit returns
+                                  S2_ERR_BUSY beyond this (default 128: an overloaded
+                                  server sheds work instead of growing its latency) */
 } s2_server_config;
 
 typedef struct {

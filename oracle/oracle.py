@@ -13,7 +13,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "_build", "libssim2_oracle.so")
 
-MODE = {"fp64": 0, "cuda32": 1, "cpu32": 2, "fir32": 3}
+MODE = {"fp64": 0, "cuda32": 1, "cpu32": 2, "fir32": 3, "fir32c": 4}
 RULE = {"cpu": 0, "min8": 1, "all6": 2}
 
 
@@ -191,7 +191,8 @@ class Result:
 
 
 def ssim2_linear(ref, dis, mode="fp64", rule="cpu"):
-    """Full metric from linear RGB (H, W, 3).  mode: fp64 | cuda32 | cpu32 | fir32."""
+    """Full metric from linear RGB (H, W, 3).  mode: fp64 | cuda32 | cpu32 | fir32 |
+    fir32c (fir32 as the cached-reference path computes it)."""
     h, w = ref.shape[:2]
     st = np.zeros(108)
     su = np.zeros(108)
@@ -210,6 +211,21 @@ def ssim2_linear(ref, dis, mode="fp64", rule="cpu"):
     if rc != 0:
         raise ValueError("invalid image size %dx%d" % (w, h))
     return Result(sc.value, st, su, ns.value)
+
+
+def ssim2_maps_fir32(ref, dis, scale, rule="cpu"):
+    """The fir32 error maps of one scale from linear RGB (H, W, 3): an array
+    (3 channels, 3 maps [ssim error, artifact, detail loss], h_s, w_s)."""
+    h, w = ref.shape[:2]
+    hs, ws = h, w
+    for _ in range(scale):
+        hs, ws = (hs + 1) // 2, (ws + 1) // 2
+    r = np.ascontiguousarray(ref, np.float32)
+    d = np.ascontiguousarray(dis, np.float32)
+    out = np.zeros((3, 3, hs, ws), np.float32)
+    if _lib.or_ssim2_maps_fir32(_f(r), _f(d), w, h, RULE[rule], scale, _f(out)) != 0:
+        raise ValueError("scale %d is not scored for %dx%d" % (scale, w, h))
+    return out
 
 
 def ssim2_srgb8(ref, dis, mode="fp64", rule="cpu"):

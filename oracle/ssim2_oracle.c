@@ -895,50 +895,74 @@ static float border_gain_f(int x, int n) {
     return (float)(s - S[0]);
 }
 
-#define FIR_TW 56
-#define FIR_BAND 63
+#define FIR_TW 120  /* output columns per tile of the fused pass */
+#define FIR_BAND 64 /* rows per shift band */
+#define FIR_SEG 8   /* pixels per f32 partial sum (one horizontal task) */
 
-/* One scale in FIR32 arithmetic.  xr/xd: planar XYB (3 planes of W*H).
- * Tiles of 56 columns x 63 rows share one shift per channel: the reference
- * XYB at the tile's first column and first row.  sums[c*6 + n*3 + m]. */
-static void score_scale_fir32(const float *xr, const float *xd, int W, int H, double sums[18]) {
+static inline float fmaxf0(float v) { return v > 0.0f ? v : 0.0f; }
+
+/* fir9f with every tap halved: exactly half of fir9f (power-of-two scaling). */
+static inline float fir9f_half(float a0, float a1, float a2, float a3, float a4, float a5, float a6,
+                               float a7, float a8) {
+    float acc = (0.5f * FT4) * (a0 + a8);
+    acc = fmaf(0.5f * FT3, a1 + a7, acc);
+    acc = fmaf(0.5f * FT2, a2 + a6, acc);
+    acc = fmaf(0.5f * FT1, a3 + a5, acc);
+    return fmaf(0.5f * FT0, a4, acc);
+}
+
+/* One scale in FIR32 arithmetic (the fused CUDA pass of this repository,
+ * csrc/ssim2_kernels.cu fused_kernel).  xr/xd: planar XYB (3 planes of W*H).
+ * Tiles of 120 columns x 64-row bands share one shift per channel (the
+ * reference XYB at the tile's first column and the band's first row).  The
+ * shifted values x', y' (0 outside the image) are blurred by the kernels'
+ * 9-tap order, vertical then horizontal: x', y', x'y' and -- direct
+ * (cached = 0) -- one plane of x'^2 + y'^2 (both squares rounded first),
+ * halved through halved taps, or -- cached reference (cached = 1) -- x'^2
+ * and y'^2 separately, then (sigma11 + sigma22) / 2 = fma(0.5, s11, 0.5 s22).
+ * Maps are pooled in f32 over 8-pixel segments of a row, then in f64.
+ * sums[c*6 + n*3 + m].  With `maps` (9 planes of W*H, [channel][ssim,
+ * artifact, detail]) every pixel's error values are stored too. */
+static void score_scale_fir32(const float *xr, const float *xd, int W, int H, double sums[18], float *maps,
+                              int cached) {
     const int TC = FIR_TW + 8, TR = FIR_BAND + 8;
-    float *P = (float *)malloc((size_t)5 * TC * TR * sizeof(float)); /* shifted planes */
-    float *V = (float *)malloc((size_t)5 * TC * FIR_BAND * sizeof(float));
+    const int NP = 5; /* x', y', s (cached: x'^2), y'^2 (cached only), xy */
+    float *P = (float *)malloc((size_t)NP * TC * TR * sizeof(float));
+    float *V = (float *)malloc((size_t)NP * TC * FIR_BAND * sizeof(float));
     float *X = (float *)malloc((size_t)2 * TC * FIR_BAND * sizeof(float));
     double acc[18] = {0};
     size_t n = (size_t)W * H;
+    const float C2 = 0.0009f;
     for (int c = 0; c < 3; c++) {
         const float *a = xr + c * n, *b = xd + c * n;
         for (int y0 = 0; y0 < H; y0 += FIR_BAND) {
             int y1 = y0 + FIR_BAND < H ? y0 + FIR_BAND : H;
             for (int x0 = 0; x0 < W; x0 += FIR_TW) {
                 const float cv = a[(size_t)y0 * W + x0];
-                /* shifted inputs over [x0-4, x0+124) x [y0-4, y1+4) */
                 for (int r = 0; r < (y1 - y0) + 8; r++) {
                     int y = y0 - 4 + r;
                     for (int k = 0; k < TC; k++) {
                         int x = x0 - 4 + k;
-                        float vx = 0, vy = 0, vxx = 0, vyy = 0, vxy = 0;
+                        float vx = 0, vy = 0, vs = 0, vyy = 0, vxy = 0;
                         if (x >= 0 && x < W && y >= 0 && y < H) {
                             vx = a[(size_t)y * W + x] - cv;
                             vy = b[(size_t)y * W + x] - cv;
-                            vxx = vx * vx;
                             vyy = vy * vy;
+                            vs = cached ? vx * vx : vx * vx + vyy;
                             vxy = vx * vy;
                         }
                         size_t o = (size_t)r * TC + k;
                         P[0 * TC * TR + o] = vx;
                         P[1 * TC * TR + o] = vy;
-                        P[2 * TC * TR + o] = vxx;
+                        P[2 * TC * TR + o] = vs;
                         P[3 * TC * TR + o] = vyy;
                         P[4 * TC * TR + o] = vxy;
                     }
                 }
-                /* vertical FIR for output rows */
                 for (int r = 0; r < y1 - y0; r++)
                     for (int k = 0; k < TC; k++) {
-                        for (int p = 0; p < 5; p++) {
+                        for (int p = 0; p < NP; p++) {
+                            if (p == 3 && !cached) continue;
                             const float *q = P + (size_t)p * TC * TR + k;
                             V[(size_t)p * TC * FIR_BAND + (size_t)r * TC + k] =
                                 fir9f(q[(size_t)(r + 0) * TC], q[(size_t)(r + 1) * TC], q[(size_t)(r + 2) * TC],
@@ -948,45 +972,53 @@ static void score_scale_fir32(const float *xr, const float *xd, int W, int H, do
                         X[(size_t)0 * TC * FIR_BAND + (size_t)r * TC + k] = P[0 * TC * TR + (size_t)(r + 4) * TC + k];
                         X[(size_t)1 * TC * FIR_BAND + (size_t)r * TC + k] = P[1 * TC * TR + (size_t)(r + 4) * TC + k];
                     }
-                /* horizontal FIR, error maps, pooled in 4-pixel f32 chunks */
                 for (int r = 0; r < y1 - y0; r++) {
                     int y = y0 + r;
                     float bv = border_gain_f(y, H);
-                    for (int c0 = 0; c0 < FIR_TW; c0 += 4) {
+                    for (int c0 = 0; c0 < FIR_TW; c0 += FIR_SEG) {
                         if (x0 + c0 >= W) break;
                         float fs[3] = {0, 0, 0}, f4[3] = {0, 0, 0};
-                        for (int j = 0; j < 4; j++) {
+                        for (int j = 0; j < FIR_SEG; j++) {
                             int xx = x0 + c0 + j;
                             if (xx >= W) break;
                             float o[5];
-                            for (int p = 0; p < 5; p++) {
+                            for (int p = 0; p < NP; p++) {
+                                if (p == 3 && !cached) continue;
                                 const float *q = V + (size_t)p * TC * FIR_BAND + (size_t)r * TC + c0 + j;
-                                o[p] = fir9f(q[0], q[1], q[2], q[3], q[4], q[5], q[6], q[7], q[8]);
+                                o[p] = (p == 2 && !cached)
+                                           ? fir9f_half(q[0], q[1], q[2], q[3], q[4], q[5], q[6], q[7], q[8])
+                                           : fir9f(q[0], q[1], q[2], q[3], q[4], q[5], q[6], q[7], q[8]);
                             }
-                            float m1 = o[0], m2 = o[1], s11 = o[2], s22 = o[3], s12 = o[4];
+                            /* hs = (sigma11 + sigma22) / 2 of the shifted values */
+                            float m1 = o[0], m2 = o[1], s12 = o[4];
+                            float hs = cached ? fmaf(0.5f, o[2], 0.5f * o[3]) : o[2];
                             float xp = X[(size_t)r * TC + c0 + j + 4];
                             float yp = X[(size_t)TC * FIR_BAND + (size_t)r * TC + c0 + j + 4];
                             float bh = border_gain_f(xx, W);
                             float corr = (bh == 1.0f && bv == 1.0f) ? 0.0f : (float)(1.0 - (double)bh * (double)bv);
                             float kk = cv * corr;
                             float e = cv - kk;
-                            float v1 = fmaf(kk, fmaf(2.0f, m1, e), fmaf(-m1, m1, s11));
-                            float v2 = fmaf(kk, fmaf(2.0f, m2, e), fmaf(-m2, m2, s22));
-                            float cov = fmaf(kk, (m1 + m2) + e, fmaf(-m1, m2, s12));
+                            float h = (m1 + m2) + e;
                             float md = m1 - m2;
+                            /* w = hs - m1 m2 - md^2 / 2; den = 2 w + C2 (see maps_px) */
+                            float w = fmaf(-0.5f * md, md, fmaf(-m1, m2, hs));
+                            w = fmaf(kk, h, w);
+                            float den = fmaf(2.0f, w, C2);
+                            float cov = fmaf(kk, h, fmaf(-m1, m2, s12));
                             float num_m = fmaf(-md, md, 1.0f);
-                            float num_s = fmaf(2.0f, cov, 0.0009f);
-                            float den = (v1 + v2) + 0.0009f;
-                            float d = eng_div(fmaf(-num_m, num_s, den), den);
-                            d = d > 0.0f ? d : 0.0f;
+                            float num_s = fmaf(2.0f, cov, C2);
+                            float d = fmaxf0(eng_div(fmaf(-num_m, num_s, den), den));
                             float aa = fabsf((xp - m1) + kk);
                             float bb = fabsf((yp - m2) + kk);
                             float d1 = eng_div(bb - aa, 1.0f + aa);
-                            float art = d1 > 0.0f ? d1 : 0.0f, det = -d1 > 0.0f ? -d1 : 0.0f;
-                            float q;
-                            fs[0] += d;   q = d * d;     f4[0] += q * q;
-                            fs[1] += art; q = art * art; f4[1] += q * q;
-                            fs[2] += det; q = det * det; f4[2] += q * q;
+                            float v[3] = {d, fmaxf0(d1), fmaxf0(-d1)};
+                            if (maps)
+                                for (int m = 0; m < 3; m++) maps[((size_t)(3 * c + m) * H + y) * W + xx] = v[m];
+                            for (int m = 0; m < 3; m++) {
+                                fs[m] += v[m];
+                                float q = v[m] * v[m];
+                                f4[m] = fmaf(q, q, f4[m]);
+                            }
                         }
                         for (int m = 0; m < 3; m++) {
                             acc[c * 6 + m] += (double)fs[m];
@@ -1013,8 +1045,9 @@ static void to_planar_xyb_f32(const float *lin, size_t n, float *pl) {
     }
 }
 
-int or_ssim2_linear(const float *ref, const float *dis, int w, int h, int mode, int rule,
-                    double stats[108], double sums_out[108], double *score, int *n_scales) {
+static int ssim2_linear_impl(const float *ref, const float *dis, int w, int h, int mode, int rule,
+                             double stats[108], double sums_out[108], double *score, int *n_scales,
+                             int maps_scale, float *maps) {
     init_blur_consts();
     if (w < 1 || h < 1) return -1;
     if (rule != OR_SCALES_ALL6 && (w < 8 || h < 8)) return -1;
@@ -1040,8 +1073,8 @@ int or_ssim2_linear(const float *ref, const float *dis, int w, int h, int mode, 
         to_planar_xyb_f32(r, n, pr);
         to_planar_xyb_f32(d, n, pd);
         double sst[18], ssu[18];
-        if (mode == OR_MODE_FIR32) {
-            score_scale_fir32(pr, pd, cw, ch, ssu);
+        if (mode == OR_MODE_FIR32 || mode == OR_MODE_FIR32C) {
+            score_scale_fir32(pr, pd, cw, ch, ssu, (maps && s == maps_scale) ? maps : NULL, mode == OR_MODE_FIR32C);
             double inv = 1.0 / (double)n;
             for (int c = 0; c < 3; c++)
                 for (int k = 0; k < 3; k++) {
@@ -1081,6 +1114,19 @@ int or_ssim2_linear(const float *ref, const float *dis, int w, int h, int mode, 
         }
     }
     return 0;
+}
+
+int or_ssim2_linear(const float *ref, const float *dis, int w, int h, int mode, int rule,
+                    double stats[108], double sums_out[108], double *score, int *n_scales) {
+    return ssim2_linear_impl(ref, dis, w, h, mode, rule, stats, sums_out, score, n_scales, -1, NULL);
+}
+
+/* FIR32 error maps of one scale: 9 planes of w_s * h_s floats,
+ * [channel X, Y, B][ssim error, artifact, detail loss], row-major. */
+int or_ssim2_maps_fir32(const float *ref, const float *dis, int w, int h, int rule, int scale, float *maps) {
+    int ns = scales_for(w, h, rule);
+    if (scale < 0 || scale >= ns) return -1;
+    return ssim2_linear_impl(ref, dis, w, h, OR_MODE_FIR32, rule, NULL, NULL, NULL, NULL, scale, maps);
 }
 
 /* FP64 oracle. */

@@ -23,10 +23,18 @@
  *                    (cpu.rs:967-1022), vertical in the VERT_* form
  *                    (cpu.rs:1054-1115), d and d1 pooled in f64
  *                    (cpu.rs:581-683).  This is the timed CPU baseline.
- *   OR_MODE_FIR32    f32 restatement of the separable 9-tap FIR in the exact
- *                    operation order the CUDA kernels of this repository use
- *                    (vertical taps, then horizontal taps).  Used to check the
- *                    device kernels stage by stage.
+ *   OR_MODE_FIR32    f32 restatement of the fused CUDA pass of this
+ *                    repository: the separable 9-tap FIR in its operation
+ *                    order (vertical taps, then horizontal taps) on values
+ *                    shifted by one anchor per 120-column x 64-row block,
+ *                    four blurred planes (x', y', x'^2 + y'^2, x'y'), the
+ *                    error maps in the kernels' form, f32 sums over 8-pixel
+ *                    row segments.  Used to check the device kernels.
+ *   OR_MODE_FIR32C   FIR32 as the cached-reference path computes it: the
+ *                    reference's blurred x' and x'^2 come from its cache and
+ *                    the candidate blurs y', y'^2 and x'y', so
+ *                    (sigma11 + sigma22) / 2 = fma(0.5, sigma11, 0.5 sigma22)
+ *                    of separately blurred planes.
  *
  * Pyramid stop rules (which scales are scored):
  *   OR_SCALES_CPU    cpu.rs:359-361 -- before producing scale s>0, stop if
@@ -51,7 +59,7 @@
 extern "C" {
 #endif
 
-enum { OR_MODE_FP64 = 0, OR_MODE_CUDA32 = 1, OR_MODE_CPU32 = 2, OR_MODE_FIR32 = 3 };
+enum { OR_MODE_FP64 = 0, OR_MODE_CUDA32 = 1, OR_MODE_CPU32 = 2, OR_MODE_FIR32 = 3, OR_MODE_FIR32C = 4 };
 enum { OR_SCALES_CPU = 0, OR_SCALES_MIN8 = 1, OR_SCALES_ALL6 = 2 };
 
 /* Recursive-Gaussian constants (f32, as the reference kernels use them) and
@@ -111,6 +119,9 @@ int or_ssim2_linear_f64(const double *ref, const double *dis, int w, int h,
                         double *score, int *n_scales);
 
 /* The engine's cube root (ssim2_device.cuh s2_cbrtf), used by every f32 mode. */
+/* FIR32 error maps of one scale (the engine's s2_error_maps): 9 planes of
+ * w_s * h_s floats, [channel][ssim error, artifact, detail loss]. */
+int or_ssim2_maps_fir32(const float *ref, const float *dis, int w, int h, int rule, int scale, float *maps);
 float or_cbrtf(float x);
 /* The engine's division for b > 0 (Newton reciprocal + correction). */
 float or_div(float a, float b);

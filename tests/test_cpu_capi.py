@@ -44,7 +44,7 @@ def test_num_scales_matches_oracle(tmb, oracle, w, h, rule, n):
 
 def test_config_validation_needs_no_gpu(tmb):
     cfg = tmb.capi.make_config()
-    cfg.strip_rows = 48  # not one of 9, 21, 63
+    cfg.strip_rows = 48  # not one of 16, 32, 64
     h = ctypes.c_void_p()
     assert tmb.lib.s2_create(ctypes.byref(cfg), 64, 64, ctypes.byref(h)) == 8  # S2_ERR_INVALID_ARG
     cfg = tmb.capi.make_config()

@@ -30,8 +30,8 @@ def test_graph_replay_follows_each_submission(tmb, cuda):
     subs = [batch_of(tmb, cuda, shape, 700 + 10 * k) for k in range(3)]
     subs.append(batch_of(tmb, cuda, [(97, 333), (512, 512)], 800))  # another shape
     subs.append(subs[0])                                              # the first shape again
-    g = tmb.Ssim2Batch(8, 4 << 20, strip_rows=21)
-    plain = tmb.Ssim2Batch(8, 4 << 20, strip_rows=21)
+    g = tmb.Ssim2Batch(8, 4 << 20, strip_rows=32)
+    plain = tmb.Ssim2Batch(8, 4 << 20, strip_rows=32)
     plain.set_graphs(False)
     for pairs in subs:
         a = g.compute_batch(pairs)
@@ -48,8 +48,8 @@ def test_graph_replay_follows_each_submission(tmb, cuda):
 def test_single_pair_graphs_on_and_off(tmb, cuda):
     ref, dis = synth.srgb_pair(400, 300, 901)
     ref2, dis2 = synth.srgb_pair(400, 300, 902)
-    s = tmb.Ssimulacra2(400, 300, strip_rows=9)
-    t = tmb.Ssimulacra2(400, 300, strip_rows=9)
+    s = tmb.Ssimulacra2(400, 300, strip_rows=16)
+    t = tmb.Ssimulacra2(400, 300, strip_rows=16)
     t.set_graphs(False)
     for r, d in ((ref, dis), (ref2, dis2), (ref, dis)):
         s.compute_srgb(dev(cuda, r), dev(cuda, d))
@@ -63,7 +63,7 @@ def test_autotuned_tile_height_matches_fixed_heights(tmb, cuda):
     first = auto.compute_batch(pairs)
     again = auto.compute_batch(pairs)
     assert [x[0] for x in first] == [x[0] for x in again]  # the choice is kept
-    for rows in (9, 21, 63):
+    for rows in (16, 32, 64):
         fixed = tmb.Ssim2Batch(4, 8 << 20, strip_rows=rows).compute_batch(pairs)
         for a, f in zip(first, fixed):
             assert abs(a[0] - f[0]) < 1e-12

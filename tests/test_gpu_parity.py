@@ -2,10 +2,13 @@
 
 Two bars, on the same seeded inputs:
   * `fir32` -- the oracle's restatement of this engine's f32 arithmetic
-    (same taps, shift anchors, FMA placement and 5-pixel f32 partial sums):
+    (same taps, shift anchors, FMA placement and 8-pixel f32 partial sums):
     every one of the 108 statistics within 2e-6 relative (or 1e-12 absolute
     for statistics that are ~0), score within 2e-6.  Differences come only
-    from CUDA's vs glibc's cbrtf/powf (both <= 1 ulp) and f64 summation order.
+    from the error maps' division (the hardware reciprocal approximation and
+    one correction on the GPU, an FMA-only Newton division in the oracle; both
+    give the IEEE quotient outside rare near-halfway cases) and the f64
+    summation order.
   * `fp64` -- the FP64 oracle: score within 1e-3 absolute (the metric's bar).
 """
 import numpy as np
@@ -219,6 +222,44 @@ def test_batch_nv12_1080p_pair(tmb, oracle, cuda):
     assert out[0][0] == out[1][0]
     exact = oracle.ssim2_linear(oracle.nv12_to_linear(ry, ruv, True), oracle.nv12_to_linear(dy, duv, True), "fp64")
     assert abs(out[0][0] - exact.score) < FP64_TOL, (out[0][0], exact.score)
+
+
+def test_nv12_1080p_per_statistic(tmb, oracle, cuda):
+    """The bench workload's size and format (one 1920x1080 NV12 BT.709
+    limited pair of the 64): every statistic against fir32, the score against
+    FP64."""
+    (ry, ruv), (dy, duv) = synth.c1_pair(5)
+    s = tmb.Ssimulacra2(1920, 1080)
+    s.compute_nv12(dev(cuda, ry), dev(cuda, ruv), dev(cuda, dy), dev(cuda, duv))
+    score, stats, _ = s.get_result()
+    s.close()
+    rl, dl = oracle.nv12_to_linear(ry, ruv), oracle.nv12_to_linear(dy, duv)
+    mirror = oracle.ssim2_linear(rl, dl, "fir32")
+    assert_stats_close(stats, mirror.stats, what="1080p nv12")
+    assert abs(score - mirror.score) < SCORE_TOL
+    exact = oracle.ssim2_linear(oracle.nv12_to_linear(ry, ruv, True), oracle.nv12_to_linear(dy, duv, True), "fp64")
+    assert abs(score - exact.score) < FP64_TOL, (score, exact.score)
+
+
+@pytest.mark.parametrize("w,h", [(2047, 1999), (1999, 64), (2048, 2047)])
+def test_uneven_sizes_near_the_top_of_the_range(tmb, oracle, cuda, w, h):
+    """Sizes near 2048 of the uneven-size workload (width and height in
+    [64, 2048], not multiples of the tile): inside one batch with a small pair,
+    every statistic against fir32 and the score against FP64."""
+    i = 3000 + w + h
+    ref, dis = synth.srgb_pair(w, h, synth.pair_seed(2, i), 24)
+    small_r, small_d = synth.srgb_pair(97, 71, synth.pair_seed(2, i + 1), 8)
+    b = tmb.Ssim2Batch(2, w * h + 97 * 71)
+    out = b.compute_batch([tmb.PairDesc(dev(cuda, ref), dev(cuda, dis), "srgb8"),
+                           tmb.PairDesc(dev(cuda, small_r), dev(cuda, small_d), "srgb8")])
+    b.close()
+    mirror = oracle.ssim2_srgb8(ref, dis, "fir32")
+    assert_stats_close(out[0][1], mirror.stats, what="%dx%d" % (w, h))
+    assert abs(out[0][0] - mirror.score) < SCORE_TOL
+    exact = oracle.ssim2_srgb8(ref, dis, "fp64")
+    assert abs(out[0][0] - exact.score) < FP64_TOL, (out[0][0], exact.score)
+    small = oracle.ssim2_srgb8(small_r, small_d, "fir32")
+    assert_stats_close(out[1][1], small.stats, what="97x71 beside %dx%d" % (w, h))
 
 
 @pytest.mark.parametrize("storage,tol", [("f16", 0.2), ("bf16", 4.0)])

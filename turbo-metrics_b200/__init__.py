@@ -13,6 +13,7 @@ CPU fallback: importing this package without the built library raises.
 """
 from .capi import (  # noqa: F401
     S2Error,
+    Busy,
     InvalidImageSize,
     DimensionMismatch,
     NoCachedReference,
@@ -25,3 +26,4 @@ from .capi import (  # noqa: F401
 from .ssimulacra2 import Ssimulacra2, Ssim2Batch, PairDesc, Dssim  # noqa: F401
 from .server import Ssim2Server  # noqa: F401
 from .frames import FramePairScorer, Stats, select_frames  # noqa: F401
+from .router import RoutingPolicy, FrontEnd, Job, ServerEngine, worker_loop  # noqa: F401

@@ -14,18 +14,22 @@
 namespace s2 {
 
 constexpr int kScales = 6;
-constexpr int kTileW = 56;           // output columns per fused tile
-constexpr int kCols = kTileW + 8;    // columns incl. the 4-px halo on each side
-constexpr int kBand = 63;            // rows per shift band (tiles never straddle one; 7 x 9)
-constexpr int kRowsPerBlk = 9;       // output rows per horizontal step (= window length)
-constexpr int kSegs = 7;             // horizontal segments per row
-constexpr int kSegW = 8;             // output pixels per segment (kSegs * kSegW == kTileW)
-constexpr int kChunk = 4;            // pixels per f32 partial sum
+constexpr int kTileW = 120;          // output columns per fused tile (1920 = 16 tiles)
+constexpr int kCols = kTileW + 8;    // columns incl. the 4-px halo on each side (one thread each)
+constexpr int kBand = 64;            // rows per shift band (tiles never straddle one)
+constexpr int kStep = 8;             // output rows per vertical / horizontal step
+constexpr int kSegW = 8;             // output pixels per horizontal task (one f32 partial sum)
+constexpr int kSegs = kTileW / kSegW;  // horizontal tasks per row (15)
+constexpr int kStripMin = 16, kStripMid = 32, kStripMax = 64;  // tile heights (divide kBand)
 constexpr int kPyrBlk = 64;          // scale-0 block edge of the prep kernel
 constexpr float kC2 = 0.0009f;
 constexpr int kDsLevels = 5;         // DSSIM scales (dssim-cuda/src/lib.rs:73)
 
 enum Format { FMT_LINEAR_F32 = 0, FMT_SRGB8 = 1, FMT_NV12 = 2, FMT_RGB16 = 3, FMT_P016 = 4 };
+// Modes of the fused tile pass (per run of tiles): score a pair from both
+// images' XYB; build a cached reference's blurred moments; score a candidate
+// against a cached reference's moments.
+enum TileMode { TM_FULL = 0, TM_REFMOM = 1, TM_CAND = 2 };
 enum Storage { ST_F32 = 0, ST_F16 = 1, ST_BF16 = 2 };
 
 // FIR taps of the exact form of the recursive Gaussian (sigma 1.5, N = 5),
@@ -68,6 +72,11 @@ struct DevPair {
     float *keep[2];
     int lab_levels;          // 0: no Lab output
     int prep_levels;         // levels the prep pass builds (XYB and Lab)
+    // A cached reference's blurred moments per scale (TM_REFMOM writes them,
+    // TM_CAND reads them): 6 f32 planes of pitch lp[s] -- the blurred
+    // shifted reference XYB (mu1) of channels X, Y, B, then its blurred
+    // square (sigma11) of X, Y, B.
+    float *mom[kScales];
 };
 
 // One pair as the DSSIM kernels see it.  Level sizes follow dssim-cuda
@@ -101,6 +110,7 @@ struct Seg {
     int scale;
     int tiles_x;
     int strip_rows;
+    int mode;  // TileMode
 };
 
 // A run of S2_BLUR_IIR_REF work items of one (pair, scale): columns x planes
@@ -340,6 +350,32 @@ __device__ __forceinline__ float s2_pow_scale_unit(unsigned b) {
 // that are summed are formed by scalar multiplies (never contracted under
 // -fmad=false), or the sum is the addend of a packed FMA, or the product is
 // exact (a multiplication by 0.5).
+// The same operations as inline PTX (add / mul / fma .rn.f32x2): the
+// optimiser sees no multiply and add to contract, and PTX does not fuse
+// operations that carry an explicit rounding modifier, so each lane rounds
+// exactly as the written scalar operation.  The fused tile pass uses these.
+__device__ __forceinline__ float2 s2_padd(float2 a, float2 b) {
+    float2 d;
+    asm("{.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "add.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;}"
+        : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
+}
+__device__ __forceinline__ float2 s2_pmul(float2 a, float2 b) {
+    float2 d;
+    asm("{.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "mul.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;}"
+        : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
+}
+__device__ __forceinline__ float2 s2_pfma(float2 a, float2 b, float2 c) {
+    float2 d;
+    asm("{.reg .b64 ra, rb, rc, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "mov.b64 rc, {%6, %7};\n\tfma.rn.f32x2 rd, ra, rb, rc;\n\tmov.b64 {%0, %1}, rd;}"
+        : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+    return d;
+}
+
 __device__ __forceinline__ float2 s2_mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
 __device__ __forceinline__ float2 s2_add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
 __device__ __forceinline__ float2 s2_mul2s(float2 a, float2 b) { return make_float2(a.x * b.x, a.y * b.y); }

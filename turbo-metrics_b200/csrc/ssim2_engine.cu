@@ -365,7 +365,8 @@ static s2_status check_cfg(const s2_config *cfg) {
     if (cfg->blur != S2_BLUR_FIR && cfg->blur != S2_BLUR_IIR_REF) return S2_ERR_INVALID_ARG;
     if (cfg->storage < 0 || cfg->storage > 2) return S2_ERR_INVALID_ARG;
     if (cfg->scale_rule < 0 || cfg->scale_rule > 2) return S2_ERR_INVALID_ARG;
-    if (cfg->strip_rows != 0 && cfg->strip_rows != 9 && cfg->strip_rows != 21 && cfg->strip_rows != 63)
+    if (cfg->strip_rows != 0 && cfg->strip_rows != kStripMin && cfg->strip_rows != kStripMid &&
+        cfg->strip_rows != kStripMax)
         return S2_ERR_INVALID_ARG;
     return S2_OK;
 }
@@ -711,9 +712,12 @@ s2_status s2_error_maps(s2_ctx *ctx, int32_t scale, float *maps, size_t pitch, v
     cudaStream_t st = (cudaStream_t)stream;
     const long long mpitch = (long long)(pitch / sizeof(float));
     S2_CUDA(cudaMemsetAsync(e.counter_d.p, 0, sizeof(int), st));
-    S2_CUDA(launch_fused_export(e.storage, (const DevPair *)dbase, (const Seg *)(dbase + pb + bb), (int)P.segs.size(), t0,
-                                t1, (int *)e.counter_d.p, (double *)e.partials_d.p, maps, mpitch,
-                                mpitch * p.h[scale], e.num_sms * e.fused_bps, st));
+    int mode = TM_FULL;
+    for (const Seg &sg : P.segs)
+        if (sg.pair == 0 && sg.scale == scale && sg.mode != TM_REFMOM) mode = sg.mode;
+    S2_CUDA(launch_fused_export(e.storage, mode, (const DevPair *)dbase, (const Seg *)(dbase + pb + bb),
+                                (int)P.segs.size(), t0, t1, (int *)e.counter_d.p, (double *)e.partials_d.p, maps,
+                                mpitch, mpitch * p.h[scale], e.num_sms * e.fused_bps, st));
     return S2_OK;
 }
 

@@ -30,45 +30,36 @@
 
 namespace s2 {
 
-// Shared memory layout of fused_kernel (one CTA = one channel of a tile).
-// Rows ("rb" = output row of the 9-row block) of the float2 arrays are
-// kRowStride2 float2 apart and rows of the float array kRowStride1 floats
-// apart.  The horizontal tasks read them with 16-byte loads, lane t taking
-// block row t % 9 and segment t / 9: with kRowStride2 / 2 and
-// kRowStride1 / 4 odd, consecutive rows fall in distinct 16-byte bank groups
-// (at most 2-way where a load phase spans two segments).  The plain
-// 64-element stride gave up to 10-way conflicts.
-constexpr int kRB = kRowsPerBlk;                         // rows of one block
-constexpr int kRowStride2 = 74;                          // float2 elements
-constexpr int kRowStride1 = 76;                          // float elements
-static_assert(kRowStride2 % 2 == 0 && (kRowStride2 / 2) % 2 == 1, "16-byte aligned rows, odd 16-byte stride");
-static_assert(kRowStride1 % 4 == 0 && (kRowStride1 / 4) % 2 == 1, "16-byte aligned rows, odd 16-byte stride");
-constexpr int kSmVo2 = 2 * kRB * kRowStride2 * 2;        // vertical FIR of (x,y), (xx,yy) [pair][rb][col] (floats)
-constexpr int kSmXo = kRB * kRowStride2 * 2;             // shifted raw XYB (x', y') of the output rows [rb][col]
-constexpr int kSmVo1 = kRB * kRowStride1;                // vertical FIR of xy [rb][col]
-constexpr int kFusedSmemFloats = kSmVo2 + kSmXo + kSmVo1;
-constexpr int kFusedThreads = kCols;
-constexpr int kTasks = kRB * kSegs;                      // horizontal tasks per 9-row block
-static_assert(kSmVo2 % 4 == 0 && kSmXo % 4 == 0, "arrays start 16-byte aligned");
+// Shared memory of fused_kernel (one CTA = one channel of a tile): two
+// buffers (step parity), each three float2 planes of kStep rows x kRS
+// columns -- plane 0 and 1 the vertical FIRs, plane 2 the raw (x', y') of the
+// output rows.  A horizontal task reads 16-byte words of one row; the 8
+// lanes of a load phase take the same segment of rows 0..7, whose starts are
+// kRS * 8 = 1040 bytes apart: 65 16-byte groups, odd, so the 8 rows fall in
+// distinct bank groups.
+constexpr int kRS = kCols + 2;                        // float2 per row
+constexpr int kPlaneF2 = kStep * kRS;                 // float2 per plane
+constexpr int kBufF2 = 3 * kPlaneF2;                  // float2 per buffer
+constexpr int kFusedThreads = kCols;                  // one vertical column each
+constexpr int kTasks = kStep * kSegs;                 // horizontal tasks per step (120)
+static_assert((kRS / 2) % 2 == 1, "odd 16-byte stride between rows");
+static_assert(kTasks <= kFusedThreads, "one horizontal task per thread");
+static_assert(kBand % kStripMax == 0 && kStripMax % kStep == 0 && kStripMid % kStep == 0 &&
+                  kStripMin % kStep == 0, "tiles never straddle a band; whole steps");
 
-__device__ __forceinline__ float fir9(float a0, float a1, float a2, float a3, float a4, float a5,
-                                      float a6, float a7, float a8) {
-    float acc = S2_T4 * (a0 + a8);
-    acc = fmaf(S2_T3, a1 + a7, acc);
-    acc = fmaf(S2_T2, a2 + a6, acc);
-    acc = fmaf(S2_T1, a3 + a5, acc);
-    return fmaf(S2_T0, a4, acc);
-}
-
-// The same FIR on two planes at once (sm_100 packed f32x2; each lane rounds
-// exactly as the scalar fir9).
-__device__ __forceinline__ float2 fir9x2(float2 a0, float2 a1, float2 a2, float2 a3, float2 a4, float2 a5,
-                                         float2 a6, float2 a7, float2 a8) {
-    float2 acc = s2_mul2(make_float2(S2_T4, S2_T4), s2_add2(a0, a8));
-    acc = __ffma2_rn(make_float2(S2_T3, S2_T3), s2_add2(a1, a7), acc);
-    acc = __ffma2_rn(make_float2(S2_T2, S2_T2), s2_add2(a2, a6), acc);
-    acc = __ffma2_rn(make_float2(S2_T1, S2_T1), s2_add2(a3, a5), acc);
-    return __ffma2_rn(make_float2(S2_T0, S2_T0), a4, acc);
+// 9-tap symmetric FIR of two planes at once (f32x2 lanes; each lane rounds as
+// acc = t4 (a0 + a8); acc = fma(t3, a1 + a7, acc); ...; fma(t0, a4, acc)).
+// HX: the x lane uses the taps halved -- a power-of-two scaling, so that lane
+// is exactly half of the plain FIR.
+template <bool HX = false>
+__device__ __forceinline__ float2 fir9p(float2 a0, float2 a1, float2 a2, float2 a3, float2 a4, float2 a5,
+                                        float2 a6, float2 a7, float2 a8) {
+    constexpr float hx = HX ? 0.5f : 1.0f;
+    float2 acc = s2_pmul(make_float2(hx * S2_T4, S2_T4), s2_padd(a0, a8));
+    acc = s2_pfma(make_float2(hx * S2_T3, S2_T3), s2_padd(a1, a7), acc);
+    acc = s2_pfma(make_float2(hx * S2_T2, S2_T2), s2_padd(a2, a6), acc);
+    acc = s2_pfma(make_float2(hx * S2_T1, S2_T1), s2_padd(a3, a5), acc);
+    return s2_pfma(make_float2(hx * S2_T0, S2_T0), a4, acc);
 }
 
 template <bool KUNIT>
@@ -161,73 +152,103 @@ __device__ __forceinline__ void store_lab(const DevPair &P, int img, int s, int 
 
 // OUT: bit 0 SSIMULACRA2's XYB planes, bit 1 DSSIM's Lab planes (both from
 // the same linear pyramid).  OUT == 1 is the SSIMULACRA2-only pass.
+//
+// A thread takes two horizontally adjacent 2x2 quads at a time (4 x 2
+// scale-0 pixels): the scale-0 XYB goes out as pixel pairs, and the two
+// quads' scale-1 pixels form one pair for the f32x2 XYB conversion too.
 template <int FMT, typename ST, int OUT>
 __device__ __forceinline__ void prep_quads(const DevPair &P, int X0, int Y0, const float *lut, const ColorConsts &cc,
                                            float (*lv1)[3][kLv1 * kLv1]) {
     constexpr bool KU = FMT != FMT_LINEAR_F32;
     constexpr bool kX = (OUT & 1) != 0, kL = (OUT & 2) != 0;
+    constexpr bool kYuv = FMT == FMT_NV12 || FMT == FMT_P016;
+    constexpr int kEs = FMT == FMT_P016 ? 2 : 1;
     const int W = P.w[0], H = P.h[0];
     const bool scale1 = (kL ? P.prep_levels : P.nscales) > 1;
-    for (int q = threadIdx.x; q < kLv1 * kLv1; q += blockDim.x) {
-        const int qx = q % kLv1, qy = q / kLv1;
+    for (int qq = threadIdx.x; qq < kLv1 * kLv1 / 2; qq += blockDim.x) {
+        const int qx = 2 * (qq % (kLv1 / 2)), qy = qq / (kLv1 / 2);  // first quad of the two
         const int x = X0 + 2 * qx, y = Y0 + 2 * qy;
         if (x >= W || y >= H) continue;
-        const bool vx = x + 1 < W, vy = y + 1 < H;
+        const bool two = x + 2 < W;  // the second quad starts inside the image
+        const bool vy = y + 1 < H;
         // 4:2:0 YUV: both images' samples are loaded before either is converted
-        constexpr bool kYuv = FMT == FMT_NV12 || FMT == FMT_P016;
-        constexpr int kEs = FMT == FMT_P016 ? 2 : 1;
-        Nv12Quad nq0{}, nq1{};
+        Nv12Quad nr0{}, nr1{}, nd0{}, nd1{};  // [reference, distorted][quad]
         if (kYuv) {
-            if (P.prep_mask & 1) nq0 = yuv_load_quad<kEs>(P, 0, x, y);
-            if (P.prep_mask & 2) nq1 = yuv_load_quad<kEs>(P, 1, x, y);
+            if (P.prep_mask & 1) {
+                nr0 = yuv_load_quad<kEs>(P, 0, x, y);
+                if (two) nr1 = yuv_load_quad<kEs>(P, 0, x + 2, y);
+            }
+            if (P.prep_mask & 2) {
+                nd0 = yuv_load_quad<kEs>(P, 1, x, y);
+                if (two) nd1 = yuv_load_quad<kEs>(P, 1, x + 2, y);
+            }
         }
 #pragma unroll 1
         for (int img = 0; img < 2; img++) {
             if (!((P.prep_mask >> img) & 1)) continue;
-            float v[4][3];
-            if (kYuv) yuv_quad_linear<kEs>(img ? nq1 : nq0, P, v);
-            else lin_quad<FMT>(P, img, x, y, vx, vy, lut, cc, v);
-            if (kX && (!kL || P.nscales > 0)) {
-                ST *dst = (ST *)P.lvl[img][0];
-                const long long plane = (long long)P.lp[0] * H;
-                const long long off = (long long)y * P.lp[0] + x;
-                if (vx) store_xyb_pair<ST, KU>(dst, plane, off, v[0], v[1]);
-                else store_xyb<ST, KU>(P, img, 0, x, y, v[0]);
-                if (vy) {
-                    if (vx) store_xyb_pair<ST, KU>(dst, plane, off + P.lp[0], v[2], v[3]);
-                    else store_xyb<ST, KU>(P, img, 0, x, y + 1, v[2]);
+            float l1[2][3];
+#pragma unroll
+            for (int k = 0; k < 2; k++) {
+                if (k == 1 && !two) break;
+                const int xq = x + 2 * k;
+                const bool vx = xq + 1 < W;
+                float v[4][3];
+                if (kYuv) yuv_quad_linear<kEs>(img ? (k ? nd1 : nd0) : (k ? nr1 : nr0), P, v);
+                else lin_quad<FMT>(P, img, xq, y, vx, vy, lut, cc, v);
+                if (kX && (!kL || P.nscales > 0)) {
+                    ST *dst = (ST *)P.lvl[img][0];
+                    const long long plane = (long long)P.lp[0] * H;
+                    const long long off = (long long)y * P.lp[0] + xq;
+                    if (vx) store_xyb_pair<ST, KU>(dst, plane, off, v[0], v[1]);
+                    else store_xyb<ST, KU>(P, img, 0, xq, y, v[0]);
+                    if (vy) {
+                        if (vx) store_xyb_pair<ST, KU>(dst, plane, off + P.lp[0], v[2], v[3]);
+                        else store_xyb<ST, KU>(P, img, 0, xq, y + 1, v[2]);
+                    }
+                }
+                if (kL) {
+                    store_lab(P, img, 0, xq, y, v[0]);
+                    if (vx) store_lab(P, img, 0, xq + 1, y, v[1]);
+                    if (vy) store_lab(P, img, 0, xq, y + 1, v[2]);
+                    if (vx && vy) store_lab(P, img, 0, xq + 1, y + 1, v[3]);
+                }
+                // scale-1 pixel: 2x2 mean, far-edge clamp (a missing column
+                // repeats the left pixel, a missing row the upper one)
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    const float a = v[0][c];
+                    const float b = vx ? v[1][c] : a;
+                    const float cc2 = vy ? v[2][c] : a;
+                    const float d = vy ? (vx ? v[3][c] : cc2) : b;
+                    float sum = a + b;
+                    sum = sum + cc2;
+                    sum = sum + d;
+                    l1[k][c] = sum * 0.25f;
                 }
             }
-            if (kL) {
-                store_lab(P, img, 0, x, y, v[0]);
-                if (vx) store_lab(P, img, 0, x + 1, y, v[1]);
-                if (vy) store_lab(P, img, 0, x, y + 1, v[2]);
-                if (vx && vy) store_lab(P, img, 0, x + 1, y + 1, v[3]);
-            }
             if (!scale1) continue;
-            // far-edge clamp: a missing column repeats the left pixel, a
-            // missing row the upper one
-            float l1[3];
+            const int x1 = (X0 >> 1) + qx, y1 = (Y0 >> 1) + qy;
 #pragma unroll
             for (int c = 0; c < 3; c++) {
-                const float a = v[0][c];
-                const float b = vx ? v[1][c] : a;
-                const float cc2 = vy ? v[2][c] : a;
-                const float d = vy ? (vx ? v[3][c] : cc2) : b;
-                float sum = a + b;
-                sum = sum + cc2;
-                sum = sum + d;
-                l1[c] = sum * 0.25f;
-                lv1[img][c][q] = l1[c];
+                lv1[img][c][qy * kLv1 + qx] = l1[0][c];
+                if (two) lv1[img][c][qy * kLv1 + qx + 1] = l1[1][c];
             }
-            if (kX && (!kL || P.nscales > 1)) store_xyb<ST, KU>(P, img, 1, (X0 >> 1) + qx, (Y0 >> 1) + qy, l1);
-            if (kL) store_lab(P, img, 1, (X0 >> 1) + qx, (Y0 >> 1) + qy, l1);
+            if (kX && (!kL || P.nscales > 1)) {
+                // x1 is even and the planes' pitch a multiple of 64 elements
+                if (two) store_xyb_pair<ST, KU>((ST *)P.lvl[img][1], (long long)P.lp[1] * P.h[1],
+                                                (long long)y1 * P.lp[1] + x1, l1[0], l1[1]);
+                else store_xyb<ST, KU>(P, img, 1, x1, y1, l1[0]);
+            }
+            if (kL) {
+                store_lab(P, img, 1, x1, y1, l1[0]);
+                if (two) store_lab(P, img, 1, x1 + 1, y1, l1[1]);
+            }
         }
     }
 }
 
 template <typename ST, int OUT>
-__global__ void __launch_bounds__(256, 3) prep_kernel(const DevPair *__restrict__ pairs, int npairs,
+__global__ void __launch_bounds__(256, 2) prep_kernel(const DevPair *__restrict__ pairs, int npairs,
                                                    const int *__restrict__ blk_first, int first_block,
                                                    int end_block,
                                                    ColorConsts cc, const float *__restrict__ lut_g) {
@@ -303,11 +324,43 @@ __global__ void __launch_bounds__(256, 3) prep_kernel(const DevPair *__restrict_
 // fused per-scale tile pass
 // ---------------------------------------------------------------------------
 //
-// Work item = (tile, channel): item = 3 * tile + channel, 64 threads (two
-// warps) per CTA, so that a block barrier waits for two warps only and up to
-// ten CTAs share an SM.  A tile's three items write the tile's 18 partial
-// sums (channel-major) and are summed in the same order as one CTA per tile
-// over all channels would.
+// Work item = one channel of a tile of kTileW (120) output columns x
+// `strip_rows` rows at one scale of one pair: item = 3 * tile + channel.  A
+// tile's three items write its 18 partial sums, channel-major.  128 threads
+// walk down the tile in steps of kStep (8) rows; each step has two phases.
+//
+//   vertical    thread c owns input column x0 - 4 + c (the tile's columns and
+//               a 4-column halo on each side).  It keeps the shifted inputs of
+//               its column in register rings of 16 rows, where x' = ref -
+//               anchor and y' = dis - anchor, and for each output row of the
+//               step forms their 9-tap vertical FIRs.  The step's 8 new input
+//               rows go to ring slots 8..15 on even steps and 0..7 on odd
+//               steps, so every ring index is a compile-time constant.
+//               Pixels outside the image load the anchor itself, which shifts
+//               to exactly 0: zero padding of the shifted values, undone at
+//               the borders by border_gain.
+//   horizontal  thread t takes row t % 8 of the step and the 8-pixel segment
+//               t / 8 (120 tasks): the horizontal FIRs give the blurred
+//               moments, then the SSIM error, artifact and detail-loss maps
+//               and their sums and fourth-power sums, in f32 over the
+//               segment, then in f64 per thread.
+//
+// Modes (one per launch; the plan numbers each mode's tiles contiguously):
+//   TM_FULL    a pair scored from both images' XYB: rings A = (x', y') and
+//              B = (x'^2 + y'^2, x'y') -- SSIM needs sigma11 and sigma22
+//              only through their sum (its denominator is sigma11 - mu1^2 +
+//              sigma22 - mu2^2 + C2), so four planes are blurred, not five,
+//              and they pair up into two f32x2 FIRs.
+//   TM_REFMOM  a cached reference: blurs A = (x', x'^2) and stores the
+//              blurred mu1 and sigma11 to the pair's moment planes (mom[s]:
+//              mu1 of the three channels, then sigma11), no maps.
+//   TM_CAND    a candidate against a cached reference: blurs (y', x'y') in
+//              f32x2 and y'^2 alone (three planes), reads mu1 and sigma11
+//              from the moment planes, and forms (sigma11 + sigma22) / 2 as
+//              fma(0.5, sigma11, 0.5 sigma22).
+// The shared buffers are double buffered by step parity: step i's horizontal
+// phase reads buffer i % 2 while step i+1's vertical phase writes the other,
+// so one barrier per step orders them.
 //
 // EXPORT (error-map export, one scale of one pair): every pixel's SSIM error,
 // artifact and detail-loss values are also stored to `maps`, 9 planes
@@ -317,26 +370,381 @@ struct MapOut {
     long long mpitch, mplane;
 };
 
-template <typename ST, bool EXPORT = false>
-__global__ void __maxnreg__(96)
-    fused_kernel(const DevPair *__restrict__ pairs, const Seg *__restrict__ segs, int nseg,
-                 int first_item, int end_item, int *__restrict__ counter, double *__restrict__ partials,
-                 MapOut mo = MapOut{nullptr, 0, 0}) {
-    extern __shared__ float sm[];
-    float2 *s_vo2 = (float2 *)sm;                  // [pair][rb][col]
-    float2 *s_xo = (float2 *)(sm + kSmVo2);        // [rb][col]
-    float *s_vo1 = sm + kSmVo2 + kSmXo;            // [rb][col]
-    __shared__ int s_item;
-    __shared__ double s_red[kFusedThreads][6];
+// Scalar 9-tap FIR, the lane arithmetic of fir9p.
+__device__ __forceinline__ float fir9s(float a0, float a1, float a2, float a3, float a4, float a5, float a6,
+                                       float a7, float a8) {
+    float acc = S2_T4 * (a0 + a8);
+    acc = fmaf(S2_T3, a1 + a7, acc);
+    acc = fmaf(S2_T2, a2 + a6, acc);
+    acc = fmaf(S2_T1, a3 + a5, acc);
+    return fmaf(S2_T0, a4, acc);
+}
 
-    const int col = threadIdx.x;
-    const int tid = col;
-    // horizontal task of this thread: segment-major over the 9 block rows
-    const int t_r = tid % kRB, t_s = tid / kRB;
+// Register rings of one vertical column (which are used depends on the mode).
+struct Rings {
+    float2 a[16];  // FULL (x', y'); REFMOM (x', x'^2); CAND (y', x'y')
+    float2 b[16];  // FULL (x'^2 + y'^2, x'y')
+    float c[16];   // CAND y'^2
+    float x[16];   // CAND x'
+};
+
+// Shift one input row into ring slot `sl`.
+template <int MODE>
+__device__ __forceinline__ void ring_in(Rings &R, int sl, float vr, float vd, float2 ncg) {
+    if (MODE == TM_FULL) {
+        // both squares rounded before the sum: for x' = y' the first lane of B
+        // is exactly twice the second
+        const float2 a = s2_padd(make_float2(vr, vd), ncg);
+        const float2 q = s2_pmul(a, a);
+        R.a[sl] = a;
+        R.b[sl] = make_float2(q.x + q.y, a.x * a.y);
+    } else if (MODE == TM_REFMOM) {
+        const float xp = vr + ncg.x;
+        R.a[sl] = make_float2(xp, xp * xp);
+    } else {
+        const float2 a = s2_padd(make_float2(vr, vd), ncg);
+        R.a[sl] = make_float2(a.y, a.x * a.y);
+        R.c[sl] = a.y * a.y;
+        R.x[sl] = a.x;
+    }
+}
+
+// One vertical step: the new input rows ybase .. ybase + 7 (those below the
+// image, or beyond the tile's nr output rows, are not needed) enter ring
+// slots S0 + 8 .. S0 + 15 (mod 16); output row k reads slots S0 + k ..
+// S0 + k + 8 and is stored to row k of the buffer: plane 0 the FIR of ring
+// a, plane 1 that of ring b (FULL) or of ring c as floats (CAND), plane 2
+// the raw (x', y') of the output row (FULL, CAND).
+template <typename ST, int MODE, int S0>
+__device__ __forceinline__ void v_step(Rings &R, const ST *__restrict__ xr, const ST *__restrict__ xd, long long lp,
+                                       int x, bool colin, int ybase, int H, int nr, float cg, float2 ncg,
+                                       float2 *__restrict__ buf, int col) {
+    float lr[kStep], ld[kStep];
+#pragma unroll
+    for (int k = 0; k < kStep; k++) {
+        const int y = ybase + k;
+        const bool in = k < nr && colin && y < H;
+        lr[k] = in ? ld_store<ST>(xr + (long long)y * lp + x) : cg;
+        ld[k] = (MODE != TM_REFMOM && in) ? ld_store<ST>(xd + (long long)y * lp + x) : cg;
+    }
+#pragma unroll
+    for (int k = 0; k < kStep; k++) {
+        if (k < nr) {
+            ring_in<MODE>(R, (S0 + 8 + k) & 15, lr[k], ld[k], ncg);
+#define S2_R(a, j) a[(S0 + k + (j)) & 15]
+            buf[k * kRS + col] = fir9p(S2_R(R.a, 0), S2_R(R.a, 1), S2_R(R.a, 2), S2_R(R.a, 3), S2_R(R.a, 4),
+                                       S2_R(R.a, 5), S2_R(R.a, 6), S2_R(R.a, 7), S2_R(R.a, 8));
+            if (MODE == TM_FULL) {
+                buf[kPlaneF2 + k * kRS + col] = fir9p(S2_R(R.b, 0), S2_R(R.b, 1), S2_R(R.b, 2), S2_R(R.b, 3),
+                                                      S2_R(R.b, 4), S2_R(R.b, 5), S2_R(R.b, 6), S2_R(R.b, 7),
+                                                      S2_R(R.b, 8));
+                buf[2 * kPlaneF2 + k * kRS + col] = S2_R(R.a, 4);
+            } else if (MODE == TM_CAND) {
+                ((float *)(buf + kPlaneF2))[k * 2 * kRS + col] =
+                    fir9s(S2_R(R.c, 0), S2_R(R.c, 1), S2_R(R.c, 2), S2_R(R.c, 3), S2_R(R.c, 4), S2_R(R.c, 5),
+                          S2_R(R.c, 6), S2_R(R.c, 7), S2_R(R.c, 8));
+                buf[2 * kPlaneF2 + k * kRS + col] = make_float2(S2_R(R.x, 4), S2_R(R.a, 4).x);
+            }
+#undef S2_R
+        }
+    }
+}
+
+// Horizontal FIR of 4 outputs from 12 float2 of a buffer row (16-byte loads).
+template <bool HX>
+__device__ __forceinline__ void h_fir4(const float2 *__restrict__ p, float2 o[4]) {
+    float2 v[12];
+    const float4 *q = (const float4 *)p;
+#pragma unroll
+    for (int j = 0; j < 6; j++) {
+        const float4 t = q[j];
+        v[2 * j] = make_float2(t.x, t.y);
+        v[2 * j + 1] = make_float2(t.z, t.w);
+    }
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+        o[j] = fir9p<HX>(v[j], v[j + 1], v[j + 2], v[j + 3], v[j + 4], v[j + 5], v[j + 6], v[j + 7], v[j + 8]);
+}
+
+// The same on a float row (12 floats, three 16-byte loads).
+__device__ __forceinline__ void h_fir4s(const float *__restrict__ p, float o[4]) {
+    float v[12];
+    const float4 *q = (const float4 *)p;
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+        const float4 t = q[j];
+        v[4 * j] = t.x;
+        v[4 * j + 1] = t.y;
+        v[4 * j + 2] = t.z;
+        v[4 * j + 3] = t.w;
+    }
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+        o[j] = fir9s(v[j], v[j + 1], v[j + 2], v[j + 3], v[j + 4], v[j + 5], v[j + 6], v[j + 7], v[j + 8]);
+}
+
+// Sums of one task's maps: (d, art, det) and their 4th powers, f32.
+struct TaskSums {
+    float fs_d, f4_d;
+    float2 fs_ad, f4_ad;  // (artifact, detail loss)
+};
+
+__device__ __forceinline__ void add_maps(TaskSums &t, float d, float art, float det) {
+    t.fs_d += d;
+    const float q = d * d;
+    t.f4_d = fmaf(q, q, t.f4_d);
+    const float2 ad = make_float2(art, det);
+    t.fs_ad = s2_padd(t.fs_ad, ad);
+    const float2 q2 = s2_pmul(ad, ad);
+    t.f4_ad = s2_pfma(q2, q2, t.f4_ad);
+}
+
+// Error maps of one pixel.  m = (mu1, mu2) and s = ((sigma11 + sigma22) / 2,
+// sigma12) of the shifted values, r = (x', y').  kk = anchor * (1 - border
+// gain): the correction of the shifted moments at the image borders (0
+// inside).  With the anchor c and the gain g the true moments are
+// mu = m + c g and sigma = s + 2 c m + c^2 g, so
+//   sigma11 - mu1^2 + sigma22 - mu2^2 = 2 (w + kk h)   and
+//   sigma12 - mu1 mu2 = cov + kk h,
+// with w = s.x - mu1 mu2 - (mu1 - mu2)^2 / 2, cov = s.y - mu1 mu2,
+// e = c - kk = c g and h = (mu1 + mu2) + e.  For identical images
+// (x' = y') s.x equals s.y exactly, so w equals cov and the SSIM error is 0.
+template <bool BORDER>
+__device__ __forceinline__ void maps_px(float2 m, float2 s, float2 r, float kk, float e, float &d, float &art,
+                                        float &det) {
+    const float m1 = m.x, m2 = m.y;
+    const float md = m1 - m2;
+    float w = fmaf(-0.5f * md, md, fmaf(-m1, m2, s.x));
+    float cov = fmaf(-m1, m2, s.y);
+    if (BORDER) {
+        const float h = (m1 + m2) + e;
+        w = fmaf(kk, h, w);
+        cov = fmaf(kk, h, cov);
+    }
+    const float den = fmaf(2.0f, w, kC2);
+    const float num_m = fmaf(-md, md, 1.0f);
+    const float num_s = fmaf(2.0f, cov, kC2);
+    d = fmaxf(s2_div(fmaf(-num_m, num_s, den), den), 0.0f);
+    float2 t = s2_pfma(m, s2_f2(-1.0f), r);  // (x' - mu1, y' - mu2)
+    if (BORDER) t = make_float2(t.x + kk, t.y + kk);
+    const float aa = fabsf(t.x), bb = fabsf(t.y);
+    const float d1 = s2_div(bb - aa, 1.0f + aa);
+    art = fmaxf(d1, 0.0f);
+    det = fmaxf(-d1, 0.0f);
+}
+
+// Pooled sums of one work item, per thread (f64).
+struct Acc6 {
+    double v[6];
+};
+
+// What a horizontal task needs of its work item.
+struct ItemGeo {
+    int x0, y0, W, H, g;
+    float cg;
+    long long lp, plane;
+    float *mom;  // the moment planes of this scale (REFMOM, CAND)
+};
+
+// Horizontal phase of one step (output rows r0 .. r0 + nr - 1 of the tile):
+// this thread's task, row t_r, segment t_s.
+template <int MODE, bool EXPORT>
+__device__ __forceinline__ void h_step(const float2 *__restrict__ buf, int r0, int nr, int t_r, int t_s, bool t_on,
+                                       const ItemGeo &G, Acc6 &acc, const MapOut &mo) {
+    if (!t_on || t_r >= nr) return;
+    const int c0 = t_s * kSegW;  // first output column of the task (tile coordinates)
+    const int xc = G.x0 + c0;
+    if (xc >= G.W) return;
+    const int y = G.y0 + r0 + t_r;
+    if (MODE == TM_REFMOM) {
+        // blurred (mu1, sigma11) of 4 pixels at a time, 16-byte stores (a
+        // 4-pixel group starting inside the image stays inside the padded row)
+        float *mu = G.mom + G.g * G.plane + (long long)y * G.lp;
+        float *sg = G.mom + (3 + G.g) * G.plane + (long long)y * G.lp;
+#pragma unroll 1
+        for (int half = 0; half < kSegW / 4; half++) {
+            const int cc = c0 + 4 * half;
+            if (G.x0 + cc >= G.W) break;
+            float2 mA[4];
+            h_fir4<false>(buf + t_r * kRS + cc, mA);
+            *(float4 *)(mu + G.x0 + cc) = make_float4(mA[0].x, mA[1].x, mA[2].x, mA[3].x);
+            *(float4 *)(sg + G.x0 + cc) = make_float4(mA[0].y, mA[1].y, mA[2].y, mA[3].y);
+        }
+        return;
+    }
+    const float bv = border_gain(y, G.H);
+    const bool interior = bv == 1.0f && xc >= 4 && xc + kSegW + 4 <= G.W;
+    TaskSums ts{0.0f, 0.0f, make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f)};
+#pragma unroll 1
+    for (int half = 0; half < kSegW / 4; half++) {
+        const int cc = c0 + 4 * half;
+        const float2 *pa = buf + t_r * kRS + cc;
+        float2 mA[4], mB[4], rw[4];
+        if (MODE == TM_FULL) {
+            h_fir4<false>(pa, mA);
+            h_fir4<true>(pa + kPlaneF2, mB);  // (sigma11 + sigma22) / 2, sigma12
+        } else {
+            if (G.x0 + cc >= G.W) break;
+            float2 ma[4];
+            float s22[4];
+            h_fir4<false>(pa, ma);  // (mu2, sigma12)
+            h_fir4s((const float *)(buf + kPlaneF2) + t_r * 2 * kRS + cc, s22);
+            const long long o = (long long)y * G.lp + G.x0 + cc;
+            const float4 mu1 = *(const float4 *)(G.mom + G.g * G.plane + o);
+            const float4 s11 = *(const float4 *)(G.mom + (3 + G.g) * G.plane + o);
+            const float m1v[4] = {mu1.x, mu1.y, mu1.z, mu1.w}, s1v[4] = {s11.x, s11.y, s11.z, s11.w};
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                mA[j] = make_float2(m1v[j], ma[j].x);
+                mB[j] = make_float2(fmaf(0.5f, s1v[j], 0.5f * s22[j]), ma[j].y);
+            }
+        }
+        {
+            const float4 *q = (const float4 *)(pa + 2 * kPlaneF2 + 4);
+            const float4 t0 = q[0], t1 = q[1];
+            rw[0] = make_float2(t0.x, t0.y);
+            rw[1] = make_float2(t0.z, t0.w);
+            rw[2] = make_float2(t1.x, t1.y);
+            rw[3] = make_float2(t1.z, t1.w);
+        }
+        if (interior) {
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                float d, art, det;
+                maps_px<false>(mA[j], mB[j], rw[j], 0.0f, 0.0f, d, art, det);
+                if (EXPORT) {
+                    float *m = mo.maps + (long long)(3 * G.g) * mo.mplane + (long long)y * mo.mpitch + G.x0 + cc + j;
+                    m[0] = d;
+                    m[mo.mplane] = art;
+                    m[2 * mo.mplane] = det;
+                }
+                add_maps(ts, d, art, det);
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int xx = G.x0 + cc + j;
+                if (xx < G.W) {
+                    const float bh = border_gain(xx, G.W);
+                    const float corr = (bh == 1.0f && bv == 1.0f) ? 0.0f : (float)(1.0 - (double)bh * (double)bv);
+                    const float kk = G.cg * corr;
+                    float d, art, det;
+                    maps_px<true>(mA[j], mB[j], rw[j], kk, G.cg - kk, d, art, det);
+                    if (EXPORT) {
+                        float *m = mo.maps + (long long)(3 * G.g) * mo.mplane + (long long)y * mo.mpitch + xx;
+                        m[0] = d;
+                        m[mo.mplane] = art;
+                        m[2 * mo.mplane] = det;
+                    }
+                    add_maps(ts, d, art, det);
+                }
+            }
+        }
+    }
+    acc.v[0] += (double)ts.fs_d;
+    acc.v[1] += (double)ts.fs_ad.x;
+    acc.v[2] += (double)ts.fs_ad.y;
+    acc.v[3] += (double)ts.f4_d;
+    acc.v[4] += (double)ts.f4_ad.x;
+    acc.v[5] += (double)ts.f4_ad.y;
+}
+
+// One work item (one channel of one tile) in mode MODE.
+template <typename ST, int MODE, bool EXPORT>
+__device__ __forceinline__ void tile_item(const DevPair &P, const Seg &sg, int tile, int g, float2 *smb,
+                                          double (*s_warp)[6], double *__restrict__ partials, int item,
+                                          const MapOut &mo) {
+    const int tid = threadIdx.x;
+    const int t_r = tid % kStep, t_s = tid / kStep;
     const bool t_on = tid < kTasks;
+    const int s = sg.scale;
+    ItemGeo G;
+    G.W = P.w[s];
+    G.H = P.h[s];
+    G.g = g;
+    const int local = tile - sg.first_tile;
+    const int tx = local % sg.tiles_x, ty = local / sg.tiles_x;
+    G.x0 = tx * kTileW;
+    G.y0 = ty * sg.strip_rows;
+    const int rows_out = min(G.y0 + sg.strip_rows, G.H) - G.y0;
+    G.lp = P.lp[s];
+    G.plane = G.lp * G.H;
+    G.mom = P.mom[s];
+    const ST *xr = (const ST *)P.lvl[0][s] + g * G.plane;
+    const ST *xd = (const ST *)P.lvl[1][s] + g * G.plane;
+    // anchor: reference XYB of channel g at the tile's first column, band start
+    G.cg = ld_store<ST>(xr + (long long)((G.y0 / kBand) * kBand) * G.lp + G.x0);
+    const float cg = G.cg;
+    const float2 ncg = make_float2(-cg, -cg);
 
-    for (;;) {
+    const int x = G.x0 - 4 + tid;
+    const bool colin = x >= 0 && x < G.W;
+    Rings R;
+    // prime ring slots 0..7 with input rows y0 - 4 .. y0 + 3
+    {
+        float lr[8], ld[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            const int y = G.y0 - 4 + k;
+            const bool in = colin && y >= 0 && y < G.H;
+            lr[k] = in ? ld_store<ST>(xr + (long long)y * G.lp + x) : cg;
+            ld[k] = (MODE != TM_REFMOM && in) ? ld_store<ST>(xd + (long long)y * G.lp + x) : cg;
+        }
+#pragma unroll
+        for (int k = 0; k < 8; k++) ring_in<MODE>(R, k, lr[k], ld[k], ncg);
+    }
+
+    Acc6 acc{};
+    const int nsteps = (rows_out + kStep - 1) / kStep;
+    float2 *buf0 = smb, *buf1 = smb + kBufF2;
+    for (int st = 0; st < nsteps; st += 2) {
+        const int r0 = st * kStep;
+        const int nr0 = min(kStep, rows_out - r0);
+        v_step<ST, MODE, 0>(R, xr, xd, G.lp, x, colin, G.y0 + r0 + 4, G.H, nr0, cg, ncg, buf0, tid);
         __syncthreads();
+        h_step<MODE, EXPORT>(buf0, r0, nr0, t_r, t_s, t_on, G, acc, mo);
+        if (st + 1 < nsteps) {
+            const int r1 = r0 + kStep;
+            const int nr1 = min(kStep, rows_out - r1);
+            v_step<ST, MODE, 8>(R, xr, xd, G.lp, x, colin, G.y0 + r1 + 4, G.H, nr1, cg, ncg, buf1, tid);
+            __syncthreads();
+            h_step<MODE, EXPORT>(buf1, r1, nr1, t_r, t_s, t_on, G, acc, mo);
+        }
+    }
+
+    // channel reduction, fixed order: lanes by a shuffle tree, then warps in
+    // order (a moment build has no sums; the caller's barriers order the buffers)
+    if constexpr (MODE != TM_REFMOM) {
+#pragma unroll
+        for (int m = 0; m < 6; m++) {
+            double v = acc.v[m];
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+            if ((tid & 31) == 0) s_warp[tid >> 5][m] = v;
+        }
+        __syncthreads();
+        if (tid < 6) {
+            double v = 0.0;
+#pragma unroll
+            for (int w = 0; w < kFusedThreads / 32; w++) v += s_warp[w][tid];
+            partials[(long long)item * 6 + tid] = v;  // = tile * 18 + channel * 6 + m
+        }
+    }
+}
+
+// One launch runs the work items of one mode, so each instance gets the
+// registers of its own mode.
+template <typename ST, int MODE, bool EXPORT = false>
+__global__ void __launch_bounds__(kFusedThreads, 4)
+    fused_kernel(const DevPair *__restrict__ pairs, const Seg *__restrict__ segs, int nseg, int first_item,
+                 int end_item, int *__restrict__ counter, double *__restrict__ partials,
+                 MapOut mo = MapOut{nullptr, 0, 0}) {
+    extern __shared__ __align__(16) float2 smb[];  // [parity][3 planes][kStep][kRS]
+    __shared__ int s_item;
+    __shared__ double s_warp[kFusedThreads / 32][6];
+    const int tid = threadIdx.x;
+    for (;;) {
+        __syncthreads();  // the previous item's readers of s_item, s_warp and the buffers are done
         if (tid == 0) s_item = first_item + atomicAdd(counter, 1);
         __syncthreads();
         const int item = s_item;
@@ -344,257 +752,7 @@ __global__ void __maxnreg__(96)
         const int tile = item / 3, g = item - 3 * tile;
         const Seg sg = segs[find_seg(segs, nseg, tile)];
         const DevPair &P = pairs[sg.pair];
-        const int s = sg.scale;
-        const int W = P.w[s], H = P.h[s];
-        const int local = tile - sg.first_tile;
-        const int tx = local % sg.tiles_x, ty = local / sg.tiles_x;
-        const int x0 = tx * kTileW, y0 = ty * sg.strip_rows;
-        const int y1 = min(y0 + sg.strip_rows, H);
-        const long long plane = (long long)P.lp[s] * H;
-        const ST *xr = (const ST *)P.lvl[0][s] + g * plane;
-        const ST *xd = (const ST *)P.lvl[1][s] + g * plane;
-        const int lp = P.lp[s];
-        // shift: reference XYB of channel g at the tile's first column, band start
-        const float cg = ld_store<ST>(xr + (long long)((y0 / kBand) * kBand) * lp + x0);
-
-        const int x = x0 - 4 + col;
-        const bool colin = (x >= 0) && (x < W);
-        float2 w2a[9], w2b[9];  // windows of (x', y') and (x'^2, y'^2)
-        float w1[9];            // window of x' y'
-#pragma unroll
-        for (int m = 0; m < 6; m++) s_red[tid][m] = 0.0;
-
-        auto shifted = [&](float vr, float vd, bool in, float2 &a, float2 &b, float &c) {
-            if (in) {
-                const float px = vr - cg, py = vd - cg;
-                a = make_float2(px, py);
-                b = s2_mul2s(a, a);  // scalar squares: the FIR sums them
-                c = px * py;
-            } else {
-                a = make_float2(0.f, 0.f);
-                b = make_float2(0.f, 0.f);
-                c = 0.f;
-            }
-        };
-
-        // prime with input rows y0-4 .. y0+3 (window slots 0..7)
-        {
-            float lr[8], ld[8];
-#pragma unroll
-            for (int k = 0; k < 8; k++) {
-                const int y = y0 - 4 + k;
-                const bool in = colin && y >= 0 && y < H;
-                lr[k] = in ? ld_store<ST>(xr + (long long)y * lp + x) : 0.f;
-                ld[k] = in ? ld_store<ST>(xd + (long long)y * lp + x) : 0.f;
-            }
-#pragma unroll
-            for (int k = 0; k < 8; k++) {
-                const int y = y0 - 4 + k;
-                shifted(lr[k], ld[k], colin && y >= 0 && y < H, w2a[k], w2b[k], w1[k]);
-            }
-        }
-
-        const int rows_out = y1 - y0;
-        for (int r0 = 0; r0 < rows_out; r0 += kRowsPerBlk) {
-            const int nr = min(kRowsPerBlk, rows_out - r0);
-            float lr[kRowsPerBlk], ld[kRowsPerBlk];
-#pragma unroll
-            for (int k = 0; k < kRowsPerBlk; k++) {
-                const int y = y0 + r0 + k + 4;
-                const bool in = k < nr && colin && y < H;
-                lr[k] = in ? ld_store<ST>(xr + (long long)y * lp + x) : 0.f;
-                ld[k] = in ? ld_store<ST>(xd + (long long)y * lp + x) : 0.f;
-            }
-#pragma unroll
-            for (int k = 0; k < kRowsPerBlk; k++) {
-                if (k < nr) {
-                    const int sl = (8 + k) % 9;
-                    const int y = y0 + r0 + k + 4;
-                    shifted(lr[k], ld[k], colin && y < H, w2a[sl], w2b[sl], w1[sl]);
-#define S2_W(a, j) a[(sl + 1 + (j)) % 9]
-                    const float2 va = fir9x2(S2_W(w2a, 0), S2_W(w2a, 1), S2_W(w2a, 2), S2_W(w2a, 3), S2_W(w2a, 4),
-                                             S2_W(w2a, 5), S2_W(w2a, 6), S2_W(w2a, 7), S2_W(w2a, 8));
-                    const float2 vb = fir9x2(S2_W(w2b, 0), S2_W(w2b, 1), S2_W(w2b, 2), S2_W(w2b, 3), S2_W(w2b, 4),
-                                             S2_W(w2b, 5), S2_W(w2b, 6), S2_W(w2b, 7), S2_W(w2b, 8));
-                    const float vc = fir9(S2_W(w1, 0), S2_W(w1, 1), S2_W(w1, 2), S2_W(w1, 3), S2_W(w1, 4),
-                                          S2_W(w1, 5), S2_W(w1, 6), S2_W(w1, 7), S2_W(w1, 8));
-                    const int rb = k;
-                    s_vo2[rb * kRowStride2 + col] = va;
-                    s_vo2[(kRB + rb) * kRowStride2 + col] = vb;
-                    s_vo1[rb * kRowStride1 + col] = vc;
-                    s_xo[rb * kRowStride2 + col] = S2_W(w2a, 4);
-#undef S2_W
-                }
-            }
-            __syncthreads();
-            // horizontal FIR + error maps: task = (row, channel, 8-px segment)
-            if (t_on && t_r < nr) {
-                const int y = y0 + r0 + t_r;
-                const int xs = t_s * kSegW;
-                if (x0 + xs < W) {
-                    const int rb = t_r;
-                    const float2 *pa = s_vo2 + rb * kRowStride2;
-                    const float2 *pb = s_vo2 + (kRB + rb) * kRowStride2;
-                    const float *pc = s_vo1 + rb * kRowStride1;
-                    const float2 *px = s_xo + rb * kRowStride2;
-                    // shift of the task's channel (same anchor as the vertical pass)
-                    const float cv = ld_store<ST>((const ST *)P.lvl[0][s] + g * plane +
-                                                  (long long)((y0 / kBand) * kBand) * lp + x0);
-                    const float bv = border_gain(y, H);
-#pragma unroll 1
-                    for (int half = 0; half < kSegW / kChunk; half++) {
-                        const int c0 = xs + half * kChunk;  // first output (tile coords), a multiple of 4
-                        float2 ma[kChunk], mb[kChunk];
-                        float mc[kChunk];
-                        {
-                            float2 v[kChunk + 8];
-                            const float4 *q = (const float4 *)(pa + c0);
-#pragma unroll
-                            for (int j = 0; j < (kChunk + 8) / 2; j++) {
-                                const float4 t4 = q[j];
-                                v[2 * j] = make_float2(t4.x, t4.y);
-                                v[2 * j + 1] = make_float2(t4.z, t4.w);
-                            }
-#pragma unroll
-                            for (int j = 0; j < kChunk; j++)
-                                ma[j] = fir9x2(v[j], v[j + 1], v[j + 2], v[j + 3], v[j + 4], v[j + 5], v[j + 6], v[j + 7], v[j + 8]);
-                        }
-                        {
-                            float2 v[kChunk + 8];
-                            const float4 *q = (const float4 *)(pb + c0);
-#pragma unroll
-                            for (int j = 0; j < (kChunk + 8) / 2; j++) {
-                                const float4 t4 = q[j];
-                                v[2 * j] = make_float2(t4.x, t4.y);
-                                v[2 * j + 1] = make_float2(t4.z, t4.w);
-                            }
-#pragma unroll
-                            for (int j = 0; j < kChunk; j++)
-                                mb[j] = fir9x2(v[j], v[j + 1], v[j + 2], v[j + 3], v[j + 4], v[j + 5], v[j + 6], v[j + 7], v[j + 8]);
-                        }
-                        {
-                            float v[kChunk + 8];
-                            const float4 *q = (const float4 *)(pc + c0);
-#pragma unroll
-                            for (int j = 0; j < (kChunk + 8) / 4; j++) {
-                                const float4 t4 = q[j];
-                                v[4 * j] = t4.x;
-                                v[4 * j + 1] = t4.y;
-                                v[4 * j + 2] = t4.z;
-                                v[4 * j + 3] = t4.w;
-                            }
-#pragma unroll
-                            for (int j = 0; j < kChunk; j++)
-                                mc[j] = fir9(v[j], v[j + 1], v[j + 2], v[j + 3], v[j + 4], v[j + 5], v[j + 6], v[j + 7], v[j + 8]);
-                        }
-                        float2 xyv[kChunk];
-                        {
-                            const float4 *q = (const float4 *)(px + c0 + 4);
-#pragma unroll
-                            for (int j = 0; j < kChunk / 2; j++) {
-                                const float4 t4 = q[j];
-                                xyv[2 * j] = make_float2(t4.x, t4.y);
-                                xyv[2 * j + 1] = make_float2(t4.z, t4.w);
-                            }
-                        }
-                        float fs[3] = {0.f, 0.f, 0.f}, f4[3] = {0.f, 0.f, 0.f};
-                        const int xc = x0 + c0;
-                        if (bv == 1.0f && xc >= 4 && xc + kChunk + 4 <= W) {
-                            // every pixel of the chunk is interior: border gain
-                            // 1, so the correction term kk of the general form
-                            // below is zero and drops out; all pixels inside
-                            // the image.  The (mu1, mu2) and (art, det) pairs
-                            // go through f32x2 operations (each lane rounds as
-                            // the scalar operation).
-                            float2 fs12 = make_float2(0.f, 0.f), f412 = make_float2(0.f, 0.f);
-#pragma unroll
-                            for (int j = 0; j < kChunk; j++) {
-                                const float2 mu = ma[j];
-                                const float2 nmu = make_float2(-mu.x, -mu.y);
-                                const float2 var = __ffma2_rn(nmu, mu, mb[j]);  // (sigma11 - mu1^2, sigma22 - mu2^2)
-                                const float cov = fmaf(nmu.x, mu.y, mc[j]);
-                                const float md = mu.x - mu.y;
-                                const float num_m = fmaf(-md, md, 1.0f);
-                                const float num_s = fmaf(2.0f, cov, kC2);
-                                const float den = (var.x + var.y) + kC2;
-                                const float d = fmaxf(s2_div(fmaf(-num_m, num_s, den), den), 0.0f);
-                                const float2 t = s2_add2(xyv[j], nmu);
-                                const float aa = fabsf(t.x), bb = fabsf(t.y);
-                                const float d1 = s2_div(bb - aa, 1.0f + aa);
-                                const float2 ad = make_float2(fmaxf(d1, 0.0f), fmaxf(-d1, 0.0f));
-                                if (EXPORT) {
-                                    float *m = mo.maps + (long long)(3 * g) * mo.mplane + (long long)y * mo.mpitch + xc + j;
-                                    m[0] = d;
-                                    m[mo.mplane] = ad.x;
-                                    m[2 * mo.mplane] = ad.y;
-                                }
-                                const float q = d * d;
-                                fs[0] += d;
-                                f4[0] += q * q;
-                                const float2 q2 = s2_mul2(ad, ad);
-                                fs12 = s2_add2(fs12, ad);
-                                f412 = s2_add2(f412, s2_mul2s(q2, q2));  // scalar: summed
-                            }
-                            fs[1] = fs12.x;
-                            fs[2] = fs12.y;
-                            f4[1] = f412.x;
-                            f4[2] = f412.y;
-                        } else {
-#pragma unroll
-                        for (int j = 0; j < kChunk; j++) {
-                            const int xx = x0 + c0 + j;
-                            if (xx < W) {
-                                const float m1 = ma[j].x, m2 = ma[j].y, s11 = mb[j].x, s22 = mb[j].y, s12 = mc[j];
-                                const float2 xy = xyv[j];
-                                const float bh = border_gain(xx, W);
-                                const float corr =
-                                    (bh == 1.0f && bv == 1.0f) ? 0.0f : (float)(1.0 - (double)bh * (double)bv);
-                                const float kk = cv * corr;
-                                const float e = cv - kk;
-                                const float v1 = fmaf(kk, fmaf(2.0f, m1, e), fmaf(-m1, m1, s11));
-                                const float v2 = fmaf(kk, fmaf(2.0f, m2, e), fmaf(-m2, m2, s22));
-                                const float cov = fmaf(kk, (m1 + m2) + e, fmaf(-m1, m2, s12));
-                                const float md = m1 - m2;
-                                const float num_m = fmaf(-md, md, 1.0f);
-                                const float num_s = fmaf(2.0f, cov, kC2);
-                                const float den = (v1 + v2) + kC2;
-                                float d = s2_div(fmaf(-num_m, num_s, den), den);
-                                d = fmaxf(d, 0.0f);
-                                const float aa = fabsf((xy.x - m1) + kk);
-                                const float bb = fabsf((xy.y - m2) + kk);
-                                const float d1 = s2_div(bb - aa, 1.0f + aa);
-                                const float art = fmaxf(d1, 0.0f), det = fmaxf(-d1, 0.0f);
-                                if (EXPORT) {
-                                    float *m = mo.maps + (long long)(3 * g) * mo.mplane + (long long)y * mo.mpitch + xx;
-                                    m[0] = d;
-                                    m[mo.mplane] = art;
-                                    m[2 * mo.mplane] = det;
-                                }
-                                float q;
-                                fs[0] += d;   q = d * d;     f4[0] += q * q;
-                                fs[1] += art; q = art * art; f4[1] += q * q;
-                                fs[2] += det; q = det * det; f4[2] += q * q;
-                            }
-                        }
-                        }
-#pragma unroll
-                        for (int m = 0; m < 3; m++) {
-                            s_red[tid][m] += (double)fs[m];
-                            s_red[tid][3 + m] += (double)f4[m];
-                        }
-                    }
-                }
-            }
-            __syncthreads();
-        }
-
-        // channel reduction, fixed order: the tasks segment-major
-        __syncthreads();
-        if (tid < 6) {
-            double v = 0.0;
-            for (int t = 0; t < kTasks; t++) v += s_red[t][tid];
-            partials[(long long)item * 6 + tid] = v;  // = tile * 18 + channel * 6 + m
-        }
+        tile_item<ST, MODE, EXPORT && MODE != TM_REFMOM>(P, sg, tile, g, smb, s_warp, partials, item, mo);
     }
 }
 
@@ -690,33 +848,42 @@ const double *host_weights() { return kWeights; }
 
 cudaError_t upload_weights() { return cudaMemcpyToSymbol(c_weight, kWeights, sizeof kWeights); }
 
-size_t fused_smem_bytes() { return (size_t)kFusedSmemFloats * sizeof(float); }
+size_t fused_smem_bytes() { return (size_t)2 * kBufF2 * sizeof(float2); }
 int fused_threads() { return kFusedThreads; }
 
-template <typename ST> static const void *fused_fn() { return (const void *)fused_kernel<ST>; }
+template <typename ST, int MODE, bool EXPORT>
+static cudaError_t fused_attrs() {
+    const void *f = (const void *)fused_kernel<ST, MODE, EXPORT>;
+    // the tile pass is limited by registers and shared memory together: ask
+    // for the largest shared-memory carveout so that 4 blocks fit per SM
+    cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fused_smem_bytes());
+}
+
+template <typename ST>
+static cudaError_t fused_attrs_all() {
+    cudaError_t e;
+    if ((e = fused_attrs<ST, TM_FULL, false>()) != cudaSuccess) return e;
+    if ((e = fused_attrs<ST, TM_FULL, true>()) != cudaSuccess) return e;
+    if ((e = fused_attrs<ST, TM_CAND, false>()) != cudaSuccess) return e;
+    if ((e = fused_attrs<ST, TM_CAND, true>()) != cudaSuccess) return e;
+    return fused_attrs<ST, TM_REFMOM, false>();
+}
 
 cudaError_t configure_kernels() {
     cudaError_t e;
-    // the fused pass is limited by registers and shared memory together: ask
-    // for the largest shared-memory carveout so that 3 blocks fit per SM
-    e = cudaFuncSetAttribute(fused_kernel<float>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-    if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(fused_kernel<__half>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-    if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(fused_kernel<__nv_bfloat16>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-    if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(fused_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fused_smem_bytes());
-    if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(fused_kernel<__half>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fused_smem_bytes());
-    if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(fused_kernel<__nv_bfloat16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fused_smem_bytes());
-    if (e != cudaSuccess) return e;
+    if ((e = fused_attrs_all<float>()) != cudaSuccess) return e;
+    if ((e = fused_attrs_all<__half>()) != cudaSuccess) return e;
+    if ((e = fused_attrs_all<__nv_bfloat16>()) != cudaSuccess) return e;
     return configure_dssim_kernels();
 }
 
 int fused_blocks_per_sm(int storage) {
     int n = 0;
-    const void *f = storage == ST_F16 ? fused_fn<__half>() : storage == ST_BF16 ? fused_fn<__nv_bfloat16>() : fused_fn<float>();
+    const void *f = storage == ST_F16    ? (const void *)fused_kernel<__half, TM_FULL, false>
+                    : storage == ST_BF16 ? (const void *)fused_kernel<__nv_bfloat16, TM_FULL, false>
+                                         : (const void *)fused_kernel<float, TM_FULL, false>;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f, kFusedThreads, fused_smem_bytes()) != cudaSuccess) return 1;
     return n > 0 ? n : 1;
 }
@@ -751,48 +918,48 @@ cudaError_t launch_pyramid(int storage, const DevPair *pairs, int npairs, const 
     return cudaGetLastError();
 }
 
-cudaError_t launch_fused(int storage, const DevPair *pairs, const Seg *segs, int nseg, int first_tile, int end_tile,
-                         int *counter, double *partials, int grid, cudaStream_t st) {
+template <typename ST, int MODE, bool EXPORT>
+static void fused_go(int grid, size_t sm, cudaStream_t st, const DevPair *pairs, const Seg *segs, int nseg, int fi,
+                     int ei, int *counter, double *partials, const MapOut &mo) {
+    fused_kernel<ST, MODE, EXPORT><<<grid, kFusedThreads, sm, st>>>(pairs, segs, nseg, fi, ei, counter, partials, mo);
+}
+
+template <typename ST, bool EXPORT>
+static void fused_mode(int mode, int grid, size_t sm, cudaStream_t st, const DevPair *pairs, const Seg *segs,
+                       int nseg, int fi, int ei, int *counter, double *partials, const MapOut &mo) {
+    if (mode == TM_REFMOM) fused_go<ST, TM_REFMOM, false>(grid, sm, st, pairs, segs, nseg, fi, ei, counter, partials, mo);
+    else if (mode == TM_CAND) fused_go<ST, TM_CAND, EXPORT>(grid, sm, st, pairs, segs, nseg, fi, ei, counter, partials, mo);
+    else fused_go<ST, TM_FULL, EXPORT>(grid, sm, st, pairs, segs, nseg, fi, ei, counter, partials, mo);
+}
+
+cudaError_t launch_fused(int storage, int mode, const DevPair *pairs, const Seg *segs, int nseg, int first_tile,
+                         int end_tile, int *counter, double *partials, int grid, cudaStream_t st) {
     const int fi = 3 * first_tile, ei = 3 * end_tile;  // work items: (tile, channel)
     const int nt = ei - fi;
     if (nt <= 0) return cudaSuccess;
     grid = grid > nt ? nt : grid;
-    dim3 block(kFusedThreads);
-    size_t sm = fused_smem_bytes();
-    if (storage == ST_F16)
-        fused_kernel<__half><<<grid, block, sm, st>>>(pairs, segs, nseg, fi, ei, counter, partials);
+    const size_t sm = fused_smem_bytes();
+    const MapOut mo{nullptr, 0, 0};
+    if (storage == ST_F16) fused_mode<__half, false>(mode, grid, sm, st, pairs, segs, nseg, fi, ei, counter, partials, mo);
     else if (storage == ST_BF16)
-        fused_kernel<__nv_bfloat16><<<grid, block, sm, st>>>(pairs, segs, nseg, fi, ei, counter, partials);
-    else
-        fused_kernel<float><<<grid, block, sm, st>>>(pairs, segs, nseg, fi, ei, counter, partials);
+        fused_mode<__nv_bfloat16, false>(mode, grid, sm, st, pairs, segs, nseg, fi, ei, counter, partials, mo);
+    else fused_mode<float, false>(mode, grid, sm, st, pairs, segs, nseg, fi, ei, counter, partials, mo);
     return cudaGetLastError();
 }
 
-cudaError_t launch_fused_export(int storage, const DevPair *pairs, const Seg *segs, int nseg, int first_tile,
-                                int end_tile, int *counter, double *partials, float *maps, long long mpitch,
-                                long long mplane, int grid, cudaStream_t st) {
+cudaError_t launch_fused_export(int storage, int mode, const DevPair *pairs, const Seg *segs, int nseg,
+                                int first_tile, int end_tile, int *counter, double *partials, float *maps,
+                                long long mpitch, long long mplane, int grid, cudaStream_t st) {
     const int fi = 3 * first_tile, ei = 3 * end_tile;
     const int nt = ei - fi;
     if (nt <= 0) return cudaSuccess;
     grid = grid > nt ? nt : grid;
-    dim3 block(kFusedThreads);
-    size_t sm = fused_smem_bytes();
+    const size_t sm = fused_smem_bytes();
     const MapOut mo{maps, mpitch, mplane};
-    cudaError_t e;
-    if (storage == ST_F16) {
-        e = cudaFuncSetAttribute(fused_kernel<__half, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        if (e != cudaSuccess) return e;
-        fused_kernel<__half, true><<<grid, block, sm, st>>>(pairs, segs, nseg, fi, ei, counter, partials, mo);
-    } else if (storage == ST_BF16) {
-        e = cudaFuncSetAttribute(fused_kernel<__nv_bfloat16, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)sm);
-        if (e != cudaSuccess) return e;
-        fused_kernel<__nv_bfloat16, true><<<grid, block, sm, st>>>(pairs, segs, nseg, fi, ei, counter, partials, mo);
-    } else {
-        e = cudaFuncSetAttribute(fused_kernel<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        if (e != cudaSuccess) return e;
-        fused_kernel<float, true><<<grid, block, sm, st>>>(pairs, segs, nseg, fi, ei, counter, partials, mo);
-    }
+    if (storage == ST_F16) fused_mode<__half, true>(mode, grid, sm, st, pairs, segs, nseg, fi, ei, counter, partials, mo);
+    else if (storage == ST_BF16)
+        fused_mode<__nv_bfloat16, true>(mode, grid, sm, st, pairs, segs, nseg, fi, ei, counter, partials, mo);
+    else fused_mode<float, true>(mode, grid, sm, st, pairs, segs, nseg, fi, ei, counter, partials, mo);
     return cudaGetLastError();
 }
 

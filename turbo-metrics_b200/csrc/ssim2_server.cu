@@ -365,7 +365,7 @@ void s2_server_config_default(s2_server_config *c) {
     c->max_batch_pairs = 256;
     c->max_batch_pixels = 32ull << 20;
     c->hbm_budget = 40ull << 30;
-    c->max_queued_jobs = 1u << 20;
+    c->max_queued_jobs = 128;  // bounds the latency of an overloaded server
 }
 
 s2_status s2_server_create(const s2_server_config *cfg_in, s2_server **out) {
@@ -382,7 +382,7 @@ s2_status s2_server_create(const s2_server_config *cfg_in, s2_server **out) {
     s2_config ec;
     s2_config_default(&ec);
     ec.device = cfg.device;
-    ec.strip_rows = 21;  // fixed tile geometry: a job scores the same alone and mixed
+    ec.strip_rows = kStripMid;  // fixed tile geometry: a job scores the same alone and mixed
     s2_status st = S2_OK;
     for (int k = 0; k < 2 && st == S2_OK; k++) st = sv->eng[k].init(&ec);
     for (int k = 0; k < 2 && st == S2_OK; k++) st = sv->eng[k].set_profiling(true);

@@ -16,23 +16,43 @@ from .capi import lib, check
 
 class Ssim2Server:
     def __init__(self, device=0, max_batch_pairs=256, max_batch_pixels=32 << 20, hbm_budget=40 << 30,
-                 max_queued_jobs=1 << 20):
+                 max_queued_jobs=None):
+        """max_queued_jobs: unfinished jobs beyond which submit raises Busy
+        (None: the library default, 128)."""
         cfg = capi.ServerConfig()
         lib.s2_server_config_default(ctypes.byref(cfg))
         cfg.device, cfg.max_batch_pairs, cfg.max_batch_pixels = device, max_batch_pairs, max_batch_pixels
-        cfg.hbm_budget, cfg.max_queued_jobs = hbm_budget, max_queued_jobs
+        cfg.hbm_budget = hbm_budget
+        if max_queued_jobs is not None:
+            cfg.max_queued_jobs = max_queued_jobs
         h = ctypes.c_void_p()
         check(lib.s2_server_create(ctypes.byref(cfg), ctypes.byref(h)), "Ssim2Server")
         self._h = h
         self._keep = {}
 
+    @staticmethod
+    def _rows(a):
+        """An (H, W, 3) uint8 image whose rows are packed pixels, as is (a crop
+        of a larger image keeps its row pitch), else a packed copy."""
+        if a.dtype == np.uint8 and a.ndim == 3 and a.shape[2] == 3 and a.strides[2] == 1 and a.strides[1] == 3 \
+                and a.strides[0] >= 3 * a.shape[1]:
+            return a
+        return np.ascontiguousarray(a, np.uint8)
+
     def submit(self, ref, candidates):
-        """ref, candidates: (H, W, 3) uint8 host arrays.  Returns a job id."""
-        ref = np.ascontiguousarray(ref, np.uint8)
-        cands = [np.ascontiguousarray(c, np.uint8) for c in candidates]
+        """ref, candidates: (H, W, 3) uint8 host arrays (crops of larger
+        images are passed with their row pitch, not copied).  Returns a job
+        id; raises Busy when the server holds max_queued_jobs unfinished
+        jobs."""
+        ref = self._rows(ref)
+        cands = [self._rows(c) for c in candidates]
         for c in cands:
             if c.shape != ref.shape:
                 raise capi.DimensionMismatch(capi.S2_ERR_DIM_MISMATCH, "submit")
+        pitch = cands[0].strides[0] if cands else ref.strides[0]
+        if any(c.strides[0] != pitch for c in cands):
+            cands = [np.ascontiguousarray(c) for c in cands]
+            pitch = cands[0].strides[0]
         arr = (ctypes.c_void_p * max(len(cands), 1))(*[c.ctypes.data for c in cands])
         jd = capi.JobDesc()
         jd.height, jd.width = ref.shape[0], ref.shape[1]
@@ -40,7 +60,7 @@ class Ssim2Server:
         jd.ref, jd.ref_pitch = ref.ctypes.data, ref.strides[0]
         jd.n_candidates = len(cands)
         jd.candidates = ctypes.cast(arr, ctypes.POINTER(ctypes.c_void_p))
-        jd.cand_pitch = ref.strides[0]
+        jd.cand_pitch = pitch
         jid = ctypes.c_uint64()
         check(lib.s2_server_submit(self._h, ctypes.byref(jd), ctypes.byref(jid)), "submit")
         self._keep[jid.value] = (ref, cands, arr)  # host images must outlive the job

@@ -250,6 +250,42 @@ def c4_jobs(n_jobs: int, rate: float, seed_index: int = 0):
     return jobs
 
 
+C4_POOL_W, C4_POOL_H, C4_POOL_CANDS = 3840, 2160, 16
+
+
+def c4_pool_reference():
+    """The serving pool's reference: a 3840x2160 sRGB8 image with C0 content
+    (gratings + noise).  Jobs crop their reference from it."""
+    st = Stream(pair_seed(4, 500))
+    return gratings(st, C4_POOL_W, C4_POOL_H, 128.0, 12.0, 16.0, 255.0).astype(np.uint8)
+
+
+def c4_pool_step(i):
+    """DCT step of pool candidate i: the midpoints of 16 equal bins of [2, 48]."""
+    return 2.0 + 46.0 * (i + 0.5) / C4_POOL_CANDS
+
+
+def c4_pool_candidate(ref, i):
+    """Pool candidate i: the reference plus Gaussian noise (sigma 4), 8x8 DCT
+    quantisation at step c4_pool_step(i), rounded to uint8."""
+    st = Stream(pair_seed(4, 600 + i))
+    h, w, _ = ref.shape
+    d = np.clip(ref.astype(np.float64) + 4.0 * st.normal(h * w * 3).reshape(h, w, 3), 0, 255)
+    for c in range(3):
+        d[:, :, c] = dct_quantize(d[:, :, c], c4_pool_step(i), 128.0, 0.0, 255.0)
+    return d.astype(np.uint8)
+
+
+def c4_job_crop(job):
+    """Crop offset (x, y) of a job inside the pool images and the pool
+    candidate of each of its DCT steps (the bin that holds the step)."""
+    st = Stream(job["seed"])
+    ox = min(int(st.scalar() * (C4_POOL_W - job["w"] + 1)), C4_POOL_W - job["w"])
+    oy = min(int(st.scalar() * (C4_POOL_H - job["h"] + 1)), C4_POOL_H - job["h"])
+    idx = [min(C4_POOL_CANDS - 1, int((s - 2.0) / 46.0 * C4_POOL_CANDS)) for s in job["steps"]]
+    return ox, oy, idx
+
+
 def serving_job_images(job):
     """Reference + candidates (uint8 HxWx3) for a serving job."""
     st = Stream(job["seed"])
