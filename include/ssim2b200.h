@@ -193,7 +193,10 @@ s2_status s2_compute_sync_linear_f32(s2_ctx *ctx, const float *ref, size_t ref_p
 
 /* ---- cached reference -------------------------------------------------- */
 /* Replaces set_reference_linear (lib.rs:440-546): keeps the reference's
- * pyramid, XYB and blurred moments resident on the device. */
+ * pyramid, XYB and (FIR blur) blurred moments mu1 and sigma11 resident on the
+ * device.  compute_with_reference then blurs three planes per channel instead
+ * of four; its scores are within 1e-5 of the direct path's (sigma11 and
+ * sigma22 are blurred separately instead of as one sum). */
 s2_status s2_set_reference_linear_f32(s2_ctx *ctx, const float *ref, size_t pitch, void *stream);
 s2_status s2_set_reference_srgb8(s2_ctx *ctx, const uint8_t *ref, size_t pitch,
                                  int32_t on_host, void *stream);
@@ -270,6 +273,22 @@ s2_status s2_batch_submit_host(s2_batch *b, const s2_pair_desc *pairs, uint32_t 
  * before submission k's results are read (its uploads and preps overlap k's
  * tile pass).  With both slots pending, a new host submission drops the
  * older one's results. */
+/* Replaces Ssim2Batch::set_reference (ssim2-gpu/src/pipeline_batch.rs:206-208):
+ * converts `ref` (its ref / ref_uv planes, on the device; any format) and keeps
+ * its XYB pyramid and blurred moments in the batch.  Returns after the device
+ * work is done.  S2_ERR_INVALID_SIZE below 8x8 or above max_pixels. */
+s2_status s2_batch_set_reference(s2_batch *b, const s2_pair_desc *ref, void *stream);
+/* Replaces Ssim2Batch::compute_batch (pipeline_batch.rs:247-330): enqueue n
+ * distorted images (the dis / dis_uv planes of each descriptor, on the
+ * device, any format) against the cached reference, as one submission; read
+ * the results with s2_batch_results.  S2_ERR_NO_REFERENCE without
+ * s2_batch_set_reference, S2_ERR_DIM_MISMATCH for a size other than the
+ * reference's, S2_ERR_INVALID_ARG beyond max_pairs / max_pixels (the
+ * reference's InvalidBatchSize).  SSIMULACRA2 only. */
+s2_status s2_batch_submit_with_reference(s2_batch *b, const s2_pair_desc *dis, uint32_t n, void *stream);
+/* Replaces clear_reference / has_cached_reference (pipeline_batch.rs:210-216). */
+s2_status s2_batch_clear_reference(s2_batch *b);
+int32_t s2_batch_has_reference(const s2_batch *b);
 s2_status s2_batch_results(s2_batch *b, s2_result *out, uint32_t n);
 s2_status s2_batch_mem_usage(const s2_batch *b, size_t *bytes);
 /* CUDA graphs (1 = on, the default): the operations of a device-input
@@ -331,7 +350,8 @@ s2_status s2_dssim_mem_usage(const s2_dssim *d, size_t *bytes);
  * at any time; they are admitted in arrival order while their device bytes
  * fit the HBM budget, their images are uploaded on a copy stream, and every
  * round scores the pending work of all admitted jobs in one submission.  A
- * job's reference pyramid is built once and shared by its candidates.  A job
+ * job's reference pyramid and blurred moments are built once and shared by its
+ * candidates (scored as s2_compute_with_reference_* scores them).  A job
  * scores bit-identically alone and mixed with others.  Host images must stay
  * valid until s2_server_wait returns for the job. */
 typedef struct {

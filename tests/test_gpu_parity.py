@@ -175,7 +175,12 @@ def test_error_paths(tmb, cuda):
         odd.compute_nv12(y, y[:32], y, y[:32])
 
 
-def test_cached_reference_equals_direct(tmb, cuda):
+def test_cached_reference_equals_direct(tmb, oracle, cuda):
+    """The cached path reads the reference's blurred mu1 and sigma11 and blurs
+    sigma22 on its own: every statistic against the oracle's restatement of
+    that arithmetic (fir32c), and the score within 1e-5 of the direct path
+    (the reference's own bar for cached == direct is 1e-4,
+    ssim2-gpu/tests/parity_lock.rs:160-277)."""
     ref, _ = synth.srgb_pair(200, 150, 31)
     s = tmb.Ssimulacra2(200, 150)
     assert not s.has_reference()
@@ -184,8 +189,15 @@ def test_cached_reference_equals_direct(tmb, cuda):
     for q in (4, 16, 40):
         _, dis = synth.srgb_pair(200, 150, 31, q)
         direct = s.compute_from_cpu_srgb_sync(ref, dis)
-        cached = s.compute_with_reference_srgb(dis, on_host=True)
-        assert abs(direct - cached) < 1e-12
+        s.compute_with_reference_srgb(dis, on_host=True)
+        cached, stats, _ = s.get_result()
+        assert abs(direct - cached) < 1e-5
+        mirror = oracle.ssim2_srgb8(ref, dis, "fir32c")
+        assert_stats_close(stats, mirror.stats, what="cached q%d" % q)
+        assert abs(cached - mirror.score) < SCORE_TOL
+    # the reference compared with itself through the cache scores exactly 100
+    s.compute_with_reference_srgb(ref, on_host=True)
+    assert s.get_score() == 100.0
     s.clear_reference()
     assert not s.has_reference()
     with pytest.raises(tmb.NoCachedReference):

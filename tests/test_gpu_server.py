@@ -22,9 +22,13 @@ def test_server_matches_single_context(tmb, cuda):
     jid = sv.submit(ref, cands)
     scores, st, lat = sv.wait(jid)
     assert list(st) == [0] * 4 and lat > 0
+    # a job's candidates are scored against its cached reference: the same
+    # arithmetic as a context's compute_with_reference, within 1e-5 of direct
     ctx = tmb.Ssimulacra2(300, 200)
+    ctx.set_reference_srgb(ref, on_host=True)
     for c, s in zip(cands, scores):
-        assert abs(ctx.compute_from_cpu_srgb_sync(ref, c) - s) < 1e-12
+        assert abs(ctx.compute_with_reference_srgb(c, on_host=True) - s) < 1e-12
+        assert abs(ctx.compute_from_cpu_srgb_sync(ref, c) - s) < 1e-5
     sv.close()
 
 

@@ -297,6 +297,11 @@ struct s2_batch {
     s2_config cfg;
     uint32_t max_pairs = 0;
     uint64_t max_pixels = 0;
+    // cached reference (s2_batch_set_reference): XYB pyramid + blurred moments
+    DevBuf ref_buf;
+    bool has_ref = false;
+    uint32_t ref_w = 0, ref_h = 0;
+    PairExtra ref_extra;  // what each candidate of submit_with_reference gets
 
     s2_status open_slot(int k) {
         if (ready[k]) return S2_OK;
@@ -602,16 +607,22 @@ s2_status s2_compute_sync_linear_f32(s2_ctx *ctx, const float *ref, size_t ref_p
 }
 
 // ---- cached reference ----------------------------------------------------
-// set_reference converts the reference once and keeps its XYB planes of every
-// scale on the device (set_reference_linear, ssimulacra2-cuda/src/lib.rs:440-546,
-// caches the same ref-side state); compute_with_reference converts only the
-// distorted image and reads the cached planes.  Scores equal the direct path's
-// (same XYB values, same tiles).  Like the reference, set_reference returns
-// after the device work is done.
+// set_reference converts the reference once and keeps on the device, for
+// every scale, its XYB planes and -- with the FIR blur -- its blurred moments
+// mu1 and sigma11 per channel (set_reference_linear, ssimulacra2-cuda/src/
+// lib.rs:440-546, caches the reference's XYB, mu1_t and sigma11_t the same
+// way).  compute_with_reference converts only the distorted image and blurs
+// three planes (y', y'^2, x'y') instead of four, reading mu1 and sigma11 from
+// the cache; its sum sigma11 + sigma22 is of separately blurred planes, so
+// scores are within 1e-5 of the direct path's (the oracle's fir32c mode
+// restates this arithmetic).  Like the reference, set_reference returns after
+// the device work is done.
 static s2_status set_ref(s2_ctx *ctx, const s2_pair_desc &d, void *stream) {
-    size_t off[kScales];
+    size_t off[kScales], moff[kScales];
     const int ns = s2_num_scales_rule(ctx->w, ctx->h, ctx->eng.scale_rule);
-    const size_t bytes = s2_image_levels_layout(ctx->w, ctx->h, ns, ctx->eng.esize(), off);
+    const bool mom = ctx->eng.blur == S2_BLUR_FIR;
+    const size_t lv = s2_align_up(s2_image_levels_layout(ctx->w, ctx->h, ns, ctx->eng.esize(), off), 256);
+    const size_t bytes = lv + (mom ? s2_moment_layout(ctx->w, ctx->h, ns, moff) : 0);
     if (ctx->ref_levels.n < bytes) {
         if (ctx->ref_levels.p) {
             S2_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
@@ -630,8 +641,11 @@ static s2_status set_ref(s2_ctx *ctx, const s2_pair_desc &d, void *stream) {
     build.prep_mask = 1;
     build.score = false;
     build.dssim = false;
-    for (int s = 0; s < kScales; s++)
+    for (int s = 0; s < kScales; s++) {
         build.ref_levels[s] = s < ns ? (char *)ctx->ref_levels.p + off[s] : nullptr;
+        build.ref_mom[s] = mom && s < ns ? (char *)ctx->ref_levels.p + lv + moff[s] : nullptr;
+    }
+    build.build_mom = mom;
     ctx->has_ref = false;
     s2_status st = ctx_run(ctx, d, stream, &build);
     if (st != S2_OK) return st;
@@ -640,6 +654,7 @@ static s2_status set_ref(s2_ctx *ctx, const s2_pair_desc &d, void *stream) {
     ctx->ref_extra = build;
     ctx->ref_extra.prep_mask = 2;
     ctx->ref_extra.score = true;
+    ctx->ref_extra.build_mom = false;
     ctx->has_ref = true;
     return S2_OK;
 }
@@ -748,6 +763,7 @@ void s2_batch_destroy(s2_batch *b) {
     if (!b) return;
     for (int k = 0; k < 2; k++)
         if (b->ready[k]) b->eng[k].release();
+    if (b->ref_buf.p) cudaFree(b->ref_buf.p);
     delete b;
 }
 
@@ -786,6 +802,98 @@ s2_status s2_batch_submit_host(s2_batch *b, const s2_pair_desc *pairs, uint32_t 
     return S2_OK;
 }
 
+// Cached reference of a batch: ssim2-gpu's Ssim2Batch::set_reference /
+// compute_batch (crates/ssim2-gpu/src/pipeline_batch.rs:206-330), where every
+// candidate of a submission is scored against one resident reference.  The
+// reference's XYB pyramid and (FIR blur) blurred moments are built once, on
+// slot 0's engine, and kept in a buffer of the batch.
+s2_status s2_batch_set_reference(s2_batch *b, const s2_pair_desc *ref, void *stream) {
+    if (!b || !ref || !ref->ref) return S2_ERR_INVALID_ARG;
+    if (!(b->metrics & S2_METRIC_SSIMULACRA2)) return S2_ERR_INVALID_ARG;
+    Engine &e = b->eng[0];
+    const uint32_t w = ref->width, h = ref->height;
+    const int ns = s2_num_scales_rule(w, h, e.scale_rule);
+    if (ns == 0 || w > (1u << 16) || h > (1u << 16)) return S2_ERR_INVALID_SIZE;
+    if ((uint64_t)w * h > b->max_pixels) return S2_ERR_INVALID_SIZE;
+    size_t off[kScales], moff[kScales];
+    const bool mom = e.blur == S2_BLUR_FIR;
+    const size_t lv = s2_align_up(s2_image_levels_layout(w, h, ns, e.esize(), off), 256);
+    const size_t bytes = lv + (mom ? s2_moment_layout(w, h, ns, moff) : 0);
+    b->has_ref = false;
+    if (b->ref_buf.n < bytes) {
+        S2_CUDA(cudaDeviceSynchronize());  // earlier submissions may still read the old cache
+        if (b->ref_buf.p) cudaFree(b->ref_buf.p);
+        b->ref_buf.p = nullptr;
+        b->ref_buf.n = 0;
+        if (e.budget && e.allocated + b->eng[1].allocated + bytes > e.budget) {
+            g_last_error = "reference cache over the HBM budget";
+            return S2_ERR_OOM;
+        }
+        S2_CUDA(cudaMalloc(&b->ref_buf.p, bytes));
+        b->ref_buf.n = bytes;
+    }
+    PairExtra build;
+    build.prep_mask = 1;
+    build.score = false;
+    build.dssim = false;
+    build.build_mom = mom;
+    for (int s = 0; s < kScales; s++) {
+        build.ref_levels[s] = s < ns ? (char *)b->ref_buf.p + off[s] : nullptr;
+        build.ref_mom[s] = mom && s < ns ? (char *)b->ref_buf.p + lv + moff[s] : nullptr;
+    }
+    s2_pair_desc d = *ref;
+    d.dis = nullptr;
+    d.dis_uv = nullptr;
+    const int k = b->take_slot(false);
+    s2_status st = e.plan(&d, 1, b->plan[k], &build);
+    if (st == S2_OK && b->plan[k].pairs[0].status != S2_OK) st = (s2_status)b->plan[k].pairs[0].status;
+    if (st == S2_OK) st = e.enqueue(b->plan[k], (cudaStream_t)stream);
+    if (st == S2_OK) st = e.wait();
+    if (st != S2_OK) return st;
+    b->ref_extra = build;
+    b->ref_extra.prep_mask = 2;
+    b->ref_extra.score = true;
+    b->ref_extra.build_mom = false;
+    b->ref_w = w;
+    b->ref_h = h;
+    b->has_ref = true;
+    return S2_OK;
+}
+
+s2_status s2_batch_submit_with_reference(s2_batch *b, const s2_pair_desc *dis, uint32_t n, void *stream) {
+    if (!b || (!dis && n)) return S2_ERR_INVALID_ARG;
+    if (!b->has_ref) return S2_ERR_NO_REFERENCE;
+    if (n > b->max_pairs || (uint64_t)n * b->ref_w * b->ref_h > b->max_pixels) return S2_ERR_INVALID_ARG;
+    std::vector<s2_pair_desc> d(dis, dis + n);
+    for (uint32_t i = 0; i < n; i++) {
+        if (d[i].width != b->ref_w || d[i].height != b->ref_h) return S2_ERR_DIM_MISMATCH;
+        if (!d[i].dis) return S2_ERR_INVALID_ARG;
+        d[i].ref = nullptr;
+        d[i].ref_uv = nullptr;
+    }
+    std::vector<PairExtra> ex(n, b->ref_extra);
+    const int k = b->take_slot(false);
+    Engine &e = b->eng[k];
+    const int m = e.metrics;
+    e.metrics = S2_METRIC_SSIMULACRA2;  // the cached reference keeps SSIMULACRA2's planes only
+    s2_status st = e.plan(d.data(), (int)n, b->plan[k], ex.data());
+    if (st == S2_OK) st = e.tune(d.data(), (int)n, b->plan[k], ex.data(), (cudaStream_t)stream);
+    if (st == S2_OK) st = e.enqueue(b->plan[k], (cudaStream_t)stream);
+    e.metrics = m;
+    if (st != S2_OK) return st;
+    b->unread.push_back(k);
+    b->last_slot = k;
+    return S2_OK;
+}
+
+s2_status s2_batch_clear_reference(s2_batch *b) {
+    if (!b) return S2_ERR_INVALID_ARG;
+    b->has_ref = false;
+    return S2_OK;
+}
+
+int32_t s2_batch_has_reference(const s2_batch *b) { return b && b->has_ref ? 1 : 0; }
+
 s2_status s2_batch_results(s2_batch *b, s2_result *out, uint32_t n) {
     if (!b || (!out && n)) return S2_ERR_INVALID_ARG;
     int k = b->last_slot;  // no unread submission: the last one again
@@ -813,7 +921,7 @@ s2_status s2_batch_results(s2_batch *b, s2_result *out, uint32_t n) {
 
 s2_status s2_batch_mem_usage(const s2_batch *b, size_t *bytes) {
     if (!b || !bytes) return S2_ERR_INVALID_ARG;
-    *bytes = b->eng[0].allocated + (b->ready[1] ? b->eng[1].allocated : 0);
+    *bytes = b->eng[0].allocated + (b->ready[1] ? b->eng[1].allocated : 0) + b->ref_buf.n;
     return S2_OK;
 }
 

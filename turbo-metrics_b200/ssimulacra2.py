@@ -385,6 +385,36 @@ class Ssim2Batch:
         self.submit(pairs, stream)
         return self.results()
 
+    # ---- cached reference: ssim2-gpu Ssim2Batch (pipeline_batch.rs:206-330) ----
+    def set_reference(self, ref, fmt="srgb8", ref_uv=None, stream=None, **kw):
+        """Cache the reference (a device tensor of any supported format)."""
+        d = PairDesc(ref, ref, fmt, ref_uv, ref_uv, **kw).to_c()
+        d.dis = d.dis_uv = None
+        self._ref_keep = (ref, ref_uv)
+        check(lib.s2_batch_set_reference(self._h, ctypes.byref(d), _stream_ptr(stream)), "set_reference")
+
+    def clear_reference(self):
+        check(lib.s2_batch_clear_reference(self._h), "clear_reference")
+
+    def has_cached_reference(self):
+        return bool(lib.s2_batch_has_reference(self._h))
+
+    def submit_with_reference(self, dis, fmt="srgb8", dis_uv=None, stream=None, **kw):
+        """Enqueue distorted images (device tensors, one size) against the
+        cached reference; `dis_uv` gives their CbCr planes for 4:2:0 input."""
+        arr = (capi.PairDescC * max(len(dis), 1))()
+        for i, t in enumerate(dis):
+            arr[i] = PairDesc(t, t, fmt, dis_uv[i] if dis_uv else None, dis_uv[i] if dis_uv else None, **kw).to_c()
+            arr[i].ref = arr[i].ref_uv = None
+        k = self._take_slot(False)
+        check(lib.s2_batch_submit_with_reference(self._h, arr, len(dis), _stream_ptr(stream)), "compute_batch")
+        self._last = (k, len(dis), (dis, dis_uv))
+        self._unread.append(self._last)
+
+    def compute_batch_with_reference(self, dis, fmt="srgb8", dis_uv=None, stream=None, **kw):
+        self.submit_with_reference(dis, fmt, dis_uv, stream, **kw)
+        return self.results()
+
     def mem_usage(self):
         n = ctypes.c_size_t()
         check(lib.s2_batch_mem_usage(self._h, ctypes.byref(n)), "mem_usage")

@@ -204,6 +204,25 @@ def c1_pair(index: int, w: int = 1920, h: int = 1080):
     return nv12_frame_pair(w, h, pair_seed(1, index))
 
 
+def nv12_candidate(ref, step: float):
+    """A distorted version of an NV12 frame (y, uv): 8x8 DCT quantisation of
+    Y, Cb and Cr at `step`, clamped to the limited range."""
+    y, uv = ref
+    u, v = uv[:, 0::2].astype(np.float64), uv[:, 1::2].astype(np.float64)
+    yd = dct_quantize(y.astype(np.float64), step, 128.0, 16.0, 235.0)
+    ud = dct_quantize(u, step, 128.0, 16.0, 240.0)
+    vd = dct_quantize(v, step, 128.0, 16.0, 240.0)
+    out = np.empty_like(uv)
+    out[:, 0::2] = ud
+    out[:, 1::2] = vd
+    return yd.astype(np.uint8), out
+
+
+def c1_candidate_step(k: int):
+    """DCT step of cached-reference candidate k: spread over [2, 48]."""
+    return 2.0 + 46.0 * ((k * 0.6180339887498949) % 1.0)
+
+
 def c2_size(index: int):
     st = Stream(pair_seed(2, index) ^ 0x5A5A)
     return st.randint(64, 2048), st.randint(64, 2048)
