@@ -901,25 +901,15 @@ static float border_gain_f(int x, int n) {
 
 static inline float fmaxf0(float v) { return v > 0.0f ? v : 0.0f; }
 
-/* fir9f with every tap halved: exactly half of fir9f (power-of-two scaling). */
-static inline float fir9f_half(float a0, float a1, float a2, float a3, float a4, float a5, float a6,
-                               float a7, float a8) {
-    float acc = (0.5f * FT4) * (a0 + a8);
-    acc = fmaf(0.5f * FT3, a1 + a7, acc);
-    acc = fmaf(0.5f * FT2, a2 + a6, acc);
-    acc = fmaf(0.5f * FT1, a3 + a5, acc);
-    return fmaf(0.5f * FT0, a4, acc);
-}
-
 /* One scale in FIR32 arithmetic (the fused CUDA pass of this repository,
  * csrc/ssim2_kernels.cu fused_kernel).  xr/xd: planar XYB (3 planes of W*H).
  * Tiles of 120 columns x 64-row bands share one shift per channel (the
  * reference XYB at the tile's first column and the band's first row).  The
  * shifted values x', y' (0 outside the image) are blurred by the kernels'
  * 9-tap order, vertical then horizontal: x', y', x'y' and -- direct
- * (cached = 0) -- one plane of x'^2 + y'^2 (both squares rounded first),
- * halved through halved taps, or -- cached reference (cached = 1) -- x'^2
- * and y'^2 separately, then (sigma11 + sigma22) / 2 = fma(0.5, s11, 0.5 s22).
+ * (cached = 0) -- one plane of x'^2 + y'^2 (both squares rounded first), or
+ * -- cached reference (cached = 1) -- x'^2 and y'^2 separately, summed after
+ * the blur.
  * Maps are pooled in f32 over 8-pixel segments of a row, then in f64.
  * sums[c*6 + n*3 + m].  With `maps` (9 planes of W*H, [channel][ssim,
  * artifact, detail]) every pixel's error values are stored too. */
@@ -985,13 +975,12 @@ static void score_scale_fir32(const float *xr, const float *xd, int W, int H, do
                             for (int p = 0; p < NP; p++) {
                                 if (p == 3 && !cached) continue;
                                 const float *q = V + (size_t)p * TC * FIR_BAND + (size_t)r * TC + c0 + j;
-                                o[p] = (p == 2 && !cached)
-                                           ? fir9f_half(q[0], q[1], q[2], q[3], q[4], q[5], q[6], q[7], q[8])
-                                           : fir9f(q[0], q[1], q[2], q[3], q[4], q[5], q[6], q[7], q[8]);
+                                o[p] = fir9f(q[0], q[1], q[2], q[3], q[4], q[5], q[6], q[7], q[8]);
                             }
-                            /* hs = (sigma11 + sigma22) / 2 of the shifted values */
+                            /* ss = sigma11 + sigma22 of the shifted values: one blurred plane,
+                             * or (cached reference) the sum of the two blurred planes */
                             float m1 = o[0], m2 = o[1], s12 = o[4];
-                            float hs = cached ? fmaf(0.5f, o[2], 0.5f * o[3]) : o[2];
+                            float ss = cached ? o[2] + o[3] : o[2];
                             float xp = X[(size_t)r * TC + c0 + j + 4];
                             float yp = X[(size_t)TC * FIR_BAND + (size_t)r * TC + c0 + j + 4];
                             float bh = border_gain_f(xx, W);
@@ -1000,13 +989,13 @@ static void score_scale_fir32(const float *xr, const float *xd, int W, int H, do
                             float e = cv - kk;
                             float h = (m1 + m2) + e;
                             float md = m1 - m2;
-                            /* w = hs - m1 m2 - md^2 / 2; den = 2 w + C2 (see maps_px) */
-                            float w = fmaf(-0.5f * md, md, fmaf(-m1, m2, hs));
-                            w = fmaf(kk, h, w);
-                            float den = fmaf(2.0f, w, C2);
-                            float cov = fmaf(kk, h, fmaf(-m1, m2, s12));
+                            float t2 = m1 + m1, k2 = kk + kk;
+                            /* w2 = ss - 2 m1 m2 - md^2, c2 = 2 s12 - 2 m1 m2 (see maps_px) */
+                            float w2 = fmaf(k2, h, fmaf(-md, md, fmaf(-t2, m2, ss)));
+                            float c2 = fmaf(k2, h, fmaf(-t2, m2, s12 + s12));
+                            float den = w2 + C2;
                             float num_m = fmaf(-md, md, 1.0f);
-                            float num_s = fmaf(2.0f, cov, C2);
+                            float num_s = c2 + C2;
                             float d = fmaxf0(eng_div(fmaf(-num_m, num_s, den), den));
                             float aa = fabsf((xp - m1) + kk);
                             float bb = fabsf((yp - m2) + kk);

@@ -33,8 +33,8 @@
  *   OR_MODE_FIR32C   FIR32 as the cached-reference path computes it: the
  *                    reference's blurred x' and x'^2 come from its cache and
  *                    the candidate blurs y', y'^2 and x'y', so
- *                    (sigma11 + sigma22) / 2 = fma(0.5, sigma11, 0.5 sigma22)
- *                    of separately blurred planes.
+ *                    sigma11 + sigma22 is the sum of separately blurred
+ *                    planes.
  *
  * Pyramid stop rules (which scales are scored):
  *   OR_SCALES_CPU    cpu.rs:359-361 -- before producing scale s>0, stop if

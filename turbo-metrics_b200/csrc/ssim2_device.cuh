@@ -350,10 +350,14 @@ __device__ __forceinline__ float s2_pow_scale_unit(unsigned b) {
 // that are summed are formed by scalar multiplies (never contracted under
 // -fmad=false), or the sum is the addend of a packed FMA, or the product is
 // exact (a multiplication by 0.5).
-// The same operations as inline PTX (add / mul / fma .rn.f32x2): the
-// optimiser sees no multiply and add to contract, and PTX does not fuse
-// operations that carry an explicit rounding modifier, so each lane rounds
-// exactly as the written scalar operation.  The fused tile pass uses these.
+// The same operations as inline PTX (add / mul / fma .rn.f32x2).  Each lane
+// rounds as the scalar operation -- but the assembler, too, was measured to
+// fuse a packed multiply whose result feeds a packed add into one fused
+// multiply-add (a probe over 1.7e7 operand triples on sm_100a, CUDA 12.9:
+// every case where the two roundings differ from one came out fused).  So
+// here as well no packed product feeds a packed sum: the fused tile pass
+// feeds products to the multiplicand or addend of an explicit FMA, or sums
+// the two lanes of a product with a scalar add.
 __device__ __forceinline__ float2 s2_padd(float2 a, float2 b) {
     float2 d;
     asm("{.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
@@ -380,8 +384,13 @@ __device__ __forceinline__ float2 s2_mul2(float2 a, float2 b) { return __fmul2_r
 __device__ __forceinline__ float2 s2_add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
 __device__ __forceinline__ float2 s2_mul2s(float2 a, float2 b) { return make_float2(a.x * b.x, a.y * b.y); }
 
-// s2_pow_20_9_unit of both lanes
-__device__ __forceinline__ float2 s2_pow_20_9_unit2(float2 p) {
+// The factors 2^(20e/9) of s2_pow_20_9_unit for e = -3..0, indexed by the
+// exponent field minus 124 (the caller keeps them in shared memory: one
+// shared load per lane instead of three compares and selects).
+#define S2_POW_TAB_INIT {0x1.428a3p-7f, 0x1.784086p-5f, 0x1.b6e8aep-3f, 0x1p+0f}
+
+// s2_pow_20_9_unit of both lanes; pw = the S2_POW_TAB_INIT table
+__device__ __forceinline__ float2 s2_pow_20_9_unit2(float2 p, const float *pw) {
     const unsigned bx = __float_as_uint(p.x), by = __float_as_uint(p.y);
     const float2 m = make_float2(__uint_as_float((bx & 0x7fffffu) | 0x3f800000u),
                                  __uint_as_float((by & 0x7fffffu) | 0x3f800000u));
@@ -393,14 +402,15 @@ __device__ __forceinline__ float2 s2_pow_20_9_unit2(float2 p) {
     y = __ffma2_rn(y, t, s2_f2(0x1.7c6f02p+0f));
     y = __ffma2_rn(y, t, s2_f2(0x1.d2e55cp+1f));
     y = __ffma2_rn(y, t, s2_f2(0x1.3b279ep+1f));
-    return s2_mul2(y, make_float2(s2_pow_scale_unit(bx), s2_pow_scale_unit(by)));
+    return s2_mul2(y, make_float2(pw[(bx >> 23) - 124u], pw[(by >> 23) - 124u]));
 }
 
-// bt709_eotf of both lanes
-__device__ __forceinline__ float2 bt709_eotf2(float2 v) {
+// bt709_eotf of both lanes; pw = the S2_POW_TAB_INIT table
+__device__ __forceinline__ float2 bt709_eotf2(float2 v, const float *pw) {
     const float thr = 0.08124285829863521110029445797874f;
     const float2 q = s2_mul2(s2_add2(v, s2_f2(0x1.96b84p-4f)), s2_f2(0x1.d1c096p-1f));
-    const float2 hi = s2_pow_20_9_unit2(make_float2(fminf(fmaxf(q.x, 0.125f), 1.5f), fminf(fmaxf(q.y, 0.125f), 1.5f)));
+    const float2 hi =
+        s2_pow_20_9_unit2(make_float2(fminf(fmaxf(q.x, 0.125f), 1.5f), fminf(fmaxf(q.y, 0.125f), 1.5f)), pw);
     const float2 lo = s2_mul2(v, s2_f2(0x1.c71c72p-3f));
     return make_float2(v.x >= thr ? hi.x : lo.x, v.y >= thr ? hi.y : lo.y);
 }
@@ -539,7 +549,7 @@ __device__ __forceinline__ Nv12Quad yuv_load_quad(const DevPair &P, int img, int
 // inverse OETF, clamp to [0, 1]) of a loaded quad: pixels (0, 1) and (2, 3)
 // as f32x2 lanes.
 template <int ES>
-__device__ __forceinline__ void yuv_quad_linear(const Nv12Quad &q, const DevPair &P, float o[4][3]) {
+__device__ __forceinline__ void yuv_quad_linear(const Nv12Quad &q, const DevPair &P, const float *pw, float o[4][3]) {
     constexpr unsigned kMask = ES == 1 ? 0xffu : 0xffffu;
     constexpr int kShift = 8 * ES;
     const float cb = (float)((int)(q.uv & kMask) - P.yuv_neutral);
@@ -555,9 +565,9 @@ __device__ __forceinline__ void yuv_quad_linear(const Nv12Quad &q, const DevPair
         const int Y0 = (int)(w & kMask), Y1 = (int)(w >> kShift);
         // scalar products: luma is summed with the chroma terms below
         const float2 luma = make_float2((float)(max(Y0, ymin) - ymin) * yc, (float)(max(Y1, ymin) - ymin) * yc);
-        const float2 r = bt709_eotf2(s2_add2(luma, s2_f2(ar)));
-        const float2 g = bt709_eotf2(s2_add2(luma, s2_f2(ag)));
-        const float2 b = bt709_eotf2(s2_add2(luma, s2_f2(ab)));
+        const float2 r = bt709_eotf2(s2_add2(luma, s2_f2(ar)), pw);
+        const float2 g = bt709_eotf2(s2_add2(luma, s2_f2(ag)), pw);
+        const float2 b = bt709_eotf2(s2_add2(luma, s2_f2(ab)), pw);
         float *p0 = o[2 * row], *p1 = o[2 * row + 1];
         p0[0] = fminf(fmaxf(r.x, 0.0f), 1.0f);
         p0[1] = fminf(fmaxf(g.x, 0.0f), 1.0f);
@@ -571,13 +581,14 @@ __device__ __forceinline__ void yuv_quad_linear(const Nv12Quad &q, const DevPair
 // Linear RGB of the 2x2 quad whose top-left pixel is (x, y) (inside the
 // image); px 0..3 = (x,y), (x+1,y), (x,y+1), (x+1,y+1); pixels outside the
 // image (vx / vy false) are not read.  NV12 chroma is one sample per quad.
+// lut: the sRGB8 table (256 entries) followed by the S2_POW_TAB_INIT table.
 template <int FMT>
 __device__ __forceinline__ void lin_quad(const DevPair &P, int img, int x, int y, bool vx, bool vy,
                                          const float *lut, const ColorConsts &cc, float o[4][3]) {
     if (FMT == FMT_NV12 || FMT == FMT_P016) {
         // 4:2:0 input has even width and height: the quad is complete
         constexpr int ES = FMT == FMT_NV12 ? 1 : 2;
-        yuv_quad_linear<ES>(yuv_load_quad<ES>(P, img, x, y), P, o);
+        yuv_quad_linear<ES>(yuv_load_quad<ES>(P, img, x, y), P, lut + 256, o);
     } else {
         // a complete quad whose rows are aligned for the format's word size is
         // read as three words per row: sRGB8 16-bit, RGB16 32-bit, linear f32
@@ -628,13 +639,18 @@ __device__ __forceinline__ void lin_quad(const DevPair &P, int img, int x, int y
 // [0, n) (the blur's response to a constant 1 under zero padding), rounded
 // to f32: exactly 1.0f in the interior, where all nine taps are inside.
 // Prefix sums S[m] = t0 + ... + tm of the double-precision taps.
+// (The prefix sums are picked by selects: an indexed local array would be
+// built in local memory on every call.)
+__device__ __forceinline__ double border_prefix(int k) {
+    return k == 0 ? 0x1.0ef8d5c79cdafp-2
+                  : (k == 1 ? 0x1.e902c9b3e2946p-2
+                            : (k == 2 ? 0x1.2c7c332eb15f4p-1 : (k == 3 ? 0x1.3eec3fae31770p-1 : 0x1.43be3571e736ap-1)));
+}
 __device__ __forceinline__ float border_gain(int x, int n) {
     int lo = min(x, 4), hi = min(n - 1 - x, 4);
     if (lo == 4 && hi == 4) return 1.0f;
-    const double S[5] = {0x1.0ef8d5c79cdafp-2, 0x1.e902c9b3e2946p-2, 0x1.2c7c332eb15f4p-1,
-                         0x1.3eec3fae31770p-1, 0x1.43be3571e736ap-1};
-    double s = S[lo] + S[hi];
-    return (float)(s - S[0]);
+    double s = border_prefix(lo) + border_prefix(hi);
+    return (float)(s - 0x1.0ef8d5c79cdafp-2);
 }
 
 }  // namespace s2

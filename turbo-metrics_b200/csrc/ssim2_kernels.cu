@@ -49,17 +49,15 @@ static_assert(kBand % kStripMax == 0 && kStripMax % kStep == 0 && kStripMid % kS
 
 // 9-tap symmetric FIR of two planes at once (f32x2 lanes; each lane rounds as
 // acc = t4 (a0 + a8); acc = fma(t3, a1 + a7, acc); ...; fma(t0, a4, acc)).
-// HX: the x lane uses the taps halved -- a power-of-two scaling, so that lane
-// is exactly half of the plain FIR.
-template <bool HX = false>
+// f32x2 operations take registers only, so the five tap pairs are the same
+// five register pairs for every FIR of the pass.
 __device__ __forceinline__ float2 fir9p(float2 a0, float2 a1, float2 a2, float2 a3, float2 a4, float2 a5,
                                         float2 a6, float2 a7, float2 a8) {
-    constexpr float hx = HX ? 0.5f : 1.0f;
-    float2 acc = s2_pmul(make_float2(hx * S2_T4, S2_T4), s2_padd(a0, a8));
-    acc = s2_pfma(make_float2(hx * S2_T3, S2_T3), s2_padd(a1, a7), acc);
-    acc = s2_pfma(make_float2(hx * S2_T2, S2_T2), s2_padd(a2, a6), acc);
-    acc = s2_pfma(make_float2(hx * S2_T1, S2_T1), s2_padd(a3, a5), acc);
-    return s2_pfma(make_float2(hx * S2_T0, S2_T0), a4, acc);
+    float2 acc = s2_pmul(s2_f2(S2_T4), s2_padd(a0, a8));
+    acc = s2_pfma(s2_f2(S2_T3), s2_padd(a1, a7), acc);
+    acc = s2_pfma(s2_f2(S2_T2), s2_padd(a2, a6), acc);
+    acc = s2_pfma(s2_f2(S2_T1), s2_padd(a3, a5), acc);
+    return s2_pfma(s2_f2(S2_T0), a4, acc);
 }
 
 template <bool KUNIT>
@@ -193,7 +191,7 @@ __device__ __forceinline__ void prep_quads(const DevPair &P, int X0, int Y0, con
                 const int xq = x + 2 * k;
                 const bool vx = xq + 1 < W;
                 float v[4][3];
-                if (kYuv) yuv_quad_linear<kEs>(img ? (k ? nd1 : nd0) : (k ? nr1 : nr0), P, v);
+                if (kYuv) yuv_quad_linear<kEs>(img ? (k ? nd1 : nd0) : (k ? nr1 : nr0), P, lut + 256, v);
                 else lin_quad<FMT>(P, img, xq, y, vx, vy, lut, cc, v);
                 if (kX && (!kL || P.nscales > 0)) {
                     ST *dst = (ST *)P.lvl[img][0];
@@ -254,12 +252,16 @@ __global__ void __launch_bounds__(256, 2) prep_kernel(const DevPair *__restrict_
                                                    ColorConsts cc, const float *__restrict__ lut_g) {
     __shared__ float lv1[2][3][kLv1 * kLv1];              // scale-1 linear block [img][ch][px]
     __shared__ float pp[2][2][3][(kLv1 / 2) * (kLv1 / 2)];  // scales >= 2, ping-pong
-    __shared__ float lut[256];
+    __shared__ float lut[256 + 4];  // the sRGB8 table, then the BT.709 power's 2^(20e/9) factors
     // the block's pair descriptor: in shared memory, so the level stores
     // (global) cannot alias it and its fields need no per-thread copy
     __shared__ DevPair sP;
     static_assert(sizeof(DevPair) % 8 == 0, "DevPair copied as 8-byte words");
     for (int i = threadIdx.x; i < 256; i += blockDim.x) lut[i] = lut_g[i];
+    if (threadIdx.x < 4) {
+        const float pw[4] = S2_POW_TAB_INIT;
+        lut[256 + threadIdx.x] = pw[threadIdx.x];
+    }
     for (int item = first_block + blockIdx.x; item < end_block; item += gridDim.x) {
         int lo = 0, hi = npairs - 1;
         while (lo < hi) {
@@ -356,8 +358,7 @@ __global__ void __launch_bounds__(256, 2) prep_kernel(const DevPair *__restrict_
 //              mu1 of the three channels, then sigma11), no maps.
 //   TM_CAND    a candidate against a cached reference: blurs (y', x'y') in
 //              f32x2 and y'^2 alone (three planes), reads mu1 and sigma11
-//              from the moment planes, and forms (sigma11 + sigma22) / 2 as
-//              fma(0.5, sigma11, 0.5 sigma22).
+//              from the moment planes, and sums sigma11 + sigma22.
 // The shared buffers are double buffered by step parity: step i's horizontal
 // phase reads buffer i % 2 while step i+1's vertical phase writes the other,
 // so one barrier per step orders them.
@@ -415,9 +416,12 @@ __device__ __forceinline__ void ring_in(Rings &R, int sl, float vr, float vd, fl
 // S0 + k + 8 and is stored to row k of the buffer: plane 0 the FIR of ring
 // a, plane 1 that of ring b (FULL) or of ring c as floats (CAND), plane 2
 // the raw (x', y') of the output row (FULL, CAND).
+__device__ __forceinline__ void s2_prefetch_l1(const void *p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
+
+// more: the tile has another step after this one.
 template <typename ST, int MODE, int S0>
 __device__ __forceinline__ void v_step(Rings &R, const ST *__restrict__ xr, const ST *__restrict__ xd, long long lp,
-                                       int x, bool colin, int ybase, int H, int nr, float cg, float2 ncg,
+                                       int x, bool colin, int ybase, int H, int nr, bool more, float cg, float2 ncg,
                                        float2 *__restrict__ buf, int col) {
     float lr[kStep], ld[kStep];
 #pragma unroll
@@ -426,6 +430,18 @@ __device__ __forceinline__ void v_step(Rings &R, const ST *__restrict__ xr, cons
         const bool in = k < nr && colin && y < H;
         lr[k] = in ? ld_store<ST>(xr + (long long)y * lp + x) : cg;
         ld[k] = (MODE != TM_REFMOM && in) ? ld_store<ST>(xd + (long long)y * lp + x) : cg;
+    }
+    // the next step's rows into L1 while this step and its horizontal phase
+    // run (their loads then wait for L1, not for HBM)
+    if (more) {
+#pragma unroll
+        for (int k = 0; k < kStep; k++) {
+            const int y = ybase + kStep + k;
+            if (colin && y < H) {
+                s2_prefetch_l1(xr + (long long)y * lp + x);
+                if (MODE != TM_REFMOM) s2_prefetch_l1(xd + (long long)y * lp + x);
+            }
+        }
     }
 #pragma unroll
     for (int k = 0; k < kStep; k++) {
@@ -451,7 +467,6 @@ __device__ __forceinline__ void v_step(Rings &R, const ST *__restrict__ xr, cons
 }
 
 // Horizontal FIR of 4 outputs from 12 float2 of a buffer row (16-byte loads).
-template <bool HX>
 __device__ __forceinline__ void h_fir4(const float2 *__restrict__ p, float2 o[4]) {
     float2 v[12];
     const float4 *q = (const float4 *)p;
@@ -463,7 +478,7 @@ __device__ __forceinline__ void h_fir4(const float2 *__restrict__ p, float2 o[4]
     }
 #pragma unroll
     for (int j = 0; j < 4; j++)
-        o[j] = fir9p<HX>(v[j], v[j + 1], v[j + 2], v[j + 3], v[j + 4], v[j + 5], v[j + 6], v[j + 7], v[j + 8]);
+        o[j] = fir9p(v[j], v[j + 1], v[j + 2], v[j + 3], v[j + 4], v[j + 5], v[j + 6], v[j + 7], v[j + 8]);
 }
 
 // The same on a float row (12 floats, three 16-byte loads).
@@ -499,31 +514,34 @@ __device__ __forceinline__ void add_maps(TaskSums &t, float d, float art, float 
     t.f4_ad = s2_pfma(q2, q2, t.f4_ad);
 }
 
-// Error maps of one pixel.  m = (mu1, mu2) and s = ((sigma11 + sigma22) / 2,
+// Error maps of one pixel.  m = (mu1, mu2) and s = (sigma11 + sigma22,
 // sigma12) of the shifted values, r = (x', y').  kk = anchor * (1 - border
 // gain): the correction of the shifted moments at the image borders (0
 // inside).  With the anchor c and the gain g the true moments are
 // mu = m + c g and sigma = s + 2 c m + c^2 g, so
-//   sigma11 - mu1^2 + sigma22 - mu2^2 = 2 (w + kk h)   and
-//   sigma12 - mu1 mu2 = cov + kk h,
-// with w = s.x - mu1 mu2 - (mu1 - mu2)^2 / 2, cov = s.y - mu1 mu2,
+//   sigma11 - mu1^2 + sigma22 - mu2^2 = w2 + 2 kk h   and
+//   2 (sigma12 - mu1 mu2) = c2 + 2 kk h,
+// with w2 = s.x - 2 mu1 mu2 - (mu1 - mu2)^2, c2 = 2 s.y - 2 mu1 mu2,
 // e = c - kk = c g and h = (mu1 + mu2) + e.  For identical images
-// (x' = y') s.x equals s.y exactly, so w equals cov and the SSIM error is 0.
+// (x' = y') s.x is exactly 2 s.y and mu1 = mu2, so w2 equals c2 and the SSIM
+// error is 0.
 template <bool BORDER>
 __device__ __forceinline__ void maps_px(float2 m, float2 s, float2 r, float kk, float e, float &d, float &art,
                                         float &det) {
     const float m1 = m.x, m2 = m.y;
     const float md = m1 - m2;
-    float w = fmaf(-0.5f * md, md, fmaf(-m1, m2, s.x));
-    float cov = fmaf(-m1, m2, s.y);
+    const float t2 = m1 + m1;
+    float w2 = fmaf(-md, md, fmaf(-t2, m2, s.x));
+    float c2 = fmaf(-t2, m2, s.y + s.y);
     if (BORDER) {
         const float h = (m1 + m2) + e;
-        w = fmaf(kk, h, w);
-        cov = fmaf(kk, h, cov);
+        const float k2 = kk + kk;
+        w2 = fmaf(k2, h, w2);
+        c2 = fmaf(k2, h, c2);
     }
-    const float den = fmaf(2.0f, w, kC2);
+    const float den = w2 + kC2;
     const float num_m = fmaf(-md, md, 1.0f);
-    const float num_s = fmaf(2.0f, cov, kC2);
+    const float num_s = c2 + kC2;
     d = fmaxf(s2_div(fmaf(-num_m, num_s, den), den), 0.0f);
     float2 t = s2_pfma(m, s2_f2(-1.0f), r);  // (x' - mu1, y' - mu2)
     if (BORDER) t = make_float2(t.x + kk, t.y + kk);
@@ -550,7 +568,7 @@ struct ItemGeo {
 // this thread's task, row t_r, segment t_s.
 template <int MODE, bool EXPORT>
 __device__ __forceinline__ void h_step(const float2 *__restrict__ buf, int r0, int nr, int t_r, int t_s, bool t_on,
-                                       const ItemGeo &G, Acc6 &acc, const MapOut &mo) {
+                                       const ItemGeo G, Acc6 &acc, const MapOut mo) {
     if (!t_on || t_r >= nr) return;
     const int c0 = t_s * kSegW;  // first output column of the task (tile coordinates)
     const int xc = G.x0 + c0;
@@ -566,7 +584,7 @@ __device__ __forceinline__ void h_step(const float2 *__restrict__ buf, int r0, i
             const int cc = c0 + 4 * half;
             if (G.x0 + cc >= G.W) break;
             float2 mA[4];
-            h_fir4<false>(buf + t_r * kRS + cc, mA);
+            h_fir4(buf + t_r * kRS + cc, mA);
             *(float4 *)(mu + G.x0 + cc) = make_float4(mA[0].x, mA[1].x, mA[2].x, mA[3].x);
             *(float4 *)(sg + G.x0 + cc) = make_float4(mA[0].y, mA[1].y, mA[2].y, mA[3].y);
         }
@@ -581,13 +599,13 @@ __device__ __forceinline__ void h_step(const float2 *__restrict__ buf, int r0, i
         const float2 *pa = buf + t_r * kRS + cc;
         float2 mA[4], mB[4], rw[4];
         if (MODE == TM_FULL) {
-            h_fir4<false>(pa, mA);
-            h_fir4<true>(pa + kPlaneF2, mB);  // (sigma11 + sigma22) / 2, sigma12
+            h_fir4(pa, mA);
+            h_fir4(pa + kPlaneF2, mB);  // (sigma11 + sigma22, sigma12)
         } else {
             if (G.x0 + cc >= G.W) break;
             float2 ma[4];
             float s22[4];
-            h_fir4<false>(pa, ma);  // (mu2, sigma12)
+            h_fir4(pa, ma);  // (mu2, sigma12)
             h_fir4s((const float *)(buf + kPlaneF2) + t_r * 2 * kRS + cc, s22);
             const long long o = (long long)y * G.lp + G.x0 + cc;
             const float4 mu1 = *(const float4 *)(G.mom + G.g * G.plane + o);
@@ -596,7 +614,7 @@ __device__ __forceinline__ void h_step(const float2 *__restrict__ buf, int r0, i
 #pragma unroll
             for (int j = 0; j < 4; j++) {
                 mA[j] = make_float2(m1v[j], ma[j].x);
-                mB[j] = make_float2(fmaf(0.5f, s1v[j], 0.5f * s22[j]), ma[j].y);
+                mB[j] = make_float2(s1v[j] + s22[j], ma[j].y);
             }
         }
         {
@@ -700,13 +718,14 @@ __device__ __forceinline__ void tile_item(const DevPair &P, const Seg &sg, int t
     for (int st = 0; st < nsteps; st += 2) {
         const int r0 = st * kStep;
         const int nr0 = min(kStep, rows_out - r0);
-        v_step<ST, MODE, 0>(R, xr, xd, G.lp, x, colin, G.y0 + r0 + 4, G.H, nr0, cg, ncg, buf0, tid);
+        v_step<ST, MODE, 0>(R, xr, xd, G.lp, x, colin, G.y0 + r0 + 4, G.H, nr0, st + 1 < nsteps, cg, ncg, buf0, tid);
         __syncthreads();
         h_step<MODE, EXPORT>(buf0, r0, nr0, t_r, t_s, t_on, G, acc, mo);
         if (st + 1 < nsteps) {
             const int r1 = r0 + kStep;
             const int nr1 = min(kStep, rows_out - r1);
-            v_step<ST, MODE, 8>(R, xr, xd, G.lp, x, colin, G.y0 + r1 + 4, G.H, nr1, cg, ncg, buf1, tid);
+            v_step<ST, MODE, 8>(R, xr, xd, G.lp, x, colin, G.y0 + r1 + 4, G.H, nr1, st + 2 < nsteps, cg, ncg, buf1,
+                                tid);
             __syncthreads();
             h_step<MODE, EXPORT>(buf1, r1, nr1, t_r, t_s, t_on, G, acc, mo);
         }
