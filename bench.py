@@ -476,6 +476,8 @@ def main():
     ap.add_argument("--serve-jobs", type=int, default=10000, help="jobs per offered rate of the serving leg")
     ap.add_argument("--no-uneven", action="store_true", help="skip the 256-pair uneven-size batch leg")
     ap.add_argument("--no-dssim", action="store_true", help="skip the DSSIM (sibling metric) leg")
+    ap.add_argument("--strip", type=int, default=0,
+                    help="tile height of the main leg (16, 32, 64; 0 = autotuned, the default)")
     ap.add_argument("--pairs", type=int, default=N_PAIRS,
                     help="pairs per step (64 is the workload; smaller only for profiler captures)")
     args = ap.parse_args()
@@ -503,7 +505,7 @@ def main():
     descs = [tmb.PairDesc(r, d, "nv12", ru, du) for r, ru, d, du in dev]
     stream = torch.cuda.current_stream()
 
-    batch = tmb.Ssim2Batch(NP, NP * W * H)
+    batch = tmb.Ssim2Batch(NP, NP * W * H, strip_rows=args.strip)
     batch.submit(descs)
     scores = [r[0] for r in batch.results()]
     lib = tmb.lib

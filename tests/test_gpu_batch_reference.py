@@ -40,7 +40,7 @@ def test_batch_reference_srgb_against_oracle_and_direct(tmb, oracle, cuda):
         mirror = oracle.ssim2_srgb8(ref, c, "fir32c")
         assert close(o[1], mirror.stats)
         assert abs(o[0] - mirror.score) < 2e-6
-        assert abs(o[0] - d[0]) < 1e-5
+        assert abs(o[0] - d[0]) < 1e-4
     # a second submission against the same cache gives the same scores
     again = b.compute_batch_with_reference([dev(cuda, c) for c in cands])
     assert [x[0] for x in again] == [x[0] for x in out]
@@ -79,5 +79,5 @@ def test_batch_reference_nv12_frames(tmb, oracle, cuda):
         mirror = oracle.ssim2_linear(rl, oracle.nv12_to_linear(*c), "fir32c")
         assert close(o[1], mirror.stats)
         direct = oracle.ssim2_linear(rl, oracle.nv12_to_linear(*c), "fir32")
-        assert abs(o[0] - direct.score) < 1e-5
+        assert abs(o[0] - direct.score) < 1e-4
     b.close()

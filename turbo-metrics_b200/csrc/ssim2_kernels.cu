@@ -416,12 +416,9 @@ __device__ __forceinline__ void ring_in(Rings &R, int sl, float vr, float vd, fl
 // S0 + k + 8 and is stored to row k of the buffer: plane 0 the FIR of ring
 // a, plane 1 that of ring b (FULL) or of ring c as floats (CAND), plane 2
 // the raw (x', y') of the output row (FULL, CAND).
-__device__ __forceinline__ void s2_prefetch_l1(const void *p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
-
-// more: the tile has another step after this one.
 template <typename ST, int MODE, int S0>
 __device__ __forceinline__ void v_step(Rings &R, const ST *__restrict__ xr, const ST *__restrict__ xd, long long lp,
-                                       int x, bool colin, int ybase, int H, int nr, bool more, float cg, float2 ncg,
+                                       int x, bool colin, int ybase, int H, int nr, float cg, float2 ncg,
                                        float2 *__restrict__ buf, int col) {
     float lr[kStep], ld[kStep];
 #pragma unroll
@@ -430,18 +427,6 @@ __device__ __forceinline__ void v_step(Rings &R, const ST *__restrict__ xr, cons
         const bool in = k < nr && colin && y < H;
         lr[k] = in ? ld_store<ST>(xr + (long long)y * lp + x) : cg;
         ld[k] = (MODE != TM_REFMOM && in) ? ld_store<ST>(xd + (long long)y * lp + x) : cg;
-    }
-    // the next step's rows into L1 while this step and its horizontal phase
-    // run (their loads then wait for L1, not for HBM)
-    if (more) {
-#pragma unroll
-        for (int k = 0; k < kStep; k++) {
-            const int y = ybase + kStep + k;
-            if (colin && y < H) {
-                s2_prefetch_l1(xr + (long long)y * lp + x);
-                if (MODE != TM_REFMOM) s2_prefetch_l1(xd + (long long)y * lp + x);
-            }
-        }
     }
 #pragma unroll
     for (int k = 0; k < kStep; k++) {
@@ -568,7 +553,7 @@ struct ItemGeo {
 // this thread's task, row t_r, segment t_s.
 template <int MODE, bool EXPORT>
 __device__ __forceinline__ void h_step(const float2 *__restrict__ buf, int r0, int nr, int t_r, int t_s, bool t_on,
-                                       const ItemGeo G, Acc6 &acc, const MapOut mo) {
+                                       const ItemGeo &G, Acc6 &acc, const MapOut &mo) {
     if (!t_on || t_r >= nr) return;
     const int c0 = t_s * kSegW;  // first output column of the task (tile coordinates)
     const int xc = G.x0 + c0;
@@ -667,16 +652,30 @@ __device__ __forceinline__ void h_step(const float2 *__restrict__ buf, int r0, i
     acc.v[5] += (double)ts.f4_ad.y;
 }
 
-// One work item (one channel of one tile) in mode MODE.
-template <typename ST, int MODE, bool EXPORT>
-__device__ __forceinline__ void tile_item(const DevPair &P, const Seg &sg, int tile, int g, float2 *smb,
-                                          double (*s_warp)[6], double *__restrict__ partials, int item,
-                                          const MapOut &mo) {
-    const int tid = threadIdx.x;
-    const int t_r = tid % kStep, t_s = tid / kStep;
-    const bool t_on = tid < kTasks;
-    const int s = sg.scale;
+// Named barriers of the two warpgroups (0 is __syncthreads): FULL[b] -- the
+// vertical group has written buffer b, EMPTY[b] -- the horizontal group has
+// read it; the horizontal group's own barrier for its reduction.
+constexpr int kBarFull0 = 1, kBarEmpty0 = 3, kBarHGroup = 5;
+constexpr int kWsThreads = 2 * kFusedThreads;  // vertical warpgroup + horizontal warpgroup
+
+__device__ __forceinline__ void s2_bar_sync(int id, int n) { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory"); }
+__device__ __forceinline__ void s2_bar_arrive(int id, int n) {
+    asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(n) : "memory");
+}
+
+// The geometry of one work item, decoded alike by both warpgroups.
+template <typename ST>
+struct Item {
     ItemGeo G;
+    int rows_out, nsteps;
+    const ST *xr, *xd;
+};
+
+template <typename ST>
+__device__ __forceinline__ Item<ST> decode_item(const DevPair &P, const Seg &sg, int tile, int g) {
+    Item<ST> it;
+    const int s = sg.scale;
+    ItemGeo &G = it.G;
     G.W = P.w[s];
     G.H = P.h[s];
     G.g = g;
@@ -684,77 +683,99 @@ __device__ __forceinline__ void tile_item(const DevPair &P, const Seg &sg, int t
     const int tx = local % sg.tiles_x, ty = local / sg.tiles_x;
     G.x0 = tx * kTileW;
     G.y0 = ty * sg.strip_rows;
-    const int rows_out = min(G.y0 + sg.strip_rows, G.H) - G.y0;
+    it.rows_out = min(G.y0 + sg.strip_rows, G.H) - G.y0;
+    it.nsteps = (it.rows_out + kStep - 1) / kStep;
     G.lp = P.lp[s];
     G.plane = G.lp * G.H;
     G.mom = P.mom[s];
-    const ST *xr = (const ST *)P.lvl[0][s] + g * G.plane;
-    const ST *xd = (const ST *)P.lvl[1][s] + g * G.plane;
+    it.xr = (const ST *)P.lvl[0][s] + g * G.plane;
+    it.xd = (const ST *)P.lvl[1][s] + g * G.plane;
     // anchor: reference XYB of channel g at the tile's first column, band start
-    G.cg = ld_store<ST>(xr + (long long)((G.y0 / kBand) * kBand) * G.lp + G.x0);
+    G.cg = ld_store<ST>(it.xr + (long long)((G.y0 / kBand) * kBand) * G.lp + G.x0);
+    return it;
+}
+
+// Vertical warpgroup: one work item.  Before it overwrites buffer b at step
+// st >= 2 it waits until the horizontal group has read that buffer (step
+// st - 2); after writing it, it signals FULL[b].
+template <typename ST, int MODE>
+__device__ __forceinline__ void v_item(const Item<ST> &it, float2 *smb, int col) {
+    const ItemGeo &G = it.G;
     const float cg = G.cg;
     const float2 ncg = make_float2(-cg, -cg);
-
-    const int x = G.x0 - 4 + tid;
+    const int x = G.x0 - 4 + col;
     const bool colin = x >= 0 && x < G.W;
     Rings R;
     // prime ring slots 0..7 with input rows y0 - 4 .. y0 + 3
-    {
-        float lr[8], ld[8];
 #pragma unroll
-        for (int k = 0; k < 8; k++) {
-            const int y = G.y0 - 4 + k;
-            const bool in = colin && y >= 0 && y < G.H;
-            lr[k] = in ? ld_store<ST>(xr + (long long)y * G.lp + x) : cg;
-            ld[k] = (MODE != TM_REFMOM && in) ? ld_store<ST>(xd + (long long)y * G.lp + x) : cg;
-        }
-#pragma unroll
-        for (int k = 0; k < 8; k++) ring_in<MODE>(R, k, lr[k], ld[k], ncg);
+    for (int k = 0; k < 8; k++) {
+        const int y = G.y0 - 4 + k;
+        const bool in = colin && y >= 0 && y < G.H;
+        const float lr = in ? ld_store<ST>(it.xr + (long long)y * G.lp + x) : cg;
+        const float ld = (MODE != TM_REFMOM && in) ? ld_store<ST>(it.xd + (long long)y * G.lp + x) : cg;
+        ring_in<MODE>(R, k, lr, ld, ncg);
     }
-
-    Acc6 acc{};
-    const int nsteps = (rows_out + kStep - 1) / kStep;
     float2 *buf0 = smb, *buf1 = smb + kBufF2;
-    for (int st = 0; st < nsteps; st += 2) {
+    for (int st = 0; st < it.nsteps; st += 2) {
         const int r0 = st * kStep;
-        const int nr0 = min(kStep, rows_out - r0);
-        v_step<ST, MODE, 0>(R, xr, xd, G.lp, x, colin, G.y0 + r0 + 4, G.H, nr0, st + 1 < nsteps, cg, ncg, buf0, tid);
-        __syncthreads();
-        h_step<MODE, EXPORT>(buf0, r0, nr0, t_r, t_s, t_on, G, acc, mo);
-        if (st + 1 < nsteps) {
+        if (st >= 2) s2_bar_sync(kBarEmpty0, kWsThreads);
+        v_step<ST, MODE, 0>(R, it.xr, it.xd, G.lp, x, colin, G.y0 + r0 + 4, G.H, min(kStep, it.rows_out - r0), cg,
+                            ncg, buf0, col);
+        s2_bar_arrive(kBarFull0, kWsThreads);
+        if (st + 1 < it.nsteps) {
             const int r1 = r0 + kStep;
-            const int nr1 = min(kStep, rows_out - r1);
-            v_step<ST, MODE, 8>(R, xr, xd, G.lp, x, colin, G.y0 + r1 + 4, G.H, nr1, st + 2 < nsteps, cg, ncg, buf1,
-                                tid);
-            __syncthreads();
-            h_step<MODE, EXPORT>(buf1, r1, nr1, t_r, t_s, t_on, G, acc, mo);
+            if (st + 1 >= 2) s2_bar_sync(kBarEmpty0 + 1, kWsThreads);
+            v_step<ST, MODE, 8>(R, it.xr, it.xd, G.lp, x, colin, G.y0 + r1 + 4, G.H, min(kStep, it.rows_out - r1),
+                                cg, ncg, buf1, col);
+            s2_bar_arrive(kBarFull0 + 1, kWsThreads);
         }
     }
+}
 
-    // channel reduction, fixed order: lanes by a shuffle tree, then warps in
-    // order (a moment build has no sums; the caller's barriers order the buffers)
+// Horizontal warpgroup: one work item, then the item's sums (fixed order:
+// lanes by a shuffle tree, then the group's four warps in order).
+template <typename ST, int MODE, bool EXPORT>
+__device__ __forceinline__ void h_item(const Item<ST> &it, float2 *smb, int ht, double (*s_warp)[6],
+                                       double *__restrict__ partials, int item, const MapOut &mo) {
+    const int t_r = ht % kStep, t_s = ht / kStep;
+    const bool t_on = ht < kTasks;
+    Acc6 acc{};
+    for (int st = 0; st < it.nsteps; st++) {
+        const int b = st & 1;
+        s2_bar_sync(kBarFull0 + b, kWsThreads);
+        const int r0 = st * kStep;
+        h_step<MODE, EXPORT>(smb + b * kBufF2, r0, min(kStep, it.rows_out - r0), t_r, t_s, t_on, it.G, acc, mo);
+        if (st + 2 < it.nsteps) s2_bar_arrive(kBarEmpty0 + b, kWsThreads);
+    }
     if constexpr (MODE != TM_REFMOM) {
 #pragma unroll
         for (int m = 0; m < 6; m++) {
             double v = acc.v[m];
 #pragma unroll
             for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-            if ((tid & 31) == 0) s_warp[tid >> 5][m] = v;
+            if ((ht & 31) == 0) s_warp[ht >> 5][m] = v;
         }
-        __syncthreads();
-        if (tid < 6) {
+        s2_bar_sync(kBarHGroup, kFusedThreads);
+        if (ht < 6) {
             double v = 0.0;
 #pragma unroll
-            for (int w = 0; w < kFusedThreads / 32; w++) v += s_warp[w][tid];
-            partials[(long long)item * 6 + tid] = v;  // = tile * 18 + channel * 6 + m
+            for (int w = 0; w < kFusedThreads / 32; w++) v += s_warp[w][ht];
+            partials[(long long)item * 6 + ht] = v;  // = tile * 18 + channel * 6 + m
         }
     }
 }
 
-// One launch runs the work items of one mode, so each instance gets the
-// registers of its own mode.
+// Registers per thread of the two warpgroups (setmaxnreg): they add up to the
+// block's launch allotment, 2 x 128 per thread pair, so neither request waits.
+constexpr int kRegsV = 120, kRegsH = 136;
+static_assert(kRegsV + kRegsH == 2 * 128 && kRegsV % 8 == 0 && kRegsH % 8 == 0, "register split");
+
+// Warp-specialized: warpgroup 0 runs the vertical phase of every step,
+// warpgroup 1 the horizontal phase, concurrently, through the double-buffered
+// shared planes.  One launch runs the work items of one mode, so each
+// instance gets the registers of its own mode.
 template <typename ST, int MODE, bool EXPORT = false>
-__global__ void __launch_bounds__(kFusedThreads, 4)
+__global__ void __launch_bounds__(kWsThreads, 2)
     fused_kernel(const DevPair *__restrict__ pairs, const Seg *__restrict__ segs, int nseg, int first_item,
                  int end_item, int *__restrict__ counter, double *__restrict__ partials,
                  MapOut mo = MapOut{nullptr, 0, 0}) {
@@ -762,6 +783,9 @@ __global__ void __launch_bounds__(kFusedThreads, 4)
     __shared__ int s_item;
     __shared__ double s_warp[kFusedThreads / 32][6];
     const int tid = threadIdx.x;
+    const bool vgroup = tid < kFusedThreads;
+    if (vgroup) asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(kRegsV));
+    else asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(kRegsH));
     for (;;) {
         __syncthreads();  // the previous item's readers of s_item, s_warp and the buffers are done
         if (tid == 0) s_item = first_item + atomicAdd(counter, 1);
@@ -770,8 +794,9 @@ __global__ void __launch_bounds__(kFusedThreads, 4)
         if (item >= end_item) break;
         const int tile = item / 3, g = item - 3 * tile;
         const Seg sg = segs[find_seg(segs, nseg, tile)];
-        const DevPair &P = pairs[sg.pair];
-        tile_item<ST, MODE, EXPORT && MODE != TM_REFMOM>(P, sg, tile, g, smb, s_warp, partials, item, mo);
+        const Item<ST> it = decode_item<ST>(pairs[sg.pair], sg, tile, g);
+        if (vgroup) v_item<ST, MODE>(it, smb, tid);
+        else h_item<ST, MODE, EXPORT && MODE != TM_REFMOM>(it, smb, tid - kFusedThreads, s_warp, partials, item, mo);
     }
 }
 
@@ -868,13 +893,13 @@ const double *host_weights() { return kWeights; }
 cudaError_t upload_weights() { return cudaMemcpyToSymbol(c_weight, kWeights, sizeof kWeights); }
 
 size_t fused_smem_bytes() { return (size_t)2 * kBufF2 * sizeof(float2); }
-int fused_threads() { return kFusedThreads; }
+int fused_threads() { return kWsThreads; }
 
 template <typename ST, int MODE, bool EXPORT>
 static cudaError_t fused_attrs() {
     const void *f = (const void *)fused_kernel<ST, MODE, EXPORT>;
-    // the tile pass is limited by registers and shared memory together: ask
-    // for the largest shared-memory carveout so that 4 blocks fit per SM
+    // two blocks of two warpgroups per SM: ask for the largest shared-memory
+    // carveout (the rest is L1)
     cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fused_smem_bytes());
@@ -903,7 +928,7 @@ int fused_blocks_per_sm(int storage) {
     const void *f = storage == ST_F16    ? (const void *)fused_kernel<__half, TM_FULL, false>
                     : storage == ST_BF16 ? (const void *)fused_kernel<__nv_bfloat16, TM_FULL, false>
                                          : (const void *)fused_kernel<float, TM_FULL, false>;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f, kFusedThreads, fused_smem_bytes()) != cudaSuccess) return 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f, kWsThreads, fused_smem_bytes()) != cudaSuccess) return 1;
     return n > 0 ? n : 1;
 }
 
@@ -940,7 +965,7 @@ cudaError_t launch_pyramid(int storage, const DevPair *pairs, int npairs, const 
 template <typename ST, int MODE, bool EXPORT>
 static void fused_go(int grid, size_t sm, cudaStream_t st, const DevPair *pairs, const Seg *segs, int nseg, int fi,
                      int ei, int *counter, double *partials, const MapOut &mo) {
-    fused_kernel<ST, MODE, EXPORT><<<grid, kFusedThreads, sm, st>>>(pairs, segs, nseg, fi, ei, counter, partials, mo);
+    fused_kernel<ST, MODE, EXPORT><<<grid, kWsThreads, sm, st>>>(pairs, segs, nseg, fi, ei, counter, partials, mo);
 }
 
 template <typename ST, bool EXPORT>
