@@ -62,8 +62,9 @@ typedef enum {
 enum {
     /* Default.  Separable 9-tap FIR (the exact closed form of the reference's
      * recursive Gaussian), fused with the error maps in one pass per scale,
-     * f32 arithmetic on block-shifted moments.  Scores within ~1e-4 of the
-     * FP64 oracle. */
+     * f32 arithmetic on block-shifted moments, the SSIM error formed from
+     * the blurred difference of the two images.  Scores within ~3e-5 of
+     * the FP64 oracle. */
     S2_BLUR_FIR = 0,
     /* The reference's own f32 recursive walk (ssimulacra2-kernel blur.rs:95-136),
      * vertical then horizontal, reproduced operation for operation, so that
@@ -193,10 +194,10 @@ s2_status s2_compute_sync_linear_f32(s2_ctx *ctx, const float *ref, size_t ref_p
 
 /* ---- cached reference -------------------------------------------------- */
 /* Replaces set_reference_linear (lib.rs:440-546): keeps the reference's
- * pyramid, XYB and (FIR blur) blurred moments mu1 and sigma11 resident on the
+ * pyramid, XYB and (FIR blur) the blurred reference mean mu1 resident on the
  * device.  compute_with_reference then blurs three planes per channel instead
- * of four; its scores are within 1e-5 of the direct path's (sigma11 and
- * sigma22 are blurred separately instead of as one sum). */
+ * of four; its scores equal the direct path's bit for bit (mu1 is the same
+ * blur of the same plane either way). */
 s2_status s2_set_reference_linear_f32(s2_ctx *ctx, const float *ref, size_t pitch, void *stream);
 s2_status s2_set_reference_srgb8(s2_ctx *ctx, const uint8_t *ref, size_t pitch,
                                  int32_t on_host, void *stream);

@@ -13,7 +13,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "_build", "libssim2_oracle.so")
 
-MODE = {"fp64": 0, "cuda32": 1, "cpu32": 2, "fir32": 3, "fir32c": 4}
+MODE = {"fp64": 0, "cuda32": 1, "cpu32": 2, "fir32": 3}
 RULE = {"cpu": 0, "min8": 1, "all6": 2}
 
 
@@ -191,8 +191,7 @@ class Result:
 
 
 def ssim2_linear(ref, dis, mode="fp64", rule="cpu"):
-    """Full metric from linear RGB (H, W, 3).  mode: fp64 | cuda32 | cpu32 | fir32 |
-    fir32c (fir32 as the cached-reference path computes it)."""
+    """Full metric from linear RGB (H, W, 3).  mode: fp64 | cuda32 | cpu32 | fir32."""
     h, w = ref.shape[:2]
     st = np.zeros(108)
     su = np.zeros(108)

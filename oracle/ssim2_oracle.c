@@ -904,19 +904,23 @@ static inline float fmaxf0(float v) { return v > 0.0f ? v : 0.0f; }
 /* One scale in FIR32 arithmetic (the fused CUDA pass of this repository,
  * csrc/ssim2_kernels.cu fused_kernel).  xr/xd: planar XYB (3 planes of W*H).
  * Tiles of 120 columns x 64-row bands share one shift per channel (the
- * reference XYB at the tile's first column and the band's first row).  The
- * shifted values x', y' (0 outside the image) are blurred by the kernels'
- * 9-tap order, vertical then horizontal: x', y', x'y' and -- direct
- * (cached = 0) -- one plane of x'^2 + y'^2 (both squares rounded first), or
- * -- cached reference (cached = 1) -- x'^2 and y'^2 separately, summed after
- * the blur.
- * Maps are pooled in f32 over 8-pixel segments of a row, then in f64.
- * sums[c*6 + n*3 + m].  With `maps` (9 planes of W*H, [channel][ssim,
- * artifact, detail]) every pixel's error values are stored too. */
-static void score_scale_fir32(const float *xr, const float *xd, int W, int H, double sums[18], float *maps,
-                              int cached) {
+ * reference XYB at the tile's first column and the band's first row):
+ * x' = ref - shift, y' = dis - shift (0 outside the image).  Four planes are
+ * blurred, in the kernels' 9-tap order, vertical then horizontal: x', the
+ * difference e = ref - dis, e^2 and x'y'.  With mu1 = blur(x'),
+ * md = blur(e) = mu1 - mu2, mu2 = mu1 - md, the SSIM terms are
+ *   num_s = 2 (blur(x'y') - mu1 mu2) + C2      (+ the border correction)
+ *   Vd    = blur(e^2) - md^2                   (var1 + var2 - 2 cov)
+ *   den   = Vd + num_s
+ *   d     = (Vd + md^2 num_s) / den           (= 1 - num_m num_s / den)
+ * so the small difference between the two images is blurred as such, not
+ * recovered from the difference of two large moments.  Maps are pooled in
+ * f32 over 8-pixel segments of a row, then in f64.  sums[c*6 + n*3 + m].
+ * With `maps` (9 planes of W*H, [channel][ssim, artifact, detail]) every
+ * pixel's error values are stored too. */
+static void score_scale_fir32(const float *xr, const float *xd, int W, int H, double sums[18], float *maps) {
     const int TC = FIR_TW + 8, TR = FIR_BAND + 8;
-    const int NP = 5; /* x', y', s (cached: x'^2), y'^2 (cached only), xy */
+    const int NP = 4; /* x', e, e^2, x'y' */
     float *P = (float *)malloc((size_t)NP * TC * TR * sizeof(float));
     float *V = (float *)malloc((size_t)NP * TC * FIR_BAND * sizeof(float));
     float *X = (float *)malloc((size_t)2 * TC * FIR_BAND * sizeof(float));
@@ -933,32 +937,31 @@ static void score_scale_fir32(const float *xr, const float *xd, int W, int H, do
                     int y = y0 - 4 + r;
                     for (int k = 0; k < TC; k++) {
                         int x = x0 - 4 + k;
-                        float vx = 0, vy = 0, vs = 0, vyy = 0, vxy = 0;
+                        float vx = 0, ve = 0, vee = 0, vxy = 0;
                         if (x >= 0 && x < W && y >= 0 && y < H) {
-                            vx = a[(size_t)y * W + x] - cv;
-                            vy = b[(size_t)y * W + x] - cv;
-                            vyy = vy * vy;
-                            vs = cached ? vx * vx : vx * vx + vyy;
-                            vxy = vx * vy;
+                            const float ra = a[(size_t)y * W + x], rb = b[(size_t)y * W + x];
+                            vx = ra - cv;
+                            ve = ra - rb;
+                            vee = ve * ve;
+                            vxy = vx * (rb - cv);
                         }
                         size_t o = (size_t)r * TC + k;
                         P[0 * TC * TR + o] = vx;
-                        P[1 * TC * TR + o] = vy;
-                        P[2 * TC * TR + o] = vs;
-                        P[3 * TC * TR + o] = vyy;
-                        P[4 * TC * TR + o] = vxy;
+                        P[1 * TC * TR + o] = ve;
+                        P[2 * TC * TR + o] = vee;
+                        P[3 * TC * TR + o] = vxy;
                     }
                 }
                 for (int r = 0; r < y1 - y0; r++)
                     for (int k = 0; k < TC; k++) {
                         for (int p = 0; p < NP; p++) {
-                            if (p == 3 && !cached) continue;
                             const float *q = P + (size_t)p * TC * TR + k;
                             V[(size_t)p * TC * FIR_BAND + (size_t)r * TC + k] =
                                 fir9f(q[(size_t)(r + 0) * TC], q[(size_t)(r + 1) * TC], q[(size_t)(r + 2) * TC],
                                       q[(size_t)(r + 3) * TC], q[(size_t)(r + 4) * TC], q[(size_t)(r + 5) * TC],
                                       q[(size_t)(r + 6) * TC], q[(size_t)(r + 7) * TC], q[(size_t)(r + 8) * TC]);
                         }
+                        /* raw x' and e of the output row */
                         X[(size_t)0 * TC * FIR_BAND + (size_t)r * TC + k] = P[0 * TC * TR + (size_t)(r + 4) * TC + k];
                         X[(size_t)1 * TC * FIR_BAND + (size_t)r * TC + k] = P[1 * TC * TR + (size_t)(r + 4) * TC + k];
                     }
@@ -971,34 +974,29 @@ static void score_scale_fir32(const float *xr, const float *xd, int W, int H, do
                         for (int j = 0; j < FIR_SEG; j++) {
                             int xx = x0 + c0 + j;
                             if (xx >= W) break;
-                            float o[5];
+                            float o[4];
                             for (int p = 0; p < NP; p++) {
-                                if (p == 3 && !cached) continue;
                                 const float *q = V + (size_t)p * TC * FIR_BAND + (size_t)r * TC + c0 + j;
                                 o[p] = fir9f(q[0], q[1], q[2], q[3], q[4], q[5], q[6], q[7], q[8]);
                             }
-                            /* ss = sigma11 + sigma22 of the shifted values: one blurred plane,
-                             * or (cached reference) the sum of the two blurred planes */
-                            float m1 = o[0], m2 = o[1], s12 = o[4];
-                            float ss = cached ? o[2] + o[3] : o[2];
+                            float m1 = o[0], md = o[1], ed2 = o[2], s12 = o[3];
+                            float m2 = m1 - md;
                             float xp = X[(size_t)r * TC + c0 + j + 4];
-                            float yp = X[(size_t)TC * FIR_BAND + (size_t)r * TC + c0 + j + 4];
+                            float ep = X[(size_t)TC * FIR_BAND + (size_t)r * TC + c0 + j + 4];
                             float bh = border_gain_f(xx, W);
                             float corr = (bh == 1.0f && bv == 1.0f) ? 0.0f : (float)(1.0 - (double)bh * (double)bv);
                             float kk = cv * corr;
-                            float e = cv - kk;
-                            float h = (m1 + m2) + e;
-                            float md = m1 - m2;
-                            float t2 = m1 + m1, k2 = kk + kk;
-                            /* w2 = ss - 2 m1 m2 - md^2, c2 = 2 s12 - 2 m1 m2 (see maps_px) */
-                            float w2 = fmaf(k2, h, fmaf(-md, md, fmaf(-t2, m2, ss)));
-                            float c2 = fmaf(k2, h, fmaf(-t2, m2, s12 + s12));
-                            float den = w2 + C2;
-                            float num_m = fmaf(-md, md, 1.0f);
-                            float num_s = c2 + C2;
-                            float d = fmaxf0(eng_div(fmaf(-num_m, num_s, den), den));
-                            float aa = fabsf((xp - m1) + kk);
-                            float bb = fabsf((yp - m2) + kk);
+                            float h = (m1 + m2) + (cv - kk);
+                            float cov = fmaf(kk, h, fmaf(-m1, m2, s12));
+                            float num_s = fmaf(2.0f, cov, C2);
+                            float vd = fmaf(-md, md, ed2);
+                            float den = vd + num_s;
+                            float nn = fmaf(md * md, num_s, vd);
+                            float d = fmaxf0(eng_div(nn, den));
+                            float t1 = xp - m1, u = ep - md;
+                            float t2 = t1 - u; /* y' - mu2 */
+                            float aa = fabsf(t1 + kk);
+                            float bb = fabsf(t2 + kk);
                             float d1 = eng_div(bb - aa, 1.0f + aa);
                             float v[3] = {d, fmaxf0(d1), fmaxf0(-d1)};
                             if (maps)
@@ -1062,8 +1060,8 @@ static int ssim2_linear_impl(const float *ref, const float *dis, int w, int h, i
         to_planar_xyb_f32(r, n, pr);
         to_planar_xyb_f32(d, n, pd);
         double sst[18], ssu[18];
-        if (mode == OR_MODE_FIR32 || mode == OR_MODE_FIR32C) {
-            score_scale_fir32(pr, pd, cw, ch, ssu, (maps && s == maps_scale) ? maps : NULL, mode == OR_MODE_FIR32C);
+        if (mode == OR_MODE_FIR32) {
+            score_scale_fir32(pr, pd, cw, ch, ssu, (maps && s == maps_scale) ? maps : NULL);
             double inv = 1.0 / (double)n;
             for (int c = 0; c < 3; c++)
                 for (int k = 0; k < 3; k++) {

@@ -26,15 +26,12 @@
  *   OR_MODE_FIR32    f32 restatement of the fused CUDA pass of this
  *                    repository: the separable 9-tap FIR in its operation
  *                    order (vertical taps, then horizontal taps) on values
- *                    shifted by one anchor per 120-column x 64-row block,
- *                    four blurred planes (x', y', x'^2 + y'^2, x'y'), the
- *                    error maps in the kernels' form, f32 sums over 8-pixel
- *                    row segments.  Used to check the device kernels.
- *   OR_MODE_FIR32C   FIR32 as the cached-reference path computes it: the
- *                    reference's blurred x' and x'^2 come from its cache and
- *                    the candidate blurs y', y'^2 and x'y', so
- *                    sigma11 + sigma22 is the sum of separately blurred
- *                    planes.
+ *                    shifted by one anchor per 120-column x 64-row block;
+ *                    four blurred planes -- the shifted reference x', the
+ *                    difference e = ref - dis, e^2 and x'y' -- and the SSIM
+ *                    error formed from the blurred difference (no
+ *                    cancellation between large moments); f32 sums over
+ *                    8-pixel row segments.  Used to check the device kernels.
  *
  * Pyramid stop rules (which scales are scored):
  *   OR_SCALES_CPU    cpu.rs:359-361 -- before producing scale s>0, stop if
@@ -59,7 +56,7 @@
 extern "C" {
 #endif
 
-enum { OR_MODE_FP64 = 0, OR_MODE_CUDA32 = 1, OR_MODE_CPU32 = 2, OR_MODE_FIR32 = 3, OR_MODE_FIR32C = 4 };
+enum { OR_MODE_FP64 = 0, OR_MODE_CUDA32 = 1, OR_MODE_CPU32 = 2, OR_MODE_FIR32 = 3 };
 enum { OR_SCALES_CPU = 0, OR_SCALES_MIN8 = 1, OR_SCALES_ALL6 = 2 };
 
 /* Recursive-Gaussian constants (f32, as the reference kernels use them) and

@@ -176,11 +176,11 @@ def test_error_paths(tmb, cuda):
 
 
 def test_cached_reference_equals_direct(tmb, oracle, cuda):
-    """The cached path reads the reference's blurred mu1 and sigma11 and blurs
-    sigma22 on its own: every statistic against the oracle's restatement of
-    that arithmetic (fir32c), and the score within 1e-5 of the direct path
-    (the reference's own bar for cached == direct is 1e-4,
-    ssim2-gpu/tests/parity_lock.rs:160-277)."""
+    """The cached path reads the reference's blurred mu1 and blurs the three
+    other planes: the score equals the direct path's bit for bit (the
+    reference's own bar for cached == direct is 1e-4,
+    ssim2-gpu/tests/parity_lock.rs:160-277), every statistic against the
+    oracle's fir32 restatement."""
     ref, _ = synth.srgb_pair(200, 150, 31)
     s = tmb.Ssimulacra2(200, 150)
     assert not s.has_reference()
@@ -191,8 +191,8 @@ def test_cached_reference_equals_direct(tmb, oracle, cuda):
         direct = s.compute_from_cpu_srgb_sync(ref, dis)
         s.compute_with_reference_srgb(dis, on_host=True)
         cached, stats, _ = s.get_result()
-        assert abs(direct - cached) < 1e-5
-        mirror = oracle.ssim2_srgb8(ref, dis, "fir32c")
+        assert direct == cached
+        mirror = oracle.ssim2_srgb8(ref, dis, "fir32")
         assert_stats_close(stats, mirror.stats, what="cached q%d" % q)
         assert abs(cached - mirror.score) < SCORE_TOL
     # the reference compared with itself through the cache scores exactly 100

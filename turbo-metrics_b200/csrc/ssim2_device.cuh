@@ -73,9 +73,8 @@ struct DevPair {
     int lab_levels;          // 0: no Lab output
     int prep_levels;         // levels the prep pass builds (XYB and Lab)
     // A cached reference's blurred moments per scale (TM_REFMOM writes them,
-    // TM_CAND reads them): 6 f32 planes of pitch lp[s] -- the blurred
-    // shifted reference XYB (mu1) of channels X, Y, B, then its blurred
-    // square (sigma11) of X, Y, B.
+    // TM_CAND reads them): 3 f32 planes of pitch lp[s] -- the blurred
+    // shifted reference XYB (mu1) of channels X, Y, B.
     float *mom[kScales];
 };
 

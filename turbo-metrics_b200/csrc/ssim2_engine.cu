@@ -608,15 +608,13 @@ s2_status s2_compute_sync_linear_f32(s2_ctx *ctx, const float *ref, size_t ref_p
 
 // ---- cached reference ----------------------------------------------------
 // set_reference converts the reference once and keeps on the device, for
-// every scale, its XYB planes and -- with the FIR blur -- its blurred moments
-// mu1 and sigma11 per channel (set_reference_linear, ssimulacra2-cuda/src/
-// lib.rs:440-546, caches the reference's XYB, mu1_t and sigma11_t the same
-// way).  compute_with_reference converts only the distorted image and blurs
-// three planes (y', y'^2, x'y') instead of four, reading mu1 and sigma11 from
-// the cache; its sum sigma11 + sigma22 is of separately blurred planes, so
-// scores are within 1e-5 of the direct path's (the oracle's fir32c mode
-// restates this arithmetic).  Like the reference, set_reference returns after
-// the device work is done.
+// every scale, its XYB planes and -- with the FIR blur -- its blurred mean
+// mu1 per channel (set_reference_linear, ssimulacra2-cuda/src/lib.rs:440-546,
+// caches the reference's XYB, mu1_t and sigma11_t in the same spirit).
+// compute_with_reference converts only the distorted image and blurs three
+// planes (e, e^2, x'y') instead of four, reading mu1 from the cache: the same
+// values the direct path computes, so the scores are equal bit for bit.
+// Like the reference, set_reference returns after the device work is done.
 static s2_status set_ref(s2_ctx *ctx, const s2_pair_desc &d, void *stream) {
     size_t off[kScales], moff[kScales];
     const int ns = s2_num_scales_rule(ctx->w, ctx->h, ctx->eng.scale_rule);

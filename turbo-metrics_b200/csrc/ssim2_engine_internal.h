@@ -128,14 +128,14 @@ inline size_t s2_image_levels_layout(uint32_t w, uint32_t h, int ns, size_t esiz
 }
 
 // Byte layout of a cached reference's blurred moments (all scored scales):
-// per scale 6 f32 planes of the XYB planes' pitch (mu1 of X, Y, B, then
-// sigma11 of X, Y, B), 256-byte aligned.
+// per scale 3 f32 planes of the XYB planes' pitch (the blurred shifted
+// reference mu1 of X, Y, B), 256-byte aligned.
 inline size_t s2_moment_layout(uint32_t w, uint32_t h, int ns, size_t off[kScales]) {
     size_t o = 0;
     uint64_t cw = w, ch = h;
     for (int s = 0; s < ns; s++) {
         off[s] = o;
-        o += s2_align_up((size_t)6 * s2_align_up((size_t)cw, 64) * ch * sizeof(float), 256);
+        o += s2_align_up((size_t)3 * s2_align_up((size_t)cw, 64) * ch * sizeof(float), 256);
         cw = (cw + 1) / 2;
         ch = (ch + 1) / 2;
     }

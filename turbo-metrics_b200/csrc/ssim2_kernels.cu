@@ -9,10 +9,10 @@
 //                    (ssimulacra2-cuda-kernel/src/downscale.rs:4-35, srgb.rs,
 //                    xyb.rs)
 //   fused_kernel     persistent; each work item is one channel of a tile of
-//                    56 columns x `strip_rows` rows at one scale of one pair.
-//                    Walking down the tile it forms the five blurred inputs on
-//                    band-shifted values, runs the vertical 9-tap FIR in
-//                    registers, then every 9 rows the horizontal FIR, the
+//                    120 columns x `strip_rows` rows at one scale of one pair.
+//                    Walking down the tile 8 rows per step it forms the four
+//                    blurred inputs on band-shifted values, runs the vertical
+//                    9-tap FIR in registers, then the horizontal FIR, the
 //                    SSIM / artifact / detail-loss maps and their L1/L4 sums
 //                    from shared memory.  Only 6 pooled sums per item leave
 //                    the SM.  (blur.rs, error_maps.rs, lib.rs:862-1016)
@@ -22,8 +22,9 @@
 // The blur is the exact closed form of the reference's recursive Gaussian:
 // the truncated-cosine recursion of blur.rs equals, in exact arithmetic, a
 // symmetric 9-tap FIR with zero padding.  Moments are taken of values shifted
-// by one reference XYB sample per (56-column tile, 63-row band), which removes
-// most of the f32 cancellation in sigma - mu^2; the shift is undone
+// by one reference XYB sample per (120-column tile, 64-row band), and the
+// SSIM error is formed from the blurred difference of the two images, which
+// removes the f32 cancellation in sigma - mu^2; the shift is undone
 // algebraically (including at image borders, where the blur of a constant is
 // not the constant).
 #include "ssim2_device.cuh"
@@ -32,7 +33,7 @@ namespace s2 {
 
 // Shared memory of fused_kernel (one CTA = one channel of a tile): two
 // buffers (step parity), each three float2 planes of kStep rows x kRS
-// columns -- plane 0 and 1 the vertical FIRs, plane 2 the raw (x', y') of the
+// columns -- plane 0 and 1 the vertical FIRs, plane 2 the raw (x', e) of the
 // output rows.  A horizontal task reads 16-byte words of one row; the 8
 // lanes of a load phase take the same segment of rows 0..7, whose starts are
 // kRS * 8 = 1040 bytes apart: 65 16-byte groups, odd, so the 8 rows fall in
@@ -347,18 +348,23 @@ __global__ void __launch_bounds__(256, 2) prep_kernel(const DevPair *__restrict_
 //               and their sums and fourth-power sums, in f32 over the
 //               segment, then in f64 per thread.
 //
+// What is blurred: with x' = ref - anchor, y' = dis - anchor and the
+// difference e = ref - dis, the four planes x', e, e^2 and x'y'.  Then
+// mu1 = blur(x'), md = blur(e) = mu1 - mu2, and the SSIM error
+//   d = 1 - num_m num_s / den = (Vd + md^2 num_s) / (Vd + num_s),
+//   Vd = blur(e^2) - md^2 = var1 + var2 - 2 cov,  num_s = 2 cov + C2,
+// is formed from the blurred difference itself: for near-identical images
+// no small quantity is recovered from the difference of two large moments,
+// which f32 cannot do to the metric's precision.
+//
 // Modes (one per launch; the plan numbers each mode's tiles contiguously):
-//   TM_FULL    a pair scored from both images' XYB: rings A = (x', y') and
-//              B = (x'^2 + y'^2, x'y') -- SSIM needs sigma11 and sigma22
-//              only through their sum (its denominator is sigma11 - mu1^2 +
-//              sigma22 - mu2^2 + C2), so four planes are blurred, not five,
-//              and they pair up into two f32x2 FIRs.
-//   TM_REFMOM  a cached reference: blurs A = (x', x'^2) and stores the
-//              blurred mu1 and sigma11 to the pair's moment planes (mom[s]:
-//              mu1 of the three channels, then sigma11), no maps.
-//   TM_CAND    a candidate against a cached reference: blurs (y', x'y') in
-//              f32x2 and y'^2 alone (three planes), reads mu1 and sigma11
-//              from the moment planes, and sums sigma11 + sigma22.
+//   TM_FULL    a pair scored from both images' XYB: rings A = (x', e) and
+//              B = (e^2, x'y'), two f32x2 FIRs.
+//   TM_REFMOM  a cached reference: blurs x' and stores mu1 to the pair's
+//              moment planes (mom[s], channels X, Y, B), no maps.
+//   TM_CAND    a candidate against a cached reference: blurs (e, x'y') in
+//              f32x2 and e^2 alone, and reads mu1 from the moment planes --
+//              the same values, to the bit, as TM_FULL computes.
 // The shared buffers are double buffered by step parity: step i's horizontal
 // phase reads buffer i % 2 while step i+1's vertical phase writes the other,
 // so one barrier per step orders them.
@@ -383,30 +389,30 @@ __device__ __forceinline__ float fir9s(float a0, float a1, float a2, float a3, f
 
 // Register rings of one vertical column (which are used depends on the mode).
 struct Rings {
-    float2 a[16];  // FULL (x', y'); REFMOM (x', x'^2); CAND (y', x'y')
-    float2 b[16];  // FULL (x'^2 + y'^2, x'y')
-    float c[16];   // CAND y'^2
-    float x[16];   // CAND x'
+    float2 a[16];  // FULL (x', e); CAND (e, x'y')
+    float2 b[16];  // FULL (e^2, x'y')
+    float c[16];   // CAND e^2; REFMOM x'
 };
 
-// Shift one input row into ring slot `sl`.
+// Shift one input row into ring slot `sl` (vr, vd: the reference and
+// distorted samples; cg: the anchor).  Outside the image both are the anchor,
+// so every plane is 0 there.
 template <int MODE>
-__device__ __forceinline__ void ring_in(Rings &R, int sl, float vr, float vd, float2 ncg) {
+__device__ __forceinline__ void ring_in(Rings &R, int sl, float vr, float vd, float cg) {
+    const float xp = vr - cg;
+    if (MODE == TM_REFMOM) {
+        R.c[sl] = xp;
+        return;
+    }
+    const float e = vr - vd;
+    const float xy = __fmul_rn(xp, vd - cg);  // products rounded on their own
+    const float ee = __fmul_rn(e, e);
     if (MODE == TM_FULL) {
-        // both squares rounded before the sum: for x' = y' the first lane of B
-        // is exactly twice the second
-        const float2 a = s2_padd(make_float2(vr, vd), ncg);
-        const float2 q = s2_pmul(a, a);
-        R.a[sl] = a;
-        R.b[sl] = make_float2(q.x + q.y, a.x * a.y);
-    } else if (MODE == TM_REFMOM) {
-        const float xp = vr + ncg.x;
-        R.a[sl] = make_float2(xp, xp * xp);
+        R.a[sl] = make_float2(xp, e);
+        R.b[sl] = make_float2(ee, xy);
     } else {
-        const float2 a = s2_padd(make_float2(vr, vd), ncg);
-        R.a[sl] = make_float2(a.y, a.x * a.y);
-        R.c[sl] = a.y * a.y;
-        R.x[sl] = a.x;
+        R.a[sl] = make_float2(e, xy);
+        R.c[sl] = ee;
     }
 }
 
@@ -415,10 +421,12 @@ __device__ __forceinline__ void ring_in(Rings &R, int sl, float vr, float vd, fl
 // slots S0 + 8 .. S0 + 15 (mod 16); output row k reads slots S0 + k ..
 // S0 + k + 8 and is stored to row k of the buffer: plane 0 the FIR of ring
 // a, plane 1 that of ring b (FULL) or of ring c as floats (CAND), plane 2
-// the raw (x', y') of the output row (FULL, CAND).
+// the raw (x', e) of the output row (FULL) or its raw e as floats (CAND; the
+// horizontal phase reads x' from the reference plane); REFMOM stores the FIR
+// of ring c to plane 0 as floats.
 template <typename ST, int MODE, int S0>
 __device__ __forceinline__ void v_step(Rings &R, const ST *__restrict__ xr, const ST *__restrict__ xd, long long lp,
-                                       int x, bool colin, int ybase, int H, int nr, float cg, float2 ncg,
+                                       int x, bool colin, int ybase, int H, int nr, float cg,
                                        float2 *__restrict__ buf, int col) {
     float lr[kStep], ld[kStep];
 #pragma unroll
@@ -431,20 +439,26 @@ __device__ __forceinline__ void v_step(Rings &R, const ST *__restrict__ xr, cons
 #pragma unroll
     for (int k = 0; k < kStep; k++) {
         if (k < nr) {
-            ring_in<MODE>(R, (S0 + 8 + k) & 15, lr[k], ld[k], ncg);
+            ring_in<MODE>(R, (S0 + 8 + k) & 15, lr[k], ld[k], cg);
 #define S2_R(a, j) a[(S0 + k + (j)) & 15]
-            buf[k * kRS + col] = fir9p(S2_R(R.a, 0), S2_R(R.a, 1), S2_R(R.a, 2), S2_R(R.a, 3), S2_R(R.a, 4),
-                                       S2_R(R.a, 5), S2_R(R.a, 6), S2_R(R.a, 7), S2_R(R.a, 8));
+            if (MODE == TM_REFMOM) {
+                ((float *)buf)[k * 2 * kRS + col] =
+                    fir9s(S2_R(R.c, 0), S2_R(R.c, 1), S2_R(R.c, 2), S2_R(R.c, 3), S2_R(R.c, 4), S2_R(R.c, 5),
+                          S2_R(R.c, 6), S2_R(R.c, 7), S2_R(R.c, 8));
+            } else {
+                buf[k * kRS + col] = fir9p(S2_R(R.a, 0), S2_R(R.a, 1), S2_R(R.a, 2), S2_R(R.a, 3), S2_R(R.a, 4),
+                                           S2_R(R.a, 5), S2_R(R.a, 6), S2_R(R.a, 7), S2_R(R.a, 8));
+            }
             if (MODE == TM_FULL) {
                 buf[kPlaneF2 + k * kRS + col] = fir9p(S2_R(R.b, 0), S2_R(R.b, 1), S2_R(R.b, 2), S2_R(R.b, 3),
                                                       S2_R(R.b, 4), S2_R(R.b, 5), S2_R(R.b, 6), S2_R(R.b, 7),
                                                       S2_R(R.b, 8));
-                buf[2 * kPlaneF2 + k * kRS + col] = S2_R(R.a, 4);
+                buf[2 * kPlaneF2 + k * kRS + col] = S2_R(R.a, 4);  // raw (x', e)
             } else if (MODE == TM_CAND) {
                 ((float *)(buf + kPlaneF2))[k * 2 * kRS + col] =
                     fir9s(S2_R(R.c, 0), S2_R(R.c, 1), S2_R(R.c, 2), S2_R(R.c, 3), S2_R(R.c, 4), S2_R(R.c, 5),
                           S2_R(R.c, 6), S2_R(R.c, 7), S2_R(R.c, 8));
-                buf[2 * kPlaneF2 + k * kRS + col] = make_float2(S2_R(R.x, 4), S2_R(R.a, 4).x);
+                ((float *)(buf + 2 * kPlaneF2))[k * 2 * kRS + col] = S2_R(R.a, 4).x;  // raw e
             }
 #undef S2_R
         }
@@ -499,38 +513,33 @@ __device__ __forceinline__ void add_maps(TaskSums &t, float d, float art, float 
     t.f4_ad = s2_pfma(q2, q2, t.f4_ad);
 }
 
-// Error maps of one pixel.  m = (mu1, mu2) and s = (sigma11 + sigma22,
-// sigma12) of the shifted values, r = (x', y').  kk = anchor * (1 - border
-// gain): the correction of the shifted moments at the image borders (0
-// inside).  With the anchor c and the gain g the true moments are
-// mu = m + c g and sigma = s + 2 c m + c^2 g, so
-//   sigma11 - mu1^2 + sigma22 - mu2^2 = w2 + 2 kk h   and
-//   2 (sigma12 - mu1 mu2) = c2 + 2 kk h,
-// with w2 = s.x - 2 mu1 mu2 - (mu1 - mu2)^2, c2 = 2 s.y - 2 mu1 mu2,
-// e = c - kk = c g and h = (mu1 + mu2) + e.  For identical images
-// (x' = y') s.x is exactly 2 s.y and mu1 = mu2, so w2 equals c2 and the SSIM
-// error is 0.
+// Error maps of one pixel.  m = (mu1, md) and s = (blur(e^2), blur(x'y')),
+// r = the raw (x', e) of the pixel.  kk = anchor * (1 - border gain): the
+// correction of the shifted moments at the image borders (0 inside).  With
+// the anchor c and the gain g the true means are mu = m + c g and
+// sigma12 - mu1 mu2 = cov + kk h, cov = blur(x'y') - mu1 mu2,
+// h = (mu1 + mu2) + ce, ce = c - kk = c g; md, blur(e) and blur(e^2) need
+// no correction (e is the same with and without the shift).  For identical
+// images e = 0, so Vd, md and the SSIM error are exactly 0.
 template <bool BORDER>
-__device__ __forceinline__ void maps_px(float2 m, float2 s, float2 r, float kk, float e, float &d, float &art,
+__device__ __forceinline__ void maps_px(float2 m, float2 s, float2 r, float kk, float ce, float &d, float &art,
                                         float &det) {
-    const float m1 = m.x, m2 = m.y;
-    const float md = m1 - m2;
-    const float t2 = m1 + m1;
-    float w2 = fmaf(-md, md, fmaf(-t2, m2, s.x));
-    float c2 = fmaf(-t2, m2, s.y + s.y);
+    const float m1 = m.x, md = m.y;
+    const float m2 = m1 - md;
+    float cov = fmaf(-m1, m2, s.y);
+    if (BORDER) cov = fmaf(kk, (m1 + m2) + ce, cov);
+    const float num_s = fmaf(2.0f, cov, kC2);
+    const float vd = fmaf(-md, md, s.x);
+    const float den = vd + num_s;
+    const float nn = fmaf(md * md, num_s, vd);
+    d = fmaxf(s2_div(nn, den), 0.0f);
+    const float2 t = s2_pfma(m, s2_f2(-1.0f), r);  // (x' - mu1, e - md)
+    float t1 = t.x, t2 = t.x - t.y;              // x' - mu1, y' - mu2
     if (BORDER) {
-        const float h = (m1 + m2) + e;
-        const float k2 = kk + kk;
-        w2 = fmaf(k2, h, w2);
-        c2 = fmaf(k2, h, c2);
+        t1 = t1 + kk;
+        t2 = t2 + kk;
     }
-    const float den = w2 + kC2;
-    const float num_m = fmaf(-md, md, 1.0f);
-    const float num_s = c2 + kC2;
-    d = fmaxf(s2_div(fmaf(-num_m, num_s, den), den), 0.0f);
-    float2 t = s2_pfma(m, s2_f2(-1.0f), r);  // (x' - mu1, y' - mu2)
-    if (BORDER) t = make_float2(t.x + kk, t.y + kk);
-    const float aa = fabsf(t.x), bb = fabsf(t.y);
+    const float aa = fabsf(t1), bb = fabsf(t2);
     const float d1 = s2_div(bb - aa, 1.0f + aa);
     art = fmaxf(d1, 0.0f);
     det = fmaxf(-d1, 0.0f);
@@ -546,32 +555,50 @@ struct ItemGeo {
     int x0, y0, W, H, g;
     float cg;
     long long lp, plane;
-    float *mom;  // the moment planes of this scale (REFMOM, CAND)
+    float *mom;       // the moment planes of this scale (REFMOM, CAND)
+    const void *xr;   // this channel's reference plane (storage type)
 };
 
+__device__ __forceinline__ void add_task(Acc6 &acc, const TaskSums &ts) {
+    acc.v[0] += (double)ts.fs_d;
+    acc.v[1] += (double)ts.fs_ad.x;
+    acc.v[2] += (double)ts.fs_ad.y;
+    acc.v[3] += (double)ts.f4_d;
+    acc.v[4] += (double)ts.f4_ad.x;
+    acc.v[5] += (double)ts.f4_ad.y;
+}
+
+// The same into per-thread sums kept in shared memory (a[m * kFusedThreads]).
+__device__ __forceinline__ void add_task(double *a, const TaskSums &ts) {
+    a[0] += (double)ts.fs_d;
+    a[kFusedThreads] += (double)ts.fs_ad.x;
+    a[2 * kFusedThreads] += (double)ts.fs_ad.y;
+    a[3 * kFusedThreads] += (double)ts.f4_d;
+    a[4 * kFusedThreads] += (double)ts.f4_ad.x;
+    a[5 * kFusedThreads] += (double)ts.f4_ad.y;
+}
+
 // Horizontal phase of one step (output rows r0 .. r0 + nr - 1 of the tile):
-// this thread's task, row t_r, segment t_s.
-template <int MODE, bool EXPORT>
+// this thread's task, row t_r, segment t_s; its sums are added to acc.
+template <typename ST, int MODE, bool EXPORT, typename ACC>
 __device__ __forceinline__ void h_step(const float2 *__restrict__ buf, int r0, int nr, int t_r, int t_s, bool t_on,
-                                       const ItemGeo &G, Acc6 &acc, const MapOut &mo) {
+                                       const ItemGeo &G, ACC &&acc, const MapOut &mo) {
     if (!t_on || t_r >= nr) return;
     const int c0 = t_s * kSegW;  // first output column of the task (tile coordinates)
     const int xc = G.x0 + c0;
     if (xc >= G.W) return;
     const int y = G.y0 + r0 + t_r;
     if (MODE == TM_REFMOM) {
-        // blurred (mu1, sigma11) of 4 pixels at a time, 16-byte stores (a
-        // 4-pixel group starting inside the image stays inside the padded row)
+        // blurred mu1 of 4 pixels at a time, 16-byte stores (a 4-pixel group
+        // starting inside the image stays inside the padded row)
         float *mu = G.mom + G.g * G.plane + (long long)y * G.lp;
-        float *sg = G.mom + (3 + G.g) * G.plane + (long long)y * G.lp;
 #pragma unroll 1
         for (int half = 0; half < kSegW / 4; half++) {
             const int cc = c0 + 4 * half;
             if (G.x0 + cc >= G.W) break;
-            float2 mA[4];
-            h_fir4(buf + t_r * kRS + cc, mA);
-            *(float4 *)(mu + G.x0 + cc) = make_float4(mA[0].x, mA[1].x, mA[2].x, mA[3].x);
-            *(float4 *)(sg + G.x0 + cc) = make_float4(mA[0].y, mA[1].y, mA[2].y, mA[3].y);
+            float m1[4];
+            h_fir4s((const float *)buf + t_r * 2 * kRS + cc, m1);
+            *(float4 *)(mu + G.x0 + cc) = make_float4(m1[0], m1[1], m1[2], m1[3]);
         }
         return;
     }
@@ -584,25 +611,29 @@ __device__ __forceinline__ void h_step(const float2 *__restrict__ buf, int r0, i
         const float2 *pa = buf + t_r * kRS + cc;
         float2 mA[4], mB[4], rw[4];
         if (MODE == TM_FULL) {
-            h_fir4(pa, mA);
-            h_fir4(pa + kPlaneF2, mB);  // (sigma11 + sigma22, sigma12)
+            h_fir4(pa, mA);               // (mu1, md)
+            h_fir4(pa + kPlaneF2, mB);    // (blur(e^2), blur(x'y'))
         } else {
             if (G.x0 + cc >= G.W) break;
             float2 ma[4];
-            float s22[4];
-            h_fir4(pa, ma);  // (mu2, sigma12)
-            h_fir4s((const float *)(buf + kPlaneF2) + t_r * 2 * kRS + cc, s22);
-            const long long o = (long long)y * G.lp + G.x0 + cc;
-            const float4 mu1 = *(const float4 *)(G.mom + G.g * G.plane + o);
-            const float4 s11 = *(const float4 *)(G.mom + (3 + G.g) * G.plane + o);
-            const float m1v[4] = {mu1.x, mu1.y, mu1.z, mu1.w}, s1v[4] = {s11.x, s11.y, s11.z, s11.w};
+            float ee[4];
+            h_fir4(pa, ma);  // (md, blur(x'y'))
+            h_fir4s((const float *)(buf + kPlaneF2) + t_r * 2 * kRS + cc, ee);
+            const float4 mu1 = *(const float4 *)(G.mom + G.g * G.plane + (long long)y * G.lp + G.x0 + cc);
+            const float m1v[4] = {mu1.x, mu1.y, mu1.z, mu1.w};
+            const float4 e4 = *(const float4 *)((const float *)(buf + 2 * kPlaneF2) + t_r * 2 * kRS + cc + 4);
+            const float ev[4] = {e4.x, e4.y, e4.z, e4.w};
+            const ST *xr = (const ST *)G.xr + (long long)y * G.lp + G.x0 + cc;
 #pragma unroll
             for (int j = 0; j < 4; j++) {
                 mA[j] = make_float2(m1v[j], ma[j].x);
-                mB[j] = make_float2(s1v[j] + s22[j], ma[j].y);
+                mB[j] = make_float2(ee[j], ma[j].y);
+                // the raw x' of the pixel (0 beyond the image's last column)
+                const float xp = G.x0 + cc + j < G.W ? ld_store<ST>(xr + j) - G.cg : 0.0f;
+                rw[j] = make_float2(xp, ev[j]);
             }
         }
-        {
+        if (MODE == TM_FULL) {
             const float4 *q = (const float4 *)(pa + 2 * kPlaneF2 + 4);
             const float4 t0 = q[0], t1 = q[1];
             rw[0] = make_float2(t0.x, t0.y);
@@ -644,26 +675,10 @@ __device__ __forceinline__ void h_step(const float2 *__restrict__ buf, int r0, i
             }
         }
     }
-    acc.v[0] += (double)ts.fs_d;
-    acc.v[1] += (double)ts.fs_ad.x;
-    acc.v[2] += (double)ts.fs_ad.y;
-    acc.v[3] += (double)ts.f4_d;
-    acc.v[4] += (double)ts.f4_ad.x;
-    acc.v[5] += (double)ts.f4_ad.y;
+    add_task(acc, ts);
 }
 
-// Named barriers of the two warpgroups (0 is __syncthreads): FULL[b] -- the
-// vertical group has written buffer b, EMPTY[b] -- the horizontal group has
-// read it; the horizontal group's own barrier for its reduction.
-constexpr int kBarFull0 = 1, kBarEmpty0 = 3, kBarHGroup = 5;
-constexpr int kWsThreads = 2 * kFusedThreads;  // vertical warpgroup + horizontal warpgroup
-
-__device__ __forceinline__ void s2_bar_sync(int id, int n) { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory"); }
-__device__ __forceinline__ void s2_bar_arrive(int id, int n) {
-    asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(n) : "memory");
-}
-
-// The geometry of one work item, decoded alike by both warpgroups.
+// The geometry of one work item.
 template <typename ST>
 struct Item {
     ItemGeo G;
@@ -690,102 +705,84 @@ __device__ __forceinline__ Item<ST> decode_item(const DevPair &P, const Seg &sg,
     G.mom = P.mom[s];
     it.xr = (const ST *)P.lvl[0][s] + g * G.plane;
     it.xd = (const ST *)P.lvl[1][s] + g * G.plane;
+    G.xr = it.xr;
     // anchor: reference XYB of channel g at the tile's first column, band start
     G.cg = ld_store<ST>(it.xr + (long long)((G.y0 / kBand) * kBand) * G.lp + G.x0);
     return it;
 }
 
-// Vertical warpgroup: one work item.  Before it overwrites buffer b at step
-// st >= 2 it waits until the horizontal group has read that buffer (step
-// st - 2); after writing it, it signals FULL[b].
-template <typename ST, int MODE>
-__device__ __forceinline__ void v_item(const Item<ST> &it, float2 *smb, int col) {
+constexpr int kTileThreads = kFusedThreads;
+
+// One warpgroup does both phases of a step in turn: the vertical phase of
+// step st to buffer st & 1, a barrier, then the horizontal phase; buffer b is
+// rewritten two steps later, after the barrier of the step in between.
+template <typename ST, int MODE, bool EXPORT>
+__device__ __forceinline__ void flat_item(const Item<ST> &it, float2 *smb, int tid, double *s_acc,
+                                          double (*s_warp)[6], double *__restrict__ partials, int item,
+                                          const MapOut &mo) {
     const ItemGeo &G = it.G;
     const float cg = G.cg;
-    const float2 ncg = make_float2(-cg, -cg);
-    const int x = G.x0 - 4 + col;
+    const int x = G.x0 - 4 + tid;
     const bool colin = x >= 0 && x < G.W;
+    const int t_r = tid % kStep, t_s = tid / kStep;
+    const bool t_on = tid < kTasks;
     Rings R;
-    // prime ring slots 0..7 with input rows y0 - 4 .. y0 + 3
 #pragma unroll
     for (int k = 0; k < 8; k++) {
         const int y = G.y0 - 4 + k;
         const bool in = colin && y >= 0 && y < G.H;
         const float lr = in ? ld_store<ST>(it.xr + (long long)y * G.lp + x) : cg;
         const float ld = (MODE != TM_REFMOM && in) ? ld_store<ST>(it.xd + (long long)y * G.lp + x) : cg;
-        ring_in<MODE>(R, k, lr, ld, ncg);
+        ring_in<MODE>(R, k, lr, ld, cg);
     }
+    // this thread's sums live in shared memory (s_acc[m * kFusedThreads +
+    // tid]), out of the registers that the vertical rings need
+    double *acc = s_acc + tid;
+#pragma unroll
+    for (int m = 0; m < 6; m++) acc[m * kFusedThreads] = 0.0;
     float2 *buf0 = smb, *buf1 = smb + kBufF2;
     for (int st = 0; st < it.nsteps; st += 2) {
         const int r0 = st * kStep;
-        if (st >= 2) s2_bar_sync(kBarEmpty0, kWsThreads);
-        v_step<ST, MODE, 0>(R, it.xr, it.xd, G.lp, x, colin, G.y0 + r0 + 4, G.H, min(kStep, it.rows_out - r0), cg,
-                            ncg, buf0, col);
-        s2_bar_arrive(kBarFull0, kWsThreads);
+        const int nr0 = min(kStep, it.rows_out - r0);
+        v_step<ST, MODE, 0>(R, it.xr, it.xd, G.lp, x, colin, G.y0 + r0 + 4, G.H, nr0, cg, buf0, tid);
+        __syncthreads();
+        h_step<ST, MODE, EXPORT>(buf0, r0, nr0, t_r, t_s, t_on, G, acc, mo);
         if (st + 1 < it.nsteps) {
             const int r1 = r0 + kStep;
-            if (st + 1 >= 2) s2_bar_sync(kBarEmpty0 + 1, kWsThreads);
-            v_step<ST, MODE, 8>(R, it.xr, it.xd, G.lp, x, colin, G.y0 + r1 + 4, G.H, min(kStep, it.rows_out - r1),
-                                cg, ncg, buf1, col);
-            s2_bar_arrive(kBarFull0 + 1, kWsThreads);
+            const int nr1 = min(kStep, it.rows_out - r1);
+            v_step<ST, MODE, 8>(R, it.xr, it.xd, G.lp, x, colin, G.y0 + r1 + 4, G.H, nr1, cg, buf1, tid);
+            __syncthreads();
+            h_step<ST, MODE, EXPORT>(buf1, r1, nr1, t_r, t_s, t_on, G, acc, mo);
         }
-    }
-}
-
-// Horizontal warpgroup: one work item, then the item's sums (fixed order:
-// lanes by a shuffle tree, then the group's four warps in order).
-template <typename ST, int MODE, bool EXPORT>
-__device__ __forceinline__ void h_item(const Item<ST> &it, float2 *smb, int ht, double (*s_warp)[6],
-                                       double *__restrict__ partials, int item, const MapOut &mo) {
-    const int t_r = ht % kStep, t_s = ht / kStep;
-    const bool t_on = ht < kTasks;
-    Acc6 acc{};
-    for (int st = 0; st < it.nsteps; st++) {
-        const int b = st & 1;
-        s2_bar_sync(kBarFull0 + b, kWsThreads);
-        const int r0 = st * kStep;
-        h_step<MODE, EXPORT>(smb + b * kBufF2, r0, min(kStep, it.rows_out - r0), t_r, t_s, t_on, it.G, acc, mo);
-        if (st + 2 < it.nsteps) s2_bar_arrive(kBarEmpty0 + b, kWsThreads);
     }
     if constexpr (MODE != TM_REFMOM) {
 #pragma unroll
         for (int m = 0; m < 6; m++) {
-            double v = acc.v[m];
+            double v = acc[m * kFusedThreads];
 #pragma unroll
             for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-            if ((ht & 31) == 0) s_warp[ht >> 5][m] = v;
+            if ((tid & 31) == 0) s_warp[tid >> 5][m] = v;
         }
-        s2_bar_sync(kBarHGroup, kFusedThreads);
-        if (ht < 6) {
+        __syncthreads();
+        if (tid < 6) {
             double v = 0.0;
 #pragma unroll
-            for (int w = 0; w < kFusedThreads / 32; w++) v += s_warp[w][ht];
-            partials[(long long)item * 6 + ht] = v;  // = tile * 18 + channel * 6 + m
+            for (int w = 0; w < kFusedThreads / 32; w++) v += s_warp[w][tid];
+            partials[(long long)item * 6 + tid] = v;  // = tile * 18 + channel * 6 + m
         }
     }
 }
 
-// Registers per thread of the two warpgroups (setmaxnreg): they add up to the
-// block's launch allotment, 2 x 128 per thread pair, so neither request waits.
-constexpr int kRegsV = 120, kRegsH = 136;
-static_assert(kRegsV + kRegsH == 2 * 128 && kRegsV % 8 == 0 && kRegsH % 8 == 0, "register split");
-
-// Warp-specialized: warpgroup 0 runs the vertical phase of every step,
-// warpgroup 1 the horizontal phase, concurrently, through the double-buffered
-// shared planes.  One launch runs the work items of one mode, so each
-// instance gets the registers of its own mode.
 template <typename ST, int MODE, bool EXPORT = false>
-__global__ void __launch_bounds__(kWsThreads, 2)
+__global__ void __launch_bounds__(kFusedThreads, 4)
     fused_kernel(const DevPair *__restrict__ pairs, const Seg *__restrict__ segs, int nseg, int first_item,
                  int end_item, int *__restrict__ counter, double *__restrict__ partials,
                  MapOut mo = MapOut{nullptr, 0, 0}) {
     extern __shared__ __align__(16) float2 smb[];  // [parity][3 planes][kStep][kRS]
     __shared__ int s_item;
     __shared__ double s_warp[kFusedThreads / 32][6];
+    __shared__ double s_acc[6 * kFusedThreads];
     const int tid = threadIdx.x;
-    const bool vgroup = tid < kFusedThreads;
-    if (vgroup) asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(kRegsV));
-    else asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(kRegsH));
     for (;;) {
         __syncthreads();  // the previous item's readers of s_item, s_warp and the buffers are done
         if (tid == 0) s_item = first_item + atomicAdd(counter, 1);
@@ -795,8 +792,7 @@ __global__ void __launch_bounds__(kWsThreads, 2)
         const int tile = item / 3, g = item - 3 * tile;
         const Seg sg = segs[find_seg(segs, nseg, tile)];
         const Item<ST> it = decode_item<ST>(pairs[sg.pair], sg, tile, g);
-        if (vgroup) v_item<ST, MODE>(it, smb, tid);
-        else h_item<ST, MODE, EXPORT && MODE != TM_REFMOM>(it, smb, tid - kFusedThreads, s_warp, partials, item, mo);
+        flat_item<ST, MODE, EXPORT && MODE != TM_REFMOM>(it, smb, tid, s_acc, s_warp, partials, item, mo);
     }
 }
 
@@ -893,13 +889,13 @@ const double *host_weights() { return kWeights; }
 cudaError_t upload_weights() { return cudaMemcpyToSymbol(c_weight, kWeights, sizeof kWeights); }
 
 size_t fused_smem_bytes() { return (size_t)2 * kBufF2 * sizeof(float2); }
-int fused_threads() { return kWsThreads; }
+int fused_threads() { return kTileThreads; }
 
 template <typename ST, int MODE, bool EXPORT>
 static cudaError_t fused_attrs() {
     const void *f = (const void *)fused_kernel<ST, MODE, EXPORT>;
-    // two blocks of two warpgroups per SM: ask for the largest shared-memory
-    // carveout (the rest is L1)
+    // the tile pass is limited by registers and shared memory together: ask
+    // for the largest shared-memory carveout so that 4 blocks fit per SM
     cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fused_smem_bytes());
@@ -928,7 +924,7 @@ int fused_blocks_per_sm(int storage) {
     const void *f = storage == ST_F16    ? (const void *)fused_kernel<__half, TM_FULL, false>
                     : storage == ST_BF16 ? (const void *)fused_kernel<__nv_bfloat16, TM_FULL, false>
                                          : (const void *)fused_kernel<float, TM_FULL, false>;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f, kWsThreads, fused_smem_bytes()) != cudaSuccess) return 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f, kTileThreads, fused_smem_bytes()) != cudaSuccess) return 1;
     return n > 0 ? n : 1;
 }
 
@@ -965,7 +961,7 @@ cudaError_t launch_pyramid(int storage, const DevPair *pairs, int npairs, const 
 template <typename ST, int MODE, bool EXPORT>
 static void fused_go(int grid, size_t sm, cudaStream_t st, const DevPair *pairs, const Seg *segs, int nseg, int fi,
                      int ei, int *counter, double *partials, const MapOut &mo) {
-    fused_kernel<ST, MODE, EXPORT><<<grid, kWsThreads, sm, st>>>(pairs, segs, nseg, fi, ei, counter, partials, mo);
+    fused_kernel<ST, MODE, EXPORT><<<grid, kTileThreads, sm, st>>>(pairs, segs, nseg, fi, ei, counter, partials, mo);
 }
 
 template <typename ST, bool EXPORT>
