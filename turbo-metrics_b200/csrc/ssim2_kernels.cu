@@ -387,6 +387,8 @@ __device__ __forceinline__ float fir9s(float a0, float a1, float a2, float a3, f
     return fmaf(S2_T0, a4, acc);
 }
 
+__device__ __forceinline__ void s2_prefetch_l2(const void *p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
 // Register rings of one vertical column (which are used depends on the mode).
 struct Rings {
     float2 a[16];  // FULL (x', e); CAND (e, x'y')
@@ -424,22 +426,48 @@ __device__ __forceinline__ void ring_in(Rings &R, int sl, float vr, float vd, fl
 // the raw (x', e) of the output row (FULL) or its raw e as floats (CAND; the
 // horizontal phase reads x' from the reference plane); REFMOM stores the FIR
 // of ring c to plane 0 as floats.
-template <typename ST, int MODE, int S0>
-__device__ __forceinline__ void v_step(Rings &R, const ST *__restrict__ xr, const ST *__restrict__ xd, long long lp,
-                                       int x, bool colin, int ybase, int H, int nr, float cg,
-                                       float2 *__restrict__ buf, int col) {
-    float lr[kStep], ld[kStep];
+// The input rows of one step: reference and distorted samples of this
+// thread's column.
+struct StepRows {
+    float r[kStep], d[kStep];
+};
+
+// Loads the rows ybase .. ybase + 7 of the column.  inner: every column of
+// the tile and all 8 rows are inside the image and the tile (no masks);
+// otherwise rows and columns outside read the anchor.
+template <typename ST, int MODE>
+__device__ __forceinline__ void v_load(StepRows &in, const ST *__restrict__ xr, const ST *__restrict__ xd,
+                                       long long lp, int x, bool colin, int ybase, int H, int nr, bool inner,
+                                       float cg) {
+    float *lr = in.r, *ld = in.d;
+    if (inner) {
+        const ST *pr = xr + (long long)ybase * lp + x;
+        const ST *pd = xd + (long long)ybase * lp + x;
 #pragma unroll
-    for (int k = 0; k < kStep; k++) {
-        const int y = ybase + k;
-        const bool in = k < nr && colin && y < H;
-        lr[k] = in ? ld_store<ST>(xr + (long long)y * lp + x) : cg;
-        ld[k] = (MODE != TM_REFMOM && in) ? ld_store<ST>(xd + (long long)y * lp + x) : cg;
+        for (int k = 0; k < kStep; k++) {
+            lr[k] = ld_store<ST>(pr);
+            ld[k] = MODE != TM_REFMOM ? ld_store<ST>(pd) : cg;
+            pr += lp;
+            pd += lp;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < kStep; k++) {
+            const int y = ybase + k;
+            const bool in = k < nr && colin && y < H;
+            lr[k] = in ? ld_store<ST>(xr + (long long)y * lp + x) : cg;
+            ld[k] = (MODE != TM_REFMOM && in) ? ld_store<ST>(xd + (long long)y * lp + x) : cg;
+        }
     }
+}
+
+template <typename ST, int MODE, int S0>
+__device__ __forceinline__ void v_step(Rings &R, const StepRows &in, int nr, float cg, float2 *__restrict__ buf,
+                                       int col) {
 #pragma unroll
     for (int k = 0; k < kStep; k++) {
         if (k < nr) {
-            ring_in<MODE>(R, (S0 + 8 + k) & 15, lr[k], ld[k], cg);
+            ring_in<MODE>(R, (S0 + 8 + k) & 15, in.r[k], in.d[k], cg);
 #define S2_R(a, j) a[(S0 + k + (j)) & 15]
             if (MODE == TM_REFMOM) {
                 ((float *)buf)[k * 2 * kRS + col] =
@@ -712,6 +740,7 @@ __device__ __forceinline__ Item<ST> decode_item(const DevPair &P, const Seg &sg,
 }
 
 constexpr int kTileThreads = kFusedThreads;
+constexpr int kTileBlocks = 4;  // resident blocks per SM (registers: 128 per thread)
 
 // One warpgroup does both phases of a step in turn: the vertical phase of
 // step st to buffer st & 1, a barrier, then the horizontal phase; buffer b is
@@ -724,8 +753,16 @@ __device__ __forceinline__ void flat_item(const Item<ST> &it, float2 *smb, int t
     const float cg = G.cg;
     const int x = G.x0 - 4 + tid;
     const bool colin = x >= 0 && x < G.W;
+    const bool cols_in = G.x0 >= 4 && G.x0 + kCols - 4 <= G.W;  // every column of the tile
     const int t_r = tid % kStep, t_s = tid / kStep;
     const bool t_on = tid < kTasks;
+    // L2 prefetch of a step's input rows: lane l takes row l & 7 of image
+    // (l >> 3) & 1 at the warp's first (l < 16) or last column, the at most
+    // two lines a warp's row spans
+    const int lane = tid & 31;
+    const ST *pf = (((lane >> 3) & 1) && MODE != TM_REFMOM ? it.xd : it.xr) +
+                   min(max(x - lane + (lane < 16 ? 0 : 31), 0), G.W - 1);
+    const int pf_y = G.y0 + 4 + (lane & 7);
     Rings R;
 #pragma unroll
     for (int k = 0; k < 8; k++) {
@@ -741,16 +778,35 @@ __device__ __forceinline__ void flat_item(const Item<ST> &it, float2 *smb, int t
 #pragma unroll
     for (int m = 0; m < 6; m++) acc[m * kFusedThreads] = 0.0;
     float2 *buf0 = smb, *buf1 = smb + kBufF2;
+    auto prefetch = [&](int st) {  // the input rows of step st
+        const int y = pf_y + st * kStep;
+        if (st < it.nsteps && y < G.H) s2_prefetch_l2(pf + (long long)y * G.lp);
+    };
+    // the rows of step st (loaded right before its vertical phase: held a
+    // step ahead, they would need registers that 4 blocks per SM do not have;
+    // the L2 prefetch two steps ahead shortens their wait instead)
+    StepRows in;
+    auto load = [&](int st) {
+        const int r = st * kStep, nr = min(kStep, it.rows_out - r);
+        const bool inner = cols_in && nr == kStep && G.y0 + r + 4 + kStep <= G.H;
+        v_load<ST, MODE>(in, it.xr, it.xd, G.lp, x, colin, G.y0 + r + 4, G.H, nr, inner, cg);
+    };
+    prefetch(0);
+    prefetch(1);
     for (int st = 0; st < it.nsteps; st += 2) {
         const int r0 = st * kStep;
         const int nr0 = min(kStep, it.rows_out - r0);
-        v_step<ST, MODE, 0>(R, it.xr, it.xd, G.lp, x, colin, G.y0 + r0 + 4, G.H, nr0, cg, buf0, tid);
+        load(st);
+        prefetch(st + 2);
+        v_step<ST, MODE, 0>(R, in, nr0, cg, buf0, tid);
         __syncthreads();
         h_step<ST, MODE, EXPORT>(buf0, r0, nr0, t_r, t_s, t_on, G, acc, mo);
         if (st + 1 < it.nsteps) {
             const int r1 = r0 + kStep;
             const int nr1 = min(kStep, it.rows_out - r1);
-            v_step<ST, MODE, 8>(R, it.xr, it.xd, G.lp, x, colin, G.y0 + r1 + 4, G.H, nr1, cg, buf1, tid);
+            load(st + 1);
+            prefetch(st + 3);
+            v_step<ST, MODE, 8>(R, in, nr1, cg, buf1, tid);
             __syncthreads();
             h_step<ST, MODE, EXPORT>(buf1, r1, nr1, t_r, t_s, t_on, G, acc, mo);
         }
@@ -774,7 +830,7 @@ __device__ __forceinline__ void flat_item(const Item<ST> &it, float2 *smb, int t
 }
 
 template <typename ST, int MODE, bool EXPORT = false>
-__global__ void __launch_bounds__(kFusedThreads, 4)
+__global__ void __launch_bounds__(kFusedThreads, kTileBlocks)
     fused_kernel(const DevPair *__restrict__ pairs, const Seg *__restrict__ segs, int nseg, int first_item,
                  int end_item, int *__restrict__ counter, double *__restrict__ partials,
                  MapOut mo = MapOut{nullptr, 0, 0}) {
