@@ -72,7 +72,11 @@ enum {
     S2_BLUR_IIR_REF = 1
 };
 
-/* Storage type of the intermediate pyramid levels and reference caches. */
+/* Storage type of the intermediate pyramid levels and reference caches.
+ * Only S2_STORAGE_F32 is accepted; the 16-bit values are kept for ABI
+ * stability and make s2_config-taking constructors return
+ * S2_ERR_INVALID_ARG (both passes are compute-bound, so 16-bit planes buy no
+ * time, and they cost up to 0.2 (F16) and 4 (BF16) in score). */
 enum { S2_STORAGE_F32 = 0, S2_STORAGE_F16 = 1, S2_STORAGE_BF16 = 2 };
 
 /* Which pyramid scales are scored. */

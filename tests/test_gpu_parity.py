@@ -274,12 +274,12 @@ def test_uneven_sizes_near_the_top_of_the_range(tmb, oracle, cuda, w, h):
     assert_stats_close(out[1][1], small.stats, what="97x71 beside %dx%d" % (w, h))
 
 
-@pytest.mark.parametrize("storage,tol", [("f16", 0.2), ("bf16", 4.0)])
-def test_reduced_precision_storage(tmb, oracle, cuda, storage, tol):
-    """FP16/BF16 storage of the XYB planes (arithmetic stays f32): the error
-    against FP64 is reported, not hidden; the bound is the stated one."""
-    ref, dis = synth.srgb_pair(512, 512, synth.pair_seed(0, 0))
-    score, _, _ = run_srgb(tmb, cuda, ref, dis, storage=storage)
-    exact = oracle.ssim2_srgb8(ref, dis, "fp64")
-    print("storage %s: score %.6f fp64 %.6f |d| %.3g" % (storage, score, exact.score, abs(score - exact.score)))
-    assert abs(score - exact.score) < tol, (storage, score, exact.score)
+@pytest.mark.parametrize("storage", ["f16", "bf16"])
+def test_reduced_precision_storage_refused(tmb, cuda, storage):
+    """16-bit storage of the XYB planes is not offered (the passes are
+    compute-bound, so it bought no time, and it cost up to 0.2 / 4 in
+    score): a context asking for it is refused with S2_ERR_INVALID_ARG."""
+    with pytest.raises(tmb.InvalidArgument):
+        tmb.Ssimulacra2(64, 64, storage=storage)
+    with pytest.raises(tmb.InvalidArgument):
+        tmb.Ssim2Batch(2, 2 * 64 * 64, storage=storage)

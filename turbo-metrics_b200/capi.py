@@ -58,13 +58,19 @@ class NoCachedReference(S2Error):
     pass
 
 
+class InvalidArgument(S2Error):
+    """A NULL pointer, an unknown enum value or a bad pitch (S2_ERR_INVALID_ARG)."""
+    pass
+
+
 class Busy(S2Error):
     """The server holds its maximum of unfinished jobs (S2_ERR_BUSY)."""
     pass
 
 
 _ERRS = {S2_ERR_OOM: OutOfMemory, S2_ERR_INVALID_SIZE: InvalidImageSize,
-         S2_ERR_DIM_MISMATCH: DimensionMismatch, S2_ERR_NO_REFERENCE: NoCachedReference, S2_ERR_BUSY: Busy}
+         S2_ERR_DIM_MISMATCH: DimensionMismatch, S2_ERR_NO_REFERENCE: NoCachedReference, S2_ERR_BUSY: Busy,
+         S2_ERR_INVALID_ARG: InvalidArgument}
 
 
 def check(status, what=""):

@@ -368,7 +368,10 @@ int s2_num_scales(uint32_t w, uint32_t h, int32_t rule) { return s2_num_scales_r
 static s2_status check_cfg(const s2_config *cfg) {
     if (!cfg || cfg->struct_size != sizeof(s2_config)) return S2_ERR_INVALID_ARG;
     if (cfg->blur != S2_BLUR_FIR && cfg->blur != S2_BLUR_IIR_REF) return S2_ERR_INVALID_ARG;
-    if (cfg->storage < 0 || cfg->storage > 2) return S2_ERR_INVALID_ARG;
+    // 16-bit storage is not offered: the passes are compute-bound, so halving
+    // the plane bytes bought no time, and it cost up to 0.2 (f16) and 4
+    // (bf16) in score
+    if (cfg->storage != S2_STORAGE_F32) return S2_ERR_INVALID_ARG;
     if (cfg->scale_rule < 0 || cfg->scale_rule > 2) return S2_ERR_INVALID_ARG;
     if (cfg->strip_rows != 0 && cfg->strip_rows != kStripMin && cfg->strip_rows != kStripMid &&
         cfg->strip_rows != kStripMax)

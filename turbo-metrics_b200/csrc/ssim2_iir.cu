@@ -190,22 +190,16 @@ __global__ void __launch_bounds__(128) iir_horizontal_kernel(const DevPair *__re
 
 cudaError_t launch_iir(int storage, const DevPair *pairs, const IirSeg *vsegs, int nvseg, int vtotal,
                        const IirSeg *hsegs, int nhseg, int htotal, double *partials, cudaStream_t st) {
+    (void)storage;  // f32 planes only
     if (vtotal > 0) {
         const int g = (vtotal + 127) / 128;
-        if (storage == ST_F16) iir_vertical_kernel<__half><<<g, 128, 0, st>>>(pairs, vsegs, nvseg, vtotal);
-        else if (storage == ST_BF16) iir_vertical_kernel<__nv_bfloat16><<<g, 128, 0, st>>>(pairs, vsegs, nvseg, vtotal);
-        else iir_vertical_kernel<float><<<g, 128, 0, st>>>(pairs, vsegs, nvseg, vtotal);
+        iir_vertical_kernel<float><<<g, 128, 0, st>>>(pairs, vsegs, nvseg, vtotal);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
     if (htotal > 0) {
         const int g = (htotal + 127) / 128;
-        if (storage == ST_F16)
-            iir_horizontal_kernel<__half><<<g, 128, 0, st>>>(pairs, hsegs, nhseg, htotal, partials);
-        else if (storage == ST_BF16)
-            iir_horizontal_kernel<__nv_bfloat16><<<g, 128, 0, st>>>(pairs, hsegs, nhseg, htotal, partials);
-        else
-            iir_horizontal_kernel<float><<<g, 128, 0, st>>>(pairs, hsegs, nhseg, htotal, partials);
+        iir_horizontal_kernel<float><<<g, 128, 0, st>>>(pairs, hsegs, nhseg, htotal, partials);
         return cudaGetLastError();
     }
     return cudaSuccess;

@@ -246,8 +246,12 @@ __device__ __forceinline__ void prep_quads(const DevPair &P, int X0, int Y0, con
     }
 }
 
+// 128 threads: 4 blocks per SM (registers), whose barrier waits over the
+// small scales overlap the other blocks' work.
+constexpr int kPrepThreads = 128;
+
 template <typename ST, int OUT>
-__global__ void __launch_bounds__(256, 2) prep_kernel(const DevPair *__restrict__ pairs, int npairs,
+__global__ void __launch_bounds__(kPrepThreads, 4) prep_kernel(const DevPair *__restrict__ pairs, int npairs,
                                                    const int *__restrict__ blk_first, int first_block,
                                                    int end_block,
                                                    ColorConsts cc, const float *__restrict__ lut_g) {
@@ -970,36 +974,23 @@ static cudaError_t fused_attrs_all() {
 cudaError_t configure_kernels() {
     cudaError_t e;
     if ((e = fused_attrs_all<float>()) != cudaSuccess) return e;
-    if ((e = fused_attrs_all<__half>()) != cudaSuccess) return e;
-    if ((e = fused_attrs_all<__nv_bfloat16>()) != cudaSuccess) return e;
     return configure_dssim_kernels();
 }
 
+// The XYB planes are f32 (S2_STORAGE_F32, the only storage type offered).
 int fused_blocks_per_sm(int storage) {
+    (void)storage;
     int n = 0;
-    const void *f = storage == ST_F16    ? (const void *)fused_kernel<__half, TM_FULL, false>
-                    : storage == ST_BF16 ? (const void *)fused_kernel<__nv_bfloat16, TM_FULL, false>
-                                         : (const void *)fused_kernel<float, TM_FULL, false>;
+    const void *f = (const void *)fused_kernel<float, TM_FULL, false>;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f, kTileThreads, fused_smem_bytes()) != cudaSuccess) return 1;
     return n > 0 ? n : 1;
 }
 
 template <int OUT>
-static void prep_launch(int storage, const DevPair *pairs, int npairs, const int *blk_first, int first_block,
-                        int end_block, const ColorConsts &cc, const float *lut, int grid, cudaStream_t st) {
-    // Lab planes are f32 whatever the storage type; XYB-less passes need one instance
-    if constexpr (OUT != 2) {
-        if (storage == ST_F16) {
-            prep_kernel<__half, OUT><<<grid, 256, 0, st>>>(pairs, npairs, blk_first, first_block, end_block, cc, lut);
-            return;
-        }
-        if (storage == ST_BF16) {
-            prep_kernel<__nv_bfloat16, OUT>
-                <<<grid, 256, 0, st>>>(pairs, npairs, blk_first, first_block, end_block, cc, lut);
-            return;
-        }
-    }
-    prep_kernel<float, OUT><<<grid, 256, 0, st>>>(pairs, npairs, blk_first, first_block, end_block, cc, lut);
+static void prep_launch(const DevPair *pairs, int npairs, const int *blk_first, int first_block, int end_block,
+                        const ColorConsts &cc, const float *lut, int grid, cudaStream_t st) {
+    prep_kernel<float, OUT>
+        <<<grid, kPrepThreads, 0, st>>>(pairs, npairs, blk_first, first_block, end_block, cc, lut);
 }
 
 cudaError_t launch_pyramid(int storage, const DevPair *pairs, int npairs, const int *blk_first, int first_block,
@@ -1008,9 +999,10 @@ cudaError_t launch_pyramid(int storage, const DevPair *pairs, int npairs, const 
     const int nb = end_block - first_block;
     if (nb <= 0) return cudaSuccess;
     grid = grid > nb ? nb : grid;
-    if (out == 3) prep_launch<3>(storage, pairs, npairs, blk_first, first_block, end_block, cc, lut, grid, st);
-    else if (out == 2) prep_launch<2>(storage, pairs, npairs, blk_first, first_block, end_block, cc, lut, grid, st);
-    else prep_launch<1>(storage, pairs, npairs, blk_first, first_block, end_block, cc, lut, grid, st);
+    (void)storage;
+    if (out == 3) prep_launch<3>(pairs, npairs, blk_first, first_block, end_block, cc, lut, grid, st);
+    else if (out == 2) prep_launch<2>(pairs, npairs, blk_first, first_block, end_block, cc, lut, grid, st);
+    else prep_launch<1>(pairs, npairs, blk_first, first_block, end_block, cc, lut, grid, st);
     return cudaGetLastError();
 }
 
@@ -1036,10 +1028,8 @@ cudaError_t launch_fused(int storage, int mode, const DevPair *pairs, const Seg 
     grid = grid > nt ? nt : grid;
     const size_t sm = fused_smem_bytes();
     const MapOut mo{nullptr, 0, 0};
-    if (storage == ST_F16) fused_mode<__half, false>(mode, grid, sm, st, pairs, segs, nseg, fi, ei, counter, partials, mo);
-    else if (storage == ST_BF16)
-        fused_mode<__nv_bfloat16, false>(mode, grid, sm, st, pairs, segs, nseg, fi, ei, counter, partials, mo);
-    else fused_mode<float, false>(mode, grid, sm, st, pairs, segs, nseg, fi, ei, counter, partials, mo);
+    (void)storage;
+    fused_mode<float, false>(mode, grid, sm, st, pairs, segs, nseg, fi, ei, counter, partials, mo);
     return cudaGetLastError();
 }
 
@@ -1052,10 +1042,8 @@ cudaError_t launch_fused_export(int storage, int mode, const DevPair *pairs, con
     grid = grid > nt ? nt : grid;
     const size_t sm = fused_smem_bytes();
     const MapOut mo{maps, mpitch, mplane};
-    if (storage == ST_F16) fused_mode<__half, true>(mode, grid, sm, st, pairs, segs, nseg, fi, ei, counter, partials, mo);
-    else if (storage == ST_BF16)
-        fused_mode<__nv_bfloat16, true>(mode, grid, sm, st, pairs, segs, nseg, fi, ei, counter, partials, mo);
-    else fused_mode<float, true>(mode, grid, sm, st, pairs, segs, nseg, fi, ei, counter, partials, mo);
+    (void)storage;
+    fused_mode<float, true>(mode, grid, sm, st, pairs, segs, nseg, fi, ei, counter, partials, mo);
     return cudaGetLastError();
 }
 
