@@ -151,8 +151,7 @@ def cached_reference_bench(tmb, ref, n_cands, steps, warmup, value, peak):
     quantisation, steps spread over [2, 48]) per step, through the batch's
     cached reference (s2_batch_set_reference + submit_with_reference, the
     semantics of ssim2-gpu's Ssim2Batch): the reference's XYB pyramid and
-    blurred mean mu1 stay resident, so each candidate's prep converts one
-    frame and its tile pass blurs three planes per channel."""
+    stays resident, so each candidate's prep converts one frame."""
     import multiprocessing as mp
     import torch
     with mp.get_context("spawn").Pool(min(16, os.cpu_count() or 1)) as pool:
@@ -183,7 +182,7 @@ def cached_reference_bench(tmb, ref, n_cands, steps, warmup, value, peak):
     tmb.lib.s2_batch_set_profiling(b._h, 0)
     acc /= 3
     sn = sum_pixels()
-    tile_bytes = n_cands * 3 * 12 * sn  # ref XYB, dis XYB, ref mu1 (3 planes f32 each) read
+    tile_bytes = n_cands * 2 * 12 * sn  # ref XYB, dis XYB (3 planes f32 each) read
     prep_bytes = n_cands * (1.5 * W * H + 12 * sn)  # NV12 of the candidate in, its XYB planes out
     b.close()
     rate = n_cands / (ms / 1e3)
@@ -192,7 +191,7 @@ def cached_reference_bench(tmb, ref, n_cands, steps, warmup, value, peak):
             "score_range": [float(min(r[0] for r in res)), float(max(r[0] for r in res))],
             "kernel_ms": {"prep": float(acc[0]), "tile": float(acc[1]), "finalize": float(acc[2])},
             "bytes_per_step": {"prep (NV12 in + candidate XYB out)": prep_bytes,
-                               "tile (reference XYB + candidate XYB + reference mu1 in)": tile_bytes},
+                               "tile (reference XYB + candidate XYB in)": tile_bytes},
             "tile_gbs": tile_bytes / (acc[1] / 1e3) / 1e9, "tile_frac": tile_bytes / (acc[1] / 1e3) / 1e9 / peak}
 
 

@@ -198,10 +198,11 @@ s2_status s2_compute_sync_linear_f32(s2_ctx *ctx, const float *ref, size_t ref_p
 
 /* ---- cached reference -------------------------------------------------- */
 /* Replaces set_reference_linear (lib.rs:440-546): keeps the reference's
- * pyramid, XYB and (FIR blur) the blurred reference mean mu1 resident on the
- * device.  compute_with_reference then blurs three planes per channel instead
- * of four; its scores equal the direct path's bit for bit (mu1 is the same
- * blur of the same plane either way). */
+ * XYB pyramid resident on the device; compute_with_reference then converts
+ * only the distorted image, and its scores equal the direct path's bit for
+ * bit (the same tile pass over the same planes).  The reference also keeps
+ * the blurred mu1 / sigma11; here they would save no work (the tile pass
+ * blurs its planes in f32x2 pairs), so they are not kept. */
 s2_status s2_set_reference_linear_f32(s2_ctx *ctx, const float *ref, size_t pitch, void *stream);
 s2_status s2_set_reference_srgb8(s2_ctx *ctx, const uint8_t *ref, size_t pitch,
                                  int32_t on_host, void *stream);
@@ -280,7 +281,7 @@ s2_status s2_batch_submit_host(s2_batch *b, const s2_pair_desc *pairs, uint32_t 
  * older one's results. */
 /* Replaces Ssim2Batch::set_reference (ssim2-gpu/src/pipeline_batch.rs:206-208):
  * converts `ref` (its ref / ref_uv planes, on the device; any format) and keeps
- * its XYB pyramid and blurred moments in the batch.  Returns after the device
+ * its XYB pyramid in the batch.  Returns after the device
  * work is done.  S2_ERR_INVALID_SIZE below 8x8 or above max_pixels. */
 s2_status s2_batch_set_reference(s2_batch *b, const s2_pair_desc *ref, void *stream);
 /* Replaces Ssim2Batch::compute_batch (pipeline_batch.rs:247-330): enqueue n
@@ -355,7 +356,7 @@ s2_status s2_dssim_mem_usage(const s2_dssim *d, size_t *bytes);
  * at any time; they are admitted in arrival order while their device bytes
  * fit the HBM budget, their images are uploaded on a copy stream, and every
  * round scores the pending work of all admitted jobs in one submission.  A
- * job's reference pyramid and blurred moments are built once and shared by its
+ * job's reference pyramid is built once and shared by its
  * candidates (scored as s2_compute_with_reference_* scores them).  A job
  * scores bit-identically alone and mixed with others.  Host images must stay
  * valid until s2_server_wait returns for the job. */

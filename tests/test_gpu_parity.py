@@ -176,8 +176,9 @@ def test_error_paths(tmb, cuda):
 
 
 def test_cached_reference_equals_direct(tmb, oracle, cuda):
-    """The cached path reads the reference's blurred mu1 and blurs the three
-    other planes: the score equals the direct path's bit for bit (the
+    """The cached path converts only the distorted image and runs the same
+    tile pass over the cached reference planes: the score equals the direct
+    path's bit for bit (the
     reference's own bar for cached == direct is 1e-4,
     ssim2-gpu/tests/parity_lock.rs:160-277), every statistic against the
     oracle's fir32 restatement."""

@@ -57,11 +57,11 @@ SMALL = dict(max_batch_pairs=8, max_batch_pixels=1 << 21)
 
 def job_bytes(w, h, k):
     """Device bytes the server admits a job with: inputs + reference XYB
-    pyramid + the reference's blurred mean (3 f32 planes per scale each)."""
+    pyramid (3 f32 planes per scale)."""
     up = lambda v, a: (v + a - 1) // a * a
     total = up(w * h * 3 * (1 + k), 256)
     for _ in range(tmb_num_scales(w, h)):
-        total += 2 * up(3 * up(w, 64) * h * 4, 256)
+        total += up(3 * up(w, 64) * h * 4, 256)
         w, h = (w + 1) // 2, (h + 1) // 2
     return total
 

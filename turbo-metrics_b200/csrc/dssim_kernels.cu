@@ -139,11 +139,11 @@ __global__ void __launch_bounds__(kDsThreads) dssim_clamp_kernel(const DsPair *_
 // Each blur stage fills an n x n buffer (n = 32 + 2 x its halo, even) from the
 // (n + 2)-wide buffer of the stage before.  A thread takes two adjacent
 // columns and kDsRun consecutive rows and slides a 3 x 4 window of the input
-// down them (two 8-byte shared loads per row).  Each tap is a scalar multiply
-// per column and one f32x2 add for both columns, in the reference's
-// row-major tap order: every lane rounds as the scalar reference does (the
-// products are scalar multiplies, which -fmad=false keeps out of any fused
-// multiply-add).  The first tap initialises the sum, which equals 0 + tap
+// down them (two 8-byte shared loads per row).  Each input row's products
+// with the three distinct taps are formed once (scalar multiplies, which
+// -fmad=false keeps out of any fused multiply-add) and summed with one f32x2
+// add per tap for both columns, in the reference's row-major tap order:
+// every lane rounds as the scalar reference does.  The first tap initialises the sum, which equals 0 + tap
 // for every tap but -0 (no Lab value or product of two is -0 where it
 // matters: the sign of a zero sum does not reach the SSIM).  x^2, y^2 and xy
 // are formed once per input position, so the first statistics blur is five
@@ -153,26 +153,43 @@ __global__ void __launch_bounds__(kDsThreads) dssim_clamp_kernel(const DsPair *_
 // next stage reads there with clamped indexes.
 constexpr int kDsRun = 4;
 
-__device__ __forceinline__ float2 ds_sum9x2(const float (&w)[3][4]) {
-    float2 sum = make_float2(w[0][0] * ds_k(0), w[0][1] * ds_k(0));
-#pragma unroll
-    for (int i = 1; i < 9; i++) {
-        const int ky = i / 3, kx = i % 3;
-        const float k = ds_k(i);
-        sum = __fadd2_rn(sum, make_float2(w[ky][kx] * k, w[ky][kx + 1] * k));
-    }
-    return sum;
-}
+// The kernel has three distinct taps (corners, edges, centre), so the
+// products of one input row (columns c - 1 .. c + 2) with them are formed
+// once and serve the row in all three of its roles -- top, middle and bottom
+// row of the 3 x 3 window -- for both output columns c and c + 1.  Each
+// product is the same single-rounded value the reference forms for that tap.
+struct DsRowP {
+    float2 k0a, k0b;  // corner tap x (v0, v1), (v2, v3)
+    float2 k1m;       // edge tap x (v1, v2): top and bottom rows
+    float2 k1a, k1b;  // edge tap x (v0, v1), (v2, v3): middle row
+    float2 k2m;       // centre tap x (v1, v2)
+};
 
-__device__ __forceinline__ void ds_load4(float (&row)[4], const float *src) {
+__device__ __forceinline__ DsRowP ds_row(const float *src) {
     const float2 a = *(const float2 *)src, b = *(const float2 *)(src + 2);
-    row[0] = a.x, row[1] = a.y, row[2] = b.x, row[3] = b.y;
+    const float k0 = ds_k(0), k1 = ds_k(1), k2 = ds_k(4);
+    DsRowP p;
+    p.k0a = make_float2(a.x * k0, a.y * k0);
+    p.k0b = make_float2(b.x * k0, b.y * k0);
+    p.k1m = make_float2(a.y * k1, b.x * k1);
+    p.k1a = make_float2(a.x * k1, a.y * k1);
+    p.k1b = make_float2(b.x * k1, b.y * k1);
+    p.k2m = make_float2(a.y * k2, b.x * k2);
+    return p;
 }
 
-__device__ __forceinline__ void ds_slide(float (&w)[3][4], const float *src) {
-#pragma unroll
-    for (int kx = 0; kx < 4; kx++) w[0][kx] = w[1][kx], w[1][kx] = w[2][kx];
-    ds_load4(w[2], src);
+// 3x3 blur at (c, c + 1): the nine taps in the reference's row-major order,
+// the first initialising the sum
+__device__ __forceinline__ float2 ds_sum9p(const DsRowP &t, const DsRowP &m, const DsRowP &b) {
+    float2 sum = t.k0a;
+    sum = __fadd2_rn(sum, t.k1m);
+    sum = __fadd2_rn(sum, t.k0b);
+    sum = __fadd2_rn(sum, m.k1a);
+    sum = __fadd2_rn(sum, m.k2m);
+    sum = __fadd2_rn(sum, m.k1b);
+    sum = __fadd2_rn(sum, b.k0a);
+    sum = __fadd2_rn(sum, b.k1m);
+    return __fadd2_rn(sum, b.k0b);
 }
 
 // `planes` planes: out[p] (n x n) = 3x3 blur of in[p] (pitch n + 2, plane (n + 2)^2)
@@ -183,14 +200,14 @@ __device__ __forceinline__ void ds_stage_blur(const float *in, float *out, int n
         const int c = 2 * (q % half), j0 = (q / half) * kDsRun;
         const float *src = in + p * m * m + c;
         float *dst = out + p * n * n + c;
-        float w[3][4];
-        ds_load4(w[1], src + j0 * m);
-        ds_load4(w[2], src + (j0 + 1) * m);
+        DsRowP t = ds_row(src + j0 * m), mid = ds_row(src + (j0 + 1) * m);
 #pragma unroll
         for (int r = 0; r < kDsRun; r++) {
             if (j0 + r >= n) break;
-            ds_slide(w, src + (j0 + r + 2) * m);
-            *(float2 *)(dst + (j0 + r) * n) = ds_sum9x2(w);
+            const DsRowP b = ds_row(src + (j0 + r + 2) * m);
+            *(float2 *)(dst + (j0 + r) * n) = ds_sum9p(t, mid, b);
+            t = mid;
+            mid = b;
         }
     }
 }
@@ -214,29 +231,40 @@ __device__ __forceinline__ void ds_cp4(float *dst, const float *src) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
 }
 
-// Issue the copies of channel c's raw region of `tile` (halo 2 for L, 4 for
-// a and b; clamped into the level) into R, pitch 32 + 2 x halo, both images.
-__device__ void ds_prefetch(const DsPair *__restrict__ pairs, const DsSeg *__restrict__ segs, int nseg, int tile,
-                            int c, float *R) {
+// Issue the copies of channel c's raw region of `tile` (halo HALO: 2 for L,
+// 4 for a and b; clamped into the level) into R, pitch 32 + 2 x halo, both
+// images.  The region's edge is a compile-time constant, so the element
+// index splits into row and column without a division.
+template <int HALO>
+__device__ __forceinline__ void ds_prefetch_h(const DsPair *__restrict__ pairs, const DsSeg *__restrict__ segs,
+                                              int nseg, int tile, int c, float *R) {
+    constexpr int n = kDsT + 2 * HALO;
     const DsSeg sg = segs[ds_find_seg(segs, nseg, tile)];
     const DsPair &P = pairs[sg.pair];
     const int s = sg.level, W = P.w[s], H = P.h[s];
     const long long pitch = P.pitch[s], plane = pitch * H;
     const int tl = tile - sg.first_tile;
     const int X0 = (tl % sg.tiles_x) * kDsT, Y0 = (tl / sg.tiles_x) * kDsT;
-    const int h = c == 0 ? 2 : 4, n = kDsT + 2 * h;
     const float *xr = P.lab[0][s] + c * plane, *yr = P.lab[1][s] + c * plane;
     for (int i = threadIdx.x; i < 2 * n * n; i += kDsThreads) {
-        const int img = i / (n * n), r = i % (n * n);
-        const int gx = ds_clamp(X0 - h + r % n, W - 1), gy = ds_clamp(Y0 - h + r / n, H - 1);
+        const int img = i >= n * n, r = img ? i - n * n : i;
+        const int row = r / n, col = r - row * n;
+        const int gx = ds_clamp(X0 - HALO + col, W - 1), gy = ds_clamp(Y0 - HALO + row, H - 1);
         ds_cp4(R + i, (img ? yr : xr) + gy * pitch + gx);
     }
     asm volatile("cp.async.commit_group;\n" ::: "memory");
 }
 
+__device__ __forceinline__ void ds_prefetch(const DsPair *__restrict__ pairs, const DsSeg *__restrict__ segs,
+                                            int nseg, int tile, int c, float *R) {
+    if (c == 0) ds_prefetch_h<2>(pairs, segs, nseg, tile, c, R);
+    else ds_prefetch_h<4>(pairs, segs, nseg, tile, c, R);
+}
+
 // positions of an n x n stage buffer (origin X0 - h, Y0 - h) outside the
 // level take the value at the position clamped into the level
-__device__ void ds_fix_edges(float *buf, int planes, int n, int h, int X0, int Y0, int W, int H) {
+template <int n, int h>
+__device__ __forceinline__ void ds_fix_edges(float *buf, int planes, int X0, int Y0, int W, int H) {
     for (int i = threadIdx.x; i < n * n; i += kDsThreads) {
         const int x = X0 - h + i % n, y = Y0 - h + i / n;
         if (x >= 0 && x < W && y >= 0 && y < H) continue;
@@ -315,13 +343,13 @@ __global__ void __launch_bounds__(kDsThreads, 3) dssim_tile_kernel(const DsPair 
             else if (tile + (int)gridDim.x < ntiles) ds_prefetch(pairs, segs, nseg, tile + gridDim.x, 0, bufR);
             if (c > 0) {
                 if (edge) {
-                    ds_fix_edges(bufB, 2, kDsP, 3, X0, Y0, W, H);
+                    ds_fix_edges<kDsP, 3>(bufB, 2, X0, Y0, W, H);
                     __syncthreads();
                 }
                 ds_stage_blur(bufB, bufA, kDsX, 2);
                 __syncthreads();
                 if (edge) {
-                    ds_fix_edges(bufA, 2, kDsX, 2, X0, Y0, W, H);
+                    ds_fix_edges<kDsX, 2>(bufA, 2, X0, Y0, W, H);
                     __syncthreads();
                 }
                 ds_products(bufA, bufA + nnX, bufA, nnX);
@@ -330,7 +358,7 @@ __global__ void __launch_bounds__(kDsThreads, 3) dssim_tile_kernel(const DsPair 
             ds_stage_blur(bufA, bufB, kDsB, 5);
             __syncthreads();
             if (edge) {
-                ds_fix_edges(bufB, 5, kDsB, 1, X0, Y0, W, H);
+                ds_fix_edges<kDsB, 1>(bufB, 5, X0, Y0, W, H);
                 __syncthreads();
             }
             // second blurs at the thread's 2 x 2 outputs
@@ -338,13 +366,13 @@ __global__ void __launch_bounds__(kDsThreads, 3) dssim_tile_kernel(const DsPair 
 #pragma unroll
             for (int pl = 0; pl < 5; pl++) {
                 const float *src = bufB + pl * nnB + c0;
-                float w[3][4];
-                ds_load4(w[1], src + r0 * kDsB);
-                ds_load4(w[2], src + (r0 + 1) * kDsB);
+                DsRowP t = ds_row(src + r0 * kDsB), mid = ds_row(src + (r0 + 1) * kDsB);
 #pragma unroll
                 for (int r = 0; r < kDsOutRows; r++) {
-                    ds_slide(w, src + (r0 + r + 2) * kDsB);
-                    q[pl][r] = ds_sum9x2(w);
+                    const DsRowP b = ds_row(src + (r0 + r + 2) * kDsB);
+                    q[pl][r] = ds_sum9p(t, mid, b);
+                    t = mid;
+                    mid = b;
                 }
             }
 #pragma unroll

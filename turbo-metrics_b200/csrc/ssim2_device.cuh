@@ -26,10 +26,6 @@ constexpr float kC2 = 0.0009f;
 constexpr int kDsLevels = 5;         // DSSIM scales (dssim-cuda/src/lib.rs:73)
 
 enum Format { FMT_LINEAR_F32 = 0, FMT_SRGB8 = 1, FMT_NV12 = 2, FMT_RGB16 = 3, FMT_P016 = 4 };
-// Modes of the fused tile pass (per run of tiles): score a pair from both
-// images' XYB; build a cached reference's blurred moments; score a candidate
-// against a cached reference's moments.
-enum TileMode { TM_FULL = 0, TM_REFMOM = 1, TM_CAND = 2 };
 enum Storage { ST_F32 = 0, ST_F16 = 1, ST_BF16 = 2 };
 
 // FIR taps of the exact form of the recursive Gaussian (sigma 1.5, N = 5),
@@ -72,10 +68,6 @@ struct DevPair {
     float *keep[2];
     int lab_levels;          // 0: no Lab output
     int prep_levels;         // levels the prep pass builds (XYB and Lab)
-    // A cached reference's blurred moments per scale (TM_REFMOM writes them,
-    // TM_CAND reads them): 3 f32 planes of pitch lp[s] -- the blurred
-    // shifted reference XYB (mu1) of channels X, Y, B.
-    float *mom[kScales];
 };
 
 // One pair as the DSSIM kernels see it.  Level sizes follow dssim-cuda
@@ -109,7 +101,6 @@ struct Seg {
     int scale;
     int tiles_x;
     int strip_rows;
-    int mode;  // TileMode
 };
 
 // A run of S2_BLUR_IIR_REF work items of one (pair, scale): columns x planes

@@ -297,7 +297,7 @@ struct s2_batch {
     s2_config cfg;
     uint32_t max_pairs = 0;
     uint64_t max_pixels = 0;
-    // cached reference (s2_batch_set_reference): XYB pyramid + blurred moments
+    // cached reference (s2_batch_set_reference): its XYB pyramid
     DevBuf ref_buf;
     bool has_ref = false;
     uint32_t ref_w = 0, ref_h = 0;
@@ -610,20 +610,20 @@ s2_status s2_compute_sync_linear_f32(s2_ctx *ctx, const float *ref, size_t ref_p
 }
 
 // ---- cached reference ----------------------------------------------------
-// set_reference converts the reference once and keeps on the device, for
-// every scale, its XYB planes and -- with the FIR blur -- its blurred mean
-// mu1 per channel (set_reference_linear, ssimulacra2-cuda/src/lib.rs:440-546,
-// caches the reference's XYB, mu1_t and sigma11_t in the same spirit).
-// compute_with_reference converts only the distorted image and blurs three
-// planes (e, e^2, x'y') instead of four, reading mu1 from the cache: the same
-// values the direct path computes, so the scores are equal bit for bit.
-// Like the reference, set_reference returns after the device work is done.
+// set_reference converts the reference once and keeps its XYB planes of
+// every scale on the device (set_reference_linear, ssimulacra2-cuda/src/
+// lib.rs:440-546, keeps the reference's XYB, and also its blurred mu1_t and
+// sigma11_t).  compute_with_reference converts only the distorted image and
+// runs the same tile pass as a direct compute over the cached planes, so the
+// scores equal the direct path's bit for bit.  The blurred reference moments
+// are not kept: the tile pass blurs its planes as f32x2 pairs, so reading a
+// cached mean saves no issue slot, and a candidate pass that did read it
+// measured slower (3.50 against 3.23 ms per 63 1080p candidates).  Like the
+// reference, set_reference returns after the device work is done.
 static s2_status set_ref(s2_ctx *ctx, const s2_pair_desc &d, void *stream) {
-    size_t off[kScales], moff[kScales];
+    size_t off[kScales];
     const int ns = s2_num_scales_rule(ctx->w, ctx->h, ctx->eng.scale_rule);
-    const bool mom = ctx->eng.blur == S2_BLUR_FIR;
-    const size_t lv = s2_align_up(s2_image_levels_layout(ctx->w, ctx->h, ns, ctx->eng.esize(), off), 256);
-    const size_t bytes = lv + (mom ? s2_moment_layout(ctx->w, ctx->h, ns, moff) : 0);
+    const size_t bytes = s2_image_levels_layout(ctx->w, ctx->h, ns, ctx->eng.esize(), off);
     if (ctx->ref_levels.n < bytes) {
         if (ctx->ref_levels.p) {
             S2_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
@@ -642,11 +642,7 @@ static s2_status set_ref(s2_ctx *ctx, const s2_pair_desc &d, void *stream) {
     build.prep_mask = 1;
     build.score = false;
     build.dssim = false;
-    for (int s = 0; s < kScales; s++) {
-        build.ref_levels[s] = s < ns ? (char *)ctx->ref_levels.p + off[s] : nullptr;
-        build.ref_mom[s] = mom && s < ns ? (char *)ctx->ref_levels.p + lv + moff[s] : nullptr;
-    }
-    build.build_mom = mom;
+    for (int s = 0; s < kScales; s++) build.ref_levels[s] = s < ns ? (char *)ctx->ref_levels.p + off[s] : nullptr;
     ctx->has_ref = false;
     s2_status st = ctx_run(ctx, d, stream, &build);
     if (st != S2_OK) return st;
@@ -655,7 +651,6 @@ static s2_status set_ref(s2_ctx *ctx, const s2_pair_desc &d, void *stream) {
     ctx->ref_extra = build;
     ctx->ref_extra.prep_mask = 2;
     ctx->ref_extra.score = true;
-    ctx->ref_extra.build_mom = false;
     ctx->has_ref = true;
     return S2_OK;
 }
@@ -728,10 +723,7 @@ s2_status s2_error_maps(s2_ctx *ctx, int32_t scale, float *maps, size_t pitch, v
     cudaStream_t st = (cudaStream_t)stream;
     const long long mpitch = (long long)(pitch / sizeof(float));
     S2_CUDA(cudaMemsetAsync(e.counter_d.p, 0, sizeof(int), st));
-    int mode = TM_FULL;
-    for (const Seg &sg : P.segs)
-        if (sg.pair == 0 && sg.scale == scale && sg.mode != TM_REFMOM) mode = sg.mode;
-    S2_CUDA(launch_fused_export(e.storage, mode, (const DevPair *)dbase, (const Seg *)(dbase + pb + bb),
+    S2_CUDA(launch_fused_export(e.storage, (const DevPair *)dbase, (const Seg *)(dbase + pb + bb),
                                 (int)P.segs.size(), t0, t1, (int *)e.counter_d.p, (double *)e.partials_d.p, maps,
                                 mpitch, mpitch * p.h[scale], e.num_sms * e.fused_bps, st));
     return S2_OK;
@@ -806,8 +798,8 @@ s2_status s2_batch_submit_host(s2_batch *b, const s2_pair_desc *pairs, uint32_t 
 // Cached reference of a batch: ssim2-gpu's Ssim2Batch::set_reference /
 // compute_batch (crates/ssim2-gpu/src/pipeline_batch.rs:206-330), where every
 // candidate of a submission is scored against one resident reference.  The
-// reference's XYB pyramid and (FIR blur) blurred moments are built once, on
-// slot 0's engine, and kept in a buffer of the batch.
+// reference's XYB pyramid is built once, on slot 0's engine, and kept in a
+// buffer of the batch.
 s2_status s2_batch_set_reference(s2_batch *b, const s2_pair_desc *ref, void *stream) {
     if (!b || !ref || !ref->ref) return S2_ERR_INVALID_ARG;
     if (!(b->metrics & S2_METRIC_SSIMULACRA2)) return S2_ERR_INVALID_ARG;
@@ -816,10 +808,8 @@ s2_status s2_batch_set_reference(s2_batch *b, const s2_pair_desc *ref, void *str
     const int ns = s2_num_scales_rule(w, h, e.scale_rule);
     if (ns == 0 || w > (1u << 16) || h > (1u << 16)) return S2_ERR_INVALID_SIZE;
     if ((uint64_t)w * h > b->max_pixels) return S2_ERR_INVALID_SIZE;
-    size_t off[kScales], moff[kScales];
-    const bool mom = e.blur == S2_BLUR_FIR;
-    const size_t lv = s2_align_up(s2_image_levels_layout(w, h, ns, e.esize(), off), 256);
-    const size_t bytes = lv + (mom ? s2_moment_layout(w, h, ns, moff) : 0);
+    size_t off[kScales];
+    const size_t bytes = s2_image_levels_layout(w, h, ns, e.esize(), off);
     b->has_ref = false;
     if (b->ref_buf.n < bytes) {
         S2_CUDA(cudaDeviceSynchronize());  // earlier submissions may still read the old cache
@@ -837,11 +827,7 @@ s2_status s2_batch_set_reference(s2_batch *b, const s2_pair_desc *ref, void *str
     build.prep_mask = 1;
     build.score = false;
     build.dssim = false;
-    build.build_mom = mom;
-    for (int s = 0; s < kScales; s++) {
-        build.ref_levels[s] = s < ns ? (char *)b->ref_buf.p + off[s] : nullptr;
-        build.ref_mom[s] = mom && s < ns ? (char *)b->ref_buf.p + lv + moff[s] : nullptr;
-    }
+    for (int s = 0; s < kScales; s++) build.ref_levels[s] = s < ns ? (char *)b->ref_buf.p + off[s] : nullptr;
     s2_pair_desc d = *ref;
     d.dis = nullptr;
     d.dis_uv = nullptr;
@@ -854,7 +840,6 @@ s2_status s2_batch_set_reference(s2_batch *b, const s2_pair_desc *ref, void *str
     b->ref_extra = build;
     b->ref_extra.prep_mask = 2;
     b->ref_extra.score = true;
-    b->ref_extra.build_mom = false;
     b->ref_w = w;
     b->ref_h = h;
     b->has_ref = true;

@@ -77,14 +77,7 @@ struct PairExtra {
     bool score = true;
     bool dssim = true;  // score DSSIM too when the engine's metrics include it
     void *ref_levels[kScales] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
-    // the cached reference's blurred moments (s2_moment_layout): build them
-    // (build_mom, a reference build) or score the candidate against them
-    void *ref_mom[kScales] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
-    bool build_mom = false;
 };
-
-// The pair is a candidate scored against cached reference moments.
-inline bool s2_is_cand(const PairExtra *ex) { return ex && ex->score && !ex->build_mom && ex->ref_mom[0]; }
 
 // DSSIM level sizes (dssim-cuda/src/lib.rs:184-205): halved rounding up,
 // never below 8.
@@ -127,21 +120,6 @@ inline size_t s2_image_levels_layout(uint32_t w, uint32_t h, int ns, size_t esiz
     return o;
 }
 
-// Byte layout of a cached reference's blurred moments (all scored scales):
-// per scale 3 f32 planes of the XYB planes' pitch (the blurred shifted
-// reference mu1 of X, Y, B), 256-byte aligned.
-inline size_t s2_moment_layout(uint32_t w, uint32_t h, int ns, size_t off[kScales]) {
-    size_t o = 0;
-    uint64_t cw = w, ch = h;
-    for (int s = 0; s < ns; s++) {
-        off[s] = o;
-        o += s2_align_up((size_t)3 * s2_align_up((size_t)cw, 64) * ch * sizeof(float), 256);
-        cw = (cw + 1) / 2;
-        ch = (ch + 1) / 2;
-    }
-    return o;
-}
-
 // One planned submission.
 struct Plan {
     std::vector<DevPair> pairs;
@@ -149,10 +127,6 @@ struct Plan {
     std::vector<Seg> segs;
     int total_blocks = 0;
     int total_tiles = 0;
-    // tiles [0, mom_tiles) build cached references' moments (TM_REFMOM),
-    // [mom_tiles, mom_tiles + cand_tiles) score candidates against them
-    // (TM_CAND), the rest score pairs from both images (TM_FULL)
-    int mom_tiles = 0, cand_tiles = 0;
     size_t level_bytes = 0;  // both images, all levels, all pairs
     int strip_rows = 63;
     // autotuning: the workload class of this plan, and whether the tile
@@ -532,8 +506,6 @@ struct Engine {
             }
             const bool ref_ext = ex && ex[i].ref_levels[0] != nullptr;
             p.lvl_ext = ref_ext ? 1 : 0;
-            if (ex && ex[i].ref_mom[0])
-                for (int s = 0; s < kScales; s++) p.mom[s] = (float *)ex[i].ref_mom[s];
             for (int s = 0; s < p.nscales; s++) {
                 p.lp[s] = (int)s2_align_up((size_t)p.w[s], 64);
                 size_t bytes = s2_align_up((size_t)3 * p.lp[s] * p.h[s] * esize(), 256);
@@ -610,34 +582,7 @@ struct Engine {
             P.total_tiles = rec;
             return S2_OK;
         }
-        // moment builds, then candidates of cached references (one group)
         int tile = 0;
-        for (int mode : {TM_REFMOM, TM_CAND}) {
-            const int first = tile;
-            for (int s = 0; s < kScales; s++) {
-                for (int i = 0; i < n; i++) {
-                    DevPair &p = P.pairs[i];
-                    const bool take = mode == TM_REFMOM ? (ex && ex[i].build_mom) : s2_is_cand(ex ? &ex[i] : nullptr);
-                    if (p.status != S2_OK || s >= p.nscales || !take) continue;
-                    Seg sg;
-                    sg.first_tile = tile;
-                    sg.pair = i;
-                    sg.scale = s;
-                    sg.tiles_x = (p.w[s] + kTileW - 1) / kTileW;
-                    sg.strip_rows = P.strip_rows;
-                    sg.mode = mode;
-                    const int cnt = sg.tiles_x * ((p.h[s] + P.strip_rows - 1) / P.strip_rows);
-                    if (mode == TM_CAND) {
-                        p.tile_base[s] = tile;
-                        p.tile_cnt[s] = cnt;
-                    }
-                    tile += cnt;
-                    P.segs.push_back(sg);
-                }
-            }
-            (mode == TM_REFMOM ? P.mom_tiles : P.cand_tiles) = tile - first;
-        }
-        if (tile > 0) ngroups = 1;
         // groups of contiguous pairs, about equal scale-0 pixels except the
         // first, which gets half a share (its upload is the one that nothing
         // overlaps): group g ends where the running pixel count reaches
@@ -659,16 +604,13 @@ struct Engine {
           for (int s = 0; s < kScales; s++) {
             for (int i = P.grp_pair[g]; i < P.grp_pair[g + 1]; i++) {
                 DevPair &p = P.pairs[i];
-                if (p.status != S2_OK || s >= p.nscales || (ex && !ex[i].score) ||
-                    s2_is_cand(ex ? &ex[i] : nullptr))
-                    continue;
+                if (p.status != S2_OK || s >= p.nscales || (ex && !ex[i].score)) continue;
                 Seg sg;
                 sg.first_tile = tile;
                 sg.pair = i;
                 sg.scale = s;
                 sg.tiles_x = (p.w[s] + kTileW - 1) / kTileW;
                 sg.strip_rows = P.strip_rows;
-                sg.mode = TM_FULL;
                 int ty = (p.h[s] + P.strip_rows - 1) / P.strip_rows;
                 p.tile_base[s] = tile;
                 p.tile_cnt[s] = sg.tiles_x * ty;
@@ -810,8 +752,7 @@ struct Engine {
         const int pout = (m_s2 ? 1 : 0) | (m_ds ? 2 : 0);
         if (graphs && !host && !profiling && ng == 1) {
             const uint64_t key[8] = {(uint64_t)n, (uint64_t)P.total_blocks,
-                                     ((uint64_t)P.mom_tiles << 42) | ((uint64_t)P.cand_tiles << 21) |
-                                         (uint64_t)P.total_tiles,
+                                     (uint64_t)P.total_tiles,
                                      P.segs.size(),
                                      P.vsegs.size(), P.hsegs.size(),
                                      ((uint64_t)(uint32_t)P.vtotal << 32) | (uint32_t)P.htotal,
@@ -844,7 +785,7 @@ struct Engine {
             S2_CUDA(cudaEventRecord(sub_start, copy_st));
             S2_CUDA(cudaStreamWaitEvent(st, sub_start, 0));
         }
-        S2_CUDA(cudaMemsetAsync(counter_d.p, 0, (ng + 2) * sizeof(int), st));
+        S2_CUDA(cudaMemsetAsync(counter_d.p, 0, ng * sizeof(int), st));
         if (profiling) S2_CUDA(cudaEventRecord(prof[0], st));
         cudaStream_t pst = split ? prep_st : st;
         for (int g = 0; g < ng; g++) {
@@ -884,19 +825,9 @@ struct Engine {
                 S2_CUDA(launch_iir(storage, dpairs, (const IirSeg *)(dbase + pb + bb + sb), (int)P.vsegs.size(),
                                    P.vtotal, (const IirSeg *)(dbase + pb + bb + sb + vsb), (int)P.hsegs.size(),
                                    P.htotal, (double *)partials_d.p, st));
-            else {
-                if (g == 0) {
-                    // cached references' moments first: the candidates read them
-                    S2_CUDA(launch_fused(storage, TM_REFMOM, dpairs, dsegs, (int)P.segs.size(), 0, P.mom_tiles,
-                                         (int *)counter_d.p + ng, (double *)partials_d.p, num_sms * fused_bps, st));
-                    S2_CUDA(launch_fused(storage, TM_CAND, dpairs, dsegs, (int)P.segs.size(), P.mom_tiles,
-                                         P.mom_tiles + P.cand_tiles, (int *)counter_d.p + ng + 1,
-                                         (double *)partials_d.p, num_sms * fused_bps, st));
-                }
-                S2_CUDA(launch_fused(storage, TM_FULL, dpairs, dsegs, (int)P.segs.size(), P.grp_tile[g],
-                                     P.grp_tile[g + 1], (int *)counter_d.p + g, (double *)partials_d.p,
-                                     num_sms * fused_bps, st));
-            }
+            else
+                S2_CUDA(launch_fused(storage, dpairs, dsegs, (int)P.segs.size(), P.grp_tile[g], P.grp_tile[g + 1],
+                                     (int *)counter_d.p + g, (double *)partials_d.p, num_sms * fused_bps, st));
         }
         // several groups interleave prep and fused: the fused slot then holds both
         if (profiling && ng > 1) S2_CUDA(cudaEventRecord(prof[1], st));
@@ -950,7 +881,7 @@ struct Engine {
         }
         cudaError_t e = desc_kernel ? launch_desc_copy(dbase, pinned_dev, desc_bytes, cap_st)
                                     : cudaMemcpyAsync(dbase, pinned, desc_bytes, cudaMemcpyHostToDevice, cap_st);
-        if (e == cudaSuccess) e = cudaMemsetAsync(counter_d.p, 0, 3 * sizeof(int), cap_st);
+        if (e == cudaSuccess) e = cudaMemsetAsync(counter_d.p, 0, sizeof(int), cap_st);
         if (e == cudaSuccess)
             e = launch_pyramid(storage, dpairs, n, (const int *)(dbase + pb), 0, P.total_blocks, cc,
                                (const float *)lut_d.p, num_sms * 8, cap_st, (m_s2 ? 1 : 0) | (m_ds ? 2 : 0));
@@ -959,19 +890,10 @@ struct Engine {
                 e = launch_iir(storage, dpairs, (const IirSeg *)(dbase + pb + bb + sb), (int)P.vsegs.size(), P.vtotal,
                                (const IirSeg *)(dbase + pb + bb + sb + vsb), (int)P.hsegs.size(), P.htotal,
                                (double *)partials_d.p, cap_st);
-            else {
-                const Seg *dsegs = (const Seg *)(dbase + pb + bb);
-                const int ns = (int)P.segs.size(), grid = num_sms * fused_bps;
-                const int c0 = P.mom_tiles, c1 = P.mom_tiles + P.cand_tiles;
-                e = launch_fused(storage, TM_REFMOM, dpairs, dsegs, ns, 0, c0, (int *)counter_d.p + 1,
-                                 (double *)partials_d.p, grid, cap_st);
-                if (e == cudaSuccess)
-                    e = launch_fused(storage, TM_CAND, dpairs, dsegs, ns, c0, c1, (int *)counter_d.p + 2,
-                                     (double *)partials_d.p, grid, cap_st);
-                if (e == cudaSuccess)
-                    e = launch_fused(storage, TM_FULL, dpairs, dsegs, ns, c1, P.total_tiles, (int *)counter_d.p,
-                                     (double *)partials_d.p, grid, cap_st);
-            }
+            else
+                e = launch_fused(storage, dpairs, (const Seg *)(dbase + pb + bb), (int)P.segs.size(), 0,
+                                 P.total_tiles, (int *)counter_d.p, (double *)partials_d.p, num_sms * fused_bps,
+                                 cap_st);
         }
         if (e == cudaSuccess && m_s2)
             e = launch_finalize(dpairs, n, (const double *)partials_d.p, (DevResult *)results_d.p, cap_st);

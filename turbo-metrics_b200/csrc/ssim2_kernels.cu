@@ -361,14 +361,8 @@ __global__ void __launch_bounds__(kPrepThreads, 4) prep_kernel(const DevPair *__
 // no small quantity is recovered from the difference of two large moments,
 // which f32 cannot do to the metric's precision.
 //
-// Modes (one per launch; the plan numbers each mode's tiles contiguously):
-//   TM_FULL    a pair scored from both images' XYB: rings A = (x', e) and
-//              B = (e^2, x'y'), two f32x2 FIRs.
-//   TM_REFMOM  a cached reference: blurs x' and stores mu1 to the pair's
-//              moment planes (mom[s], channels X, Y, B), no maps.
-//   TM_CAND    a candidate against a cached reference: blurs (e, x'y') in
-//              f32x2 and e^2 alone, and reads mu1 from the moment planes --
-//              the same values, to the bit, as TM_FULL computes.
+// The four planes are blurred as two f32x2 pairs: ring A = (x', e) and
+// ring B = (e^2, x'y').
 // The shared buffers are double buffered by step parity: step i's horizontal
 // phase reads buffer i % 2 while step i+1's vertical phase writes the other,
 // so one barrier per step orders them.
@@ -381,55 +375,26 @@ struct MapOut {
     long long mpitch, mplane;
 };
 
-// Scalar 9-tap FIR, the lane arithmetic of fir9p.
-__device__ __forceinline__ float fir9s(float a0, float a1, float a2, float a3, float a4, float a5, float a6,
-                                       float a7, float a8) {
-    float acc = S2_T4 * (a0 + a8);
-    acc = fmaf(S2_T3, a1 + a7, acc);
-    acc = fmaf(S2_T2, a2 + a6, acc);
-    acc = fmaf(S2_T1, a3 + a5, acc);
-    return fmaf(S2_T0, a4, acc);
-}
-
 __device__ __forceinline__ void s2_prefetch_l2(const void *p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 
-// Register rings of one vertical column (which are used depends on the mode).
+// Register rings of one vertical column.
 struct Rings {
-    float2 a[16];  // FULL (x', e); CAND (e, x'y')
-    float2 b[16];  // FULL (e^2, x'y')
-    float c[16];   // CAND e^2; REFMOM x'
+    float2 a[16];  // (x', e)
+    float2 b[16];  // (e^2, x'y')
 };
 
 // Shift one input row into ring slot `sl` (vr, vd: the reference and
 // distorted samples; cg: the anchor).  Outside the image both are the anchor,
 // so every plane is 0 there.
-template <int MODE>
 __device__ __forceinline__ void ring_in(Rings &R, int sl, float vr, float vd, float cg) {
     const float xp = vr - cg;
-    if (MODE == TM_REFMOM) {
-        R.c[sl] = xp;
-        return;
-    }
     const float e = vr - vd;
     const float xy = __fmul_rn(xp, vd - cg);  // products rounded on their own
     const float ee = __fmul_rn(e, e);
-    if (MODE == TM_FULL) {
-        R.a[sl] = make_float2(xp, e);
-        R.b[sl] = make_float2(ee, xy);
-    } else {
-        R.a[sl] = make_float2(e, xy);
-        R.c[sl] = ee;
-    }
+    R.a[sl] = make_float2(xp, e);
+    R.b[sl] = make_float2(ee, xy);
 }
 
-// One vertical step: the new input rows ybase .. ybase + 7 (those below the
-// image, or beyond the tile's nr output rows, are not needed) enter ring
-// slots S0 + 8 .. S0 + 15 (mod 16); output row k reads slots S0 + k ..
-// S0 + k + 8 and is stored to row k of the buffer: plane 0 the FIR of ring
-// a, plane 1 that of ring b (FULL) or of ring c as floats (CAND), plane 2
-// the raw (x', e) of the output row (FULL) or its raw e as floats (CAND; the
-// horizontal phase reads x' from the reference plane); REFMOM stores the FIR
-// of ring c to plane 0 as floats.
 // The input rows of one step: reference and distorted samples of this
 // thread's column.
 struct StepRows {
@@ -439,7 +404,7 @@ struct StepRows {
 // Loads the rows ybase .. ybase + 7 of the column.  inner: every column of
 // the tile and all 8 rows are inside the image and the tile (no masks);
 // otherwise rows and columns outside read the anchor.
-template <typename ST, int MODE>
+template <typename ST>
 __device__ __forceinline__ void v_load(StepRows &in, const ST *__restrict__ xr, const ST *__restrict__ xd,
                                        long long lp, int x, bool colin, int ybase, int H, int nr, bool inner,
                                        float cg) {
@@ -450,7 +415,7 @@ __device__ __forceinline__ void v_load(StepRows &in, const ST *__restrict__ xr, 
 #pragma unroll
         for (int k = 0; k < kStep; k++) {
             lr[k] = ld_store<ST>(pr);
-            ld[k] = MODE != TM_REFMOM ? ld_store<ST>(pd) : cg;
+            ld[k] = ld_store<ST>(pd);
             pr += lp;
             pd += lp;
         }
@@ -460,38 +425,29 @@ __device__ __forceinline__ void v_load(StepRows &in, const ST *__restrict__ xr, 
             const int y = ybase + k;
             const bool in = k < nr && colin && y < H;
             lr[k] = in ? ld_store<ST>(xr + (long long)y * lp + x) : cg;
-            ld[k] = (MODE != TM_REFMOM && in) ? ld_store<ST>(xd + (long long)y * lp + x) : cg;
+            ld[k] = in ? ld_store<ST>(xd + (long long)y * lp + x) : cg;
         }
     }
 }
 
-template <typename ST, int MODE, int S0>
+// One vertical step: the step's input rows enter ring slots S0 + 8 ..
+// S0 + 15 (mod 16); output row k reads slots S0 + k .. S0 + k + 8 and is
+// stored to row k of the buffer: plane 0 the FIR of ring a, plane 1 that of
+// ring b, plane 2 the raw (x', e) of the output row.
+template <int S0>
 __device__ __forceinline__ void v_step(Rings &R, const StepRows &in, int nr, float cg, float2 *__restrict__ buf,
                                        int col) {
 #pragma unroll
     for (int k = 0; k < kStep; k++) {
         if (k < nr) {
-            ring_in<MODE>(R, (S0 + 8 + k) & 15, in.r[k], in.d[k], cg);
+            ring_in(R, (S0 + 8 + k) & 15, in.r[k], in.d[k], cg);
 #define S2_R(a, j) a[(S0 + k + (j)) & 15]
-            if (MODE == TM_REFMOM) {
-                ((float *)buf)[k * 2 * kRS + col] =
-                    fir9s(S2_R(R.c, 0), S2_R(R.c, 1), S2_R(R.c, 2), S2_R(R.c, 3), S2_R(R.c, 4), S2_R(R.c, 5),
-                          S2_R(R.c, 6), S2_R(R.c, 7), S2_R(R.c, 8));
-            } else {
-                buf[k * kRS + col] = fir9p(S2_R(R.a, 0), S2_R(R.a, 1), S2_R(R.a, 2), S2_R(R.a, 3), S2_R(R.a, 4),
-                                           S2_R(R.a, 5), S2_R(R.a, 6), S2_R(R.a, 7), S2_R(R.a, 8));
-            }
-            if (MODE == TM_FULL) {
-                buf[kPlaneF2 + k * kRS + col] = fir9p(S2_R(R.b, 0), S2_R(R.b, 1), S2_R(R.b, 2), S2_R(R.b, 3),
-                                                      S2_R(R.b, 4), S2_R(R.b, 5), S2_R(R.b, 6), S2_R(R.b, 7),
-                                                      S2_R(R.b, 8));
-                buf[2 * kPlaneF2 + k * kRS + col] = S2_R(R.a, 4);  // raw (x', e)
-            } else if (MODE == TM_CAND) {
-                ((float *)(buf + kPlaneF2))[k * 2 * kRS + col] =
-                    fir9s(S2_R(R.c, 0), S2_R(R.c, 1), S2_R(R.c, 2), S2_R(R.c, 3), S2_R(R.c, 4), S2_R(R.c, 5),
-                          S2_R(R.c, 6), S2_R(R.c, 7), S2_R(R.c, 8));
-                ((float *)(buf + 2 * kPlaneF2))[k * 2 * kRS + col] = S2_R(R.a, 4).x;  // raw e
-            }
+            buf[k * kRS + col] = fir9p(S2_R(R.a, 0), S2_R(R.a, 1), S2_R(R.a, 2), S2_R(R.a, 3), S2_R(R.a, 4),
+                                       S2_R(R.a, 5), S2_R(R.a, 6), S2_R(R.a, 7), S2_R(R.a, 8));
+            buf[kPlaneF2 + k * kRS + col] = fir9p(S2_R(R.b, 0), S2_R(R.b, 1), S2_R(R.b, 2), S2_R(R.b, 3),
+                                                  S2_R(R.b, 4), S2_R(R.b, 5), S2_R(R.b, 6), S2_R(R.b, 7),
+                                                  S2_R(R.b, 8));
+            buf[2 * kPlaneF2 + k * kRS + col] = S2_R(R.a, 4);  // raw (x', e)
 #undef S2_R
         }
     }
@@ -510,23 +466,6 @@ __device__ __forceinline__ void h_fir4(const float2 *__restrict__ p, float2 o[4]
 #pragma unroll
     for (int j = 0; j < 4; j++)
         o[j] = fir9p(v[j], v[j + 1], v[j + 2], v[j + 3], v[j + 4], v[j + 5], v[j + 6], v[j + 7], v[j + 8]);
-}
-
-// The same on a float row (12 floats, three 16-byte loads).
-__device__ __forceinline__ void h_fir4s(const float *__restrict__ p, float o[4]) {
-    float v[12];
-    const float4 *q = (const float4 *)p;
-#pragma unroll
-    for (int j = 0; j < 3; j++) {
-        const float4 t = q[j];
-        v[4 * j] = t.x;
-        v[4 * j + 1] = t.y;
-        v[4 * j + 2] = t.z;
-        v[4 * j + 3] = t.w;
-    }
-#pragma unroll
-    for (int j = 0; j < 4; j++)
-        o[j] = fir9s(v[j], v[j + 1], v[j + 2], v[j + 3], v[j + 4], v[j + 5], v[j + 6], v[j + 7], v[j + 8]);
 }
 
 // Sums of one task's maps: (d, art, det) and their 4th powers, f32.
@@ -587,8 +526,6 @@ struct ItemGeo {
     int x0, y0, W, H, g;
     float cg;
     long long lp, plane;
-    float *mom;       // the moment planes of this scale (REFMOM, CAND)
-    const void *xr;   // this channel's reference plane (storage type)
 };
 
 __device__ __forceinline__ void add_task(Acc6 &acc, const TaskSums &ts) {
@@ -612,7 +549,7 @@ __device__ __forceinline__ void add_task(double *a, const TaskSums &ts) {
 
 // Horizontal phase of one step (output rows r0 .. r0 + nr - 1 of the tile):
 // this thread's task, row t_r, segment t_s; its sums are added to acc.
-template <typename ST, int MODE, bool EXPORT, typename ACC>
+template <bool EXPORT, typename ACC>
 __device__ __forceinline__ void h_step(const float2 *__restrict__ buf, int r0, int nr, int t_r, int t_s, bool t_on,
                                        const ItemGeo &G, ACC &&acc, const MapOut &mo) {
     if (!t_on || t_r >= nr) return;
@@ -620,20 +557,6 @@ __device__ __forceinline__ void h_step(const float2 *__restrict__ buf, int r0, i
     const int xc = G.x0 + c0;
     if (xc >= G.W) return;
     const int y = G.y0 + r0 + t_r;
-    if (MODE == TM_REFMOM) {
-        // blurred mu1 of 4 pixels at a time, 16-byte stores (a 4-pixel group
-        // starting inside the image stays inside the padded row)
-        float *mu = G.mom + G.g * G.plane + (long long)y * G.lp;
-#pragma unroll 1
-        for (int half = 0; half < kSegW / 4; half++) {
-            const int cc = c0 + 4 * half;
-            if (G.x0 + cc >= G.W) break;
-            float m1[4];
-            h_fir4s((const float *)buf + t_r * 2 * kRS + cc, m1);
-            *(float4 *)(mu + G.x0 + cc) = make_float4(m1[0], m1[1], m1[2], m1[3]);
-        }
-        return;
-    }
     const float bv = border_gain(y, G.H);
     const bool interior = bv == 1.0f && xc >= 4 && xc + kSegW + 4 <= G.W;
     TaskSums ts{0.0f, 0.0f, make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f)};
@@ -642,30 +565,9 @@ __device__ __forceinline__ void h_step(const float2 *__restrict__ buf, int r0, i
         const int cc = c0 + 4 * half;
         const float2 *pa = buf + t_r * kRS + cc;
         float2 mA[4], mB[4], rw[4];
-        if (MODE == TM_FULL) {
-            h_fir4(pa, mA);               // (mu1, md)
-            h_fir4(pa + kPlaneF2, mB);    // (blur(e^2), blur(x'y'))
-        } else {
-            if (G.x0 + cc >= G.W) break;
-            float2 ma[4];
-            float ee[4];
-            h_fir4(pa, ma);  // (md, blur(x'y'))
-            h_fir4s((const float *)(buf + kPlaneF2) + t_r * 2 * kRS + cc, ee);
-            const float4 mu1 = *(const float4 *)(G.mom + G.g * G.plane + (long long)y * G.lp + G.x0 + cc);
-            const float m1v[4] = {mu1.x, mu1.y, mu1.z, mu1.w};
-            const float4 e4 = *(const float4 *)((const float *)(buf + 2 * kPlaneF2) + t_r * 2 * kRS + cc + 4);
-            const float ev[4] = {e4.x, e4.y, e4.z, e4.w};
-            const ST *xr = (const ST *)G.xr + (long long)y * G.lp + G.x0 + cc;
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-                mA[j] = make_float2(m1v[j], ma[j].x);
-                mB[j] = make_float2(ee[j], ma[j].y);
-                // the raw x' of the pixel (0 beyond the image's last column)
-                const float xp = G.x0 + cc + j < G.W ? ld_store<ST>(xr + j) - G.cg : 0.0f;
-                rw[j] = make_float2(xp, ev[j]);
-            }
-        }
-        if (MODE == TM_FULL) {
+        h_fir4(pa, mA);             // (mu1, md)
+        h_fir4(pa + kPlaneF2, mB);  // (blur(e^2), blur(x'y'))
+        {
             const float4 *q = (const float4 *)(pa + 2 * kPlaneF2 + 4);
             const float4 t0 = q[0], t1 = q[1];
             rw[0] = make_float2(t0.x, t0.y);
@@ -734,10 +636,8 @@ __device__ __forceinline__ Item<ST> decode_item(const DevPair &P, const Seg &sg,
     it.nsteps = (it.rows_out + kStep - 1) / kStep;
     G.lp = P.lp[s];
     G.plane = G.lp * G.H;
-    G.mom = P.mom[s];
     it.xr = (const ST *)P.lvl[0][s] + g * G.plane;
     it.xd = (const ST *)P.lvl[1][s] + g * G.plane;
-    G.xr = it.xr;
     // anchor: reference XYB of channel g at the tile's first column, band start
     G.cg = ld_store<ST>(it.xr + (long long)((G.y0 / kBand) * kBand) * G.lp + G.x0);
     return it;
@@ -749,7 +649,7 @@ constexpr int kTileBlocks = 4;  // resident blocks per SM (registers: 128 per th
 // One warpgroup does both phases of a step in turn: the vertical phase of
 // step st to buffer st & 1, a barrier, then the horizontal phase; buffer b is
 // rewritten two steps later, after the barrier of the step in between.
-template <typename ST, int MODE, bool EXPORT>
+template <typename ST, bool EXPORT>
 __device__ __forceinline__ void flat_item(const Item<ST> &it, float2 *smb, int tid, double *s_acc,
                                           double (*s_warp)[6], double *__restrict__ partials, int item,
                                           const MapOut &mo) {
@@ -764,7 +664,7 @@ __device__ __forceinline__ void flat_item(const Item<ST> &it, float2 *smb, int t
     // (l >> 3) & 1 at the warp's first (l < 16) or last column, the at most
     // two lines a warp's row spans
     const int lane = tid & 31;
-    const ST *pf = (((lane >> 3) & 1) && MODE != TM_REFMOM ? it.xd : it.xr) +
+    const ST *pf = (((lane >> 3) & 1) ? it.xd : it.xr) +
                    min(max(x - lane + (lane < 16 ? 0 : 31), 0), G.W - 1);
     const int pf_y = G.y0 + 4 + (lane & 7);
     Rings R;
@@ -773,8 +673,8 @@ __device__ __forceinline__ void flat_item(const Item<ST> &it, float2 *smb, int t
         const int y = G.y0 - 4 + k;
         const bool in = colin && y >= 0 && y < G.H;
         const float lr = in ? ld_store<ST>(it.xr + (long long)y * G.lp + x) : cg;
-        const float ld = (MODE != TM_REFMOM && in) ? ld_store<ST>(it.xd + (long long)y * G.lp + x) : cg;
-        ring_in<MODE>(R, k, lr, ld, cg);
+        const float ld = in ? ld_store<ST>(it.xd + (long long)y * G.lp + x) : cg;
+        ring_in(R, k, lr, ld, cg);
     }
     // this thread's sums live in shared memory (s_acc[m * kFusedThreads +
     // tid]), out of the registers that the vertical rings need
@@ -793,7 +693,7 @@ __device__ __forceinline__ void flat_item(const Item<ST> &it, float2 *smb, int t
     auto load = [&](int st) {
         const int r = st * kStep, nr = min(kStep, it.rows_out - r);
         const bool inner = cols_in && nr == kStep && G.y0 + r + 4 + kStep <= G.H;
-        v_load<ST, MODE>(in, it.xr, it.xd, G.lp, x, colin, G.y0 + r + 4, G.H, nr, inner, cg);
+        v_load<ST>(in, it.xr, it.xd, G.lp, x, colin, G.y0 + r + 4, G.H, nr, inner, cg);
     };
     prefetch(0);
     prefetch(1);
@@ -802,38 +702,36 @@ __device__ __forceinline__ void flat_item(const Item<ST> &it, float2 *smb, int t
         const int nr0 = min(kStep, it.rows_out - r0);
         load(st);
         prefetch(st + 2);
-        v_step<ST, MODE, 0>(R, in, nr0, cg, buf0, tid);
+        v_step<0>(R, in, nr0, cg, buf0, tid);
         __syncthreads();
-        h_step<ST, MODE, EXPORT>(buf0, r0, nr0, t_r, t_s, t_on, G, acc, mo);
+        h_step<EXPORT>(buf0, r0, nr0, t_r, t_s, t_on, G, acc, mo);
         if (st + 1 < it.nsteps) {
             const int r1 = r0 + kStep;
             const int nr1 = min(kStep, it.rows_out - r1);
             load(st + 1);
             prefetch(st + 3);
-            v_step<ST, MODE, 8>(R, in, nr1, cg, buf1, tid);
+            v_step<8>(R, in, nr1, cg, buf1, tid);
             __syncthreads();
-            h_step<ST, MODE, EXPORT>(buf1, r1, nr1, t_r, t_s, t_on, G, acc, mo);
+            h_step<EXPORT>(buf1, r1, nr1, t_r, t_s, t_on, G, acc, mo);
         }
     }
-    if constexpr (MODE != TM_REFMOM) {
 #pragma unroll
-        for (int m = 0; m < 6; m++) {
-            double v = acc[m * kFusedThreads];
+    for (int m = 0; m < 6; m++) {
+        double v = acc[m * kFusedThreads];
 #pragma unroll
-            for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-            if ((tid & 31) == 0) s_warp[tid >> 5][m] = v;
-        }
-        __syncthreads();
-        if (tid < 6) {
-            double v = 0.0;
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+        if ((tid & 31) == 0) s_warp[tid >> 5][m] = v;
+    }
+    __syncthreads();
+    if (tid < 6) {
+        double v = 0.0;
 #pragma unroll
-            for (int w = 0; w < kFusedThreads / 32; w++) v += s_warp[w][tid];
-            partials[(long long)item * 6 + tid] = v;  // = tile * 18 + channel * 6 + m
-        }
+        for (int w = 0; w < kFusedThreads / 32; w++) v += s_warp[w][tid];
+        partials[(long long)item * 6 + tid] = v;  // = tile * 18 + channel * 6 + m
     }
 }
 
-template <typename ST, int MODE, bool EXPORT = false>
+template <typename ST, bool EXPORT = false>
 __global__ void __launch_bounds__(kFusedThreads, kTileBlocks)
     fused_kernel(const DevPair *__restrict__ pairs, const Seg *__restrict__ segs, int nseg, int first_item,
                  int end_item, int *__restrict__ counter, double *__restrict__ partials,
@@ -852,7 +750,7 @@ __global__ void __launch_bounds__(kFusedThreads, kTileBlocks)
         const int tile = item / 3, g = item - 3 * tile;
         const Seg sg = segs[find_seg(segs, nseg, tile)];
         const Item<ST> it = decode_item<ST>(pairs[sg.pair], sg, tile, g);
-        flat_item<ST, MODE, EXPORT && MODE != TM_REFMOM>(it, smb, tid, s_acc, s_warp, partials, item, mo);
+        flat_item<ST, EXPORT>(it, smb, tid, s_acc, s_warp, partials, item, mo);
     }
 }
 
@@ -951,9 +849,9 @@ cudaError_t upload_weights() { return cudaMemcpyToSymbol(c_weight, kWeights, siz
 size_t fused_smem_bytes() { return (size_t)2 * kBufF2 * sizeof(float2); }
 int fused_threads() { return kTileThreads; }
 
-template <typename ST, int MODE, bool EXPORT>
+template <bool EXPORT>
 static cudaError_t fused_attrs() {
-    const void *f = (const void *)fused_kernel<ST, MODE, EXPORT>;
+    const void *f = (const void *)fused_kernel<float, EXPORT>;
     // the tile pass is limited by registers and shared memory together: ask
     // for the largest shared-memory carveout so that 4 blocks fit per SM
     cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
@@ -961,19 +859,10 @@ static cudaError_t fused_attrs() {
     return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fused_smem_bytes());
 }
 
-template <typename ST>
-static cudaError_t fused_attrs_all() {
-    cudaError_t e;
-    if ((e = fused_attrs<ST, TM_FULL, false>()) != cudaSuccess) return e;
-    if ((e = fused_attrs<ST, TM_FULL, true>()) != cudaSuccess) return e;
-    if ((e = fused_attrs<ST, TM_CAND, false>()) != cudaSuccess) return e;
-    if ((e = fused_attrs<ST, TM_CAND, true>()) != cudaSuccess) return e;
-    return fused_attrs<ST, TM_REFMOM, false>();
-}
-
 cudaError_t configure_kernels() {
     cudaError_t e;
-    if ((e = fused_attrs_all<float>()) != cudaSuccess) return e;
+    if ((e = fused_attrs<false>()) != cudaSuccess) return e;
+    if ((e = fused_attrs<true>()) != cudaSuccess) return e;
     return configure_dssim_kernels();
 }
 
@@ -981,7 +870,7 @@ cudaError_t configure_kernels() {
 int fused_blocks_per_sm(int storage) {
     (void)storage;
     int n = 0;
-    const void *f = (const void *)fused_kernel<float, TM_FULL, false>;
+    const void *f = (const void *)fused_kernel<float, false>;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f, kTileThreads, fused_smem_bytes()) != cudaSuccess) return 1;
     return n > 0 ? n : 1;
 }
@@ -1006,44 +895,28 @@ cudaError_t launch_pyramid(int storage, const DevPair *pairs, int npairs, const 
     return cudaGetLastError();
 }
 
-template <typename ST, int MODE, bool EXPORT>
-static void fused_go(int grid, size_t sm, cudaStream_t st, const DevPair *pairs, const Seg *segs, int nseg, int fi,
-                     int ei, int *counter, double *partials, const MapOut &mo) {
-    fused_kernel<ST, MODE, EXPORT><<<grid, kTileThreads, sm, st>>>(pairs, segs, nseg, fi, ei, counter, partials, mo);
-}
-
-template <typename ST, bool EXPORT>
-static void fused_mode(int mode, int grid, size_t sm, cudaStream_t st, const DevPair *pairs, const Seg *segs,
-                       int nseg, int fi, int ei, int *counter, double *partials, const MapOut &mo) {
-    if (mode == TM_REFMOM) fused_go<ST, TM_REFMOM, false>(grid, sm, st, pairs, segs, nseg, fi, ei, counter, partials, mo);
-    else if (mode == TM_CAND) fused_go<ST, TM_CAND, EXPORT>(grid, sm, st, pairs, segs, nseg, fi, ei, counter, partials, mo);
-    else fused_go<ST, TM_FULL, EXPORT>(grid, sm, st, pairs, segs, nseg, fi, ei, counter, partials, mo);
-}
-
-cudaError_t launch_fused(int storage, int mode, const DevPair *pairs, const Seg *segs, int nseg, int first_tile,
-                         int end_tile, int *counter, double *partials, int grid, cudaStream_t st) {
+cudaError_t launch_fused(int storage, const DevPair *pairs, const Seg *segs, int nseg, int first_tile, int end_tile,
+                         int *counter, double *partials, int grid, cudaStream_t st) {
     const int fi = 3 * first_tile, ei = 3 * end_tile;  // work items: (tile, channel)
     const int nt = ei - fi;
     if (nt <= 0) return cudaSuccess;
     grid = grid > nt ? nt : grid;
-    const size_t sm = fused_smem_bytes();
-    const MapOut mo{nullptr, 0, 0};
     (void)storage;
-    fused_mode<float, false>(mode, grid, sm, st, pairs, segs, nseg, fi, ei, counter, partials, mo);
+    fused_kernel<float, false><<<grid, kTileThreads, fused_smem_bytes(), st>>>(pairs, segs, nseg, fi, ei, counter,
+                                                                              partials, MapOut{nullptr, 0, 0});
     return cudaGetLastError();
 }
 
-cudaError_t launch_fused_export(int storage, int mode, const DevPair *pairs, const Seg *segs, int nseg,
-                                int first_tile, int end_tile, int *counter, double *partials, float *maps,
-                                long long mpitch, long long mplane, int grid, cudaStream_t st) {
+cudaError_t launch_fused_export(int storage, const DevPair *pairs, const Seg *segs, int nseg, int first_tile,
+                                int end_tile, int *counter, double *partials, float *maps, long long mpitch,
+                                long long mplane, int grid, cudaStream_t st) {
     const int fi = 3 * first_tile, ei = 3 * end_tile;
     const int nt = ei - fi;
     if (nt <= 0) return cudaSuccess;
     grid = grid > nt ? nt : grid;
-    const size_t sm = fused_smem_bytes();
-    const MapOut mo{maps, mpitch, mplane};
     (void)storage;
-    fused_mode<float, true>(mode, grid, sm, st, pairs, segs, nseg, fi, ei, counter, partials, mo);
+    fused_kernel<float, true><<<grid, kTileThreads, fused_smem_bytes(), st>>>(pairs, segs, nseg, fi, ei, counter,
+                                                                             partials, MapOut{maps, mpitch, mplane});
     return cudaGetLastError();
 }
 

@@ -17,8 +17,7 @@ int fused_blocks_per_sm(int storage);
 cudaError_t launch_pyramid(int storage, const DevPair *pairs, int npairs, const int *blk_first, int first_block,
                            int end_block, const ColorConsts &cc, const float *lut, int grid, cudaStream_t st,
                            int out = 1);
-// mode: the TileMode of every tile in [first_tile, end_tile).
-cudaError_t launch_fused(int storage, int mode, const DevPair *pairs, const Seg *segs, int nseg, int first_tile,
+cudaError_t launch_fused(int storage, const DevPair *pairs, const Seg *segs, int nseg, int first_tile,
                          int end_tile, int *counter, double *partials, int grid, cudaStream_t st);
 cudaError_t launch_iir(int storage, const DevPair *pairs, const IirSeg *vsegs, int nvseg, int vtotal,
                        const IirSeg *hsegs, int nhseg, int htotal, double *partials, cudaStream_t st);
@@ -30,7 +29,7 @@ cudaError_t launch_desc_copy(void *dst, const void *src_host_mapped, size_t byte
 // pair, also storing each pixel's three error-map values to `maps` (9 float
 // planes [channel][ssim, artifact, detail], mpitch floats per row, mplane
 // floats per plane).
-cudaError_t launch_fused_export(int storage, int mode, const DevPair *pairs, const Seg *segs, int nseg,
+cudaError_t launch_fused_export(int storage, const DevPair *pairs, const Seg *segs, int nseg,
                                 int first_tile, int end_tile, int *counter, double *partials, float *maps,
                                 long long mpitch, long long mplane, int grid, cudaStream_t st);
 cudaError_t launch_finalize(const DevPair *pairs, int npairs, const double *partials, DevResult *out,

@@ -149,7 +149,6 @@ extern "C" s2_status s2_compute_srgb8_noalloc(const uint8_t *ref, size_t ref_pit
         sg.scale = s;
         sg.tiles_x = (P.w[s] + kTileW - 1) / kTileW;
         sg.strip_rows = strip;
-        sg.mode = TM_FULL;
         P.tile_base[s] = tiles;
         P.tile_cnt[s] = sg.tiles_x * ((P.h[s] + strip - 1) / strip);
         tiles += P.tile_cnt[s];
@@ -208,7 +207,7 @@ extern "C" s2_status s2_compute_srgb8_noalloc(const uint8_t *ref, size_t ref_pit
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (launch_pyramid(ST_F32, dp, 1, (const int *)(base + off_blk), 0, P.blk_x * P.blk_y, cc, lut, sms * 8, cs) !=
             cudaSuccess ||
-        launch_fused(ST_F32, TM_FULL, dp, (const Seg *)(base + off_seg), nseg, 0, tiles, (int *)(base + kOffCounter),
+        launch_fused(ST_F32, dp, (const Seg *)(base + off_seg), nseg, 0, tiles, (int *)(base + kOffCounter),
                      (double *)(base + off_part), sms * bps, cs) != cudaSuccess ||
         launch_finalize(dp, 1, (const double *)(base + off_part), (DevResult *)out_device, cs) != cudaSuccess)
         return fail("kernel launch");

@@ -18,9 +18,9 @@
 //               pending work -- the reference pyramid build (once per job) and
 //               candidates -- up to a pair / pixel cap, and runs it as one
 //               submission (prep + persistent fused + finalize launches);
-//               candidates read the job's resident reference pyramid and
-//               its blurred moments (built once per job, in the round that
-//               converts the reference, by a launch ahead of the candidates');
+//               candidates read the job's resident reference pyramid
+//               (built once per job, by the prep launch of the round that
+//               converts the reference, ahead of the candidates' tiles);
 //   overlap     two submission workspaces alternate: the worker plans and
 //               enqueues round i+1 while round i runs, then harvests round i;
 //   completion  a job completes when all its candidates are harvested; its
@@ -61,8 +61,6 @@ struct Job {
     size_t bytes = 0;
     size_t ref_levels_off = 0;
     size_t lvl_off[s2::kScales] = {0, 0, 0, 0, 0, 0};
-    size_t mom_off = 0;                                  // the reference's blurred moments
-    size_t mom_lvl[s2::kScales] = {0, 0, 0, 0, 0, 0};
     int ns = 0;
     cudaEvent_t uploaded = nullptr, up_start = nullptr;  // the job's uploads on the copy stream
     bool admitted = false, uploading = false, ref_scheduled = false, cancelled = false, finished = false;
@@ -110,15 +108,13 @@ struct s2_server {
 
     // Device bytes a job needs while admitted.
     // Layout: the images (reference, then candidates, packed rows), the
-    // reference's XYB pyramid, its blurred moments.
+    // reference's XYB pyramid.
     static size_t job_bytes(Job &j, size_t esize) {
         const size_t img = (size_t)j.w * 3 * j.h;
         size_t off = s2_align_up(img * (1 + j.cand_host.size()), 256);
         j.ref_levels_off = off;
         j.ns = s2_num_scales(j.w, j.h, S2_SCALES_CPU);
         off += s2_align_up(s2_image_levels_layout(j.w, j.h, j.ns, esize, j.lvl_off), 256);
-        j.mom_off = off;
-        off += s2_moment_layout(j.w, j.h, j.ns, j.mom_lvl);
         return off;
     }
 
@@ -237,11 +233,8 @@ struct s2_server {
             d[i].width = j->w;
             d[i].height = j->h;
             d[i].format = S2_FMT_SRGB8;
-            for (int s = 0; s < s2::kScales; s++) {
+            for (int s = 0; s < s2::kScales; s++)
                 ex[i].ref_levels[s] = s < j->ns ? j->dev + j->ref_levels_off + j->lvl_off[s] : nullptr;
-                ex[i].ref_mom[s] = s < j->ns ? j->dev + j->mom_off + j->mom_lvl[s] : nullptr;
-            }
-            ex[i].build_mom = r[i].cand < 0;  // the reference build also blurs its moments
             if (r[i].cand < 0) {
                 d[i].ref = j->dev;
                 d[i].ref_pitch = row;
