@@ -139,11 +139,11 @@ __global__ void __launch_bounds__(kDsThreads) dssim_clamp_kernel(const DsPair *_
 // Each blur stage fills an n x n buffer (n = 32 + 2 x its halo, even) from the
 // (n + 2)-wide buffer of the stage before.  A thread takes two adjacent
 // columns and kDsRun consecutive rows and slides a 3 x 4 window of the input
-// down them (two 8-byte shared loads per row).  Each input row's products
-// with the three distinct taps are formed once (scalar multiplies, which
-// -fmad=false keeps out of any fused multiply-add) and summed with one f32x2
-// add per tap for both columns, in the reference's row-major tap order:
-// every lane rounds as the scalar reference does.  The first tap initialises the sum, which equals 0 + tap
+// down them (two 8-byte shared loads per row).  Each tap is a scalar multiply
+// per column and one f32x2 add for both columns, in the reference's
+// row-major tap order: every lane rounds as the scalar reference does (the
+// products are scalar multiplies, which -fmad=false keeps out of any fused
+// multiply-add).  The first tap initialises the sum, which equals 0 + tap
 // for every tap but -0 (no Lab value or product of two is -0 where it
 // matters: the sign of a zero sum does not reach the SSIM).  x^2, y^2 and xy
 // are formed once per input position, so the first statistics blur is five
@@ -153,43 +153,26 @@ __global__ void __launch_bounds__(kDsThreads) dssim_clamp_kernel(const DsPair *_
 // next stage reads there with clamped indexes.
 constexpr int kDsRun = 4;
 
-// The kernel has three distinct taps (corners, edges, centre), so the
-// products of one input row (columns c - 1 .. c + 2) with them are formed
-// once and serve the row in all three of its roles -- top, middle and bottom
-// row of the 3 x 3 window -- for both output columns c and c + 1.  Each
-// product is the same single-rounded value the reference forms for that tap.
-struct DsRowP {
-    float2 k0a, k0b;  // corner tap x (v0, v1), (v2, v3)
-    float2 k1m;       // edge tap x (v1, v2): top and bottom rows
-    float2 k1a, k1b;  // edge tap x (v0, v1), (v2, v3): middle row
-    float2 k2m;       // centre tap x (v1, v2)
-};
-
-__device__ __forceinline__ DsRowP ds_row(const float *src) {
-    const float2 a = *(const float2 *)src, b = *(const float2 *)(src + 2);
-    const float k0 = ds_k(0), k1 = ds_k(1), k2 = ds_k(4);
-    DsRowP p;
-    p.k0a = make_float2(a.x * k0, a.y * k0);
-    p.k0b = make_float2(b.x * k0, b.y * k0);
-    p.k1m = make_float2(a.y * k1, b.x * k1);
-    p.k1a = make_float2(a.x * k1, a.y * k1);
-    p.k1b = make_float2(b.x * k1, b.y * k1);
-    p.k2m = make_float2(a.y * k2, b.x * k2);
-    return p;
+__device__ __forceinline__ float2 ds_sum9x2(const float (&w)[3][4]) {
+    float2 sum = make_float2(w[0][0] * ds_k(0), w[0][1] * ds_k(0));
+#pragma unroll
+    for (int i = 1; i < 9; i++) {
+        const int ky = i / 3, kx = i % 3;
+        const float k = ds_k(i);
+        sum = __fadd2_rn(sum, make_float2(w[ky][kx] * k, w[ky][kx + 1] * k));
+    }
+    return sum;
 }
 
-// 3x3 blur at (c, c + 1): the nine taps in the reference's row-major order,
-// the first initialising the sum
-__device__ __forceinline__ float2 ds_sum9p(const DsRowP &t, const DsRowP &m, const DsRowP &b) {
-    float2 sum = t.k0a;
-    sum = __fadd2_rn(sum, t.k1m);
-    sum = __fadd2_rn(sum, t.k0b);
-    sum = __fadd2_rn(sum, m.k1a);
-    sum = __fadd2_rn(sum, m.k2m);
-    sum = __fadd2_rn(sum, m.k1b);
-    sum = __fadd2_rn(sum, b.k0a);
-    sum = __fadd2_rn(sum, b.k1m);
-    return __fadd2_rn(sum, b.k0b);
+__device__ __forceinline__ void ds_load4(float (&row)[4], const float *src) {
+    const float2 a = *(const float2 *)src, b = *(const float2 *)(src + 2);
+    row[0] = a.x, row[1] = a.y, row[2] = b.x, row[3] = b.y;
+}
+
+__device__ __forceinline__ void ds_slide(float (&w)[3][4], const float *src) {
+#pragma unroll
+    for (int kx = 0; kx < 4; kx++) w[0][kx] = w[1][kx], w[1][kx] = w[2][kx];
+    ds_load4(w[2], src);
 }
 
 // `planes` planes: out[p] (n x n) = 3x3 blur of in[p] (pitch n + 2, plane (n + 2)^2)
@@ -200,14 +183,14 @@ __device__ __forceinline__ void ds_stage_blur(const float *in, float *out, int n
         const int c = 2 * (q % half), j0 = (q / half) * kDsRun;
         const float *src = in + p * m * m + c;
         float *dst = out + p * n * n + c;
-        DsRowP t = ds_row(src + j0 * m), mid = ds_row(src + (j0 + 1) * m);
+        float w[3][4];
+        ds_load4(w[1], src + j0 * m);
+        ds_load4(w[2], src + (j0 + 1) * m);
 #pragma unroll
         for (int r = 0; r < kDsRun; r++) {
             if (j0 + r >= n) break;
-            const DsRowP b = ds_row(src + (j0 + r + 2) * m);
-            *(float2 *)(dst + (j0 + r) * n) = ds_sum9p(t, mid, b);
-            t = mid;
-            mid = b;
+            ds_slide(w, src + (j0 + r + 2) * m);
+            *(float2 *)(dst + (j0 + r) * n) = ds_sum9x2(w);
         }
     }
 }
@@ -366,13 +349,13 @@ __global__ void __launch_bounds__(kDsThreads, 3) dssim_tile_kernel(const DsPair 
 #pragma unroll
             for (int pl = 0; pl < 5; pl++) {
                 const float *src = bufB + pl * nnB + c0;
-                DsRowP t = ds_row(src + r0 * kDsB), mid = ds_row(src + (r0 + 1) * kDsB);
+                float w[3][4];
+                ds_load4(w[1], src + r0 * kDsB);
+                ds_load4(w[2], src + (r0 + 1) * kDsB);
 #pragma unroll
                 for (int r = 0; r < kDsOutRows; r++) {
-                    const DsRowP b = ds_row(src + (r0 + r + 2) * kDsB);
-                    q[pl][r] = ds_sum9p(t, mid, b);
-                    t = mid;
-                    mid = b;
+                    ds_slide(w, src + (r0 + r + 2) * kDsB);
+                    q[pl][r] = ds_sum9x2(w);
                 }
             }
 #pragma unroll

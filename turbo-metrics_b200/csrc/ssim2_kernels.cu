@@ -525,7 +525,7 @@ struct Acc6 {
 struct ItemGeo {
     int x0, y0, W, H, g;
     float cg;
-    long long lp, plane;
+    int lp;  // row pitch of the planes (elements)
 };
 
 __device__ __forceinline__ void add_task(Acc6 &acc, const TaskSums &ts) {
@@ -635,9 +635,9 @@ __device__ __forceinline__ Item<ST> decode_item(const DevPair &P, const Seg &sg,
     it.rows_out = min(G.y0 + sg.strip_rows, G.H) - G.y0;
     it.nsteps = (it.rows_out + kStep - 1) / kStep;
     G.lp = P.lp[s];
-    G.plane = G.lp * G.H;
-    it.xr = (const ST *)P.lvl[0][s] + g * G.plane;
-    it.xd = (const ST *)P.lvl[1][s] + g * G.plane;
+    const long long plane = (long long)G.lp * G.H;
+    it.xr = (const ST *)P.lvl[0][s] + g * plane;
+    it.xd = (const ST *)P.lvl[1][s] + g * plane;
     // anchor: reference XYB of channel g at the tile's first column, band start
     G.cg = ld_store<ST>(it.xr + (long long)((G.y0 / kBand) * kBand) * G.lp + G.x0);
     return it;
