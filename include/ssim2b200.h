@@ -223,9 +223,9 @@ int32_t s2_has_reference(const s2_ctx *ctx);
  * detail-loss maps of `scale` to the device buffer `maps` as 9 float planes
  * [channel X, Y, B][ssim, artifact, detail], each h_s rows of `pitch` bytes
  * (w_s = ceil(w / 2^scale), h_s likewise).  Enqueued on `stream` after that
- * compute (its planes must not have been overwritten by another compute).
- * FIR blur only (S2_ERR_INVALID_ARG for S2_BLUR_IIR_REF); S2_ERR_NOT_READY
- * before a scored compute. */
+ * compute (its planes must not have been overwritten by another compute);
+ * returns when the maps are written.  FIR blur only (S2_ERR_INVALID_ARG for
+ * S2_BLUR_IIR_REF); S2_ERR_NOT_READY before a scored compute. */
 s2_status s2_error_maps(s2_ctx *ctx, int32_t scale, float *maps, size_t pitch, void *stream);
 
 /* ---- batches of pairs of uneven sizes ---------------------------------- */

@@ -722,10 +722,19 @@ s2_status s2_error_maps(s2_ctx *ctx, int32_t scale, float *maps, size_t pitch, v
     char *dbase = (char *)e.pairs_d.p;
     cudaStream_t st = (cudaStream_t)stream;
     const long long mpitch = (long long)(pitch / sizeof(float));
-    S2_CUDA(cudaMemsetAsync(e.counter_d.p, 0, sizeof(int), st));
+    S2_CUDA(cudaMemsetAsync(e.counter_d.p, 0, Engine::kCounterBytes, st));
     S2_CUDA(launch_fused_export(e.storage, (const DevPair *)dbase, (const Seg *)(dbase + pb + bb),
-                                (int)P.segs.size(), t0, t1, (int *)e.counter_d.p, (double *)e.partials_d.p, maps,
-                                mpitch, mpitch * p.h[scale], e.num_sms * e.fused_bps, st));
+                                (int)P.segs.size(), t0, t1, (int *)e.counter_d.p, e.err_word(),
+                                (double *)e.partials_d.p, maps, mpitch, mpitch * p.h[scale], e.num_sms * e.fused_bps,
+                                st));
+    // the tile pass's time-out word (set only if its row copies never landed)
+    int err = 0;
+    S2_CUDA(cudaMemcpyAsync(&err, e.err_word(), sizeof err, cudaMemcpyDeviceToHost, st));
+    S2_CUDA(cudaStreamSynchronize(st));
+    if (err) {
+        g_last_error = "tile pass: row copies timed out";
+        return S2_ERR_CUDA;
+    }
     return S2_OK;
 }
 

@@ -185,6 +185,10 @@ struct Engine {
     ColorConsts cc;
 
     DevBuf pairs_d, blk_d, segs_d, counter_d, partials_d, results_d, levels_d, lut_d, iir_d;
+    // counter_d: the tile groups' work counters (ints 0..), and at its last
+    // int the tile pass's error word; all zeroed before every submission
+    static constexpr size_t kCounterBytes = 256;
+    int *err_word() const { return (int *)counter_d.p + kCounterBytes / sizeof(int) - 1; }
     DevBuf ds_d;  // DSSIM: per-tile SSIM sums, per-tile |avg - ssim| sums, per-level avg
     void *pinned = nullptr;  // staging: pairs | blk_first | segs
     size_t pinned_n = 0;
@@ -245,7 +249,7 @@ struct Engine {
         st = ensure(lut_d, sizeof s2_srgb8_lut);
         if (st != S2_OK) return st;
         S2_CUDA(cudaMemcpy(lut_d.p, s2_srgb8_lut, sizeof s2_srgb8_lut, cudaMemcpyHostToDevice));
-        st = ensure(counter_d, 256);
+        st = ensure(counter_d, kCounterBytes);
         return st;
     }
 
@@ -785,7 +789,7 @@ struct Engine {
             S2_CUDA(cudaEventRecord(sub_start, copy_st));
             S2_CUDA(cudaStreamWaitEvent(st, sub_start, 0));
         }
-        S2_CUDA(cudaMemsetAsync(counter_d.p, 0, ng * sizeof(int), st));
+        S2_CUDA(cudaMemsetAsync(counter_d.p, 0, kCounterBytes, st));
         if (profiling) S2_CUDA(cudaEventRecord(prof[0], st));
         cudaStream_t pst = split ? prep_st : st;
         for (int g = 0; g < ng; g++) {
@@ -827,12 +831,14 @@ struct Engine {
                                    P.htotal, (double *)partials_d.p, st));
             else
                 S2_CUDA(launch_fused(storage, dpairs, dsegs, (int)P.segs.size(), P.grp_tile[g], P.grp_tile[g + 1],
-                                     (int *)counter_d.p + g, (double *)partials_d.p, num_sms * fused_bps, st));
+                                     (int *)counter_d.p + g, err_word(), (double *)partials_d.p, num_sms * fused_bps,
+                                     st));
         }
         // several groups interleave prep and fused: the fused slot then holds both
         if (profiling && ng > 1) S2_CUDA(cudaEventRecord(prof[1], st));
         if (profiling) S2_CUDA(cudaEventRecord(prof[2], st));
-        if (m_s2) S2_CUDA(launch_finalize(dpairs, n, (const double *)partials_d.p, (DevResult *)results_d.p, st));
+        if (m_s2)
+            S2_CUDA(launch_finalize(dpairs, n, (const double *)partials_d.p, err_word(), (DevResult *)results_d.p, st));
         if (profiling) S2_CUDA(cudaEventRecord(prof[3], st));
         if (m_ds) S2_CUDA(launch_ds(P, dbase, st));
         if (profiling) S2_CUDA(cudaEventRecord(prof[4], st));
@@ -881,7 +887,7 @@ struct Engine {
         }
         cudaError_t e = desc_kernel ? launch_desc_copy(dbase, pinned_dev, desc_bytes, cap_st)
                                     : cudaMemcpyAsync(dbase, pinned, desc_bytes, cudaMemcpyHostToDevice, cap_st);
-        if (e == cudaSuccess) e = cudaMemsetAsync(counter_d.p, 0, sizeof(int), cap_st);
+        if (e == cudaSuccess) e = cudaMemsetAsync(counter_d.p, 0, kCounterBytes, cap_st);
         if (e == cudaSuccess)
             e = launch_pyramid(storage, dpairs, n, (const int *)(dbase + pb), 0, P.total_blocks, cc,
                                (const float *)lut_d.p, num_sms * 8, cap_st, (m_s2 ? 1 : 0) | (m_ds ? 2 : 0));
@@ -892,11 +898,11 @@ struct Engine {
                                (double *)partials_d.p, cap_st);
             else
                 e = launch_fused(storage, dpairs, (const Seg *)(dbase + pb + bb), (int)P.segs.size(), 0,
-                                 P.total_tiles, (int *)counter_d.p, (double *)partials_d.p, num_sms * fused_bps,
-                                 cap_st);
+                                 P.total_tiles, (int *)counter_d.p, err_word(), (double *)partials_d.p,
+                                 num_sms * fused_bps, cap_st);
         }
         if (e == cudaSuccess && m_s2)
-            e = launch_finalize(dpairs, n, (const double *)partials_d.p, (DevResult *)results_d.p, cap_st);
+            e = launch_finalize(dpairs, n, (const double *)partials_d.p, err_word(), (DevResult *)results_d.p, cap_st);
         if (e == cudaSuccess && m_ds) e = launch_ds(P, dbase, cap_st);
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(results_h, results_d.p, n * sizeof(DevResult), cudaMemcpyDeviceToHost, cap_st);

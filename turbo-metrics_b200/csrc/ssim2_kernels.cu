@@ -27,14 +27,15 @@
 // removes the f32 cancellation in sigma - mu^2; the shift is undone
 // algebraically (including at image borders, where the blur of a constant is
 // not the constant).
+#include "../../include/ssim2b200.h"
 #include "ssim2_device.cuh"
 
 namespace s2 {
 
-// Shared memory of fused_kernel (one CTA = one channel of a tile): two
-// buffers (step parity), each three float2 planes of kStep rows x kRS
-// columns -- plane 0 and 1 the vertical FIRs, plane 2 the raw (x', e) of the
-// output rows.  A horizontal task reads 16-byte words of one row; the 8
+// Shared memory of fused_kernel (one CTA = one channel of a tile): the step
+// buffer, three float2 planes of kStep rows x kRS columns -- plane 0 and 1
+// the vertical FIRs, plane 2 the raw (x', e) of the output rows -- then two
+// stages of input rows (filled by bulk copies) and the threads' f64 sums.  A horizontal task reads 16-byte words of one row; the 8
 // lanes of a load phase take the same segment of rows 0..7, whose starts are
 // kRS * 8 = 1040 bytes apart: 65 16-byte groups, odd, so the 8 rows fall in
 // distinct bank groups.
@@ -337,20 +338,23 @@ __global__ void __launch_bounds__(kPrepThreads, 4) prep_kernel(const DevPair *__
 // walk down the tile in steps of kStep (8) rows; each step has two phases.
 //
 //   vertical    thread c owns input column x0 - 4 + c (the tile's columns and
-//               a 4-column halo on each side).  It keeps the shifted inputs of
-//               its column in register rings of 16 rows, where x' = ref -
+//               a 4-column halo on each side).  The step's 8 input rows of
+//               both images are already in shared memory: the bulk-copy
+//               engine (cp.async.bulk, completion on an mbarrier) brought
+//               them in two steps ahead.  The thread keeps the shifted inputs
+//               of its column in register rings of 16 rows, where x' = ref -
 //               anchor and y' = dis - anchor, and for each output row of the
 //               step forms their 9-tap vertical FIRs.  The step's 8 new input
 //               rows go to ring slots 8..15 on even steps and 0..7 on odd
 //               steps, so every ring index is a compile-time constant.
-//               Pixels outside the image load the anchor itself, which shifts
+//               Pixels outside the image read the anchor itself, which shifts
 //               to exactly 0: zero padding of the shifted values, undone at
 //               the borders by border_gain.
 //   horizontal  thread t takes row t % 8 of the step and the 8-pixel segment
 //               t / 8 (120 tasks): the horizontal FIRs give the blurred
 //               moments, then the SSIM error, artifact and detail-loss maps
 //               and their sums and fourth-power sums, in f32 over the
-//               segment, then in f64 per thread.
+//               segment, then in f64 per thread (kept in shared memory).
 //
 // What is blurred: with x' = ref - anchor, y' = dis - anchor and the
 // difference e = ref - dis, the four planes x', e, e^2 and x'y'.  Then
@@ -362,10 +366,8 @@ __global__ void __launch_bounds__(kPrepThreads, 4) prep_kernel(const DevPair *__
 // which f32 cannot do to the metric's precision.
 //
 // The four planes are blurred as two f32x2 pairs: ring A = (x', e) and
-// ring B = (e^2, x'y').
-// The shared buffers are double buffered by step parity: step i's horizontal
-// phase reads buffer i % 2 while step i+1's vertical phase writes the other,
-// so one barrier per step orders them.
+// ring B = (e^2, x'y').  A barrier follows each phase (one step buffer: a
+// second one would not leave room for four blocks per SM).
 //
 // EXPORT (error-map export, one scale of one pair): every pixel's SSIM error,
 // artifact and detail-loss values are also stored to `maps`, 9 planes
@@ -374,8 +376,6 @@ struct MapOut {
     float *maps;
     long long mpitch, mplane;
 };
-
-__device__ __forceinline__ void s2_prefetch_l2(const void *p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 
 // Register rings of one vertical column.
 struct Rings {
@@ -395,38 +395,74 @@ __device__ __forceinline__ void ring_in(Rings &R, int sl, float vr, float vd, fl
     R.b[sl] = make_float2(ee, xy);
 }
 
-// The input rows of one step: reference and distorted samples of this
-// thread's column.
+// ---- input rows through the bulk-copy engine -------------------------------
+// A stage holds 8 input rows of the tile's 128 columns of both images
+// ([image][row][column] floats, 8 KB).  Each row of each image is one
+// cp.async.bulk copy (global -> shared, completion counted in bytes on the
+// stage's mbarrier): the columns [x0 - 4, x0 + 124) clipped to [0, pitch), so
+// every copy starts 16-byte aligned (x0 is a multiple of 120, the pitch of 64
+// elements, the planes 256-byte aligned) and never leaves its row.  Rows and
+// columns outside the image are not copied; their stage words are stale and
+// the vertical phase replaces them by the anchor.
+constexpr int kStageFloats = 2 * kStep * kCols;  // 8 KB
+constexpr int kStages = 2;
+
+__device__ __forceinline__ unsigned s2_smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void s2_mbar_init(uint64_t *bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(s2_smem_addr(bar)) : "memory");
+}
+
+__device__ __forceinline__ void s2_mbar_expect(uint64_t *bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(s2_smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void s2_bulk_g2s(void *dst, const void *src, unsigned bytes, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            s2_smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(s2_smem_addr(bar))
+        : "memory");
+}
+
+// Wait for the stage's phase `parity`, at most about one second (clock64 at
+// the SM clock); on time-out set *err and return false.
+__device__ __forceinline__ bool s2_mbar_wait(uint64_t *bar, unsigned parity, int *err) {
+    const unsigned a = s2_smem_addr(bar);
+    const long long t0 = clock64();
+    for (;;) {
+        unsigned done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, "
+            "p;\n\t}"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if (clock64() - t0 > (1ll << 31)) {
+            atomicExch(err, 1);
+            return false;
+        }
+    }
+}
+
+// The 8 rows of a stage for this thread's column.  inner: every column of
+// the tile and all 8 rows are inside the image; otherwise rows and columns
+// outside read the anchor (rows beyond the tile's nr output rows are not
+// used).
 struct StepRows {
     float r[kStep], d[kStep];
 };
 
-// Loads the rows ybase .. ybase + 7 of the column.  inner: every column of
-// the tile and all 8 rows are inside the image and the tile (no masks);
-// otherwise rows and columns outside read the anchor.
-template <typename ST>
-__device__ __forceinline__ void v_load(StepRows &in, const ST *__restrict__ xr, const ST *__restrict__ xd,
-                                       long long lp, int x, bool colin, int ybase, int H, int nr, bool inner,
-                                       float cg) {
-    float *lr = in.r, *ld = in.d;
-    if (inner) {
-        const ST *pr = xr + (long long)ybase * lp + x;
-        const ST *pd = xd + (long long)ybase * lp + x;
+__device__ __forceinline__ void v_load(StepRows &in, const float *stage, int col, bool colin, int ybase, int H,
+                                       bool inner, float cg) {
 #pragma unroll
-        for (int k = 0; k < kStep; k++) {
-            lr[k] = ld_store<ST>(pr);
-            ld[k] = ld_store<ST>(pd);
-            pr += lp;
-            pd += lp;
-        }
-    } else {
-#pragma unroll
-        for (int k = 0; k < kStep; k++) {
-            const int y = ybase + k;
-            const bool in = k < nr && colin && y < H;
-            lr[k] = in ? ld_store<ST>(xr + (long long)y * lp + x) : cg;
-            ld[k] = in ? ld_store<ST>(xd + (long long)y * lp + x) : cg;
-        }
+    for (int k = 0; k < kStep; k++) {
+        const float vr = stage[k * kCols + col], vd = stage[(kStep + k) * kCols + col];
+        const bool ok = inner || (colin && ybase + k >= 0 && ybase + k < H);
+        in.r[k] = ok ? vr : cg;
+        in.d[k] = ok ? vd : cg;
     }
 }
 
@@ -516,10 +552,6 @@ __device__ __forceinline__ void maps_px(float2 m, float2 s, float2 r, float kk, 
     det = fmaxf(-d1, 0.0f);
 }
 
-// Pooled sums of one work item, per thread (f64).
-struct Acc6 {
-    double v[6];
-};
 
 // What a horizontal task needs of its work item.
 struct ItemGeo {
@@ -528,16 +560,7 @@ struct ItemGeo {
     int lp;  // row pitch of the planes (elements)
 };
 
-__device__ __forceinline__ void add_task(Acc6 &acc, const TaskSums &ts) {
-    acc.v[0] += (double)ts.fs_d;
-    acc.v[1] += (double)ts.fs_ad.x;
-    acc.v[2] += (double)ts.fs_ad.y;
-    acc.v[3] += (double)ts.f4_d;
-    acc.v[4] += (double)ts.f4_ad.x;
-    acc.v[5] += (double)ts.f4_ad.y;
-}
 
-// The same into per-thread sums kept in shared memory (a[m * kFusedThreads]).
 __device__ __forceinline__ void add_task(double *a, const TaskSums &ts) {
     a[0] += (double)ts.fs_d;
     a[kFusedThreads] += (double)ts.fs_ad.x;
@@ -644,15 +667,47 @@ __device__ __forceinline__ Item<ST> decode_item(const DevPair &P, const Seg &sg,
 }
 
 constexpr int kTileThreads = kFusedThreads;
-constexpr int kTileBlocks = 4;  // resident blocks per SM (registers: 128 per thread)
+constexpr int kTileBlocks = 4;  // resident blocks per SM (128 registers per thread, 47 KB shared)
 
 // One warpgroup does both phases of a step in turn: the vertical phase of
 // step st to buffer st & 1, a barrier, then the horizontal phase; buffer b is
 // rewritten two steps later, after the barrier of the step in between.
+// Issue the copies of stage load L of the item (input rows
+// y0 - 4 + 8 L .. + 7) into `stage`, completing on `bar`.  Run by warp 0:
+// lane 0 announces the bytes, lanes 0..15 copy one row each (lane >> 3 the
+// image, lane & 7 the row).
+template <typename ST>
+__device__ __forceinline__ void issue_rows(const Item<ST> &it, int L, float *stage, uint64_t *bar, int lane) {
+    const ItemGeo &G = it.G;
+    const int ybase = G.y0 - 4 + kStep * L;
+    const int xs = max(G.x0 - 4, 0), xe = min(G.x0 + kCols - 4, G.lp);
+    const unsigned bytes = (unsigned)(xe - xs) * (unsigned)sizeof(ST);
+    const int rows = max(0, min(kStep, G.H - ybase) - max(0, -ybase));  // rows inside [0, H)
+    // order this CTA's earlier generic reads of the stage before the async
+    // copies that overwrite it
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if (lane == 0) s2_mbar_expect(bar, 2u * (unsigned)rows * bytes);
+    __syncwarp();
+    if (lane < 2 * kStep) {
+        const int img = lane >> 3, k = lane & 7, y = ybase + k;
+        if (y >= 0 && y < G.H) {
+            const ST *src = (img ? it.xd : it.xr) + (long long)y * G.lp + xs;
+            s2_bulk_g2s(stage + (img * kStep + k) * kCols + (xs - (G.x0 - 4)), src, bytes, bar);
+        }
+    }
+}
+
+// One work item.  Stage load L (L = 0: the 8 priming rows y0 - 4 .. y0 + 3;
+// L = st + 1: the rows of step st) goes to stage L % 2, issued two loads
+// ahead: loads 0 and 1 at the start, load 2 after the priming rows are read,
+// load st + 3 right after the barrier that follows step st's vertical phase
+// (every thread has then read stage (st + 1) % 2, which it overwrites).  All
+// loads of an item are consumed before it ends.  `phase` holds each stage's
+// expected mbarrier parity (bit s), the same in every thread.
 template <typename ST, bool EXPORT>
-__device__ __forceinline__ void flat_item(const Item<ST> &it, float2 *smb, int tid, double *s_acc,
-                                          double (*s_warp)[6], double *__restrict__ partials, int item,
-                                          const MapOut &mo) {
+__device__ __forceinline__ bool flat_item(const Item<ST> &it, float2 *smb, float *stages, uint64_t *bars,
+                                          unsigned &phase, int *err, int tid, double (*s_warp)[6],
+                                          double *__restrict__ partials, int item, const MapOut &mo) {
     const ItemGeo &G = it.G;
     const float cg = G.cg;
     const int x = G.x0 - 4 + tid;
@@ -660,64 +715,52 @@ __device__ __forceinline__ void flat_item(const Item<ST> &it, float2 *smb, int t
     const bool cols_in = G.x0 >= 4 && G.x0 + kCols - 4 <= G.W;  // every column of the tile
     const int t_r = tid % kStep, t_s = tid / kStep;
     const bool t_on = tid < kTasks;
-    // L2 prefetch of a step's input rows: lane l takes row l & 7 of image
-    // (l >> 3) & 1 at the warp's first (l < 16) or last column, the at most
-    // two lines a warp's row spans
     const int lane = tid & 31;
-    const ST *pf = (((lane >> 3) & 1) ? it.xd : it.xr) +
-                   min(max(x - lane + (lane < 16 ? 0 : 31), 0), G.W - 1);
-    const int pf_y = G.y0 + 4 + (lane & 7);
-    Rings R;
-#pragma unroll
-    for (int k = 0; k < 8; k++) {
-        const int y = G.y0 - 4 + k;
-        const bool in = colin && y >= 0 && y < G.H;
-        const float lr = in ? ld_store<ST>(it.xr + (long long)y * G.lp + x) : cg;
-        const float ld = in ? ld_store<ST>(it.xd + (long long)y * G.lp + x) : cg;
-        ring_in(R, k, lr, ld, cg);
+    const bool producer = tid < 32;
+    bool ok = true;
+    auto stage = [&](int L) { return stages + (L & 1) * kStageFloats; };
+    auto wait = [&](int L) {
+        const int sidx = L & 1;
+        ok &= s2_mbar_wait(&bars[sidx], (phase >> sidx) & 1u, err);
+        phase ^= 1u << sidx;
+    };
+    if (producer) {
+        issue_rows<ST>(it, 0, stage(0), &bars[0], lane);
+        issue_rows<ST>(it, 1, stage(1), &bars[1], lane);
     }
-    // this thread's sums live in shared memory (s_acc[m * kFusedThreads +
-    // tid]), out of the registers that the vertical rings need
-    double *acc = s_acc + tid;
+    Rings R;
+    wait(0);
+    {
+        StepRows in;
+        v_load(in, stage(0), tid, colin, G.y0 - 4, G.H, cols_in && G.y0 >= 4 && G.y0 + 4 <= G.H, cg);
 #pragma unroll
-    for (int m = 0; m < 6; m++) acc[m * kFusedThreads] = 0.0;
-    float2 *buf0 = smb, *buf1 = smb + kBufF2;
-    auto prefetch = [&](int st) {  // the input rows of step st
-        const int y = pf_y + st * kStep;
-        if (st < it.nsteps && y < G.H) s2_prefetch_l2(pf + (long long)y * G.lp);
-    };
-    // the rows of step st (loaded right before its vertical phase: held a
-    // step ahead, they would need registers that 4 blocks per SM do not have;
-    // the L2 prefetch two steps ahead shortens their wait instead)
-    StepRows in;
-    auto load = [&](int st) {
+        for (int k = 0; k < 8; k++) ring_in(R, k, in.r[k], in.d[k], cg);
+    }
+    __syncthreads();  // stage 0 read by every thread
+    if (producer && it.nsteps >= 2) issue_rows<ST>(it, 2, stage(2), &bars[0], lane);
+    float2 *const buf = smb;
+    double *sacc = (double *)(stages + kStages * kStageFloats) + tid;
+#pragma unroll
+    for (int m = 0; m < 6; m++) sacc[m * kFusedThreads] = 0.0;
+    auto step = [&](int st, auto s0) {
         const int r = st * kStep, nr = min(kStep, it.rows_out - r);
-        const bool inner = cols_in && nr == kStep && G.y0 + r + 4 + kStep <= G.H;
-        v_load<ST>(in, it.xr, it.xd, G.lp, x, colin, G.y0 + r + 4, G.H, nr, inner, cg);
-    };
-    prefetch(0);
-    prefetch(1);
-    for (int st = 0; st < it.nsteps; st += 2) {
-        const int r0 = st * kStep;
-        const int nr0 = min(kStep, it.rows_out - r0);
-        load(st);
-        prefetch(st + 2);
-        v_step<0>(R, in, nr0, cg, buf0, tid);
+        const int ybase = G.y0 + r + 4;
+        wait(st + 1);
+        StepRows in;
+        v_load(in, stage(st + 1), tid, colin, ybase, G.H, cols_in && nr == kStep && ybase + kStep <= G.H, cg);
+        v_step<decltype(s0)::value>(R, in, nr, cg, buf, tid);
         __syncthreads();
-        h_step<EXPORT>(buf0, r0, nr0, t_r, t_s, t_on, G, acc, mo);
-        if (st + 1 < it.nsteps) {
-            const int r1 = r0 + kStep;
-            const int nr1 = min(kStep, it.rows_out - r1);
-            load(st + 1);
-            prefetch(st + 3);
-            v_step<8>(R, in, nr1, cg, buf1, tid);
-            __syncthreads();
-            h_step<EXPORT>(buf1, r1, nr1, t_r, t_s, t_on, G, acc, mo);
-        }
+        if (producer && st + 3 <= it.nsteps) issue_rows<ST>(it, st + 3, stage(st + 3), &bars[(st + 3) & 1], lane);
+        h_step<EXPORT>(buf, r, nr, t_r, t_s, t_on, G, sacc, mo);
+        __syncthreads();
+    };
+    for (int st = 0; st < it.nsteps; st += 2) {
+        step(st, std::integral_constant<int, 0>());
+        if (st + 1 < it.nsteps) step(st + 1, std::integral_constant<int, 8>());
     }
 #pragma unroll
     for (int m = 0; m < 6; m++) {
-        double v = acc[m * kFusedThreads];
+        double v = sacc[m * kFusedThreads];
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
         if ((tid & 31) == 0) s_warp[tid >> 5][m] = v;
@@ -729,29 +772,45 @@ __device__ __forceinline__ void flat_item(const Item<ST> &it, float2 *smb, int t
         for (int w = 0; w < kFusedThreads / 32; w++) v += s_warp[w][tid];
         partials[(long long)item * 6 + tid] = v;  // = tile * 18 + channel * 6 + m
     }
+    return ok;
 }
 
+// Persistent: each block claims work items from the atomic counter until
+// they run out.  Dynamic shared memory: the step buffer, the two row stages,
+// the threads' f64 sums.  A block whose row copies time out (err set) stops claiming.
 template <typename ST, bool EXPORT = false>
 __global__ void __launch_bounds__(kFusedThreads, kTileBlocks)
     fused_kernel(const DevPair *__restrict__ pairs, const Seg *__restrict__ segs, int nseg, int first_item,
-                 int end_item, int *__restrict__ counter, double *__restrict__ partials,
+                 int end_item, int *__restrict__ counter, int *__restrict__ err, double *__restrict__ partials,
                  MapOut mo = MapOut{nullptr, 0, 0}) {
-    extern __shared__ __align__(16) float2 smb[];  // [parity][3 planes][kStep][kRS]
-    __shared__ int s_item;
+    extern __shared__ __align__(128) float2 smb[];  // [3 planes][kStep][kRS], then the stages and sums
+    float *const stages = (float *)(smb + kBufF2);
+    __shared__ int s_item, s_bad;
     __shared__ double s_warp[kFusedThreads / 32][6];
-    __shared__ double s_acc[6 * kFusedThreads];
+    __shared__ __align__(8) uint64_t s_bar[kStages];
     const int tid = threadIdx.x;
+    if (tid == 0) {
+        for (int i = 0; i < kStages; i++) s2_mbar_init(&s_bar[i]);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_bad = 0;
+    }
+    unsigned phase = 0;
     for (;;) {
         __syncthreads();  // the previous item's readers of s_item, s_warp and the buffers are done
-        if (tid == 0) s_item = first_item + atomicAdd(counter, 1);
+        if (tid == 0) s_item = s_bad ? end_item : first_item + atomicAdd(counter, 1);
         __syncthreads();
         const int item = s_item;
         if (item >= end_item) break;
         const int tile = item / 3, g = item - 3 * tile;
         const Seg sg = segs[find_seg(segs, nseg, tile)];
         const Item<ST> it = decode_item<ST>(pairs[sg.pair], sg, tile, g);
-        flat_item<ST, EXPORT>(it, smb, tid, s_acc, s_warp, partials, item, mo);
+        if (!flat_item<ST, EXPORT>(it, smb, stages, s_bar, phase, err, tid, s_warp, partials, item, mo))
+            s_bad = 1;
     }
+    // after a time-out, give copies still in flight a bounded wait before the
+    // block's shared memory goes away
+    if (s_bad)
+        for (int i = 0; i < kStages; i++) s2_mbar_wait(&s_bar[i], (phase >> i) & 1u, err);
 }
 
 // ---------------------------------------------------------------------------
@@ -766,8 +825,11 @@ __constant__ double c_weight[108];
 // independent of the rest of the batch).
 constexpr int kFinThreads = 256, kFinChunk = 128;
 
+// err: set by a tile pass whose row copies timed out; every pair of the
+// submission then reports S2_ERR_CUDA.
 __global__ void __launch_bounds__(kFinThreads) finalize_kernel(const DevPair *__restrict__ pairs, int npairs,
                                                                const double *__restrict__ partials,
+                                                               const int *__restrict__ err,
                                                                DevResult *__restrict__ out) {
     __shared__ double st[108];
     __shared__ double rec[kFinChunk * 18];
@@ -808,7 +870,7 @@ __global__ void __launch_bounds__(kFinThreads) finalize_kernel(const DevPair *__
         sc = sc > 0.0 ? fma(pow(sc, 0.6276336467831387), -10.0, 100.0) : 100.0;
         out[p].score = P.status == 0 ? sc : 0.0;
         out[p].n_scales = P.status == 0 ? P.nscales : 0;
-        out[p].status = P.status;
+        out[p].status = (P.status == 0 && err && *err) ? (int)S2_ERR_CUDA : P.status;
     }
 }
 
@@ -846,7 +908,7 @@ const double *host_weights() { return kWeights; }
 
 cudaError_t upload_weights() { return cudaMemcpyToSymbol(c_weight, kWeights, sizeof kWeights); }
 
-size_t fused_smem_bytes() { return (size_t)2 * kBufF2 * sizeof(float2); }
+size_t fused_smem_bytes() { return (size_t)kBufF2 * sizeof(float2) + (size_t)kStages * kStageFloats * sizeof(float) + 6 * kFusedThreads * sizeof(double); }
 int fused_threads() { return kTileThreads; }
 
 template <bool EXPORT>
@@ -896,27 +958,27 @@ cudaError_t launch_pyramid(int storage, const DevPair *pairs, int npairs, const 
 }
 
 cudaError_t launch_fused(int storage, const DevPair *pairs, const Seg *segs, int nseg, int first_tile, int end_tile,
-                         int *counter, double *partials, int grid, cudaStream_t st) {
+                         int *counter, int *err, double *partials, int grid, cudaStream_t st) {
     const int fi = 3 * first_tile, ei = 3 * end_tile;  // work items: (tile, channel)
     const int nt = ei - fi;
     if (nt <= 0) return cudaSuccess;
     grid = grid > nt ? nt : grid;
     (void)storage;
     fused_kernel<float, false><<<grid, kTileThreads, fused_smem_bytes(), st>>>(pairs, segs, nseg, fi, ei, counter,
-                                                                              partials, MapOut{nullptr, 0, 0});
+                                                                              err, partials, MapOut{nullptr, 0, 0});
     return cudaGetLastError();
 }
 
 cudaError_t launch_fused_export(int storage, const DevPair *pairs, const Seg *segs, int nseg, int first_tile,
-                                int end_tile, int *counter, double *partials, float *maps, long long mpitch,
-                                long long mplane, int grid, cudaStream_t st) {
+                                int end_tile, int *counter, int *err, double *partials, float *maps,
+                                long long mpitch, long long mplane, int grid, cudaStream_t st) {
     const int fi = 3 * first_tile, ei = 3 * end_tile;
     const int nt = ei - fi;
     if (nt <= 0) return cudaSuccess;
     grid = grid > nt ? nt : grid;
     (void)storage;
     fused_kernel<float, true><<<grid, kTileThreads, fused_smem_bytes(), st>>>(pairs, segs, nseg, fi, ei, counter,
-                                                                             partials, MapOut{maps, mpitch, mplane});
+                                                                             err, partials, MapOut{maps, mpitch, mplane});
     return cudaGetLastError();
 }
 
@@ -934,10 +996,10 @@ cudaError_t launch_desc_copy(void *dst, const void *src_host_mapped, size_t byte
     return cudaGetLastError();
 }
 
-cudaError_t launch_finalize(const DevPair *pairs, int npairs, const double *partials, DevResult *out,
-                            cudaStream_t st) {
+cudaError_t launch_finalize(const DevPair *pairs, int npairs, const double *partials, const int *err,
+                            DevResult *out, cudaStream_t st) {
     if (npairs <= 0) return cudaSuccess;
-    finalize_kernel<<<npairs, kFinThreads, 0, st>>>(pairs, npairs, partials, out);
+    finalize_kernel<<<npairs, kFinThreads, 0, st>>>(pairs, npairs, partials, err, out);
     return cudaGetLastError();
 }
 

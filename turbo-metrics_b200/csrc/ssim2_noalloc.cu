@@ -104,7 +104,8 @@ __global__ void desc_kernel(NoallocDesc d, unsigned char *base) {
     for (int i = t; i < (int)(d.nseg * sizeof(Seg) / 4); i += blockDim.x) ((unsigned *)(base + d.off_seg))[i] = sw[i];
     if (t == 0) {
         *(int *)(base + d.off_blk) = d.blk_first;
-        *(int *)(base + kOffCounter) = 0;
+        *(int *)(base + kOffCounter) = 0;      // the tile pass's work counter
+        *(int *)(base + kOffCounter + 4) = 0;  // and its time-out word
     }
 }
 
@@ -208,8 +209,9 @@ extern "C" s2_status s2_compute_srgb8_noalloc(const uint8_t *ref, size_t ref_pit
     if (launch_pyramid(ST_F32, dp, 1, (const int *)(base + off_blk), 0, P.blk_x * P.blk_y, cc, lut, sms * 8, cs) !=
             cudaSuccess ||
         launch_fused(ST_F32, dp, (const Seg *)(base + off_seg), nseg, 0, tiles, (int *)(base + kOffCounter),
-                     (double *)(base + off_part), sms * bps, cs) != cudaSuccess ||
-        launch_finalize(dp, 1, (const double *)(base + off_part), (DevResult *)out_device, cs) != cudaSuccess)
+                     (int *)(base + kOffCounter + 4), (double *)(base + off_part), sms * bps, cs) != cudaSuccess ||
+        launch_finalize(dp, 1, (const double *)(base + off_part), (const int *)(base + kOffCounter + 4),
+                        (DevResult *)out_device, cs) != cudaSuccess)
         return fail("kernel launch");
     return S2_OK;
 }
