@@ -207,11 +207,13 @@ __device__ __forceinline__ void ds_products(const float *X, const float *Y, floa
     }
 }
 
-// Asynchronous 4-byte global -> shared copies (cp.async): the next channel's
-// raw Lab region is fetched while the current channel computes.
-__device__ __forceinline__ void ds_cp4(float *dst, const float *src) {
+// Asynchronous global -> shared copies (cp.async) of 4, 8 or 16 bytes: the
+// next channel's raw Lab region is fetched while the current channel
+// computes.
+template <int BYTES>
+__device__ __forceinline__ void ds_cp(float *dst, const float *src) {
     const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(d), "l"(src), "n"(BYTES) : "memory");
 }
 
 // Issue the copies of channel c's raw region of `tile` (halo HALO: 2 for L,
@@ -229,11 +231,26 @@ __device__ __forceinline__ void ds_prefetch_h(const DsPair *__restrict__ pairs, 
     const int tl = tile - sg.first_tile;
     const int X0 = (tl % sg.tiles_x) * kDsT, Y0 = (tl / sg.tiles_x) * kDsT;
     const float *xr = P.lab[0][s] + c * plane, *yr = P.lab[1][s] + c * plane;
-    for (int i = threadIdx.x; i < 2 * n * n; i += kDsThreads) {
-        const int img = i >= n * n, r = img ? i - n * n : i;
-        const int row = r / n, col = r - row * n;
-        const int gx = ds_clamp(X0 - HALO + col, W - 1), gy = ds_clamp(Y0 - HALO + row, H - 1);
-        ds_cp4(R + i, (img ? yr : xr) + gy * pitch + gx);
+    if (X0 >= HALO && X0 - HALO + n <= W && Y0 >= HALO && Y0 - HALO + n <= H) {
+        // the region lies inside the level: whole rows in 16-byte (halo 4:
+        // X0 - 4 is a multiple of 4 floats) or 8-byte (halo 2) pieces; the
+        // Lab planes' pitch is a multiple of 64 floats and the planes are
+        // 256-byte aligned
+        constexpr int kCh = HALO % 4 == 0 ? 16 : 8, kPer = n * 4 / kCh, kF = kCh / 4;
+        static_assert((n * 4) % kCh == 0 && (kDsT - HALO) * 4 % kCh == 0, "aligned pieces");
+        for (int i = threadIdx.x; i < 2 * n * kPer; i += kDsThreads) {
+            const int img = i >= n * kPer, r = img ? i - n * kPer : i;
+            const int row = r / kPer, ch = r - row * kPer;
+            ds_cp<kCh>(R + img * n * n + row * n + ch * kF,
+                       (img ? yr : xr) + (long long)(Y0 - HALO + row) * pitch + (X0 - HALO) + ch * kF);
+        }
+    } else {
+        for (int i = threadIdx.x; i < 2 * n * n; i += kDsThreads) {
+            const int img = i >= n * n, r = img ? i - n * n : i;
+            const int row = r / n, col = r - row * n;
+            const int gx = ds_clamp(X0 - HALO + col, W - 1), gy = ds_clamp(Y0 - HALO + row, H - 1);
+            ds_cp<4>(R + i, (img ? yr : xr) + gy * pitch + gx);
+        }
     }
     asm volatile("cp.async.commit_group;\n" ::: "memory");
 }

@@ -146,11 +146,16 @@ struct DevResult {
 // platform rounds the same way.  Two iterations from the ~3% seed leave
 // ~1e-5, which the final correction squares away: <= 1 ulp over
 // [1e-30, 1e30] (checked in the tests).
+// i / 3 for i < 2^31 (the bits of a non-negative float) as one high multiply:
+// 0x55555556 = (2^32 + 2) / 3, so the high word of i * 0x55555556 is
+// floor(i / 3 + 2 i / (3 * 2^32)), and the added fraction is below 1/3.
+__device__ __forceinline__ unsigned s2_div3(unsigned i) { return __umulhi(i, 0x55555556u); }
+
 __device__ __forceinline__ float s2_cbrtf(float x) {
     const bool pos = x > 0.0f, tiny = x < 0x1p-100f;
     float xs = tiny ? x * 0x1p102f : x;
     xs = pos ? xs : 1.0f;
-    float r = __uint_as_float(0x54a2fa8cu - __float_as_uint(xs) / 3u);
+    float r = __uint_as_float(0x54a2fa8cu - s2_div3(__float_as_uint(xs)));
     const float third = 0x1.555556p-2f;
 #pragma unroll
     for (int k = 0; k < 2; k++) {
@@ -172,7 +177,7 @@ __device__ __forceinline__ float s2_cbrtf(float x) {
 // linear RGB, which are >= the bias 0.0038): the same operations without the
 // scaling of tiny and the zero of non-positive arguments, so the same result.
 __device__ __forceinline__ float s2_cbrtf_unit(float x) {
-    float r = __uint_as_float(0x54a2fa8cu - __float_as_uint(x) / 3u);
+    float r = __uint_as_float(0x54a2fa8cu - s2_div3(__float_as_uint(x)));
     const float third = 0x1.555556p-2f;
 #pragma unroll
     for (int k = 0; k < 2; k++) {
@@ -407,8 +412,8 @@ __device__ __forceinline__ float2 bt709_eotf2(float2 v, const float *pw) {
 
 // s2_cbrtf_unit of both lanes
 __device__ __forceinline__ float2 s2_cbrtf_unit2(float2 x) {
-    float2 r = make_float2(__uint_as_float(0x54a2fa8cu - __float_as_uint(x.x) / 3u),
-                           __uint_as_float(0x54a2fa8cu - __float_as_uint(x.y) / 3u));
+    float2 r = make_float2(__uint_as_float(0x54a2fa8cu - s2_div3(__float_as_uint(x.x))),
+                           __uint_as_float(0x54a2fa8cu - s2_div3(__float_as_uint(x.y))));
     const float2 third = s2_f2(0x1.555556p-2f);
 #pragma unroll
     for (int k = 0; k < 2; k++) {
