@@ -438,6 +438,42 @@ s2_status s2_compute_srgb8_noalloc(const uint8_t *ref, size_t ref_pitch, const u
 /* (The no-allocation entry point scores SSIMULACRA2 only and leaves the
  * dssim fields of *out_device unwritten.) */
 
+/* ---- zensim features (crates/zensim-cuda) ------------------------------ *
+ * The feature side of zensim's GPU port: positive XYB at the SIMD-padded
+ * width, 4 box-pyramid scales, radius-5 box blurs and, per scale and
+ * channel, 13 pooled features + 6 peak features: 228 in all, in the order of
+ * Zensim::compute_features (zensim-cuda/src/lib.rs:686-819; scales that the
+ * image is too small for are 0).  The score itself needs the trained table
+ * WEIGHTS_PREVIEW_V0_2 of the zensim crate, which is not part of the
+ * reference tree, so no score is offered.  Sums are reduced in a fixed order
+ * (the reference adds columns with float atomics). */
+#define S2_ZENSIM_FEATURES 228
+typedef struct s2_zensim s2_zensim;
+/* Replaces Zensim::new (lib.rs:198-287): S2_ERR_INVALID_SIZE below 8x8. */
+s2_status s2_zensim_create(int32_t device, uint32_t width, uint32_t height, s2_zensim **out);
+void s2_zensim_destroy(s2_zensim *z);
+/* Replaces Zensim::set_reference (lib.rs:340-376): packed sRGB8 rows of
+ * `pitch` bytes, on the device or (on_host) in host memory; the reference's
+ * pyramid stays resident.  Returns after the device work is done. */
+s2_status s2_zensim_set_reference_srgb8(s2_zensim *z, const uint8_t *ref, size_t pitch, int32_t on_host,
+                                        void *stream);
+/* Replaces Zensim::compute_with_reference (lib.rs:388-395): the 228 features
+ * of `dis` against the cached reference; *n_scales = scales computed.
+ * S2_ERR_NO_REFERENCE without a reference.  Synchronous. */
+s2_status s2_zensim_compute_with_reference_srgb8(s2_zensim *z, const uint8_t *dis, size_t pitch, int32_t on_host,
+                                                 void *stream, double *features, int32_t *n_scales);
+/* Replaces Zensim::compute_features (lib.rs:322-329): set_reference + compute. */
+s2_status s2_zensim_compute_features_srgb8(s2_zensim *z, const uint8_t *ref, size_t ref_pitch, const uint8_t *dis,
+                                           size_t dis_pitch, int32_t on_host, void *stream, double *features,
+                                           int32_t *n_scales);
+int32_t s2_zensim_has_reference(const s2_zensim *z);
+s2_status s2_zensim_clear_reference(s2_zensim *z);
+/* Replaces Zensim::debug_compute_raw (lib.rs:303-310): the last compute's
+ * 17 sums per [scale][channel] (acc: 4 * 3 * 17 doubles) and 3 maxima per
+ * [scale][channel] as f32 bits (peaks: 4 * 3 * 3). */
+s2_status s2_zensim_raw(const s2_zensim *z, double *acc, uint32_t *peaks);
+s2_status s2_zensim_mem_usage(const s2_zensim *z, size_t *bytes);
+
 /* ---- kernel timing (no reference counterpart; the reference has commented-
  * out cuProfilerStart/Stop calls, ssimulacra2-cuda/src/lib.rs:311,963) ----
  * When enabled, CUDA events bracket the three launches of every submission;

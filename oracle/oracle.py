@@ -267,3 +267,33 @@ def dssim_srgb8(ref, dis, mode="cuda32"):
     """DSSIM of two sRGB8 images (H, W, 3): the reference's 256-entry LUT,
     then dssim_linear (dssim-cuda's srgb_to_linear, srgb.rs:23-73)."""
     return dssim_linear(srgb8_to_linear(ref), srgb8_to_linear(dis), mode)
+
+
+_lib.zs_features_srgb8.restype = ctypes.c_int
+_lib.zs_padded_width.restype = ctypes.c_int
+
+
+class ZensimResult:
+    def __init__(self, features, acc, peaks, n_scales):
+        self.features, self.acc, self.peaks, self.n_scales = features, acc, peaks, n_scales
+
+
+def zensim_padded_width(w):
+    return _lib.zs_padded_width(w)
+
+
+def zensim_features_srgb8(ref, dis):
+    """zensim's 228 features of two sRGB8 images (H, W, 3) (restatement of
+    crates/zensim-cuda; see zensim_oracle.c).  acc: (4, 3, 17) f64 sums,
+    peaks: (4, 3, 3) maxima (f32), features: 228."""
+    h, w = ref.shape[:2]
+    r = np.ascontiguousarray(ref, np.uint8)
+    d = np.ascontiguousarray(dis, np.uint8)
+    acc = np.zeros((4, 3, 17))
+    peaks = np.zeros((4, 3, 3), np.uint32)
+    feat = np.zeros(228)
+    ns = _lib.zs_features_srgb8(r.ctypes.data_as(_U8), d.ctypes.data_as(_U8), w, h, ctypes.c_size_t(3 * w),
+                                _d(acc), peaks.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), _d(feat))
+    if ns < 0:
+        raise ValueError("zensim needs at least 8x8, got %dx%d" % (w, h))
+    return ZensimResult(feat, acc, peaks.view(np.float32), ns)

@@ -24,7 +24,7 @@ from .capi import (  # noqa: F401
     num_scales,
     version,
 )
-from .ssimulacra2 import Ssimulacra2, Ssim2Batch, PairDesc, Dssim  # noqa: F401
+from .ssimulacra2 import Ssimulacra2, Ssim2Batch, PairDesc, Dssim, Zensim  # noqa: F401
 from .server import Ssim2Server  # noqa: F401
 from .frames import FramePairScorer, Stats, select_frames  # noqa: F401
 from .router import RoutingPolicy, FrontEnd, Job, ServerEngine, worker_loop  # noqa: F401

@@ -24,6 +24,8 @@ UNITS = [
     ("ssim2_engine.cu", []),
     ("ssim2_noalloc.cu", []),
     ("ssim2_server.cu", []),
+    ("zensim_kernels.cu", ["-fmad=false"]),
+    ("zensim_engine.cu", []),
 ]
 
 

@@ -192,6 +192,17 @@ _sig = {
     "s2_dssim_compute_srgb8": (ctypes.c_int, [P, P, ctypes.c_size_t, P, ctypes.c_size_t, ctypes.c_int32, P, D]),
     "s2_dssim_compute_dis_only_srgb8": (ctypes.c_int, [P, P, ctypes.c_size_t, ctypes.c_int32, P, D]),
     "s2_dssim_mem_usage": (ctypes.c_int, [P, ctypes.POINTER(ctypes.c_size_t)]),
+    "s2_zensim_create": (ctypes.c_int, [ctypes.c_int32, ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(P)]),
+    "s2_zensim_destroy": (None, [P]),
+    "s2_zensim_set_reference_srgb8": (ctypes.c_int, [P, P, ctypes.c_size_t, ctypes.c_int32, P]),
+    "s2_zensim_compute_with_reference_srgb8": (ctypes.c_int, [P, P, ctypes.c_size_t, ctypes.c_int32, P, D,
+                                                              ctypes.POINTER(ctypes.c_int32)]),
+    "s2_zensim_compute_features_srgb8": (ctypes.c_int, [P, P, ctypes.c_size_t, P, ctypes.c_size_t, ctypes.c_int32,
+                                                        P, D, ctypes.POINTER(ctypes.c_int32)]),
+    "s2_zensim_has_reference": (ctypes.c_int32, [P]),
+    "s2_zensim_clear_reference": (ctypes.c_int, [P]),
+    "s2_zensim_raw": (ctypes.c_int, [P, D, ctypes.POINTER(ctypes.c_uint32)]),
+    "s2_zensim_mem_usage": (ctypes.c_int, [P, ctypes.POINTER(ctypes.c_size_t)]),
 }
 for _name, (_res, _args) in _sig.items():
     _f = getattr(lib, _name)

@@ -472,3 +472,76 @@ class Dssim:
         n = ctypes.c_size_t()
         check(lib.s2_dssim_mem_usage(self._h, ctypes.byref(n)), "mem_usage")
         return n.value
+
+
+class Zensim:
+    """zensim's 228-feature extraction of one size: the drop-in for
+    zensim-cuda's `Zensim` (crates/zensim-cuda/src/lib.rs:168-819).  Images
+    are packed sRGB8 (H, W, 3): torch CUDA tensors, or host arrays for the
+    `*_from_cpu` calls.  The score needs the trained weight table of the zensim
+    crate, which the reference tree does not hold: features only."""
+
+    FEATURES = 228
+
+    def __init__(self, width, height, *, device=0):
+        self.width, self.height = int(width), int(height)
+        h = ctypes.c_void_p()
+        check(lib.s2_zensim_create(device, self.width, self.height, ctypes.byref(h)), "Zensim::new")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None) and lib is not None:
+            lib.s2_zensim_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def _img(self, img, on_host):
+        if on_host:
+            p, pitch, keep = _host(img)
+            return p, pitch, keep
+        p, pitch = _dev(img, 1)
+        return p, pitch, None
+
+    def set_reference(self, ref_srgb, on_host=False, stream=None):
+        """Zensim::set_reference (lib.rs:340-376)."""
+        p, pitch, _ = self._img(ref_srgb, on_host)
+        check(lib.s2_zensim_set_reference_srgb8(self._h, p, pitch, 1 if on_host else 0, _stream_ptr(stream)),
+              "Zensim::set_reference")
+
+    def compute_with_reference(self, dis_srgb, on_host=False, stream=None):
+        """Zensim::compute_with_reference (lib.rs:388-395): 228 features."""
+        p, pitch, _ = self._img(dis_srgb, on_host)
+        feat = np.zeros(self.FEATURES)
+        ns = ctypes.c_int32()
+        check(lib.s2_zensim_compute_with_reference_srgb8(self._h, p, pitch, 1 if on_host else 0, _stream_ptr(stream),
+                                                         feat.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                                         ctypes.byref(ns)), "Zensim::compute_with_reference")
+        self.n_scales = ns.value
+        return feat
+
+    def compute_features(self, ref_srgb, dis_srgb, on_host=False, stream=None):
+        """Zensim::compute_features (lib.rs:322-329)."""
+        self.set_reference(ref_srgb, on_host, stream)
+        return self.compute_with_reference(dis_srgb, on_host, stream)
+
+    def has_reference(self):
+        return bool(lib.s2_zensim_has_reference(self._h))
+
+    def clear_reference(self):
+        check(lib.s2_zensim_clear_reference(self._h), "Zensim::clear_reference")
+
+    def raw(self):
+        """Zensim::debug_compute_raw's sums of the last compute: acc (4, 3, 17)
+        and the maxima (4, 3, 3) as float32."""
+        acc = np.zeros((4, 3, 17))
+        peaks = np.zeros((4, 3, 3), np.uint32)
+        check(lib.s2_zensim_raw(self._h, acc.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                peaks.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32))), "raw")
+        return acc, peaks.view(np.float32)
+
+    def mem_usage(self):
+        n = ctypes.c_size_t()
+        check(lib.s2_zensim_mem_usage(self._h, ctypes.byref(n)), "mem_usage")
+        return n.value
