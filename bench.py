@@ -331,6 +331,43 @@ def cpu_baseline(seconds=15.0, threads=None):
                       "one pair per thread); single-thread %.2f s/pair" % (n, one)}
 
 
+def zensim_bench(tmb, n_cands=16, reps=3):
+    """zensim features (the other sibling metric of the shared pyramid row):
+    one 1920x1080 sRGB8 reference cached with Zensim::set_reference, then
+    n_cands distorted versions through compute_with_reference (each call
+    returns its 228 features to the host, so the time includes the readback);
+    and the oracle restatement on one host thread for one pair."""
+    import synth
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    ref, _ = synth.srgb_pair(W, H, synth.pair_seed(0, 5000))
+    cands = [synth.srgb_pair(W, H, synth.pair_seed(0, 5000), 2.0 + 46.0 * k / n_cands)[1] for k in range(n_cands)]
+    dref = torch.from_numpy(ref).cuda()
+    dcs = [torch.from_numpy(c).cuda() for c in cands]
+    z = tmb.Zensim(W, H)
+    z.set_reference(dref)
+    for c in dcs[:2]:
+        z.compute_with_reference(c)
+    torch.cuda.synchronize()
+    best = None
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        for c in dcs:
+            z.compute_with_reference(c)
+        dt = time.perf_counter() - t0
+        best = dt if best is None else min(best, dt)
+    z.close()
+    t0 = time.perf_counter()
+    oracle.zensim_features_srgb8(ref, cands[0])
+    cpu_s = time.perf_counter() - t0
+    return {"workload": "1 x 1920x1080 sRGB8 reference (cached) + %d candidates, 228 features each" % n_cands,
+            "pairs_per_s": n_cands / best, "ms_per_pair": best / n_cands * 1e3,
+            "cpu_baseline": {"value": 1.0 / cpu_s, "unit": "pairs/s", "cores": 1, "kind": "port",
+                             "sample": "1 pair, oracle zensim_oracle.c (-O3 -march=x86-64-v3), one thread"},
+            "score": "unavailable: the zensim weight table is not in the reference tree"}
+
+
 def dssim_bench(tmb, descs, n_pairs, steps, warmup, s2_value, peak):
     """DSSIM, the sibling metric, on the same batch: both metrics from one
     prep pass, and DSSIM alone; device-timed like the main leg, with the
@@ -475,6 +512,7 @@ def main():
     ap.add_argument("--serve-jobs", type=int, default=10000, help="jobs per offered rate of the serving leg")
     ap.add_argument("--no-uneven", action="store_true", help="skip the 256-pair uneven-size batch leg")
     ap.add_argument("--no-dssim", action="store_true", help="skip the DSSIM (sibling metric) leg")
+    ap.add_argument("--no-zensim", action="store_true", help="skip the zensim features leg")
     ap.add_argument("--strip", type=int, default=0,
                     help="tile height of the main leg (16, 32, 64; 0 = autotuned, the default)")
     ap.add_argument("--pairs", type=int, default=N_PAIRS,
@@ -636,6 +674,10 @@ def main():
     if not args.no_dssim:
         dssim = dssim_bench(tmb, descs, NP, args.steps, args.warmup, value / world, peak)
 
+    zensim = None
+    if not args.no_zensim and world == 1:
+        zensim = zensim_bench(tmb)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline()
@@ -661,6 +703,7 @@ def main():
             "served": served,
             "uneven": uneven,
             "dssim": dssim,
+            "zensim": zensim,
             "score_mean": float(np.mean(scores)),
         }
         print(json.dumps(line), flush=True)
