@@ -457,10 +457,18 @@ struct StepRows {
 
 __device__ __forceinline__ void v_load(StepRows &in, const float *stage, int col, bool colin, int ybase, int H,
                                        bool inner, float cg) {
+    if (inner) {  // no masks: a branch of its own, so the selects are not executed
+#pragma unroll
+        for (int k = 0; k < kStep; k++) {
+            in.r[k] = stage[k * kCols + col];
+            in.d[k] = stage[(kStep + k) * kCols + col];
+        }
+        return;
+    }
 #pragma unroll
     for (int k = 0; k < kStep; k++) {
         const float vr = stage[k * kCols + col], vd = stage[(kStep + k) * kCols + col];
-        const bool ok = inner || (colin && ybase + k >= 0 && ybase + k < H);
+        const bool ok = colin && ybase + k >= 0 && ybase + k < H;
         in.r[k] = ok ? vr : cg;
         in.d[k] = ok ? vd : cg;
     }
