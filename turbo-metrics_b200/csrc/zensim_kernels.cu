@@ -117,6 +117,8 @@ __global__ void __launch_bounds__(kZsCols) zs_feat_kernel(const ZsScale *__restr
 #pragma unroll
     for (int i = 0; i < kZsOut; i++) acc[i] = 0.0;
     if (on) {
+        // columns whose 11 taps stay inside the row need no mirror index
+        const bool xin = x >= kZsRadius && x + kZsRadius < n;
         int done = -1;  // horizontal sums computed for rows 0 .. done
         auto ensure = [&](int row) {
             while (done < row) {
@@ -124,7 +126,7 @@ __global__ void __launch_bounds__(kZsCols) zs_feat_kernel(const ZsScale *__restr
                 float s1 = 0.0f, s2 = 0.0f, sq = 0.0f, s12 = 0.0f;
                 const float *a = A + (size_t)done * pitch, *d = D + (size_t)done * pitch;
                 for (int k = 0; k < diam; k++) {
-                    const int ix = mirror(x + k - kZsRadius, n);
+                    const int ix = xin ? x + k - kZsRadius : mirror(x + k - kZsRadius, n);
                     const float s = a[ix], t = d[ix];
                     s1 += s;
                     s2 += t;
@@ -187,7 +189,8 @@ __global__ void __launch_bounds__(kZsCols) zs_feat_kernel(const ZsScale *__restr
             const float pd = sv - dv;
             acc[9] += (double)(pd * pd);
             // slide the vertical window: (sum + entering row) - leaving row
-            const int ai = mirror(y + kZsRadius + 1, h), ri = mirror(y - kZsRadius, h);
+            const int ai = y + kZsRadius + 1 < h ? y + kZsRadius + 1 : mirror(y + kZsRadius + 1, h);
+            const int ri = y >= kZsRadius ? y - kZsRadius : mirror(y - kZsRadius, h);
             ensure(ai);
             sm1 = sm1 + get(ai, 0) - get(ri, 0);
             sm2 = sm2 + get(ai, 1) - get(ri, 1);
