@@ -486,6 +486,15 @@ s2_status s2_batch_last_timings(s2_batch *b, float ms[3]);
 /* Device time of the DSSIM passes (clamp, tile, mean, MAD, final) of the
  * last profiled submission that scored DSSIM. */
 s2_status s2_batch_last_dssim_ms(s2_batch *b, float *ms);
+/* Failure-detection hook of the tile pass.  Every wait of the tile pass on
+ * its bulk row copies is bounded (wait_cycles SM clock cycles; 0 restores
+ * the default, about one second); a wait that runs out makes the submission
+ * report S2_ERR_TIMEOUT instead of hanging.  drop_item >= 0 makes the pass
+ * withhold the row copies of that work item, so that its waits run out: the
+ * way the tests exercise that path without any fault.  -1 (the default)
+ * withholds nothing.  Process-wide; read when a submission is enqueued (a
+ * CUDA graph keeps the values it was captured with). */
+s2_status s2_debug_tile_timeout(int32_t drop_item, int64_t wait_cycles);
 /* Resident blocks per SM of the fused kernel for a storage type (0 on error). */
 int32_t s2_fused_blocks_per_sm(int32_t storage);
 

@@ -78,3 +78,11 @@ def test_dssim_entry_points_validate_without_gpu(tmb):
     assert lib.s2_set_metrics(None, 3) == 8
     assert lib.s2_batch_set_metrics(None, 2) == 8
     assert lib.s2_get_dssim(None, None, None) == 8
+
+
+def test_tile_timeout_hook_validates_without_gpu(tmb):
+    lib = tmb.lib
+    assert lib.s2_debug_tile_timeout(-1, -5) == 8  # negative wait bound
+    assert lib.s2_debug_tile_timeout(3, 1 << 20) == 0
+    assert lib.s2_debug_tile_timeout(-1, 0) == 0  # back to the defaults
+    assert tmb.capi._ERRS[tmb.capi.S2_ERR_TIMEOUT] is tmb.Timeout

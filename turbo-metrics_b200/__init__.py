@@ -14,6 +14,7 @@ CPU fallback: importing this package without the built library raises.
 from .capi import (  # noqa: F401
     S2Error,
     Busy,
+    Timeout,
     InvalidArgument,
     InvalidImageSize,
     DimensionMismatch,

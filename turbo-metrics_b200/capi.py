@@ -68,9 +68,14 @@ class Busy(S2Error):
     pass
 
 
+class Timeout(S2Error):
+    """A bounded device-side wait ran out (S2_ERR_TIMEOUT)."""
+    pass
+
+
 _ERRS = {S2_ERR_OOM: OutOfMemory, S2_ERR_INVALID_SIZE: InvalidImageSize,
          S2_ERR_DIM_MISMATCH: DimensionMismatch, S2_ERR_NO_REFERENCE: NoCachedReference, S2_ERR_BUSY: Busy,
-         S2_ERR_INVALID_ARG: InvalidArgument}
+         S2_ERR_INVALID_ARG: InvalidArgument, S2_ERR_TIMEOUT: Timeout}
 
 
 def check(status, what=""):
@@ -173,6 +178,7 @@ _sig = {
     "s2_batch_set_profiling": (ctypes.c_int, [P, ctypes.c_int32]),
     "s2_batch_last_timings": (ctypes.c_int, [P, ctypes.POINTER(ctypes.c_float)]),
     "s2_fused_blocks_per_sm": (ctypes.c_int32, [ctypes.c_int32]),
+    "s2_debug_tile_timeout": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int64]),
     "s2_server_config_default": (None, [ctypes.POINTER(ServerConfig)]),
     "s2_server_create": (ctypes.c_int, [ctypes.POINTER(ServerConfig), ctypes.POINTER(P)]),
     "s2_server_destroy": (None, [P]),

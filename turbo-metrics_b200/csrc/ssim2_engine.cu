@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -328,6 +329,14 @@ struct s2_batch {
     }
 };
 
+// The tile pass's wait bound and the failure test's withheld work item.
+static std::atomic<long long> g_tile_wait_cycles{1ll << 31};
+static std::atomic<int> g_tile_drop_item{-1};
+
+namespace s2 {
+TileCheck tile_check(int *err) { return TileCheck{err, g_tile_wait_cycles.load(), g_tile_drop_item.load()}; }
+}  // namespace s2
+
 extern "C" {
 
 const char *s2_version(void) { return "ssim2b200 1.0.0 (sm_100a)"; }
@@ -350,6 +359,13 @@ const char *s2_status_string(s2_status st) {
 }
 
 const char *s2_last_error(void) { return g_last_error.c_str(); }
+
+s2_status s2_debug_tile_timeout(int32_t drop_item, int64_t wait_cycles) {
+    if (wait_cycles < 0) return S2_ERR_INVALID_ARG;
+    g_tile_drop_item.store(drop_item < 0 ? -1 : drop_item);
+    g_tile_wait_cycles.store(wait_cycles == 0 ? (1ll << 31) : wait_cycles);
+    return S2_OK;
+}
 
 void s2_config_default(s2_config *cfg) {
     if (!cfg) return;
@@ -724,7 +740,7 @@ s2_status s2_error_maps(s2_ctx *ctx, int32_t scale, float *maps, size_t pitch, v
     const long long mpitch = (long long)(pitch / sizeof(float));
     S2_CUDA(cudaMemsetAsync(e.counter_d.p, 0, Engine::kCounterBytes, st));
     S2_CUDA(launch_fused_export(e.storage, (const DevPair *)dbase, (const Seg *)(dbase + pb + bb),
-                                (int)P.segs.size(), t0, t1, (int *)e.counter_d.p, e.err_word(),
+                                (int)P.segs.size(), t0, t1, (int *)e.counter_d.p, tile_check(e.err_word()),
                                 (double *)e.partials_d.p, maps, mpitch, mpitch * p.h[scale], e.num_sms * e.fused_bps,
                                 st));
     // the tile pass's time-out word (set only if its row copies never landed)
@@ -733,7 +749,7 @@ s2_status s2_error_maps(s2_ctx *ctx, int32_t scale, float *maps, size_t pitch, v
     S2_CUDA(cudaStreamSynchronize(st));
     if (err) {
         g_last_error = "tile pass: row copies timed out";
-        return S2_ERR_CUDA;
+        return S2_ERR_TIMEOUT;
     }
     return S2_OK;
 }

@@ -831,7 +831,7 @@ struct Engine {
                                    P.htotal, (double *)partials_d.p, st));
             else
                 S2_CUDA(launch_fused(storage, dpairs, dsegs, (int)P.segs.size(), P.grp_tile[g], P.grp_tile[g + 1],
-                                     (int *)counter_d.p + g, err_word(), (double *)partials_d.p, num_sms * fused_bps,
+                                     (int *)counter_d.p + g, tile_check(err_word()), (double *)partials_d.p, num_sms * fused_bps,
                                      st));
         }
         // several groups interleave prep and fused: the fused slot then holds both
@@ -898,7 +898,7 @@ struct Engine {
                                (double *)partials_d.p, cap_st);
             else
                 e = launch_fused(storage, dpairs, (const Seg *)(dbase + pb + bb), (int)P.segs.size(), 0,
-                                 P.total_tiles, (int *)counter_d.p, err_word(), (double *)partials_d.p,
+                                 P.total_tiles, (int *)counter_d.p, tile_check(err_word()), (double *)partials_d.p,
                                  num_sms * fused_bps, cap_st);
         }
         if (e == cudaSuccess && m_s2)

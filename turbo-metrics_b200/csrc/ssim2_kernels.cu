@@ -29,6 +29,7 @@
 // not the constant).
 #include "../../include/ssim2b200.h"
 #include "ssim2_device.cuh"
+#include "ssim2_launch.h"
 
 namespace s2 {
 
@@ -426,8 +427,12 @@ __device__ __forceinline__ void s2_bulk_g2s(void *dst, const void *src, unsigned
         : "memory");
 }
 
-// Wait for the stage's phase `parity`, at most about one second (clock64 at
-// the SM clock); on time-out set *err and return false.
+// The tile pass's wait bound in SM cycles, set by each block from its
+// TileCheck (in shared memory so that the spin loops hold no register for it).
+__shared__ long long s2_wait_limit;
+
+// Wait for the stage's phase `parity`, at most s2_wait_limit SM clock
+// cycles; on time-out set *err and return false.
 __device__ __forceinline__ bool s2_mbar_wait(uint64_t *bar, unsigned parity, int *err) {
     const unsigned a = s2_smem_addr(bar);
     const long long t0 = clock64();
@@ -440,7 +445,7 @@ __device__ __forceinline__ bool s2_mbar_wait(uint64_t *bar, unsigned parity, int
             : "r"(a), "r"(parity)
             : "memory");
         if (done) return true;
-        if (clock64() - t0 > (1ll << 31)) {
+        if (clock64() - t0 > s2_wait_limit) {
             atomicExch(err, 1);
             return false;
         }
@@ -684,8 +689,14 @@ constexpr int kTileBlocks = 4;  // resident blocks per SM (128 registers per thr
 // y0 - 4 + 8 L .. + 7) into `stage`, completing on `bar`.  Run by warp 0:
 // lane 0 announces the bytes, lanes 0..15 copy one row each (lane >> 3 the
 // image, lane & 7 the row).
+// withhold: announce the bytes but copy nothing (the failure test's way to
+// make the stage's waits run out).  ok: this lane's waits so far succeeded;
+// once any lane of the warp has timed out the warp issues nothing more for
+// the item, so no barrier ever sees a second arrival in an unfinished phase.
 template <typename ST>
-__device__ __forceinline__ void issue_rows(const Item<ST> &it, int L, float *stage, uint64_t *bar, int lane) {
+__device__ __forceinline__ void issue_rows(const Item<ST> &it, int L, float *stage, uint64_t *bar, int lane,
+                                           bool withhold, bool ok) {
+    if (!__all_sync(0xffffffffu, ok)) return;
     const ItemGeo &G = it.G;
     const int ybase = G.y0 - 4 + kStep * L;
     const int xs = max(G.x0 - 4, 0), xe = min(G.x0 + kCols - 4, G.lp);
@@ -696,7 +707,7 @@ __device__ __forceinline__ void issue_rows(const Item<ST> &it, int L, float *sta
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     if (lane == 0) s2_mbar_expect(bar, 2u * (unsigned)rows * bytes);
     __syncwarp();
-    if (lane < 2 * kStep) {
+    if (lane < 2 * kStep && !withhold) {
         const int img = lane >> 3, k = lane & 7, y = ybase + k;
         if (y >= 0 && y < G.H) {
             const ST *src = (img ? it.xd : it.xr) + (long long)y * G.lp + xs;
@@ -714,7 +725,7 @@ __device__ __forceinline__ void issue_rows(const Item<ST> &it, int L, float *sta
 // expected mbarrier parity (bit s), the same in every thread.
 template <typename ST, bool EXPORT>
 __device__ __forceinline__ bool flat_item(const Item<ST> &it, float2 *smb, float *stages, uint64_t *bars,
-                                          unsigned &phase, int *err, int tid, double (*s_warp)[6],
+                                          unsigned &phase, const TileCheck &ck, int tid, double (*s_warp)[6],
                                           double *__restrict__ partials, int item, const MapOut &mo) {
     const ItemGeo &G = it.G;
     const float cg = G.cg;
@@ -725,16 +736,17 @@ __device__ __forceinline__ bool flat_item(const Item<ST> &it, float2 *smb, float
     const bool t_on = tid < kTasks;
     const int lane = tid & 31;
     const bool producer = tid < 32;
+    const bool withhold = item == ck.drop_item;
     bool ok = true;
     auto stage = [&](int L) { return stages + (L & 1) * kStageFloats; };
     auto wait = [&](int L) {
         const int sidx = L & 1;
-        ok &= s2_mbar_wait(&bars[sidx], (phase >> sidx) & 1u, err);
+        ok &= s2_mbar_wait(&bars[sidx], (phase >> sidx) & 1u, ck.err);
         phase ^= 1u << sidx;
     };
     if (producer) {
-        issue_rows<ST>(it, 0, stage(0), &bars[0], lane);
-        issue_rows<ST>(it, 1, stage(1), &bars[1], lane);
+        issue_rows<ST>(it, 0, stage(0), &bars[0], lane, withhold, ok);
+        issue_rows<ST>(it, 1, stage(1), &bars[1], lane, withhold, ok);
     }
     Rings R;
     wait(0);
@@ -745,7 +757,7 @@ __device__ __forceinline__ bool flat_item(const Item<ST> &it, float2 *smb, float
         for (int k = 0; k < 8; k++) ring_in(R, k, in.r[k], in.d[k], cg);
     }
     __syncthreads();  // stage 0 read by every thread
-    if (producer && it.nsteps >= 2) issue_rows<ST>(it, 2, stage(2), &bars[0], lane);
+    if (producer && it.nsteps >= 2) issue_rows<ST>(it, 2, stage(2), &bars[0], lane, withhold, ok);
     float2 *const buf = smb;
     double *sacc = (double *)(stages + kStages * kStageFloats) + tid;
 #pragma unroll
@@ -758,7 +770,7 @@ __device__ __forceinline__ bool flat_item(const Item<ST> &it, float2 *smb, float
         v_load(in, stage(st + 1), tid, colin, ybase, G.H, cols_in && nr == kStep && ybase + kStep <= G.H, cg);
         v_step<decltype(s0)::value>(R, in, nr, cg, buf, tid);
         __syncthreads();
-        if (producer && st + 3 <= it.nsteps) issue_rows<ST>(it, st + 3, stage(st + 3), &bars[(st + 3) & 1], lane);
+        if (producer && st + 3 <= it.nsteps) issue_rows<ST>(it, st + 3, stage(st + 3), &bars[(st + 3) & 1], lane, withhold, ok);
         h_step<EXPORT>(buf, r, nr, t_r, t_s, t_on, G, sacc, mo);
         __syncthreads();
     };
@@ -789,7 +801,7 @@ __device__ __forceinline__ bool flat_item(const Item<ST> &it, float2 *smb, float
 template <typename ST, bool EXPORT = false>
 __global__ void __launch_bounds__(kFusedThreads, kTileBlocks)
     fused_kernel(const DevPair *__restrict__ pairs, const Seg *__restrict__ segs, int nseg, int first_item,
-                 int end_item, int *__restrict__ counter, int *__restrict__ err, double *__restrict__ partials,
+                 int end_item, int *__restrict__ counter, TileCheck ck, double *__restrict__ partials,
                  MapOut mo = MapOut{nullptr, 0, 0}) {
     extern __shared__ __align__(128) float2 smb[];  // [3 planes][kStep][kRS], then the stages and sums
     float *const stages = (float *)(smb + kBufF2);
@@ -801,6 +813,7 @@ __global__ void __launch_bounds__(kFusedThreads, kTileBlocks)
         for (int i = 0; i < kStages; i++) s2_mbar_init(&s_bar[i]);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         s_bad = 0;
+        s2_wait_limit = ck.wait_cycles;
     }
     unsigned phase = 0;
     for (;;) {
@@ -812,13 +825,13 @@ __global__ void __launch_bounds__(kFusedThreads, kTileBlocks)
         const int tile = item / 3, g = item - 3 * tile;
         const Seg sg = segs[find_seg(segs, nseg, tile)];
         const Item<ST> it = decode_item<ST>(pairs[sg.pair], sg, tile, g);
-        if (!flat_item<ST, EXPORT>(it, smb, stages, s_bar, phase, err, tid, s_warp, partials, item, mo))
+        if (!flat_item<ST, EXPORT>(it, smb, stages, s_bar, phase, ck, tid, s_warp, partials, item, mo))
             s_bad = 1;
     }
     // after a time-out, give copies still in flight a bounded wait before the
     // block's shared memory goes away
     if (s_bad)
-        for (int i = 0; i < kStages; i++) s2_mbar_wait(&s_bar[i], (phase >> i) & 1u, err);
+        for (int i = 0; i < kStages; i++) s2_mbar_wait(&s_bar[i], (phase >> i) & 1u, ck.err);
 }
 
 // ---------------------------------------------------------------------------
@@ -834,7 +847,7 @@ __constant__ double c_weight[108];
 constexpr int kFinThreads = 256, kFinChunk = 128;
 
 // err: set by a tile pass whose row copies timed out; every pair of the
-// submission then reports S2_ERR_CUDA.
+// submission then reports S2_ERR_TIMEOUT.
 __global__ void __launch_bounds__(kFinThreads) finalize_kernel(const DevPair *__restrict__ pairs, int npairs,
                                                                const double *__restrict__ partials,
                                                                const int *__restrict__ err,
@@ -878,7 +891,7 @@ __global__ void __launch_bounds__(kFinThreads) finalize_kernel(const DevPair *__
         sc = sc > 0.0 ? fma(pow(sc, 0.6276336467831387), -10.0, 100.0) : 100.0;
         out[p].score = P.status == 0 ? sc : 0.0;
         out[p].n_scales = P.status == 0 ? P.nscales : 0;
-        out[p].status = (P.status == 0 && err && *err) ? (int)S2_ERR_CUDA : P.status;
+        out[p].status = (P.status == 0 && err && *err) ? (int)S2_ERR_TIMEOUT : P.status;
     }
 }
 
@@ -966,19 +979,19 @@ cudaError_t launch_pyramid(int storage, const DevPair *pairs, int npairs, const 
 }
 
 cudaError_t launch_fused(int storage, const DevPair *pairs, const Seg *segs, int nseg, int first_tile, int end_tile,
-                         int *counter, int *err, double *partials, int grid, cudaStream_t st) {
+                         int *counter, const TileCheck &ck, double *partials, int grid, cudaStream_t st) {
     const int fi = 3 * first_tile, ei = 3 * end_tile;  // work items: (tile, channel)
     const int nt = ei - fi;
     if (nt <= 0) return cudaSuccess;
     grid = grid > nt ? nt : grid;
     (void)storage;
     fused_kernel<float, false><<<grid, kTileThreads, fused_smem_bytes(), st>>>(pairs, segs, nseg, fi, ei, counter,
-                                                                              err, partials, MapOut{nullptr, 0, 0});
+                                                                              ck, partials, MapOut{nullptr, 0, 0});
     return cudaGetLastError();
 }
 
 cudaError_t launch_fused_export(int storage, const DevPair *pairs, const Seg *segs, int nseg, int first_tile,
-                                int end_tile, int *counter, int *err, double *partials, float *maps,
+                                int end_tile, int *counter, const TileCheck &ck, double *partials, float *maps,
                                 long long mpitch, long long mplane, int grid, cudaStream_t st) {
     const int fi = 3 * first_tile, ei = 3 * end_tile;
     const int nt = ei - fi;
@@ -986,7 +999,7 @@ cudaError_t launch_fused_export(int storage, const DevPair *pairs, const Seg *se
     grid = grid > nt ? nt : grid;
     (void)storage;
     fused_kernel<float, true><<<grid, kTileThreads, fused_smem_bytes(), st>>>(pairs, segs, nseg, fi, ei, counter,
-                                                                             err, partials, MapOut{maps, mpitch, mplane});
+                                                                             ck, partials, MapOut{maps, mpitch, mplane});
     return cudaGetLastError();
 }
 

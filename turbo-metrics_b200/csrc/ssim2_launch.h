@@ -17,10 +17,20 @@ int fused_blocks_per_sm(int storage);
 cudaError_t launch_pyramid(int storage, const DevPair *pairs, int npairs, const int *blk_first, int first_block,
                            int end_block, const ColorConsts &cc, const float *lut, int grid, cudaStream_t st,
                            int out = 1);
-// err: a device word (zeroed before the submission) that a tile pass whose
-// row copies time out sets; launch_finalize then marks every pair S2_ERR_CUDA.
+// The tile pass's bounded waits: err is a device word (zeroed before the
+// submission) that a pass whose row copies time out sets (launch_finalize
+// then marks every pair S2_ERR_TIMEOUT); wait_cycles bounds each wait (SM
+// clock cycles); drop_item >= 0 withholds the row copies of that work item
+// so that its waits run out (the failure test; -1 in normal use).
+struct TileCheck {
+    int *err;
+    long long wait_cycles;
+    int drop_item;
+};
+TileCheck tile_check(int *err);  // the process-wide setting (s2_debug_tile_timeout)
 cudaError_t launch_fused(int storage, const DevPair *pairs, const Seg *segs, int nseg, int first_tile,
-                         int end_tile, int *counter, int *err, double *partials, int grid, cudaStream_t st);
+                         int end_tile, int *counter, const TileCheck &ck, double *partials, int grid,
+                         cudaStream_t st);
 cudaError_t launch_iir(int storage, const DevPair *pairs, const IirSeg *vsegs, int nvseg, int vtotal,
                        const IirSeg *hsegs, int nhseg, int htotal, double *partials, cudaStream_t st);
 // Copy `bytes` (a multiple of 16, both pointers 16-byte aligned) from
@@ -32,7 +42,8 @@ cudaError_t launch_desc_copy(void *dst, const void *src_host_mapped, size_t byte
 // planes [channel][ssim, artifact, detail], mpitch floats per row, mplane
 // floats per plane).
 cudaError_t launch_fused_export(int storage, const DevPair *pairs, const Seg *segs, int nseg,
-                                int first_tile, int end_tile, int *counter, int *err, double *partials, float *maps,
+                                int first_tile, int end_tile, int *counter, const TileCheck &ck, double *partials,
+                                float *maps,
                                 long long mpitch, long long mplane, int grid, cudaStream_t st);
 cudaError_t launch_finalize(const DevPair *pairs, int npairs, const double *partials, const int *err,
                             DevResult *out, cudaStream_t st);

@@ -209,7 +209,8 @@ extern "C" s2_status s2_compute_srgb8_noalloc(const uint8_t *ref, size_t ref_pit
     if (launch_pyramid(ST_F32, dp, 1, (const int *)(base + off_blk), 0, P.blk_x * P.blk_y, cc, lut, sms * 8, cs) !=
             cudaSuccess ||
         launch_fused(ST_F32, dp, (const Seg *)(base + off_seg), nseg, 0, tiles, (int *)(base + kOffCounter),
-                     (int *)(base + kOffCounter + 4), (double *)(base + off_part), sms * bps, cs) != cudaSuccess ||
+                     tile_check((int *)(base + kOffCounter + 4)), (double *)(base + off_part), sms * bps,
+                     cs) != cudaSuccess ||
         launch_finalize(dp, 1, (const double *)(base + off_part), (const int *)(base + kOffCounter + 4),
                         (DevResult *)out_device, cs) != cudaSuccess)
         return fail("kernel launch");
