@@ -379,6 +379,20 @@ __device__ __forceinline__ float2 s2_mul2(float2 a, float2 b) { return __fmul2_r
 __device__ __forceinline__ float2 s2_add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
 __device__ __forceinline__ float2 s2_mul2s(float2 a, float2 b) { return make_float2(a.x * b.x, a.y * b.y); }
 
+// The negated quotients -(a.x / b.x, a.y / b.y) by s2_div's steps on both
+// lanes, with the reciprocals of -b: r' = -r, q' = a r' = -q, e = b q' + a =
+// a - b q, e r' + q' = -(e r + q); each step rounds to the negation of the
+// scalar step's result (round-to-nearest is symmetric, and so is the
+// hardware reciprocal), so -n is s2_div of each lane.
+__device__ __forceinline__ float2 s2_div2_neg(float2 a, float2 b) {
+    float2 r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r.x) : "f"(-b.x));
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r.y) : "f"(-b.y));
+    const float2 q = s2_pmul(a, r);
+    const float2 e = s2_pfma(b, q, a);
+    return s2_pfma(e, r, q);
+}
+
 // The factors 2^(20e/9) of s2_pow_20_9_unit for e = -3..0, indexed by the
 // exponent field minus 124 (the caller keeps them in shared memory: one
 // shared load per lane instead of three compares and selects).

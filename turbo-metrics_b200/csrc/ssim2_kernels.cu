@@ -482,23 +482,24 @@ __device__ __forceinline__ void v_load(StepRows &in, const float *stage, int col
 // One vertical step: the step's input rows enter ring slots S0 + 8 ..
 // S0 + 15 (mod 16); output row k reads slots S0 + k .. S0 + k + 8 and is
 // stored to row k of the buffer: plane 0 the FIR of ring a, plane 1 that of
-// ring b, plane 2 the raw (x', e) of the output row.
+// ring b, plane 2 the raw (x', e) of the output row.  All 8 rows are formed
+// even in an item's last, partial step (nr < 8, which happens only at the
+// image's bottom edge): its rows beyond nr lie below the image, read the
+// anchor (0 after the shift) and are neither read by the horizontal phase
+// nor used by a later step.
 template <int S0>
-__device__ __forceinline__ void v_step(Rings &R, const StepRows &in, int nr, float cg, float2 *__restrict__ buf,
-                                       int col) {
+__device__ __forceinline__ void v_step(Rings &R, const StepRows &in, float cg, float2 *__restrict__ buf, int col) {
 #pragma unroll
     for (int k = 0; k < kStep; k++) {
-        if (k < nr) {
-            ring_in(R, (S0 + 8 + k) & 15, in.r[k], in.d[k], cg);
+        ring_in(R, (S0 + 8 + k) & 15, in.r[k], in.d[k], cg);
 #define S2_R(a, j) a[(S0 + k + (j)) & 15]
-            buf[k * kRS + col] = fir9p(S2_R(R.a, 0), S2_R(R.a, 1), S2_R(R.a, 2), S2_R(R.a, 3), S2_R(R.a, 4),
-                                       S2_R(R.a, 5), S2_R(R.a, 6), S2_R(R.a, 7), S2_R(R.a, 8));
-            buf[kPlaneF2 + k * kRS + col] = fir9p(S2_R(R.b, 0), S2_R(R.b, 1), S2_R(R.b, 2), S2_R(R.b, 3),
-                                                  S2_R(R.b, 4), S2_R(R.b, 5), S2_R(R.b, 6), S2_R(R.b, 7),
-                                                  S2_R(R.b, 8));
-            buf[2 * kPlaneF2 + k * kRS + col] = S2_R(R.a, 4);  // raw (x', e)
+        buf[k * kRS + col] = fir9p(S2_R(R.a, 0), S2_R(R.a, 1), S2_R(R.a, 2), S2_R(R.a, 3), S2_R(R.a, 4),
+                                   S2_R(R.a, 5), S2_R(R.a, 6), S2_R(R.a, 7), S2_R(R.a, 8));
+        buf[kPlaneF2 + k * kRS + col] = fir9p(S2_R(R.b, 0), S2_R(R.b, 1), S2_R(R.b, 2), S2_R(R.b, 3),
+                                              S2_R(R.b, 4), S2_R(R.b, 5), S2_R(R.b, 6), S2_R(R.b, 7),
+                                              S2_R(R.b, 8));
+        buf[2 * kPlaneF2 + k * kRS + col] = S2_R(R.a, 4);  // raw (x', e)
 #undef S2_R
-        }
     }
 }
 
@@ -552,7 +553,6 @@ __device__ __forceinline__ void maps_px(float2 m, float2 s, float2 r, float kk, 
     const float vd = fmaf(-md, md, s.x);
     const float den = vd + num_s;
     const float nn = fmaf(md * md, num_s, vd);
-    d = fmaxf(s2_div(nn, den), 0.0f);
     const float2 t = s2_pfma(m, s2_f2(-1.0f), r);  // (x' - mu1, e - md)
     float t1 = t.x, t2 = t.x - t.y;              // x' - mu1, y' - mu2
     if (BORDER) {
@@ -560,9 +560,18 @@ __device__ __forceinline__ void maps_px(float2 m, float2 s, float2 r, float kk, 
         t2 = t2 + kk;
     }
     const float aa = fabsf(t1), bb = fabsf(t2);
-    const float d1 = s2_div(bb - aa, 1.0f + aa);
-    art = fmaxf(d1, 0.0f);
-    det = fmaxf(-d1, 0.0f);
+    if (BORDER) {
+        d = fmaxf(s2_div(nn, den), 0.0f);
+        const float d1 = s2_div(bb - aa, 1.0f + aa);
+        art = fmaxf(d1, 0.0f);
+        det = fmaxf(-d1, 0.0f);
+    } else {
+        // both quotients at once: n = -(nn / den, (bb - aa) / (1 + aa))
+        const float2 n = s2_div2_neg(make_float2(nn, bb - aa), make_float2(den, 1.0f + aa));
+        d = fmaxf(-n.x, 0.0f);
+        art = fmaxf(-n.y, 0.0f);
+        det = fmaxf(n.y, 0.0f);
+    }
 }
 
 
@@ -768,7 +777,7 @@ __device__ __forceinline__ bool flat_item(const Item<ST> &it, float2 *smb, float
         wait(st + 1);
         StepRows in;
         v_load(in, stage(st + 1), tid, colin, ybase, G.H, cols_in && nr == kStep && ybase + kStep <= G.H, cg);
-        v_step<decltype(s0)::value>(R, in, nr, cg, buf, tid);
+        v_step<decltype(s0)::value>(R, in, cg, buf, tid);
         __syncthreads();
         if (producer && st + 3 <= it.nsteps) issue_rows<ST>(it, st + 3, stage(st + 3), &bars[(st + 3) & 1], lane, withhold, ok);
         h_step<EXPORT>(buf, r, nr, t_r, t_s, t_on, G, sacc, mo);
