@@ -138,8 +138,8 @@ __global__ void __launch_bounds__(kDsThreads) dssim_clamp_kernel(const DsPair *_
 //
 // Each blur stage fills an n x n buffer (n = 32 + 2 x its halo, even) from the
 // (n + 2)-wide buffer of the stage before.  A thread takes two adjacent
-// columns and kDsRun consecutive rows and slides a 3 x 4 window of the input
-// down them (two 8-byte shared loads per row).  Each tap is a scalar multiply
+// columns and a run of consecutive rows and slides a 3 x 4 window of the
+// input down them (two 8-byte shared loads per row).  Each tap is a scalar multiply
 // per column and one f32x2 add for both columns, in the reference's
 // row-major tap order: every lane rounds as the scalar reference does (the
 // products are scalar multiplies, which -fmad=false keeps out of any fused
@@ -151,7 +151,7 @@ __global__ void __launch_bounds__(kDsThreads) dssim_clamp_kernel(const DsPair *_
 // touch the level's edge, positions outside the level then take the value of
 // the position clamped into it (ds_fix_edges), which is what the reference's
 // next stage reads there with clamped indexes.
-constexpr int kDsRun = 4;
+constexpr int kDsRun = 4;  // rows per thread of the MAD pass
 
 __device__ __forceinline__ float2 ds_sum9x2(const float (&w)[3][4]) {
     float2 sum = make_float2(w[0][0] * ds_k(0), w[0][1] * ds_k(0));
@@ -175,23 +175,31 @@ __device__ __forceinline__ void ds_slide(float (&w)[3][4], const float *src) {
     ds_load4(w[2], src);
 }
 
-// `planes` planes: out[p] (n x n) = 3x3 blur of in[p] (pitch n + 2, plane (n + 2)^2)
-__device__ __forceinline__ void ds_stage_blur(const float *in, float *out, int n, int planes) {
-    const int m = n + 2, half = n / 2, runs = (n + kDsRun - 1) / kDsRun;
-    for (int it = threadIdx.x; it < planes * half * runs; it += kDsThreads) {
-        const int p = it / (half * runs), q = it % (half * runs);
-        const int c = 2 * (q % half), j0 = (q / half) * kDsRun;
-        const float *src = in + p * m * m + c;
-        float *dst = out + p * n * n + c;
-        float w[3][4];
-        ds_load4(w[1], src + j0 * m);
-        ds_load4(w[2], src + (j0 + 1) * m);
+// `planes` planes: out[p] (n x n) = 3x3 blur of in[p] (pitch n + 2, plane
+// (n + 2)^2).  Thread t takes one column pair of one plane and a run of L
+// rows: the plane's n / 2 column pairs times S row segments, at most one
+// item per thread; segment k starts at row min(k L, n - L), so the last run
+// may overlap the one before it (those rows are written twice, with the same
+// values).  Every size is a compile-time constant: the item's plane, columns
+// and rows are found once, and the run is unrolled without row checks.
+template <int n, int planes, int S, int L>
+__device__ __forceinline__ void ds_stage_blur(const float *in, float *out) {
+    constexpr int m = n + 2, half = n / 2, items = planes * half * S;
+    static_assert(items <= kDsThreads && S * L >= n && L <= n && n % 2 == 0, "one run per thread");
+    const int t = threadIdx.x;
+    if (t >= items) return;
+    const int p = t / (half * S), q = t - p * (half * S);
+    const int seg = q / half, c = 2 * (q - seg * half);
+    const int j0 = min(seg * L, n - L);
+    const float *src = in + p * m * m + j0 * m + c;
+    float *dst = out + p * n * n + j0 * n + c;
+    float w[3][4];
+    ds_load4(w[1], src);
+    ds_load4(w[2], src + m);
 #pragma unroll
-        for (int r = 0; r < kDsRun; r++) {
-            if (j0 + r >= n) break;
-            ds_slide(w, src + (j0 + r + 2) * m);
-            *(float2 *)(dst + (j0 + r) * n) = ds_sum9x2(w);
-        }
+    for (int r = 0; r < L; r++) {
+        ds_slide(w, src + (r + 2) * m);
+        *(float2 *)(dst + r * n) = ds_sum9x2(w);
     }
 }
 
@@ -334,7 +342,7 @@ __global__ void __launch_bounds__(kDsThreads, 3) dssim_tile_kernel(const DsPair 
                 __syncthreads();
             } else {
                 // a, b: pre-blurred twice first (lib.rs:296-316)
-                ds_stage_blur(bufR, bufB, kDsP, 2);
+                ds_stage_blur<kDsP, 2, 6, 7>(bufR, bufB);
                 __syncthreads();
             }
             // R is free: fetch the next channel (or the next tile's L) during
@@ -346,7 +354,7 @@ __global__ void __launch_bounds__(kDsThreads, 3) dssim_tile_kernel(const DsPair 
                     ds_fix_edges<kDsP, 3>(bufB, 2, X0, Y0, W, H);
                     __syncthreads();
                 }
-                ds_stage_blur(bufB, bufA, kDsX, 2);
+                ds_stage_blur<kDsX, 2, 6, 6>(bufB, bufA);
                 __syncthreads();
                 if (edge) {
                     ds_fix_edges<kDsX, 2>(bufA, 2, X0, Y0, W, H);
@@ -355,7 +363,7 @@ __global__ void __launch_bounds__(kDsThreads, 3) dssim_tile_kernel(const DsPair 
                 ds_products(bufA, bufA + nnX, bufA, nnX);
                 __syncthreads();
             }
-            ds_stage_blur(bufA, bufB, kDsB, 5);
+            ds_stage_blur<kDsB, 5, 3, 12>(bufA, bufB);
             __syncthreads();
             if (edge) {
                 ds_fix_edges<kDsB, 1>(bufB, 5, X0, Y0, W, H);
