@@ -598,15 +598,42 @@ float or_pow_20_9(float p) { return eng_pow_20_9(p); }
 
 float or_cbrtf(float x) { return eng_cbrtf(x); }
 
+/* The XYB cube root: the correctly rounded f32 cube root of x > 0 (0 for
+ * x <= 0), from libm's double cbrt rounded once to f32.  The engine's XYB
+ * cube root (ssim2_device.cuh s2_cbrtf_unit / s2_cbrtf_xyb) ends in a
+ * Newton step with an exact residual, which gives this value in all but a
+ * few cases per 10^5, and otherwise a neighbour within 1 ulp.  It stands in
+ * for the reference's cbrtf (libdevice, xyb.rs:42-78; <= 1 ulp) in every
+ * f32 mode. */
+static inline float xyb_cbrtf(float x) { return x > 0.0f ? (float)cbrt((double)x) : 0.0f; }
+float or_xyb_cbrtf(float x) { return xyb_cbrtf(x); }
+
+/* The last step of the engine's XYB cube root (ssim2_device.cuh
+ * s2_cbrt_step) from a seed r ~ x^(-1/3): y = x r^2, then one Newton step
+ * with the residual y^3 - x formed from y^2 = hi + lo split exactly.  The
+ * engine's seed comes from the SFU, which C cannot restate; the tests feed
+ * this step perturbed exact seeds to show that its result is the correctly
+ * rounded cube root whatever the seed's last bits. */
+float or_cbrt_step(float x, float r) {
+    float y = x * r;
+    y = y * r;
+    const float hi = y * y;
+    const float lo = fmaf(y, y, -hi);
+    float e = fmaf(hi, y, -x);
+    e = fmaf(lo, y, e);
+    const float c = (r * r) * 0x1.555556p-2f;
+    return fmaf(-e, c, y);
+}
+
 static inline void xyb_f32(float r, float g, float b, float out[3]) {
     const float m01 = 1.0f - XM02 - XM00, m11 = 1.0f - XM12 - XM10, m22 = 1.0f - XM20 - XM21;
     const float root = 0.1559542025327239180319220163705f;
     float rg = fmaf(XM00, r, fmaf(m01, g, fmaf(XM02, b, XB0)));
     float gr = fmaf(XM10, r, fmaf(m11, g, fmaf(XM12, b, XB0)));
     float bb = fmaf(XM20, r, fmaf(XM21, g, fmaf(m22, b, XB0)));
-    rg = eng_cbrtf(rg > 0.0f ? rg : 0.0f) - root;
-    gr = eng_cbrtf(gr > 0.0f ? gr : 0.0f) - root;
-    bb = eng_cbrtf(bb > 0.0f ? bb : 0.0f) - root;
+    rg = xyb_cbrtf(rg) - root;
+    gr = xyb_cbrtf(gr) - root;
+    bb = xyb_cbrtf(bb) - root;
     float x = 0.5f * (rg - gr), y = 0.5f * (rg + gr);
     out[0] = fmaf(x, 14.0f, 0.42f);
     out[1] = y + 0.01f;

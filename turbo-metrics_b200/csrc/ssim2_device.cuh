@@ -173,24 +173,45 @@ __device__ __forceinline__ float s2_cbrtf(float x) {
     return pos ? y : 0.0f;
 }
 
-// s2_cbrtf for x in [2^-100, 2^100] (the opsin values of non-negative
-// linear RGB, which are >= the bias 0.0038): the same operations without the
-// scaling of tiny and the zero of non-positive arguments, so the same result.
-__device__ __forceinline__ float s2_cbrtf_unit(float x) {
-    float r = __uint_as_float(0x54a2fa8cu - s2_div3(__float_as_uint(x)));
-    const float third = 0x1.555556p-2f;
-#pragma unroll
-    for (int k = 0; k < 2; k++) {
-        float t = x * r;
-        t = t * r;
-        t = t * r;
-        r = fmaf(r * third, 1.0f - t, r);
-    }
+// ---- the XYB cube root --------------------------------------------------
+// Correctly rounded in all but a few cases per 10^5 (<= 1 ulp always): a
+// seed r ~ x^(-1/3) from the SFU, 2^(-log2(x) / 3) (lg2.approx / ex2.approx,
+// about 4e-7 relative), y = x r^2, and one Newton step for y^3 = x whose
+// residual y^3 - x is formed with y^2 split exactly into hi + lo (the
+// FMA-based TwoProduct of Ogita, Rump and Oishi, "Accurate sum and dot
+// product", 2005), so the step's error is second order in the seed's: the
+// result then no longer depends on how the seed was found, and a CPU can
+// check it against the correctly rounded cube root.  (s2_cbrtf above, with a
+// plain residual, is within an ulp but its last bit follows its seed.)
+__device__ __forceinline__ float s2_rcbrt_sfu(float x) {
+    float l, r;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(l) : "f"(x));
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(l * -0x1.555556p-2f));
+    return r;
+}
+
+__device__ __forceinline__ float s2_cbrt_step(float x, float r) {
     float y = x * r;
     y = y * r;
-    const float e = fmaf(y * y, y, -x);
-    const float c = (r * r) * third;
+    const float hi = y * y;
+    const float lo = fmaf(y, y, -hi);  // y^2 = hi + lo exactly
+    float e = fmaf(hi, y, -x);
+    e = fmaf(lo, y, e);  // y^3 - x
+    const float c = (r * r) * 0x1.555556p-2f;  // 1 / (3 y^2)
     return fmaf(-e, c, y);
+}
+
+// x in [2^-100, 2^100] (the opsin values of non-negative linear RGB, which
+// are >= the bias 0.0038)
+__device__ __forceinline__ float s2_cbrtf_unit(float x) { return s2_cbrt_step(x, s2_rcbrt_sfu(x)); }
+
+// any x: 0 for x <= 0 or NaN; tiny x scaled by 2^102 and the root by 2^-34
+__device__ __forceinline__ float s2_cbrtf_xyb(float x) {
+    const bool pos = x > 0.0f, tiny = x < 0x1p-100f;
+    float xs = tiny ? x * 0x1p102f : x;
+    xs = pos ? xs : 1.0f;
+    const float y = s2_cbrt_step(xs, s2_rcbrt_sfu(xs)) * (tiny ? 0x1p-34f : 1.0f);
+    return pos ? y : 0.0f;
 }
 
 // dssim-core's scaled Lab of one linear-RGB pixel, with the reference GPU's
@@ -300,7 +321,7 @@ __device__ __forceinline__ float opsin_row(int g, float r, float gg, float b) {
     else
         v = fmaf(S2_M20, r, fmaf(S2_M21, gg, fmaf(m22, b, S2_B0)));
     if (KUNIT) return s2_cbrtf_unit(v) - S2_B0_ROOT;
-    return s2_cbrtf(fmaxf(v, 0.0f)) - S2_B0_ROOT;
+    return s2_cbrtf_xyb(v) - S2_B0_ROOT;
 }
 
 // XYB channel g from the three opsin cube roots (xyb.rs:42-78).
@@ -424,24 +445,17 @@ __device__ __forceinline__ float2 bt709_eotf2(float2 v, const float *pw) {
     return make_float2(v.x >= thr ? hi.x : lo.x, v.y >= thr ? hi.y : lo.y);
 }
 
-// s2_cbrtf_unit of both lanes
+// s2_cbrtf_unit of both lanes (each lane rounds as the scalar steps: no
+// packed product feeds a packed sum)
 __device__ __forceinline__ float2 s2_cbrtf_unit2(float2 x) {
-    float2 r = make_float2(__uint_as_float(0x54a2fa8cu - s2_div3(__float_as_uint(x.x))),
-                           __uint_as_float(0x54a2fa8cu - s2_div3(__float_as_uint(x.y))));
-    const float2 third = s2_f2(0x1.555556p-2f);
-#pragma unroll
-    for (int k = 0; k < 2; k++) {
-        float2 t = s2_mul2(x, r);
-        t = s2_mul2(t, r);
-        t = s2_mul2(t, r);
-        // 1 - t as fma(t, -1, 1): same rounding, and t (a product) is not
-        // fed to a packed add
-        r = __ffma2_rn(s2_mul2(r, third), __ffma2_rn(t, s2_f2(-1.0f), s2_f2(1.0f)), r);
-    }
+    const float2 r = make_float2(s2_rcbrt_sfu(x.x), s2_rcbrt_sfu(x.y));
     float2 y = s2_mul2(x, r);
     y = s2_mul2(y, r);
-    const float2 e = __ffma2_rn(s2_mul2(y, y), y, s2_neg2(x));
-    const float2 c = s2_mul2(s2_mul2(r, r), third);
+    const float2 hi = s2_mul2(y, y);
+    const float2 lo = __ffma2_rn(y, y, s2_neg2(hi));
+    float2 e = __ffma2_rn(hi, y, s2_neg2(x));
+    e = __ffma2_rn(lo, y, e);
+    const float2 c = s2_mul2(s2_mul2(r, r), s2_f2(0x1.555556p-2f));
     return __ffma2_rn(s2_neg2(e), c, y);
 }
 
