@@ -134,6 +134,24 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def with_issue_roofline(roofline, clk, peaks):
+    """The fused pass is bound by instruction issue, not HBM: beside the HBM
+    fraction, its warp instructions per launch (ncu smsp__inst_executed.sum of
+    a capture, scaled to the bench launch by the pairs it processes) over the
+    issue peak at the SM clock sampled during the timed region (148 SMs x 4
+    schedulers x one warp instruction per cycle)."""
+    winst = roofline.get("warp_instructions_per_launch")
+    mhz = clk.get("sm_mhz") or peaks.get("sm_max_mhz")
+    ms = roofline["kernel_ms"]["fused"]
+    if winst and mhz and ms > 0:
+        peak = 148 * 4 * mhz * 1e6
+        achieved = winst / (ms / 1e3)
+        roofline["issue"] = {"bound": "issue", "achieved": achieved / 1e9, "peak": peak / 1e9,
+                             "unit": "G warp instructions/s", "frac": achieved / peak, "sm_mhz": mhz,
+                             "source": "instructions from the ncu capture in profiles/, clock sampled"}
+    return roofline
+
+
 def serve_pool_candidate(args):
     import synth
     ref, i = args
@@ -589,10 +607,13 @@ def main():
     ab = algorithmic_bytes_fused(NP)
     achieved = ab / (fused_ms / 1e3) / 1e9
     traffic = None
+    winst = None
     tpath = os.path.join(ROOT, "profiles", "fused_traffic.json")
     if os.path.exists(tpath):
         try:
-            traffic = json.load(open(tpath)).get("bytes_per_launch")
+            tj = json.load(open(tpath))
+            traffic = tj.get("bytes_per_launch")
+            winst = tj.get("warp_instructions_per_launch")
         except (OSError, ValueError):
             traffic = None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
@@ -601,6 +622,7 @@ def main():
                 "kernel_ms": {"prep": float(acc[0]), "fused": fused_ms, "finalize": float(acc[2])},
                 "fused_blocks_per_sm": int(lib.s2_fused_blocks_per_sm(0)),
                 "algorithmic_bytes_per_launch": ab,
+                "warp_instructions_per_launch": winst,
                 "prep_gbs": algorithmic_bytes_prep(NP) / (float(acc[0]) / 1e3) / 1e9,
                 # every pass's declared I/O over the sum of their times (prep: NV12 in + XYB
                 # planes out; fused: XYB planes in; finalize: negligible)
@@ -685,6 +707,7 @@ def main():
             dssim["cpu_baseline"] = dssim_cpu_baseline()
 
     if rank == 0:
+        clk = clocks.summary()
         line = {
             "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
@@ -695,9 +718,9 @@ def main():
                        "parallelism": "replicas" if world > 1 else "single"},
             "plain_pairs_per_s": plain, "batched_vs_plain": value / world / plain,
             "e2e": {"value": e2e, "unit": "pairs/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
-            "roofline": roofline,
+            "roofline": with_issue_roofline(roofline, clk, peaks),
             "gpu_launches": 3 * args.steps,
-            "clocks": clocks.summary(),
+            "clocks": clk,
             "cpu_baseline": cpu,
             "cached_reference": cached,
             "served": served,
