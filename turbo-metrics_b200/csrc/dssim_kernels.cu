@@ -139,11 +139,10 @@ __global__ void __launch_bounds__(kDsThreads) dssim_clamp_kernel(const DsPair *_
 // Each blur stage fills an n x n buffer (n = 32 + 2 x its halo, even) from the
 // (n + 2)-wide buffer of the stage before.  A thread takes two adjacent
 // columns and a run of consecutive rows and slides a 3 x 4 window of the
-// input down them (two 8-byte shared loads per row).  Each tap is a scalar multiply
-// per column and one f32x2 add for both columns, in the reference's
-// row-major tap order: every lane rounds as the scalar reference does (the
-// products are scalar multiplies, which -fmad=false keeps out of any fused
-// multiply-add).  The first tap initialises the sum, which equals 0 + tap
+// input down them (two 8-byte shared loads per row).  The taps' products
+// are formed once per input row (ds_prod) and added, one f32x2 add for both
+// columns per tap, in the reference's row-major tap order: every lane rounds
+// as the scalar reference does.  The first tap initialises the sum, which equals 0 + tap
 // for every tap but -0 (no Lab value or product of two is -0 where it
 // matters: the sign of a zero sum does not reach the SSIM).  x^2, y^2 and xy
 // are formed once per input position, so the first statistics blur is five
@@ -151,28 +150,71 @@ __global__ void __launch_bounds__(kDsThreads) dssim_clamp_kernel(const DsPair *_
 // touch the level's edge, positions outside the level then take the value of
 // the position clamped into it (ds_fix_edges), which is what the reference's
 // next stage reads there with clamped indexes.
-constexpr int kDsRun = 4;  // rows per thread of the MAD pass
+// One input row of a thread's window: columns c .. c + 3 as two aligned
+// register pairs (w0, w1), (w2, w3).
+struct DsRow {
+    float2 a, b;
+};
 
-__device__ __forceinline__ float2 ds_sum9x2(const float (&w)[3][4]) {
-    float2 sum = make_float2(w[0][0] * ds_k(0), w[0][1] * ds_k(0));
+__device__ __forceinline__ DsRow ds_row(const float *src) {
+    return DsRow{*(const float2 *)src, *(const float2 *)(src + 2)};
+}
+
+// The products of one window row with its taps for both columns, in tap
+// order kx = 0, 1, 2: (k0 w0, k0 w1), (k1 w1, k1 w2), (k0 w2, k0 w3), where
+// k0 is the row's outer tap and k1 its middle one (corner / edge for the top
+// and bottom rows, edge / centre for the middle row).  A product is the same
+// rounded value whichever output and window position uses it, so a row's
+// outer products are formed once and used by the two outputs whose top and
+// bottom row it is, and its middle products once when it is the middle row
+// (8 instructions per row instead of 18 multiplies).  The aligned pairs are
+// packed FMAs with the addend -0 (nz): k w + (-0) rounds exactly as k w,
+// signed zeros included, and an FMA cannot be fused with the add that
+// follows (a packed multiply feeding a packed add is fused even under
+// -fmad=false); the middle pair (w1, w2) is not an aligned register pair, so
+// its two products are scalar multiplies (never fused under -fmad=false).
+struct DsProd {
+    float2 p0, p1, p2;
+};
+
+__device__ __forceinline__ DsProd ds_prod(const DsRow &w, float k0, float k1, float2 nz) {
+    DsProd p;
+    p.p0 = __ffma2_rn(make_float2(k0, k0), w.a, nz);
+    p.p1 = make_float2(w.a.y * k1, w.b.x * k1);
+    p.p2 = __ffma2_rn(make_float2(k0, k0), w.b, nz);
+    return p;
+}
+
+// The 3 x 3 window of both columns, the nine products added in the
+// reference's row-major tap order.
+__device__ __forceinline__ float2 ds_sum3(const DsProd &t, const DsProd &m, const DsProd &b) {
+    float2 s = t.p0;
+    s = __fadd2_rn(s, t.p1);
+    s = __fadd2_rn(s, t.p2);
+    s = __fadd2_rn(s, m.p0);
+    s = __fadd2_rn(s, m.p1);
+    s = __fadd2_rn(s, m.p2);
+    s = __fadd2_rn(s, b.p0);
+    s = __fadd2_rn(s, b.p1);
+    return __fadd2_rn(s, b.p2);
+}
+
+// L output rows of one column pair from input rows src[0 .. L + 1] (pitch m)
+template <int L, int m, typename F>
+__device__ __forceinline__ void ds_blur_run(const float *src, float2 nz, F &&emit) {
+    const float kc = ds_k(0), ke = ds_k(1), km = ds_k(4);
+    DsProd top = ds_prod(ds_row(src), kc, ke, nz);
+    DsRow mid = ds_row(src + m);
+    DsProd mid_outer = ds_prod(mid, kc, ke, nz);
 #pragma unroll
-    for (int i = 1; i < 9; i++) {
-        const int ky = i / 3, kx = i % 3;
-        const float k = ds_k(i);
-        sum = __fadd2_rn(sum, make_float2(w[ky][kx] * k, w[ky][kx + 1] * k));
+    for (int r = 0; r < L; r++) {
+        const DsRow nw = ds_row(src + (r + 2) * m);
+        const DsProd bot = ds_prod(nw, kc, ke, nz);
+        emit(r, ds_sum3(top, ds_prod(mid, ke, km, nz), bot));
+        top = mid_outer;
+        mid = nw;
+        mid_outer = bot;
     }
-    return sum;
-}
-
-__device__ __forceinline__ void ds_load4(float (&row)[4], const float *src) {
-    const float2 a = *(const float2 *)src, b = *(const float2 *)(src + 2);
-    row[0] = a.x, row[1] = a.y, row[2] = b.x, row[3] = b.y;
-}
-
-__device__ __forceinline__ void ds_slide(float (&w)[3][4], const float *src) {
-#pragma unroll
-    for (int kx = 0; kx < 4; kx++) w[0][kx] = w[1][kx], w[1][kx] = w[2][kx];
-    ds_load4(w[2], src);
 }
 
 // `planes` planes: out[p] (n x n) = 3x3 blur of in[p] (pitch n + 2, plane
@@ -183,7 +225,7 @@ __device__ __forceinline__ void ds_slide(float (&w)[3][4], const float *src) {
 // values).  Every size is a compile-time constant: the item's plane, columns
 // and rows are found once, and the run is unrolled without row checks.
 template <int n, int planes, int S, int L>
-__device__ __forceinline__ void ds_stage_blur(const float *in, float *out) {
+__device__ __forceinline__ void ds_stage_blur(const float *in, float *out, float2 nz) {
     constexpr int m = n + 2, half = n / 2, items = planes * half * S;
     static_assert(items <= kDsThreads && S * L >= n && L <= n && n % 2 == 0, "one run per thread");
     const int t = threadIdx.x;
@@ -193,14 +235,7 @@ __device__ __forceinline__ void ds_stage_blur(const float *in, float *out) {
     const int j0 = min(seg * L, n - L);
     const float *src = in + p * m * m + j0 * m + c;
     float *dst = out + p * n * n + j0 * n + c;
-    float w[3][4];
-    ds_load4(w[1], src);
-    ds_load4(w[2], src + m);
-#pragma unroll
-    for (int r = 0; r < L; r++) {
-        ds_slide(w, src + (r + 2) * m);
-        *(float2 *)(dst + r * n) = ds_sum9x2(w);
-    }
+    ds_blur_run<L, m>(src, nz, [&](int r, float2 v) { *(float2 *)(dst + r * n) = v; });
 }
 
 // the five blur inputs x, y, x^2, y^2, xy of every position (out: 5 planes)
@@ -304,8 +339,15 @@ constexpr int kDsSmemFloats = 5 * kDsX * kDsX + 5 * kDsB * kDsB + 2 * kDsR * kDs
 
 __global__ void __launch_bounds__(kDsThreads, 3) dssim_tile_kernel(const DsPair *__restrict__ pairs,
                                                                    const DsSeg *__restrict__ segs, int nseg,
-                                                                   int ntiles, double *__restrict__ partials) {
+                                                                   int ntiles, double *__restrict__ partials,
+                                                                   float negz) {
     extern __shared__ __align__(16) float ds_smem[];
+    // (-0, -0): the addend that makes the squares of the blurred means packed
+    // FMAs (k w + (-0) rounds exactly as k w, signed zeros included), which the
+    // compiler, not knowing the argument, cannot turn into a multiply fused
+    // with the packed add that follows (a packed multiply feeding a packed add
+    // is fused even under -fmad=false)
+    const float2 nz = make_float2(negz, negz);
     float *const bufA = ds_smem;
     float *const bufB = bufA + 5 * kDsX * kDsX;
     float *const bufR = bufB + 5 * kDsB * kDsB;
@@ -342,7 +384,7 @@ __global__ void __launch_bounds__(kDsThreads, 3) dssim_tile_kernel(const DsPair 
                 __syncthreads();
             } else {
                 // a, b: pre-blurred twice first (lib.rs:296-316)
-                ds_stage_blur<kDsP, 2, 6, 7>(bufR, bufB);
+                ds_stage_blur<kDsP, 2, 6, 7>(bufR, bufB, nz);
                 __syncthreads();
             }
             // R is free: fetch the next channel (or the next tile's L) during
@@ -354,7 +396,7 @@ __global__ void __launch_bounds__(kDsThreads, 3) dssim_tile_kernel(const DsPair 
                     ds_fix_edges<kDsP, 3>(bufB, 2, X0, Y0, W, H);
                     __syncthreads();
                 }
-                ds_stage_blur<kDsX, 2, 6, 6>(bufB, bufA);
+                ds_stage_blur<kDsX, 2, 6, 6>(bufB, bufA, nz);
                 __syncthreads();
                 if (edge) {
                     ds_fix_edges<kDsX, 2>(bufA, 2, X0, Y0, W, H);
@@ -363,7 +405,7 @@ __global__ void __launch_bounds__(kDsThreads, 3) dssim_tile_kernel(const DsPair 
                 ds_products(bufA, bufA + nnX, bufA, nnX);
                 __syncthreads();
             }
-            ds_stage_blur<kDsB, 5, 3, 12>(bufA, bufB);
+            ds_stage_blur<kDsB, 5, 3, 12>(bufA, bufB, nz);
             __syncthreads();
             if (edge) {
                 ds_fix_edges<kDsB, 1>(bufB, 5, X0, Y0, W, H);
@@ -373,22 +415,15 @@ __global__ void __launch_bounds__(kDsThreads, 3) dssim_tile_kernel(const DsPair 
             float2 q[5][kDsOutRows];
 #pragma unroll
             for (int pl = 0; pl < 5; pl++) {
-                const float *src = bufB + pl * nnB + c0;
-                float w[3][4];
-                ds_load4(w[1], src + r0 * kDsB);
-                ds_load4(w[2], src + (r0 + 1) * kDsB);
-#pragma unroll
-                for (int r = 0; r < kDsOutRows; r++) {
-                    ds_slide(w, src + (r0 + r + 2) * kDsB);
-                    q[pl][r] = ds_sum9x2(w);
-                }
+                ds_blur_run<kDsOutRows, kDsB>(bufB + pl * nnB + r0 * kDsB + c0, nz,
+                                              [&](int r, float2 v) { q[pl][r] = v; });
             }
 #pragma unroll
             for (int r = 0; r < kDsOutRows; r++) {
                 const float2 m1 = q[0][r], m2 = q[1][r];
-                const float2 a0 = make_float2(m1.x * m1.x, m1.y * m1.y);
-                const float2 a1 = make_float2(m2.x * m2.x, m2.y * m2.y);
-                const float2 a2 = make_float2(m1.x * m2.x, m1.y * m2.y);
+                const float2 a0 = __ffma2_rn(m1, m1, nz);
+                const float2 a1 = __ffma2_rn(m2, m2, nz);
+                const float2 a2 = __ffma2_rn(m1, m2, nz);
                 if (c == 0) {
                     acc[r][0] = a0, acc[r][1] = a1, acc[r][2] = a2;
                     acc[r][3] = q[2][r], acc[r][4] = q[3][r], acc[r][5] = q[4][r];
@@ -445,30 +480,44 @@ __global__ void __launch_bounds__(kDsThreads) dssim_mean_kernel(const DsPair *__
     }
 }
 
+// One warp per tile: lane l sums |avg - ssim| down column l of the tile in
+// row order (f64), then the warp adds the lanes by a fixed shuffle tree.  No
+// block barriers, and each lane has its column's rows in flight at once.
+constexpr int kMadWarps = kDsThreads / 32;
+static_assert(kDsT == 32, "one lane per tile column");
+
 __global__ void __launch_bounds__(kDsThreads) dssim_mad_kernel(const DsPair *__restrict__ pairs,
                                                                const DsSeg *__restrict__ segs, int nseg, int ntiles,
                                                                const float *__restrict__ avg,
                                                                double *__restrict__ mad) {
-    __shared__ double red[kDsThreads];
-    const int t = threadIdx.x;
-    const int tx = t % kDsT, j0 = (t / kDsT) * kDsRun;  // one column, kDsRun rows
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int lane = threadIdx.x & 31;
+    const int nwarps = gridDim.x * kMadWarps;
+    for (int tile = blockIdx.x * kMadWarps + (threadIdx.x >> 5); tile < ntiles; tile += nwarps) {
         const DsSeg sg = segs[ds_find_seg(segs, nseg, tile)];
         const DsPair &P = pairs[sg.pair];
         const int s = sg.level;
         const int tl = tile - sg.first_tile;
         const int X0 = (tl % sg.tiles_x) * kDsT, Y0 = (tl / sg.tiles_x) * kDsT;
         const float a = avg[sg.pair * kDsLevels + s];
-        const float *map = P.map[s];
         const long long pitch = P.pitch[s];
+        const int ox = X0 + lane;
+        const int rows = min(kDsT, P.h[s] - Y0);
         double acc = 0.0;
+        if (ox < P.w[s]) {
+            const float *col = P.map[s] + (long long)Y0 * pitch + ox;
+            if (rows == kDsT) {
+                float v[kDsT];
 #pragma unroll
-        for (int k = 0; k < kDsRun; k++) {
-            const int ox = X0 + tx, oy = Y0 + j0 + k;
-            if (ox < P.w[s] && oy < P.h[s]) acc += (double)fabsf(a - map[oy * pitch + ox]);
+                for (int k = 0; k < kDsT; k++) v[k] = col[k * pitch];
+#pragma unroll
+                for (int k = 0; k < kDsT; k++) acc += (double)fabsf(a - v[k]);
+            } else {
+                for (int k = 0; k < rows; k++) acc += (double)fabsf(a - col[k * pitch]);
+            }
         }
-        const double r = ds_block_reduce(acc, red);
-        if (t == 0) mad[tile] = r;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+        if (lane == 0) mad[tile] = acc;
     }
 }
 
@@ -525,9 +574,11 @@ cudaError_t launch_dssim(const DsPair *pairs, int npairs, const DsSeg *segs, int
         // striding over the tiles
         const int grid = ntiles < num_sms * 3 ? ntiles : num_sms * 3;
         dssim_tile_kernel<<<grid, kDsThreads, kDsSmemFloats * sizeof(float), st>>>(pairs, segs, nseg, ntiles,
-                                                                                  partials);
+                                                                                  partials, -0.0f);
         dssim_mean_kernel<<<npairs * kDsLevels, kDsThreads, 0, st>>>(pairs, partials, avg);
-        dssim_mad_kernel<<<grid, kDsThreads, 0, st>>>(pairs, segs, nseg, ntiles, avg, partials + ntiles);
+        const int mgrid = (ntiles + kMadWarps - 1) / kMadWarps < num_sms * 8 ? (ntiles + kMadWarps - 1) / kMadWarps
+                                                                               : num_sms * 8;
+        dssim_mad_kernel<<<mgrid, kDsThreads, 0, st>>>(pairs, segs, nseg, ntiles, avg, partials + ntiles);
     }
     dssim_final_kernel<<<npairs, kDsThreads, 0, st>>>(pairs, partials + ntiles, out, write_all ? 1 : 0);
     return cudaGetLastError();
