@@ -353,6 +353,55 @@ __device__ __forceinline__ float bt709_eotf(float v) {
 __device__ __forceinline__ float2 s2_f2(float a) { return make_float2(a, a); }
 __device__ __forceinline__ float2 s2_neg2(float2 a) { return make_float2(-a.x, -a.y); }
 
+// s2_cbrtf of two values at once (f32x2 where both lanes do the same
+// operation; each lane rounds as the scalar steps).  The product that
+// 1 - t subtracts is formed by two scalar multiplies: a packed product
+// feeding a packed add would be fused into one rounding.
+__device__ __forceinline__ float2 s2_cbrtf2(float2 x) {
+    const bool p0 = x.x > 0.0f, p1 = x.y > 0.0f, t0 = x.x < 0x1p-100f, t1 = x.y < 0x1p-100f;
+    float2 xs = make_float2(t0 ? x.x * 0x1p102f : x.x, t1 ? x.y * 0x1p102f : x.y);
+    xs = make_float2(p0 ? xs.x : 1.0f, p1 ? xs.y : 1.0f);
+    float2 r = make_float2(__uint_as_float(0x54a2fa8cu - s2_div3(__float_as_uint(xs.x))),
+                           __uint_as_float(0x54a2fa8cu - s2_div3(__float_as_uint(xs.y))));
+    const float2 third = s2_f2(0x1.555556p-2f);
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+        float2 t = __fmul2_rn(xs, r);
+        t = __fmul2_rn(t, r);
+        t = make_float2(t.x * r.x, t.y * r.y);
+        r = __ffma2_rn(__fmul2_rn(r, third), __fadd2_rn(s2_f2(1.0f), s2_neg2(t)), r);
+    }
+    float2 y = __fmul2_rn(xs, r);
+    y = __fmul2_rn(y, r);
+    const float2 e = __ffma2_rn(__fmul2_rn(y, y), y, s2_neg2(xs));
+    const float2 c = __fmul2_rn(__fmul2_rn(r, r), third);
+    y = __ffma2_rn(s2_neg2(e), c, y);
+    y = __fmul2_rn(y, make_float2(t0 ? 0x1p-34f : 1.0f, t1 ? 0x1p-34f : 1.0f));
+    return make_float2(p0 ? y.x : 0.0f, p1 ? y.y : 0.0f);
+}
+
+__device__ __forceinline__ float2 ds_lab_f2(float2 t) {
+    const float thr = 216.0f / 24389.0f;
+    const float2 c = s2_cbrtf2(t);
+    const float2 l = __ffma2_rn(s2_f2(24389.0f / (27.0f * 116.0f)), t, s2_f2(16.0f / 116.0f));
+    return make_float2(t.x > thr ? c.x : l.x, t.y > thr ? c.y : l.y);
+}
+
+// ds_lab of two pixels (lanes), each lane rounding as ds_lab: the products
+// of the colour matrix feed the addends of FMAs, never a packed add.
+__device__ __forceinline__ void ds_lab2(float2 r, float2 g, float2 b, float2 o[3]) {
+    const float2 xn = __ffma2_rn(s2_f2(0.4124f), r, __ffma2_rn(s2_f2(0.3576f), g, __fmul2_rn(s2_f2(0.1805f), b)));
+    const float2 y = __ffma2_rn(s2_f2(0.2126f), r, __ffma2_rn(s2_f2(0.7152f), g, __fmul2_rn(s2_f2(0.0722f), b)));
+    const float2 zn = __ffma2_rn(s2_f2(0.0193f), r, __ffma2_rn(s2_f2(0.1192f), g, __fmul2_rn(s2_f2(0.9505f), b)));
+    const float2 fx = ds_lab_f2(make_float2(xn.x / 0.9505f, xn.y / 0.9505f));
+    const float2 fy = ds_lab_f2(y);
+    const float2 fz = ds_lab_f2(make_float2(zn.x / 1.089f, zn.y / 1.089f));
+    o[0] = __fmul2_rn(__fadd2_rn(fy, s2_f2(-(16.0f / 116.0f))), s2_f2(1.05f));
+    o[1] = __ffma2_rn(__fadd2_rn(fx, s2_neg2(fy)), s2_f2(500.0f / 220.0f), s2_f2(86.2f / 220.0f));
+    o[2] = __ffma2_rn(__fadd2_rn(fy, s2_neg2(fz)), s2_f2(200.0f / 220.0f), s2_f2(107.9f / 220.0f));
+}
+
+
 __device__ __forceinline__ float s2_pow_scale_unit(unsigned b) {
     const int e = (int)(b >> 23) - 127;
     return e == 0 ? 1.0f : (e == -1 ? 0x1.b6e8aep-3f : (e == -2 ? 0x1.784086p-5f : 0x1.428a3p-7f));

@@ -151,6 +151,33 @@ __device__ __forceinline__ void store_lab(const DevPair &P, int img, int s, int 
     }
 }
 
+// The same for pixels (x, y) and, when `two`, (x + 1, y) of one row, their
+// Lab formed two at a time (ds_lab2, each lane as ds_lab).
+__device__ __forceinline__ void store_lab_pair(const DevPair &P, int img, int s, int x, int y, const float a[3],
+                                               const float b[3], bool two) {
+    const long long plane = (long long)P.lp[s] * P.h[s];
+    const long long off = (long long)y * P.lp[s] + x;
+    if (s < P.lab_levels) {
+        float2 o[3];
+        ds_lab2(make_float2(a[0], two ? b[0] : a[0]), make_float2(a[1], two ? b[1] : a[1]),
+                make_float2(a[2], two ? b[2] : a[2]), o);
+        float *dst = P.lab[img][s];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            dst[c * plane + off] = o[c].x;
+            if (two) dst[c * plane + off + 1] = o[c].y;
+        }
+    }
+    if (s == P.lab_levels - 1 && P.keep[img]) {
+        float *dst = P.keep[img];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            dst[c * plane + off] = a[c];
+            if (two) dst[c * plane + off + 1] = b[c];
+        }
+    }
+}
+
 // OUT: bit 0 SSIMULACRA2's XYB planes, bit 1 DSSIM's Lab planes (both from
 // the same linear pyramid).  OUT == 1 is the SSIMULACRA2-only pass.
 //
@@ -208,10 +235,8 @@ __device__ __forceinline__ void prep_quads(const DevPair &P, int X0, int Y0, con
                     }
                 }
                 if (kL) {
-                    store_lab(P, img, 0, xq, y, v[0]);
-                    if (vx) store_lab(P, img, 0, xq + 1, y, v[1]);
-                    if (vy) store_lab(P, img, 0, xq, y + 1, v[2]);
-                    if (vx && vy) store_lab(P, img, 0, xq + 1, y + 1, v[3]);
+                    store_lab_pair(P, img, 0, xq, y, v[0], v[1], vx);
+                    if (vy) store_lab_pair(P, img, 0, xq, y + 1, v[2], v[3], vx);
                 }
                 // scale-1 pixel: 2x2 mean, far-edge clamp (a missing column
                 // repeats the left pixel, a missing row the upper one)
@@ -240,10 +265,7 @@ __device__ __forceinline__ void prep_quads(const DevPair &P, int X0, int Y0, con
                                                 (long long)y1 * P.lp[1] + x1, l1[0], l1[1]);
                 else store_xyb<ST, KU>(P, img, 1, x1, y1, l1[0]);
             }
-            if (kL) {
-                store_lab(P, img, 1, x1, y1, l1[0]);
-                if (two) store_lab(P, img, 1, x1 + 1, y1, l1[1]);
-            }
+            if (kL) store_lab_pair(P, img, 1, x1, y1, l1[0], l1[1], two);
         }
     }
 }
