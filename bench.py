@@ -612,8 +612,13 @@ def main():
     if os.path.exists(tpath):
         try:
             tj = json.load(open(tpath))
+            # both were measured for the 64-pair launch; each pair's planes
+            # are read once and its items are the same, so they scale with
+            # the pairs of this run
             traffic = tj.get("bytes_per_launch")
+            traffic = None if traffic is None else int(traffic * NP / N_PAIRS)
             winst = tj.get("warp_instructions_per_launch")
+            winst = None if winst is None else int(winst * NP / N_PAIRS)
         except (OSError, ValueError):
             traffic = None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
