@@ -145,8 +145,8 @@ __global__ void __launch_bounds__(kDsThreads) dssim_clamp_kernel(const DsPair *_
 // as the scalar reference does.  The first tap initialises the sum, which equals 0 + tap
 // for every tap but -0 (no Lab value or product of two is -0 where it
 // matters: the sign of a zero sum does not reach the SSIM).  x^2, y^2 and xy
-// are formed once per input position, so the first statistics blur is five
-// plain blurs.  The window is evaluated at every position; on tiles that
+// are formed as the first statistics blur reads its window rows
+// (ds_stat_blur).  The window is evaluated at every position; on tiles that
 // touch the level's edge, positions outside the level then take the value of
 // the position clamped into it (ds_fix_edges), which is what the reference's
 // next stage reads there with clamped indexes.
@@ -199,22 +199,28 @@ __device__ __forceinline__ float2 ds_sum3(const DsProd &t, const DsProd &m, cons
     return __fadd2_rn(s, b.p2);
 }
 
-// L output rows of one column pair from input rows src[0 .. L + 1] (pitch m)
-template <int L, int m, typename F>
-__device__ __forceinline__ void ds_blur_run(const float *src, float2 nz, F &&emit) {
+// L output rows of one column pair from input rows row(0) .. row(L + 1)
+template <int L, typename R, typename F>
+__device__ __forceinline__ void ds_blur_rows(R &&row, float2 nz, F &&emit) {
     const float kc = ds_k(0), ke = ds_k(1), km = ds_k(4);
-    DsProd top = ds_prod(ds_row(src), kc, ke, nz);
-    DsRow mid = ds_row(src + m);
+    DsProd top = ds_prod(row(0), kc, ke, nz);
+    DsRow mid = row(1);
     DsProd mid_outer = ds_prod(mid, kc, ke, nz);
 #pragma unroll
     for (int r = 0; r < L; r++) {
-        const DsRow nw = ds_row(src + (r + 2) * m);
+        const DsRow nw = row(r + 2);
         const DsProd bot = ds_prod(nw, kc, ke, nz);
         emit(r, ds_sum3(top, ds_prod(mid, ke, km, nz), bot));
         top = mid_outer;
         mid = nw;
         mid_outer = bot;
     }
+}
+
+// the same from rows src[0 .. L + 1] of pitch m
+template <int L, int m, typename F>
+__device__ __forceinline__ void ds_blur_run(const float *src, float2 nz, F &&emit) {
+    ds_blur_rows<L>([&](int i) { return ds_row(src + i * m); }, nz, emit);
 }
 
 // `planes` planes: out[p] (n x n) = 3x3 blur of in[p] (pitch n + 2, plane
@@ -238,16 +244,43 @@ __device__ __forceinline__ void ds_stage_blur(const float *in, float *out, float
     ds_blur_run<L, m>(src, nz, [&](int r, float2 v) { *(float2 *)(dst + r * n) = v; });
 }
 
-// the five blur inputs x, y, x^2, y^2, xy of every position (out: 5 planes)
-__device__ __forceinline__ void ds_products(const float *X, const float *Y, float *out, int nn) {
-    for (int i = threadIdx.x; i < nn; i += kDsThreads) {
-        const float x = X[i], y = Y[i];
-        out[i] = x;
-        out[nn + i] = y;
-        out[2 * nn + i] = x * x;
-        out[3 * nn + i] = y * y;
-        out[4 * nn + i] = x * y;
-    }
+// The first statistics blur: the five planes x, y, x^2, y^2, xy (n = 34
+// outputs, pitch 36) from the two input planes x and y.  Each plane is read
+// as the product a b of two rows: x = x * 1, y = y * 1 (b read from four 1s
+// at pitch 0), x^2, y^2, xy, each a packed FMA with the addend -0, so every
+// input is the reference's separately rounded product (or the value
+// itself); the products are not stored, which keeps the block's shared
+// memory within four blocks per SM.  Every thread runs the same code for
+// every plane (no divergence where a warp straddles two planes).
+template <int S, int L>
+__device__ __forceinline__ void ds_stat_blur(const float *in, const float *ones, float *out, float2 nz) {
+    constexpr int n = kDsB, m = n + 2, mm = m * m, half = n / 2, items = 5 * half * S;
+    static_assert(items <= kDsThreads && S * L >= n && L <= n && n % 2 == 0, "one run per thread");
+    const int t = threadIdx.x;
+    if (t >= items) return;
+    const int p = t / (half * S), q = t - p * (half * S);
+    const int seg = q / half, c = 2 * (q - seg * half);
+    const int j0 = min(seg * L, n - L);
+    const int pa = (p == 1 || p == 3) ? 1 : 0;           // x, y, x, y, x
+    const int pb = p == 2 ? 0 : (p >= 3 ? 1 : -1);       // 1, 1, x, y, y
+    const float *srcA = in + pa * mm + j0 * m + c;
+    const float *srcB = pb < 0 ? ones : in + pb * mm + j0 * m + c;
+    const int mB = pb < 0 ? 0 : m;
+    float *dst = out + p * n * n + j0 * n + c;
+    ds_blur_rows<L>(
+        [&](int i) {
+            const DsRow a = ds_row(srcA + i * m), b = ds_row(srcB + i * mB);
+            return DsRow{__ffma2_rn(a.a, b.a, nz), __ffma2_rn(a.b, b.b, nz)};
+        },
+        nz, [&](int r, float2 v) { *(float2 *)(dst + r * n) = v; });
+}
+
+// L's blur inputs x and y: the raw region (2 planes of nn floats) copied out
+// of R, which then takes the next channel's prefetch
+__device__ __forceinline__ void ds_copy2(const float *in, float *out, int nn) {
+    const float4 *s = (const float4 *)in;
+    float4 *d = (float4 *)out;
+    for (int i = threadIdx.x; i < 2 * nn / 4; i += kDsThreads) d[i] = s[i];
 }
 
 // Asynchronous global -> shared copies (cp.async) of 4, 8 or 16 bytes: the
@@ -332,12 +365,14 @@ constexpr int kDsOutCols = kDsT / 2;             // column pairs of a tile
 constexpr int kDsOutRows = 2;                    // output rows per thread
 static_assert(kDsThreads == kDsOutCols * (kDsT / kDsOutRows), "one 2 x 2 output block per thread");
 
-// dynamic shared memory: A (5 planes of 36^2: x, y, x^2, y^2, xy, and the
-// second a/b pre-blur), B (5 planes of 34^2: the first blurs, and the first
-// a/b pre-blur), R (the raw region being fetched: 2 planes of up to 40^2)
-constexpr int kDsSmemFloats = 5 * kDsX * kDsX + 5 * kDsB * kDsB + 2 * kDsR * kDsR;
+// dynamic shared memory: A (2 planes of 36^2: the blur inputs x and y, for
+// a and b the second pre-blur), B (5 planes of 34^2: the first blurs, and the
+// first a/b pre-blur), R (the raw region being fetched: 2 planes of up to
+// 40^2), four 1s (the b rows of the x and y planes in ds_stat_blur)
+constexpr int kDsSmemFloats = 2 * kDsX * kDsX + 5 * kDsB * kDsB + 2 * kDsR * kDsR + 4;
+constexpr int kDsBlocks = 4;  // resident blocks per SM (46 KB shared, at most 64 registers)
 
-__global__ void __launch_bounds__(kDsThreads, 3) dssim_tile_kernel(const DsPair *__restrict__ pairs,
+__global__ void __launch_bounds__(kDsThreads, kDsBlocks) dssim_tile_kernel(const DsPair *__restrict__ pairs,
                                                                    const DsSeg *__restrict__ segs, int nseg,
                                                                    int ntiles, double *__restrict__ partials,
                                                                    float negz) {
@@ -349,11 +384,14 @@ __global__ void __launch_bounds__(kDsThreads, 3) dssim_tile_kernel(const DsPair 
     // is fused even under -fmad=false)
     const float2 nz = make_float2(negz, negz);
     float *const bufA = ds_smem;
-    float *const bufB = bufA + 5 * kDsX * kDsX;
+    float *const bufB = bufA + 2 * kDsX * kDsX;
     float *const bufR = bufB + 5 * kDsB * kDsB;
+    float *const ones = bufR + 2 * kDsR * kDsR;
     __shared__ double wsum[kDsThreads / 32];
-    static_assert(2 * kDsX * kDsX <= 5 * kDsX * kDsX && 2 * kDsP * kDsP <= 5 * kDsB * kDsB, "buffer reuse");
-    static_assert((5 * kDsX * kDsX) % 4 == 0 && (5 * kDsB * kDsB) % 4 == 0, "16-byte aligned buffers");
+    static_assert(2 * kDsP * kDsP <= 5 * kDsB * kDsB, "buffer reuse");
+    static_assert((2 * kDsX * kDsX) % 4 == 0 && (5 * kDsB * kDsB) % 4 == 0 && (2 * kDsR * kDsR) % 4 == 0,
+                  "16-byte aligned buffers");
+    if (threadIdx.x < 4) ones[threadIdx.x] = 1.0f;  // first read after the loop's first barrier
     const int t = threadIdx.x;
     const int c0 = 2 * (t % kDsOutCols), r0 = (t / kDsOutCols) * kDsOutRows;
     constexpr int nnX = kDsX * kDsX, nnB = kDsB * kDsB;
@@ -380,7 +418,7 @@ __global__ void __launch_bounds__(kDsThreads, 3) dssim_tile_kernel(const DsPair 
             __syncthreads();
             if (c == 0) {
                 // L: the blur input is the plane itself (halo 2, clamped loads)
-                ds_products(bufR, bufR + nnX, bufA, nnX);
+                ds_copy2(bufR, bufA, nnX);
                 __syncthreads();
             } else {
                 // a, b: pre-blurred twice first (lib.rs:296-316)
@@ -402,10 +440,8 @@ __global__ void __launch_bounds__(kDsThreads, 3) dssim_tile_kernel(const DsPair 
                     ds_fix_edges<kDsX, 2>(bufA, 2, X0, Y0, W, H);
                     __syncthreads();
                 }
-                ds_products(bufA, bufA + nnX, bufA, nnX);
-                __syncthreads();
             }
-            ds_stage_blur<kDsB, 5, 3, 12>(bufA, bufB, nz);
+            ds_stat_blur<3, 12>(bufA, ones, bufB, nz);
             __syncthreads();
             if (edge) {
                 ds_fix_edges<kDsB, 1>(bufB, 5, X0, Y0, W, H);
@@ -570,9 +606,9 @@ cudaError_t launch_dssim(const DsPair *pairs, int npairs, const DsSeg *segs, int
     if (npairs <= 0) return cudaSuccess;
     if (clamp) dssim_clamp_kernel<<<npairs, kDsThreads, 0, st>>>(pairs);
     if (ntiles > 0) {
-        // persistent: the resident blocks of the tile kernel (3 per SM), each
+        // persistent: the resident blocks of the tile kernel (4 per SM), each
         // striding over the tiles
-        const int grid = ntiles < num_sms * 3 ? ntiles : num_sms * 3;
+        const int grid = ntiles < num_sms * kDsBlocks ? ntiles : num_sms * kDsBlocks;
         dssim_tile_kernel<<<grid, kDsThreads, kDsSmemFloats * sizeof(float), st>>>(pairs, segs, nseg, ntiles,
                                                                                   partials, -0.0f);
         dssim_mean_kernel<<<npairs * kDsLevels, kDsThreads, 0, st>>>(pairs, partials, avg);
