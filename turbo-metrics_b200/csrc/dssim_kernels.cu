@@ -223,10 +223,37 @@ __device__ __forceinline__ void ds_blur_run(const float *src, float2 nz, F &&emi
     ds_blur_rows<L>([&](int i) { return ds_row(src + i * m); }, nz, emit);
 }
 
+// Thread t's item of a blur stage: plane p, row segment seg, column pair
+// c (even).  The first 16 column pairs of every (plane, segment) go to one
+// aligned half-warp, whose 16 lanes read 32 consecutive floats of a row (no
+// shared-memory bank conflicts); the remaining half - 16 pairs of every
+// (plane, segment) go to the threads after those.  Returns false for a
+// thread without an item.
+template <int half, int S, int planes>
+__device__ __forceinline__ bool ds_item(int t, int &p, int &seg, int &c) {
+    static_assert(half >= 16, "a half-warp of column pairs per row segment");
+    constexpr int G = planes * S, extra = half - 16;
+    if (t < 16 * G) {
+        const int g = t >> 4;
+        p = g / S;
+        seg = g - p * S;
+        c = 2 * (t & 15);
+        return true;
+    }
+    if (extra == 0) return false;
+    const int u = t - 16 * G;
+    if (u >= G * extra) return false;
+    const int g = u / extra;
+    p = g / S;
+    seg = g - p * S;
+    c = 2 * (16 + (u - g * extra));
+    return true;
+}
+
 // `planes` planes: out[p] (n x n) = 3x3 blur of in[p] (pitch n + 2, plane
 // (n + 2)^2).  Thread t takes one column pair of one plane and a run of L
-// rows: the plane's n / 2 column pairs times S row segments, at most one
-// item per thread; segment k starts at row min(k L, n - L), so the last run
+// rows (ds_item): the plane's n / 2 column pairs times S row segments, at
+// most one item per thread; segment k starts at row min(k L, n - L), so the last run
 // may overlap the one before it (those rows are written twice, with the same
 // values).  Every size is a compile-time constant: the item's plane, columns
 // and rows are found once, and the run is unrolled without row checks.
@@ -234,10 +261,8 @@ template <int n, int planes, int S, int L>
 __device__ __forceinline__ void ds_stage_blur(const float *in, float *out, float2 nz) {
     constexpr int m = n + 2, half = n / 2, items = planes * half * S;
     static_assert(items <= kDsThreads && S * L >= n && L <= n && n % 2 == 0, "one run per thread");
-    const int t = threadIdx.x;
-    if (t >= items) return;
-    const int p = t / (half * S), q = t - p * (half * S);
-    const int seg = q / half, c = 2 * (q - seg * half);
+    int p, seg, c;
+    if (!ds_item<half, S, planes>(threadIdx.x, p, seg, c)) return;
     const int j0 = min(seg * L, n - L);
     const float *src = in + p * m * m + j0 * m + c;
     float *dst = out + p * n * n + j0 * n + c;
@@ -256,10 +281,8 @@ template <int S, int L>
 __device__ __forceinline__ void ds_stat_blur(const float *in, const float *ones, float *out, float2 nz) {
     constexpr int n = kDsB, m = n + 2, mm = m * m, half = n / 2, items = 5 * half * S;
     static_assert(items <= kDsThreads && S * L >= n && L <= n && n % 2 == 0, "one run per thread");
-    const int t = threadIdx.x;
-    if (t >= items) return;
-    const int p = t / (half * S), q = t - p * (half * S);
-    const int seg = q / half, c = 2 * (q - seg * half);
+    int p, seg, c;
+    if (!ds_item<half, S, 5>(threadIdx.x, p, seg, c)) return;
     const int j0 = min(seg * L, n - L);
     const int pa = (p == 1 || p == 3) ? 1 : 0;           // x, y, x, y, x
     const int pb = p == 2 ? 0 : (p >= 3 ? 1 : -1);       // 1, 1, x, y, y
