@@ -658,6 +658,16 @@ struct Engine {
         return S2_OK;
     }
 
+    // The input format of every pair of a plan, or -1 when they differ: the
+    // prep launch then runs a kernel compiled for that one format.
+    static int uniform_fmt(const Plan &P) {
+        if (P.pairs.empty()) return -1;
+        const int f = P.pairs[0].fmt;
+        for (const DevPair &q : P.pairs)
+            if (q.fmt != f) return -1;
+        return f;
+    }
+
     // Enqueue a planned submission on `st`.  With `host` (the submission's
     // descriptors, planes in host memory), the planes are uploaded group by
     // group on the copy stream and each group's prep + fused launches wait
@@ -755,7 +765,7 @@ struct Engine {
         const Seg *dsegs = (const Seg *)(dbase + pb + bb);
         const int pout = (m_s2 ? 1 : 0) | (m_ds ? 2 : 0);
         if (graphs && !host && !profiling && ng == 1) {
-            const uint64_t key[8] = {(uint64_t)n, (uint64_t)P.total_blocks,
+            const uint64_t key[8] = {(uint64_t)n | ((uint64_t)(uniform_fmt(P) + 1) << 40), (uint64_t)P.total_blocks,
                                      (uint64_t)P.total_tiles,
                                      P.segs.size(),
                                      P.vsegs.size(), P.hsegs.size(),
@@ -817,7 +827,7 @@ struct Engine {
             const int b0 = pa < n ? P.blk_first[pa] : P.total_blocks;
             const int b1 = pe < n ? P.blk_first[pe] : P.total_blocks;
             S2_CUDA(launch_pyramid(storage, dpairs, n, dblk, b0, b1, cc, (const float *)lut_d.p, num_sms * 8, pst,
-                                   pout));
+                                   pout, uniform_fmt(P)));
             if (host && g + 1 == ng) S2_CUDA(cudaEventRecord(stage_free, pst));
             if (split) {
                 S2_CUDA(cudaEventRecord(grp_prepped[g], prep_st));
@@ -890,7 +900,8 @@ struct Engine {
         if (e == cudaSuccess) e = cudaMemsetAsync(counter_d.p, 0, kCounterBytes, cap_st);
         if (e == cudaSuccess)
             e = launch_pyramid(storage, dpairs, n, (const int *)(dbase + pb), 0, P.total_blocks, cc,
-                               (const float *)lut_d.p, num_sms * 8, cap_st, (m_s2 ? 1 : 0) | (m_ds ? 2 : 0));
+                               (const float *)lut_d.p, num_sms * 8, cap_st, (m_s2 ? 1 : 0) | (m_ds ? 2 : 0),
+                               uniform_fmt(P));
         if (e == cudaSuccess && m_s2) {
             if (blur == S2_BLUR_IIR_REF)
                 e = launch_iir(storage, dpairs, (const IirSeg *)(dbase + pb + bb + sb), (int)P.vsegs.size(), P.vtotal,

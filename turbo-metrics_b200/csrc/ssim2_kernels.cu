@@ -274,7 +274,11 @@ __device__ __forceinline__ void prep_quads(const DevPair &P, int X0, int Y0, con
 // small scales overlap the other blocks' work.
 constexpr int kPrepThreads = 128;
 
-template <typename ST, int OUT>
+// FMT: the input format of every pair of the launch, or -1 for a mix (each
+// block then switches on its pair's format).  A kernel compiled for one
+// format carries one conversion instead of five, which the instruction
+// cache notices.
+template <typename ST, int OUT, int FMT>
 __global__ void __launch_bounds__(kPrepThreads, 4) prep_kernel(const DevPair *__restrict__ pairs, int npairs,
                                                    const int *__restrict__ blk_first, int first_block,
                                                    int end_block,
@@ -306,12 +310,16 @@ __global__ void __launch_bounds__(kPrepThreads, 4) prep_kernel(const DevPair *__
         const int b = item - blk_first[lo];
         const int bx = b % P.blk_x, by = b / P.blk_x;
         const int X0 = bx * kPyrBlk, Y0 = by * kPyrBlk;
-        switch (P.fmt) {
-        case FMT_LINEAR_F32: prep_quads<FMT_LINEAR_F32, ST, OUT>(P, X0, Y0, lut, cc, lv1); break;
-        case FMT_SRGB8: prep_quads<FMT_SRGB8, ST, OUT>(P, X0, Y0, lut, cc, lv1); break;
-        case FMT_NV12: prep_quads<FMT_NV12, ST, OUT>(P, X0, Y0, lut, cc, lv1); break;
-        case FMT_P016: prep_quads<FMT_P016, ST, OUT>(P, X0, Y0, lut, cc, lv1); break;
-        default: prep_quads<FMT_RGB16, ST, OUT>(P, X0, Y0, lut, cc, lv1); break;
+        if constexpr (FMT >= 0) {
+            prep_quads<(FMT >= 0 ? FMT : 0), ST, OUT>(P, X0, Y0, lut, cc, lv1);
+        } else {
+            switch (P.fmt) {
+            case FMT_LINEAR_F32: prep_quads<FMT_LINEAR_F32, ST, OUT>(P, X0, Y0, lut, cc, lv1); break;
+            case FMT_SRGB8: prep_quads<FMT_SRGB8, ST, OUT>(P, X0, Y0, lut, cc, lv1); break;
+            case FMT_NV12: prep_quads<FMT_NV12, ST, OUT>(P, X0, Y0, lut, cc, lv1); break;
+            case FMT_P016: prep_quads<FMT_P016, ST, OUT>(P, X0, Y0, lut, cc, lv1); break;
+            default: prep_quads<FMT_RGB16, ST, OUT>(P, X0, Y0, lut, cc, lv1); break;
+            }
         }
         __syncthreads();
         const int nlev = (OUT & 2) ? P.prep_levels : P.nscales;
@@ -990,23 +998,46 @@ int fused_blocks_per_sm(int storage) {
     return n > 0 ? n : 1;
 }
 
+template <int OUT, int FMT>
+static void prep_launch_f(const DevPair *pairs, int npairs, const int *blk_first, int first_block, int end_block,
+                          const ColorConsts &cc, const float *lut, int grid, cudaStream_t st) {
+    prep_kernel<float, OUT, FMT>
+        <<<grid, kPrepThreads, 0, st>>>(pairs, npairs, blk_first, first_block, end_block, cc, lut);
+}
+
 template <int OUT>
 static void prep_launch(const DevPair *pairs, int npairs, const int *blk_first, int first_block, int end_block,
-                        const ColorConsts &cc, const float *lut, int grid, cudaStream_t st) {
-    prep_kernel<float, OUT>
-        <<<grid, kPrepThreads, 0, st>>>(pairs, npairs, blk_first, first_block, end_block, cc, lut);
+                        const ColorConsts &cc, const float *lut, int grid, cudaStream_t st, int fmt) {
+    switch (fmt) {
+    case FMT_LINEAR_F32:
+        prep_launch_f<OUT, FMT_LINEAR_F32>(pairs, npairs, blk_first, first_block, end_block, cc, lut, grid, st);
+        break;
+    case FMT_SRGB8:
+        prep_launch_f<OUT, FMT_SRGB8>(pairs, npairs, blk_first, first_block, end_block, cc, lut, grid, st);
+        break;
+    case FMT_NV12:
+        prep_launch_f<OUT, FMT_NV12>(pairs, npairs, blk_first, first_block, end_block, cc, lut, grid, st);
+        break;
+    case FMT_P016:
+        prep_launch_f<OUT, FMT_P016>(pairs, npairs, blk_first, first_block, end_block, cc, lut, grid, st);
+        break;
+    case FMT_RGB16:
+        prep_launch_f<OUT, FMT_RGB16>(pairs, npairs, blk_first, first_block, end_block, cc, lut, grid, st);
+        break;
+    default: prep_launch_f<OUT, -1>(pairs, npairs, blk_first, first_block, end_block, cc, lut, grid, st); break;
+    }
 }
 
 cudaError_t launch_pyramid(int storage, const DevPair *pairs, int npairs, const int *blk_first, int first_block,
                            int end_block, const ColorConsts &cc, const float *lut, int grid, cudaStream_t st,
-                           int out) {
+                           int out, int fmt) {
     const int nb = end_block - first_block;
     if (nb <= 0) return cudaSuccess;
     grid = grid > nb ? nb : grid;
     (void)storage;
-    if (out == 3) prep_launch<3>(pairs, npairs, blk_first, first_block, end_block, cc, lut, grid, st);
-    else if (out == 2) prep_launch<2>(pairs, npairs, blk_first, first_block, end_block, cc, lut, grid, st);
-    else prep_launch<1>(pairs, npairs, blk_first, first_block, end_block, cc, lut, grid, st);
+    if (out == 3) prep_launch<3>(pairs, npairs, blk_first, first_block, end_block, cc, lut, grid, st, fmt);
+    else if (out == 2) prep_launch<2>(pairs, npairs, blk_first, first_block, end_block, cc, lut, grid, st, fmt);
+    else prep_launch<1>(pairs, npairs, blk_first, first_block, end_block, cc, lut, grid, st, fmt);
     return cudaGetLastError();
 }
 

@@ -13,10 +13,11 @@ int fused_blocks_per_sm(int storage);
 // prep over the pyramid blocks [first_block, end_block) (absolute numbering
 // of blk_first), fused over the tiles [first_tile, end_tile) with its own
 // zeroed work counter.  out: 1 XYB planes (SSIMULACRA2), 2 Lab planes
-// (DSSIM), 3 both from one pass.
+// (DSSIM), 3 both from one pass.  fmt: the input format shared by every
+// pair of the launch (a kernel compiled for it), or -1 for a mix.
 cudaError_t launch_pyramid(int storage, const DevPair *pairs, int npairs, const int *blk_first, int first_block,
                            int end_block, const ColorConsts &cc, const float *lut, int grid, cudaStream_t st,
-                           int out = 1);
+                           int out = 1, int fmt = -1);
 // The tile pass's bounded waits: err is a device word (zeroed before the
 // submission) that a pass whose row copies time out sets (launch_finalize
 // then marks every pair S2_ERR_TIMEOUT); wait_cycles bounds each wait (SM
