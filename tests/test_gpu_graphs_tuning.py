@@ -68,3 +68,36 @@ def test_autotuned_tile_height_matches_fixed_heights(tmb, cuda):
         for a, f in zip(first, fixed):
             assert abs(a[0] - f[0]) < 1e-12
             assert np.allclose(a[1], f[1], rtol=1e-12, atol=1e-15)
+
+
+def nv12_batch_of(tmb, torch, sizes, seed):
+    out = []
+    for i, (w, h) in enumerate(sizes):
+        (ry, ruv), (dy, duv) = synth.nv12_frame_pair(w, h, seed + i)
+        out.append(tmb.PairDesc(dev(torch, ry), dev(torch, dy), "nv12", dev(torch, ruv), dev(torch, duv)))
+    return out
+
+
+def test_graph_replay_follows_the_input_format(tmb, cuda):
+    """A submission whose pairs share one input format runs a prep kernel
+    compiled for that format, so a replayed graph must be the one recorded
+    for the same format: sRGB8, NV12 and a mix of both, all of one shape
+    (same sizes, same tile plan), alternate on one batch with graphs on and
+    score exactly as on a batch with graphs off."""
+    shape = [(320, 180), (256, 144)]
+    srgb = batch_of(tmb, cuda, shape, 1200)
+    nv12 = nv12_batch_of(tmb, cuda, shape, 1300)
+    mixed = [srgb[0], nv12[1]]
+    g = tmb.Ssim2Batch(4, 1 << 20, strip_rows=32)
+    plain = tmb.Ssim2Batch(4, 1 << 20, strip_rows=32)
+    plain.set_graphs(False)
+    for pairs in (srgb, nv12, mixed, srgb, mixed, nv12):
+        a = g.compute_batch(pairs)
+        b = plain.compute_batch(pairs)
+        assert [x[0] for x in a] == [x[0] for x in b]
+        for x, y in zip(a, b):
+            assert np.array_equal(x[1], y[1])
+    # the mixed submission scores each pair as its own-format submission does
+    m = g.compute_batch(mixed)
+    assert m[0][0] == g.compute_batch(srgb)[0][0]
+    assert m[1][0] == g.compute_batch(nv12)[1][0]
