@@ -134,6 +134,27 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def h2d_link_rate(nbytes, reps=5):
+    """Host-to-device bandwidth of one plain copy of `nbytes` from pinned
+    host memory (GB/s, CUDA events, best of `reps`): the ceiling of the e2e
+    leg, whose every step uploads that many bytes."""
+    import torch
+    src = torch.empty(int(nbytes), dtype=torch.uint8).pin_memory()
+    dst = torch.empty(int(nbytes), dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+    best = None
+    for _ in range(reps + 1):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        dst.copy_(src, non_blocking=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        best = ms if best is None else min(best, ms)
+    del src, dst
+    return nbytes / (best / 1e3) / 1e9
+
+
 def with_issue_roofline(roofline, clk, peaks):
     """The fused pass is bound by instruction issue, not HBM: beside the HBM
     fraction, its warp instructions per launch (ncu smsp__inst_executed.sum of
@@ -685,6 +706,7 @@ def main():
     e2e_ms = max_over_ranks(e0.elapsed_time(e1), dist, "cuda")
     e2e = whole_job_rate(world, NP, args.steps, e2e_ms)
     assert np.allclose([r[0] for r in res], scores, atol=1e-9)
+    link = h2d_link_rate(h2d)
 
     cached = None
     if not args.no_cached:
@@ -722,7 +744,11 @@ def main():
                        "l2": "inputs 398 MB per step > 126 MB L2 (no flush)",
                        "parallelism": "replicas" if world > 1 else "single"},
             "plain_pairs_per_s": plain, "batched_vs_plain": value / world / plain,
-            "e2e": {"value": e2e, "unit": "pairs/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+            "e2e": {"value": e2e, "unit": "pairs/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                    # the step's upload over the host link: its rate inside the
+                    # e2e run against a plain pinned copy of the same bytes
+                    "upload_gbs": h2d * e2e / NP / world / 1e9, "link_h2d_gbs": link,
+                    "link_frac": (h2d * e2e / NP / world / 1e9) / link if link else None},
             "roofline": with_issue_roofline(roofline, clk, peaks),
             "gpu_launches": 3 * args.steps,
             "clocks": clk,
