@@ -27,16 +27,10 @@
 // pair's DSSIM does not depend on the rest of its batch.
 #include <cfloat>
 
+#include "dssim_tile_map.h"
 #include "ssim2_launch.h"
 
 namespace s2 {
-
-constexpr int kDsT = 32;             // output tile edge
-constexpr int kDsThreads = 256;
-constexpr int kDsR = kDsT + 8;       // raw a/b region (halo 4)
-constexpr int kDsP = kDsT + 6;       // first a/b pre-blur (halo 3)
-constexpr int kDsX = kDsT + 4;       // blur input x, y (halo 2)
-constexpr int kDsB = kDsT + 2;       // first statistics blur (halo 1)
 
 // dssim-cuda-kernel/src/blur.rs:13-17
 __device__ __forceinline__ float ds_k(int i) {
@@ -221,33 +215,6 @@ __device__ __forceinline__ void ds_blur_rows(R &&row, float2 nz, F &&emit) {
 template <int L, int m, typename F>
 __device__ __forceinline__ void ds_blur_run(const float *src, float2 nz, F &&emit) {
     ds_blur_rows<L>([&](int i) { return ds_row(src + i * m); }, nz, emit);
-}
-
-// Thread t's item of a blur stage: plane p, row segment seg, column pair
-// c (even).  The first 16 column pairs of every (plane, segment) go to one
-// aligned half-warp, whose 16 lanes read 32 consecutive floats of a row (no
-// shared-memory bank conflicts); the remaining half - 16 pairs of every
-// (plane, segment) go to the threads after those.  Returns false for a
-// thread without an item.
-template <int half, int S, int planes>
-__device__ __forceinline__ bool ds_item(int t, int &p, int &seg, int &c) {
-    static_assert(half >= 16, "a half-warp of column pairs per row segment");
-    constexpr int G = planes * S, extra = half - 16;
-    if (t < 16 * G) {
-        const int g = t >> 4;
-        p = g / S;
-        seg = g - p * S;
-        c = 2 * (t & 15);
-        return true;
-    }
-    if (extra == 0) return false;
-    const int u = t - 16 * G;
-    if (u >= G * extra) return false;
-    const int g = u / extra;
-    p = g / S;
-    seg = g - p * S;
-    c = 2 * (16 + (u - g * extra));
-    return true;
 }
 
 // `planes` planes: out[p] (n x n) = 3x3 blur of in[p] (pitch n + 2, plane
@@ -445,7 +412,7 @@ __global__ void __launch_bounds__(kDsThreads, kDsBlocks) dssim_tile_kernel(const
                 __syncthreads();
             } else {
                 // a, b: pre-blurred twice first (lib.rs:296-316)
-                ds_stage_blur<kDsP, 2, 6, 7>(bufR, bufB, nz);
+                ds_stage_blur<kDsP, 2, kDsPre1S, kDsPre1L>(bufR, bufB, nz);
                 __syncthreads();
             }
             // R is free: fetch the next channel (or the next tile's L) during
@@ -457,14 +424,14 @@ __global__ void __launch_bounds__(kDsThreads, kDsBlocks) dssim_tile_kernel(const
                     ds_fix_edges<kDsP, 3>(bufB, 2, X0, Y0, W, H);
                     __syncthreads();
                 }
-                ds_stage_blur<kDsX, 2, 6, 6>(bufB, bufA, nz);
+                ds_stage_blur<kDsX, 2, kDsPre2S, kDsPre2L>(bufB, bufA, nz);
                 __syncthreads();
                 if (edge) {
                     ds_fix_edges<kDsX, 2>(bufA, 2, X0, Y0, W, H);
                     __syncthreads();
                 }
             }
-            ds_stat_blur<3, 12>(bufA, ones, bufB, nz);
+            ds_stat_blur<kDsStatS, kDsStatL>(bufA, ones, bufB, nz);
             __syncthreads();
             if (edge) {
                 ds_fix_edges<kDsB, 1>(bufB, 5, X0, Y0, W, H);
